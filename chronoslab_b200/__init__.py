@@ -1,0 +1,414 @@
+"""chronoslab_b200 -- B200-native (sm_100a) AMG-preconditioned SPD solve path of
+ChronosLab, behind a C ABI (include/chronos_b200.h) with this Python binding.
+
+The names mirror the reference's entry points on this path:
+  cpt_aspAMG(param, A, TV0)            -> Hierarchy   (aspAMG/cpt_aspAMG.m)
+  AMG_Vcycle(hrc, b)                   -> x           (aspAMG/AMG_Vcycle.m)
+  PCG_CJ(hrc, b, x0, itmax, tol)       -> x, iter, resvec, flag   (LinearSolver/PCG_CJ.m)
+  SQMR(hrc, rhs, tol, itmax)           -> x, info, relres, niter  (LinearSolver/SQMR.m)
+  SYM_aFSAI_compute(...)               -> the MEX outputs         (MEX_SYM_AFSAI)
+  afsai_cpp(M, nthread, nstep, step_size, eps) -> F, is_posdef    (smoother/afsai_cpp.m)
+  readDefaultParams(fnames)            -> chronos_params          (utils/readDefaultParams.m)
+Vectors are numpy FP64 arrays; matrices scipy.sparse CSR (0-based).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import scipy.sparse as sp
+
+from ._lib import (CHRONOS_FP32, CHRONOS_FP64, ChronosError, chronos_level_info, chronos_params,
+                   check, last_error, load)
+
+__all__ = [
+    "CHRONOS_FP32", "CHRONOS_FP64", "ChronosError", "Hierarchy", "params", "readDefaultParams",
+    "cpt_aspAMG", "AMG_Vcycle", "PCG_CJ", "SQMR", "SYM_aFSAI_compute", "afsai_cpp",
+    "fsai_numeric", "fsai_pattern", "coarsen", "bamg", "galerkin", "dense_chol", "spmv",
+    "diag_fix", "version",
+]
+
+_P_I = C.POINTER(C.c_int)
+_P_I64 = C.POINTER(C.c_int64)
+_P_D = C.POINTER(C.c_double)
+
+
+def _pi(a):
+    return a.ctypes.data_as(_P_I)
+
+
+def _pi64(a):
+    return a.ctypes.data_as(_P_I64)
+
+
+def _pd(a):
+    return a.ctypes.data_as(_P_D)
+
+
+def version():
+    return load().chronos_version().decode()
+
+
+def _csr(A, ncols=None):
+    A = sp.csr_matrix(A)
+    if not A.has_sorted_indices:
+        A = A.copy()
+        A.sort_indices()
+    indptr = np.ascontiguousarray(A.indptr, dtype=np.int32)
+    indices = np.ascontiguousarray(A.indices, dtype=np.int32)
+    data = np.ascontiguousarray(A.data, dtype=np.float64)
+    return A.shape[0], indptr, indices, data
+
+
+_STR_FIELDS = {"smoother_method", "tspace_method", "SoC_type", "proltype", "prol_emin",
+               "rhs_build", "solv_method"}
+
+
+def params(**overrides):
+    """Reference regression-test defaults (Tests/parm_*), then overrides."""
+    p = chronos_params()
+    load().chronos_params_default(C.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise KeyError(f"unknown parameter {k}")
+        setattr(p, k, v.encode() if k in _STR_FIELDS else v)
+    return p
+
+
+def readDefaultParams(fnames_path, **overrides):
+    """Reads aspAMG.fnames and the seven parm_* files it names."""
+    p = params()
+    check(load().chronos_params_read(str(fnames_path).encode(), C.byref(p)))
+    for k, v in overrides.items():
+        setattr(p, k, v.encode() if k in _STR_FIELDS else v)
+    return p
+
+
+class _CsrHandle:
+    """Fetches a chronos_csr result into scipy and frees it."""
+
+    @staticmethod
+    def take(handle):
+        lib = load()
+        nr, nc, nnz = C.c_int(), C.c_int(), C.c_int64()
+        check(lib.chronos_csr_info(handle, C.byref(nr), C.byref(nc), C.byref(nnz)))
+        iat = np.zeros(nr.value + 1, np.int32)
+        ja = np.zeros(max(nnz.value, 1), np.int32)
+        v = np.zeros(max(nnz.value, 1), np.float64)
+        check(lib.chronos_csr_fetch(handle, _pi(iat), _pi(ja), _pd(v)))
+        check(lib.chronos_csr_free(handle))
+        return sp.csr_matrix((v[:nnz.value], ja[:nnz.value], iat), shape=(nr.value, nc.value))
+
+
+# ---------------------------------------------------------------------------
+# FSAI
+# ---------------------------------------------------------------------------
+
+def SYM_aFSAI_compute(nthread, n_step, step_size, tau, eps, nrows, nrows_M, nterm_M, iat_M,
+                      ja_M, coef_M):
+    """Mirror of the MEX gateway SYM_aFSAI_compute.cpp:15-20: 1-based CSR with
+    int64 iat / int32 ja; returns (nterm_G, iat_G, ja_G, coef_G, is_posdef)."""
+    iat_M = np.ascontiguousarray(iat_M, dtype=np.int64)
+    ja_M = np.ascontiguousarray(ja_M, dtype=np.int32)
+    coef_M = np.ascontiguousarray(coef_M, dtype=np.float64)
+    kmax = 1 + n_step * step_size
+    iat_G = np.zeros(nrows + 1, np.int64)
+    ja_G = np.zeros(nrows * kmax, np.int32)
+    coef_G = np.zeros(nrows * kmax, np.float64)
+    nterm = C.c_int64()
+    posdef = C.c_int()
+    check(load().chronos_fsai_compute(nthread, n_step, step_size, tau, eps, nrows, nrows_M,
+                                      nterm_M, _pi64(iat_M), _pi(ja_M), _pd(coef_M),
+                                      C.byref(nterm), _pi64(iat_G), _pi(ja_G), _pd(coef_G),
+                                      C.byref(posdef)))
+    nt = nterm.value
+    return nt, iat_G, ja_G[:nt], coef_G[:nt], bool(posdef.value)
+
+
+def afsai_cpp(M, nthread, nstep, step_size, eps):
+    """afsai_cpp.m:1-65: F (lower-triangular CSR, diagonal last in each row)
+    and is_posdef; F is None when the matrix was deemed indefinite."""
+    M = sp.csr_matrix(M)
+    M.sort_indices()
+    n = M.shape[0]
+    nt, iat, ja, coef, ok = SYM_aFSAI_compute(nthread, nstep, step_size, 0.0, eps, n, n, M.nnz,
+                                              M.indptr.astype(np.int64) + 1,
+                                              M.indices.astype(np.int32) + 1, M.data)
+    if not ok:
+        return None, False
+    F = sp.csr_matrix((coef, ja.astype(np.int64) - 1, iat - 1), shape=(n, n))
+    return F, True
+
+
+def fsai_pattern(A, nstep=15, step_size=1, eps=1e-3, nthread=1, fsai_fabs=0):
+    """Host adaptive pattern search (no GPU): (G with host FP64 values, posdef)."""
+    n, ip, ix, dv = _csr(A)
+    ok = C.c_int()
+    h = C.c_void_p()
+    check(load().chronos_fsai_pattern(n, _pi(ip), _pi(ix), _pd(dv), nstep, step_size, eps,
+                                      nthread, fsai_fabs, C.byref(ok), C.byref(h)))
+    return _CsrHandle.take(h), bool(ok.value)
+
+
+def fsai_numeric(A, G):
+    """GPU numeric phase on the pattern of G (rows: strictly-lower ascending,
+    diagonal last).  Returns (values in G's order, is_posdef)."""
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    G = sp.csr_matrix(G)
+    n = A.shape[0]
+    out = np.zeros(G.nnz, np.float64)
+    ok = C.c_int()
+    iatA = A.indptr.astype(np.int64) + 1
+    jaA = A.indices.astype(np.int32) + 1
+    iatG = G.indptr.astype(np.int64) + 1
+    jaG = G.indices.astype(np.int32) + 1
+    dA = np.ascontiguousarray(A.data, np.float64)
+    check(load().chronos_fsai_numeric(n, _pi64(iatA), _pi(jaA), _pd(dA), _pi64(iatG), _pi(jaG),
+                                      _pd(out), C.byref(ok)))
+    return out, bool(ok.value)
+
+
+# ---------------------------------------------------------------------------
+# Coarsening, prolongation, Galerkin, coarse factor
+# ---------------------------------------------------------------------------
+
+def coarsen(A, prm=None, rng_skip=0):
+    """SoC + PMIS on the host: (fcnode numbered as the reference, nc, S)."""
+    prm = prm or params()
+    n, ip, ix, dv = _csr(A)
+    fc = np.zeros(n, np.int32)
+    nc = C.c_int()
+    h = C.c_void_p()
+    check(load().chronos_coarsen(C.byref(prm), n, _pi(ip), _pi(ix), _pd(dv), rng_skip, _pi(fc),
+                                 C.byref(nc), C.byref(h)))
+    return fc.astype(np.int64), nc.value, _CsrHandle.take(h)
+
+
+def bamg(S, fcnode, TV, prm=None):
+    """BAMG prolongation on the host: (P, c_mark)."""
+    prm = prm or params()
+    S = sp.csr_matrix(S)
+    S.sort_indices()
+    n = S.shape[0]
+    ip = S.indptr.astype(np.int32)
+    ix = S.indices.astype(np.int32)
+    fc = np.ascontiguousarray(fcnode, dtype=np.int32)
+    TV = np.asfortranarray(np.asarray(TV, dtype=np.float64).reshape(n, -1))
+    ntv = TV.shape[1]
+    tvc = np.ascontiguousarray(TV.T).ravel()      # column-major
+    cm = np.zeros(n, np.int32)
+    h = C.c_void_p()
+    check(load().chronos_bamg(C.byref(prm), n, _pi(ip), _pi(ix), _pi(fc), ntv, _pd(tvc), _pi(cm),
+                              C.byref(h)))
+    return _CsrHandle.take(h), cm
+
+
+def galerkin(A, P):
+    """GPU Galerkin product P'*(A*P) (exact zeros dropped, sorted rows)."""
+    n, ip, ix, dv = _csr(A)
+    P = sp.csr_matrix(P)
+    nc = P.shape[1]
+    pp = P.indptr.astype(np.int32)
+    px = P.indices.astype(np.int32)
+    pv = np.ascontiguousarray(P.data, np.float64)
+    nnz = C.c_int64()
+    plan = C.c_void_p()
+    lib = load()
+    check(lib.chronos_galerkin_compute(n, nc, _pi(ip), _pi(ix), _pd(dv), _pi(pp), _pi(px),
+                                       _pd(pv), C.byref(nnz), C.byref(plan)))
+    try:
+        iat = np.zeros(nc + 1, np.int32)
+        ja = np.zeros(max(nnz.value, 1), np.int32)
+        v = np.zeros(max(nnz.value, 1), np.float64)
+        check(lib.chronos_galerkin_fetch(plan, _pi(iat), _pi(ja), _pd(v)))
+    finally:
+        lib.chronos_galerkin_free(plan)
+    return sp.csr_matrix((v[:nnz.value], ja[:nnz.value], iat), shape=(nc, nc))
+
+
+def dense_chol(A):
+    """GPU dense FP64 Cholesky: lower L with A = L L'."""
+    A = np.asfortranarray(np.asarray(A, dtype=np.float64))
+    n = A.shape[0]
+    a = np.ascontiguousarray(A.T).ravel()     # column-major
+    L = np.zeros(n * n, np.float64)
+    check(load().chronos_dense_chol(n, _pd(a), _pd(L)))
+    return L.reshape(n, n).T.copy()
+
+
+def spmv(A, x, precision=CHRONOS_FP64):
+    n, ip, ix, dv = _csr(A)
+    x = np.ascontiguousarray(x, np.float64)
+    y = np.zeros(n, np.float64)
+    check(load().chronos_spmv(n, A.shape[1], _pi(ip), _pi(ix), _pd(dv), _pd(x), _pd(y), precision))
+    return y
+
+
+def diag_fix(A):
+    """computeAMG.m:5-10 on the GPU: diagonal entries equal to 1 become
+    lambda_max(A)/10.  Returns a new matrix."""
+    A = sp.csr_matrix(A, copy=True)
+    A.sort_indices()
+    n, ip, ix, dv = _csr(A)
+    dv = dv.copy()
+    check(load().chronos_diag_fix(n, _pi(ip), _pi(ix), _pd(dv)))
+    return sp.csr_matrix((dv, ix, ip), shape=A.shape)
+
+
+# ---------------------------------------------------------------------------
+# Hierarchy, V-cycle, Krylov
+# ---------------------------------------------------------------------------
+
+class Hierarchy:
+    """Handle of a GPU AMG hierarchy (chronos_hier)."""
+
+    def __init__(self, A, TV0=None, prm=None):
+        self._lib = load()
+        self.prm = prm or params()
+        n, ip, ix, dv = _csr(A)
+        self.n = n
+        if TV0 is None:
+            ntv0, tv = 0, np.zeros(1)
+        else:
+            TV0 = np.asarray(TV0, dtype=np.float64).reshape(n, -1)
+            ntv0 = TV0.shape[1]
+            tv = np.ascontiguousarray(TV0.T).ravel()
+        h = C.c_void_p()
+        check(self._lib.chronos_amg_setup(C.byref(self.prm), n, _pi(ip), _pi(ix), _pd(dv), ntv0,
+                                          _pd(tv), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.chronos_hier_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def nlevels(self):
+        v = C.c_int()
+        check(self._lib.chronos_hier_nlevels(self._h, C.byref(v)))
+        return v.value
+
+    def level_info(self, level):
+        info = chronos_level_info()
+        check(self._lib.chronos_hier_level_info(self._h, level, C.byref(info)))
+        return {"n": info.n, "nnz_A": info.nnz_A, "nnz_G": info.nnz_G, "nnz_P": info.nnz_P,
+                "nc": info.nc, "omega": info.omega, "lambda": info.lambda_,
+                "threads_per_row": info.threads_per_row}
+
+    def export(self, level, which):
+        nr, ncl, nnz = C.c_int(), C.c_int(), C.c_int64()
+        w = C.c_char(which.encode() if isinstance(which, str) else which)
+        check(self._lib.chronos_hier_export(self._h, level, w, C.byref(nr), C.byref(ncl),
+                                            C.byref(nnz), None, None, None))
+        iat = np.zeros(nr.value + 1, np.int32)
+        ja = np.zeros(max(nnz.value, 1), np.int32)
+        v = np.zeros(max(nnz.value, 1), np.float64)
+        check(self._lib.chronos_hier_export(self._h, level, w, C.byref(nr), C.byref(ncl),
+                                            C.byref(nnz), _pi(iat), _pi(ja), _pd(v)))
+        return sp.csr_matrix((v[:nnz.value], ja[:nnz.value], iat), shape=(nr.value, ncl.value))
+
+    def setup_times(self):
+        t = np.zeros(8)
+        check(self._lib.chronos_hier_setup_times(self._h, _pd(t)))
+        keys = ["fsai_pattern", "fsai_numeric", "omega", "coarsen", "prolong", "galerkin",
+                "coarse_factor", "total"]
+        return dict(zip(keys, t.tolist()))
+
+    def vcycle(self, b):
+        b = np.asarray(b, dtype=np.float64)
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        bc = np.ascontiguousarray(b.T if b.ndim == 2 else b).ravel()
+        x = np.zeros_like(bc)
+        check(self._lib.chronos_vcycle(self._h, _pd(bc), _pd(x), nrhs))
+        return x if b.ndim == 1 else x.reshape(nrhs, self.n).T
+
+    def pcg(self, b, x0=None, itmax=1000, tol=1e-8):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        it, flag, sec = C.c_int(), C.c_int(), C.c_double()
+        rv = np.zeros(max(itmax, 0) + 1)
+        check(self._lib.chronos_pcg(self._h, _pd(b), _pd(x), itmax, tol, C.byref(it), _pd(rv),
+                                    C.byref(flag), C.byref(sec)))
+        return x, it.value, rv[:it.value + 1], flag.value, sec.value
+
+    def pcg_dev(self, b_ptr, x_ptr, itmax=1000, tol=1e-8):
+        """PCG on device FP64 vectors (raw pointers, e.g. torch tensor.data_ptr())."""
+        it, flag, sec = C.c_int(), C.c_int(), C.c_double()
+        check(self._lib.chronos_pcg_dev(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr), itmax, tol,
+                                        C.byref(it), None, C.byref(flag), C.byref(sec)))
+        return it.value, flag.value, sec.value
+
+    def pcg_block(self, B, X0=None, itmax=1000, tol=1e-8):
+        B = np.asarray(B, dtype=np.float64)
+        nrhs = B.shape[1]
+        bc = np.ascontiguousarray(B.T).ravel()
+        xc = np.zeros_like(bc) if X0 is None else np.ascontiguousarray(np.asarray(X0).T).ravel()
+        its = np.zeros(nrhs, np.int32)
+        fl = np.zeros(nrhs, np.int32)
+        sec = C.c_double()
+        check(self._lib.chronos_pcg_block(self._h, nrhs, _pd(bc), _pd(xc), itmax, tol, _pi(its),
+                                          _pi(fl), C.byref(sec)))
+        return xc.reshape(nrhs, self.n).T, its, fl, sec.value
+
+    def sqmr(self, b, tol=1e-6, itmax=100, x0=None, A=None):
+        """SQMR with the V-cycle as left preconditioner; A (optional) is the
+        operator, else the level-1 operator of the hierarchy."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        it, info, rel = C.c_int(), C.c_int(), C.c_double()
+        if A is not None:
+            _, ip, ix, dv = _csr(A)
+            ops = (_pi(ip), _pi(ix), _pd(dv))
+        else:
+            ops = (None, None, None)
+        check(self._lib.chronos_sqmr(self._h, *ops, _pd(b), _pd(x), itmax, tol, C.byref(it),
+                                     C.byref(rel), C.byref(info)))
+        return x, info.value, rel.value, it.value
+
+    def adjoint_grad(self, u, g, itmax=1000, tol=1e-10):
+        """dJ/dA on A's pattern for J with dJ/du = g (A SPD): returns
+        (lambda, grad values in A's CSR order, iterations)."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        lam = np.zeros(self.n)
+        A0 = self.level_info(0)
+        grad = np.zeros(max(A0["nnz_A"], 1))
+        it = C.c_int()
+        check(self._lib.chronos_adjoint_grad(self._h, _pd(u), _pd(g), itmax, tol, _pd(lam),
+                                             _pd(grad), C.byref(it)))
+        return lam, grad[:A0["nnz_A"]], it.value
+
+
+def cpt_aspAMG(param, A, TV0=None):
+    """cpt_aspAMG.m:1: builds the hierarchy (param: chronos_params)."""
+    return Hierarchy(A, TV0, param)
+
+
+def AMG_Vcycle(hrc, b):
+    """AMG_Vcycle.m (x0 absent): x = M^{-1} b."""
+    return hrc.vcycle(b)
+
+
+def PCG_CJ(hrc, b, x0=None, itmax=15000, tol=1e-8):
+    """PCG_CJ.m:1: returns (x, iter, resvec, flag)."""
+    x, it, rv, flag, _ = hrc.pcg(b, x0, itmax, tol)
+    return x, it, rv, flag
+
+
+def SQMR(hrc, rhs, tol=1e-6, itmax=100, x0=None, A=None):
+    """SQMR.m:1 with the V-cycle as left preconditioner: (x, info, relres, niter)."""
+    return hrc.sqmr(rhs, tol, itmax, x0, A)

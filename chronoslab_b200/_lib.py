@@ -1,0 +1,130 @@
+"""ctypes declarations of the C ABI in include/chronos_b200.h.
+
+Loads chronoslab_b200/libchronos_b200.so (built in-tree by
+chronoslab_b200.build).  There is no fallback: a missing library raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libchronos_b200.so")
+
+CHRONOS_FP64 = 0
+CHRONOS_FP32 = 1
+
+STATUS = {0: "OK", -1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENOTSPD", -5: "EBREAKDOWN",
+          -6: "EIO", -7: "ENOTSUP"}
+
+
+class ChronosError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"chronos {STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class chronos_params(C.Structure):
+    _fields_ = [
+        ("nLevMax", C.c_int), ("maxCoarseSZ", C.c_int),
+        ("nthread", C.c_int), ("nupre", C.c_int), ("nupost", C.c_int), ("nstep", C.c_int),
+        ("step_size", C.c_int), ("epsilon", C.c_double), ("smoother_method", C.c_char * 32),
+        ("ntv", C.c_int), ("tspace_itmax", C.c_int), ("tspace_tol", C.c_double),
+        ("tspace_method", C.c_char * 32), ("init_approx", C.c_int),
+        ("SoC_type", C.c_char * 16), ("soc_tau", C.c_double), ("nl_agg", C.c_int),
+        ("proltype", C.c_char * 16), ("prol_emin", C.c_char * 16), ("prol_np", C.c_int),
+        ("itmax_vol", C.c_int), ("tol_vol", C.c_double), ("dist_min", C.c_int),
+        ("dist_max", C.c_int), ("maxcond", C.c_double), ("maxrownrm", C.c_double),
+        ("eps_prol", C.c_double), ("updateCF", C.c_int),
+        ("filt_np", C.c_int), ("filt_wgt", C.c_double), ("filt_tol", C.c_double),
+        ("filt_tau", C.c_double), ("min_patt", C.c_int),
+        ("ascii_input", C.c_int), ("rhs_build", C.c_char * 16), ("symmetric", C.c_int),
+        ("solv_method", C.c_char * 16), ("itmax", C.c_int), ("tol", C.c_double),
+        ("restart", C.c_int),
+        ("precision", C.c_int), ("use_graph", C.c_int), ("seed", C.c_uint64),
+        ("fsai_fabs", C.c_int),
+    ]
+
+
+class chronos_level_info(C.Structure):
+    _fields_ = [("n", C.c_int), ("nnz_A", C.c_int64), ("nnz_G", C.c_int64),
+                ("nnz_P", C.c_int64), ("nc", C.c_int), ("omega", C.c_double),
+                ("lambda_", C.c_double), ("threads_per_row", C.c_int)]
+
+
+_i = C.c_int
+_i64 = C.c_int64
+_u64 = C.c_uint64
+_d = C.c_double
+_pi = C.POINTER(C.c_int)
+_pi64 = C.POINTER(C.c_int64)
+_pd = C.POINTER(C.c_double)
+_vp = C.c_void_p
+_pp = C.POINTER(C.c_void_p)
+
+# name -> argtypes (every function returns int unless listed in _RESTYPE)
+SIGNATURES = {
+    "chronos_params_default": [C.POINTER(chronos_params)],
+    "chronos_params_read": [C.c_char_p, C.POINTER(chronos_params)],
+    "chronos_last_error": [C.c_char_p, _i],
+    "chronos_version": [],
+    "chronos_csr_info": [_vp, _pi, _pi, _pi64],
+    "chronos_csr_fetch": [_vp, _pi, _pi, _pd],
+    "chronos_csr_free": [_vp],
+    "chronos_fsai_pattern": [_i, _pi, _pi, _pd, _i, _i, _d, _i, _i, _pi, _pp],
+    "chronos_coarsen": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _u64, _pi, _pi, _pp],
+    "chronos_bamg": [C.POINTER(chronos_params), _i, _pi, _pi, _pi, _i, _pd, _pi, _pp],
+    "chronos_fsai_compute": [_i, _i, _i, _d, _d, _i, _i, _i64, _pi64, _pi, _pd, _pi64, _pi64,
+                             _pi, _pd, _pi],
+    "chronos_fsai_numeric": [_i, _pi64, _pi, _pd, _pi64, _pi, _pd, _pi],
+    "chronos_galerkin_compute": [_i, _i, _pi, _pi, _pd, _pi, _pi, _pd, _pi64, _pp],
+    "chronos_galerkin_fetch": [_vp, _pi, _pi, _pd],
+    "chronos_galerkin_free": [_vp],
+    "chronos_dense_chol": [_i, _pd, _pd],
+    "chronos_spmv": [_i, _i, _pi, _pi, _pd, _pd, _pd, _i],
+    "chronos_amg_setup": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _i, _pd, _pp],
+    "chronos_hier_free": [_vp],
+    "chronos_hier_nlevels": [_vp, _pi],
+    "chronos_hier_level_info": [_vp, _i, C.POINTER(chronos_level_info)],
+    "chronos_hier_export": [_vp, _i, C.c_char, _pi, _pi, _pi64, _pi, _pi, _pd],
+    "chronos_hier_setup_times": [_vp, _pd],
+    "chronos_diag_fix": [_i, _pi, _pi, _pd],
+    "chronos_vcycle": [_vp, _pd, _pd, _i],
+    "chronos_pcg": [_vp, _pd, _pd, _i, _d, _pi, _pd, _pi, _pd],
+    "chronos_pcg_dev": [_vp, _vp, _vp, _i, _d, _pi, _pd, _pi, _pd],
+    "chronos_pcg_block": [_vp, _i, _pd, _pd, _i, _d, _pi, _pi, _pd],
+    "chronos_sqmr": [_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _pi, _pd, _pi],
+    "chronos_adjoint_grad": [_vp, _pd, _pd, _i, _d, _pd, _pd, _pi],
+}
+_RESTYPE = {"chronos_params_default": None, "chronos_version": C.c_char_p}
+
+_lib = None
+
+
+def load():
+    """Loads the library once and declares every signature."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m chronoslab_b200.build` "
+                "(or __graft_entry__.build()); there is no CPU fallback")
+        lib = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPE.get(name, C.c_int)
+        _lib = lib
+    return _lib
+
+
+def last_error():
+    buf = C.create_string_buffer(4096)
+    load().chronos_last_error(buf, 4096)
+    return buf.value.decode(errors="replace")
+
+
+def check(code):
+    if code != 0:
+        raise ChronosError(code, last_error())
+    return code

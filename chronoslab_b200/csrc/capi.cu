@@ -1,0 +1,647 @@
+// extern "C" boundary of the library (include/chronos_b200.h).  Every entry
+// point converts C++ errors into a status code and records the message for
+// chronos_last_error(); no exception crosses the boundary.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "hier.h"
+#include "spmv.cuh"
+
+namespace chronos {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+
+template <typename F>
+static int guard(F &&f) {
+  try {
+    f();
+    return CHRONOS_OK;
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return CHRONOS_ENOMEM;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return CHRONOS_EINVAL;
+  } catch (...) {
+    set_last_error("unknown error");
+    return CHRONOS_EINVAL;
+  }
+}
+
+// 1-based CSR with int64 row pointers (the MEX layout, afsai_cpp.m:26-39) -> HostCSR.
+static HostCSR from_mex_csr(int n, int ncols, const int64_t *iat, const int *ja, const double *v) {
+  CHRONOS_REQUIRE(n > 0 && iat && ja && v, CHRONOS_EINVAL, "null CSR input");
+  CHRONOS_REQUIRE(iat[0] == 1, CHRONOS_EINVAL, "1-based CSR expected (iat[0] == 1)");
+  HostCSR h;
+  h.nrows = n;
+  h.ncols = ncols;
+  h.rp.resize((size_t)n + 1);
+  for (int i = 0; i <= n; ++i) {
+    h.rp[i] = iat[i] - 1;
+    CHRONOS_REQUIRE(i == 0 || h.rp[i] >= h.rp[i - 1], CHRONOS_EINVAL, "decreasing row pointers");
+  }
+  const int64_t nnz = h.rp[n];
+  h.ci.resize(nnz);
+  h.v.assign(v, v + nnz);
+  for (int64_t k = 0; k < nnz; ++k) {
+    h.ci[k] = ja[k] - 1;
+    CHRONOS_REQUIRE(h.ci[k] >= 0 && h.ci[k] < ncols, CHRONOS_EINVAL, "column index out of range");
+  }
+  for (int i = 0; i < n; ++i)
+    for (int64_t k = h.rp[i] + 1; k < h.rp[i + 1]; ++k)
+      CHRONOS_REQUIRE(h.ci[k] > h.ci[k - 1], CHRONOS_EINVAL, "columns must increase within a row");
+  return h;
+}
+
+static HostCSR from_csr0(int n, int ncols, const int *iat, const int *ja, const double *v) {
+  CHRONOS_REQUIRE(n > 0 && iat && (iat[n] == 0 || (ja && v)), CHRONOS_EINVAL, "null CSR input");
+  CHRONOS_REQUIRE(iat[0] == 0, CHRONOS_EINVAL, "0-based CSR expected (iat[0] == 0)");
+  HostCSR h;
+  h.nrows = n;
+  h.ncols = ncols;
+  h.rp.assign(iat, iat + n + 1);
+  const int64_t nnz = h.rp[n];
+  for (int i = 0; i < n; ++i)
+    CHRONOS_REQUIRE(h.rp[i + 1] >= h.rp[i], CHRONOS_EINVAL, "decreasing row pointers");
+  h.ci.assign(ja, ja + nnz);
+  h.v.assign(v, v + nnz);
+  for (int64_t k = 0; k < nnz; ++k)
+    CHRONOS_REQUIRE(h.ci[k] >= 0 && h.ci[k] < ncols, CHRONOS_EINVAL, "column index out of range");
+  for (int i = 0; i < n; ++i)
+    for (int64_t k = h.rp[i] + 1; k < h.rp[i + 1]; ++k)
+      CHRONOS_REQUIRE(h.ci[k] > h.ci[k - 1], CHRONOS_EINVAL,
+                      "CSR columns must be strictly increasing within a row");
+  return h;
+}
+
+struct ScopedStream {
+  cudaStream_t st = nullptr;
+  ScopedStream() { CHRONOS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)); }
+  ~ScopedStream() { if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); } }
+};
+
+// Device-side FSAI numeric phase on a host pattern; vals out in G's order.
+static int fsai_values(const HostCSR &A, const HostCSR &G, std::vector<double> &gval) {
+  ScopedStream s;
+  DMat dA, dG;
+  upload_csr(A, dA, false, s.st);
+  upload_csr(G, dG, false, s.st);
+  std::vector<int> rowlen(G.nrows);
+  for (int i = 0; i < G.nrows; ++i) {
+    rowlen[i] = (int)(G.rp[i + 1] - G.rp[i]);
+    CHRONOS_REQUIRE(rowlen[i] >= 1 && G.ci[G.rp[i + 1] - 1] == i, CHRONOS_EINVAL,
+                    "FSAI pattern rows must end with their diagonal");
+    for (int64_t k = G.rp[i]; k + 1 < G.rp[i + 1]; ++k)
+      CHRONOS_REQUIRE(G.ci[k] < i && (k == G.rp[i] || G.ci[k] > G.ci[k - 1]), CHRONOS_EINVAL,
+                      "FSAI pattern rows must list strictly-lower columns ascending");
+  }
+  const int fl = fsai_numeric_device(A.nrows, dA.rp, dA.ci, dA.v64, dG.rp, dG.ci, dG.v64,
+                                     rowlen, s.st);
+  gval.resize(G.nnz());
+  dG.v64.download(gval.data(), G.nnz(), s.st);
+  CHRONOS_CUDA(cudaStreamSynchronize(s.st));
+  return fl;
+}
+
+}  // namespace chronos
+
+using namespace chronos;
+
+struct chronos_hier {
+  std::unique_ptr<Hier> h;
+};
+
+struct chronos_galerkin_plan {
+  int nc = 0;
+  int64_t nnz = 0;
+  DBuf<int> rp, ci;
+  DBuf<double> v;
+};
+
+struct chronos_csr {
+  HostCSR m;
+};
+
+static chronos_csr *wrap_csr(HostCSR &&m) {
+  auto *r = new chronos_csr();
+  r->m = std::move(m);
+  return r;
+}
+
+extern "C" {
+
+int chronos_csr_info(const chronos_csr *m, int *nrows, int *ncols, int64_t *nnz) {
+  return guard([&] {
+    CHRONOS_REQUIRE(m && nrows && ncols && nnz, CHRONOS_EINVAL, "null argument");
+    *nrows = m->m.nrows;
+    *ncols = m->m.ncols;
+    *nnz = m->m.nnz();
+  });
+}
+
+int chronos_csr_fetch(const chronos_csr *m, int *iat_h, int *ja_h, double *val_h) {
+  return guard([&] {
+    CHRONOS_REQUIRE(m && iat_h && ja_h && val_h, CHRONOS_EINVAL, "null argument");
+    for (int i = 0; i <= m->m.nrows; ++i) iat_h[i] = (int)m->m.rp[i];
+    std::memcpy(ja_h, m->m.ci.data(), sizeof(int) * m->m.ci.size());
+    std::memcpy(val_h, m->m.v.data(), sizeof(double) * m->m.v.size());
+  });
+}
+
+int chronos_csr_free(chronos_csr *m) {
+  return guard([&] { delete m; });
+}
+
+int chronos_fsai_pattern(int n, const int *iat_h, const int *ja_h, const double *val_h, int nstep,
+                         int step_size, double eps, int nthread, int fsai_fabs, int *is_posdef,
+                         chronos_csr **G) {
+  return guard([&] {
+    CHRONOS_REQUIRE(is_posdef && G, CHRONOS_EINVAL, "null argument");
+    CHRONOS_REQUIRE(nstep >= 0 && step_size >= 1 && nstep * step_size <= 64, CHRONOS_EINVAL,
+                    "nstep*step_size must be <= 64");
+    HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
+    FsaiResult fr = fsai_adaptive(A, nstep, step_size, eps, nthread > 0 ? nthread : 1,
+                                  fsai_fabs == 0);
+    *is_posdef = fr.posdef ? 1 : 0;
+    *G = wrap_csr(std::move(fr.G));
+  });
+}
+
+int chronos_coarsen(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
+                    const double *val_h, uint64_t rng_skip, int *fcnode_h, int *nc,
+                    chronos_csr **S) {
+  return guard([&] {
+    CHRONOS_REQUIRE(prm && fcnode_h && nc, CHRONOS_EINVAL, "null argument");
+    HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
+    MT19937 rng((uint32_t)(prm->seed ? prm->seed : 5489));
+    for (uint64_t k = 0; k < rng_skip; ++k) rng.next_res53();
+    HostCSR Sm = soc_matrix(A, prm->SoC_type, prm->soc_tau);
+    std::vector<int> fc = pmis_split(A, Sm, rng, nc);
+    std::memcpy(fcnode_h, fc.data(), sizeof(int) * n);
+    if (S) *S = wrap_csr(std::move(Sm));
+  });
+}
+
+int chronos_bamg(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
+                 const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
+                 chronos_csr **P) {
+  return guard([&] {
+    CHRONOS_REQUIRE(prm && iat_S_h && ja_S_h && fcnode_h && TV_h && P && ntv >= 1 && n > 0,
+                    CHRONOS_EINVAL, "bad argument");
+    HostCSR S;
+    S.nrows = S.ncols = n;
+    S.rp.assign(iat_S_h, iat_S_h + n + 1);
+    S.ci.assign(ja_S_h, ja_S_h + S.rp[n]);
+    S.v.assign(S.rp[n], 1.0);
+    std::vector<int> fc0(n);
+    int nc = 0;
+    for (int i = 0; i < n; ++i) {
+      fc0[i] = fcnode_h[i] > 0 ? fcnode_h[i] - 1 : -1;
+      if (fcnode_h[i] > 0) ++nc;
+    }
+    std::vector<double> TVr((size_t)n * ntv);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < ntv; ++j) TVr[(size_t)i * ntv + j] = TV_h[(size_t)j * n + i];
+    int nth = prm->prol_np;
+    if (nth <= 0) nth = 1;
+    BamgParams bp{prm->itmax_vol, prm->dist_min, prm->dist_max, ntv, nth, prm->maxcond,
+                  prm->maxrownrm, prm->tol_vol, prm->eps_prol};
+    std::vector<int> cm;
+    HostCSR Pm = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, cm);
+    if (c_mark_h) std::memcpy(c_mark_h, cm.data(), sizeof(int) * n);
+    *P = wrap_csr(std::move(Pm));
+  });
+}
+
+void chronos_params_default(chronos_params *p) {
+  if (p) params_default(p);
+}
+
+int chronos_params_read(const char *fnames_path, chronos_params *p) {
+  return guard([&] {
+    CHRONOS_REQUIRE(fnames_path && p, CHRONOS_EINVAL, "null argument");
+    params_read(fnames_path, p);
+  });
+}
+
+int chronos_last_error(char *buf, int len) {
+  if (!buf || len <= 0) return CHRONOS_EINVAL;
+  std::snprintf(buf, (size_t)len, "%s", g_last_error.c_str());
+  return CHRONOS_OK;
+}
+
+const char *chronos_version(void) { return "chronos_b200 1.0 (sm_100a)"; }
+
+int chronos_fsai_compute(int nthread, int n_step, int step_size, double tau, double eps,
+                         int nrows, int nrows_M, int64_t nterm_M, const int64_t *iat_M_h,
+                         const int *ja_M_h, const double *coef_M_h, int64_t *nterm_G,
+                         int64_t *iat_G_h, int *ja_G_h, double *coef_G_h, int *is_posdef) {
+  return guard([&] {
+    CHRONOS_REQUIRE(nterm_G && iat_G_h && ja_G_h && coef_G_h && is_posdef, CHRONOS_EINVAL,
+                    "null output");
+    CHRONOS_REQUIRE(nrows == nrows_M, CHRONOS_ENOTSUP,
+                    "trailing-block FSAI (nrows_M > nrows) is outside this path");
+    CHRONOS_REQUIRE(tau == 0.0, CHRONOS_ENOTSUP, "FSAI dropping (tau > 0) is outside this path");
+    CHRONOS_REQUIRE(n_step >= 0 && step_size >= 1 && n_step * step_size <= 64, CHRONOS_EINVAL,
+                    "n_step*step_size must be <= 64");
+    HostCSR A = from_mex_csr(nrows, nrows, iat_M_h, ja_M_h, coef_M_h);
+    CHRONOS_REQUIRE(A.nnz() == nterm_M, CHRONOS_EINVAL, "nterm_M does not match iat_M");
+    FsaiResult fr = fsai_adaptive(A, n_step, step_size, eps, nthread, true);
+    std::vector<double> gval;
+    const int fl = fsai_values(A, fr.G, gval);
+    const HostCSR &G = fr.G;
+    for (int i = 0; i <= nrows; ++i) iat_G_h[i] = G.rp[i] + 1;
+    for (int64_t k = 0; k < G.nnz(); ++k) {
+      ja_G_h[k] = G.ci[k] + 1;
+      coef_G_h[k] = gval[k];
+    }
+    *nterm_G = G.nnz();
+    *is_posdef = (fr.posdef && fl == 0) ? 1 : 0;
+  });
+}
+
+int chronos_fsai_numeric(int n, const int64_t *iat_A_h, const int *ja_A_h, const double *val_A_h,
+                         const int64_t *iat_G_h, const int *ja_G_h, double *val_G_h,
+                         int *is_posdef) {
+  return guard([&] {
+    CHRONOS_REQUIRE(val_G_h && is_posdef && iat_G_h && ja_G_h, CHRONOS_EINVAL, "null argument");
+    HostCSR A = from_mex_csr(n, n, iat_A_h, ja_A_h, val_A_h);
+    HostCSR G;
+    G.nrows = G.ncols = n;
+    G.rp.resize((size_t)n + 1);
+    for (int i = 0; i <= n; ++i) G.rp[i] = iat_G_h[i] - 1;
+    CHRONOS_REQUIRE(G.rp[0] == 0, CHRONOS_EINVAL, "1-based G pattern expected");
+    G.ci.resize(G.rp[n]);
+    for (int64_t k = 0; k < G.rp[n]; ++k) {
+      G.ci[k] = ja_G_h[k] - 1;
+      CHRONOS_REQUIRE(G.ci[k] >= 0 && G.ci[k] < n, CHRONOS_EINVAL, "G column out of range");
+    }
+    G.v.assign(G.rp[n], 0.0);
+    std::vector<double> gval;
+    const int fl = fsai_values(A, G, gval);
+    std::memcpy(val_G_h, gval.data(), sizeof(double) * gval.size());
+    *is_posdef = fl == 0 ? 1 : 0;
+  });
+}
+
+int chronos_galerkin_compute(int n, int nc, const int *iat_A_h, const int *ja_A_h,
+                             const double *val_A_h, const int *iat_P_h, const int *ja_P_h,
+                             const double *val_P_h, int64_t *nnz_Ac, chronos_galerkin_plan **plan) {
+  return guard([&] {
+    CHRONOS_REQUIRE(plan && nnz_Ac && nc > 0, CHRONOS_EINVAL, "bad argument");
+    HostCSR A = from_csr0(n, n, iat_A_h, ja_A_h, val_A_h);
+    HostCSR P = from_csr0(n, nc, iat_P_h, ja_P_h, val_P_h);
+    for (int i = 0; i < n; ++i)
+      for (int64_t k = A.rp[i] + 1; k < A.rp[i + 1]; ++k)
+        CHRONOS_REQUIRE(A.ci[k] > A.ci[k - 1], CHRONOS_EINVAL, "A rows must be sorted");
+    HostCSR Pt = csr_transpose(P);
+    ScopedStream s;
+    DMat dA, dP, dPt;
+    upload_csr(A, dA, false, s.st);
+    upload_csr(P, dP, false, s.st);
+    upload_csr(Pt, dPt, false, s.st);
+    DBuf<int> aprp, apci;
+    DBuf<double> apv;
+    int64_t nnz_ap = 0;
+    spgemm_device(n, nc, dA.rp, dA.ci, dA.v64, dP.rp, dP.ci, dP.v64, aprp, apci, apv, &nnz_ap, s.st);
+    auto *pl = new chronos_galerkin_plan();
+    try {
+      pl->nc = nc;
+      spgemm_device(nc, nc, dPt.rp, dPt.ci, dPt.v64, aprp, apci, apv, pl->rp, pl->ci, pl->v,
+                    &pl->nnz, s.st);
+    } catch (...) {
+      delete pl;
+      throw;
+    }
+    *nnz_Ac = pl->nnz;
+    *plan = pl;
+  });
+}
+
+int chronos_galerkin_fetch(chronos_galerkin_plan *plan, int *iat_Ac_h, int *ja_Ac_h,
+                           double *val_Ac_h) {
+  return guard([&] {
+    CHRONOS_REQUIRE(plan && iat_Ac_h && ja_Ac_h && val_Ac_h, CHRONOS_EINVAL, "null argument");
+    plan->rp.download(iat_Ac_h, (size_t)plan->nc + 1);
+    plan->ci.download(ja_Ac_h, plan->nnz);
+    plan->v.download(val_Ac_h, plan->nnz);
+    CHRONOS_CUDA(cudaDeviceSynchronize());
+  });
+}
+
+int chronos_galerkin_free(chronos_galerkin_plan *plan) {
+  return guard([&] { delete plan; });
+}
+
+int chronos_dense_chol(int n, const double *A_h, double *L_h) {
+  return guard([&] {
+    CHRONOS_REQUIRE(n > 0 && n <= 8192 && A_h && L_h, CHRONOS_EINVAL, "bad argument (n <= 8192)");
+    ScopedStream s;
+    DBuf<double> d;
+    d.upload(A_h, (size_t)n * n, s.st);
+    const int info = dense_cholesky_device(n, d.get(), s.st);
+    CHRONOS_REQUIRE(info == 0, CHRONOS_ENOTSPD, "non-positive pivot " + std::to_string(info));
+    d.download(L_h, (size_t)n * n, s.st);
+    CHRONOS_CUDA(cudaStreamSynchronize(s.st));
+  });
+}
+
+int chronos_spmv(int n, int ncols, const int *iat_h, const int *ja_h, const double *val_h,
+                 const double *x_h, double *y_h, int precision) {
+  return guard([&] {
+    CHRONOS_REQUIRE(x_h && y_h, CHRONOS_EINVAL, "null vector");
+    HostCSR A = from_csr0(n, ncols, iat_h, ja_h, val_h);
+    ScopedStream s;
+    DMat d;
+    const bool fp32 = precision == CHRONOS_FP32;
+    upload_csr(A, d, fp32, s.st);
+    autotune_lanes(d, fp32, s.st);
+    if (fp32) {
+      std::vector<float> xf(x_h, x_h + ncols), yf(n);
+      DBuf<float> x, y(n);
+      x.upload(xf, s.st);
+      csr_apply<float, float, float, float, MODE_PLAIN, false>(s.st, d.lanes, n, d.rp, d.ci, d.v32,
+                                                              x.get(), nullptr, y.get(), 1.0f);
+      y.download(yf.data(), n, s.st);
+      CHRONOS_CUDA(cudaStreamSynchronize(s.st));
+      for (int i = 0; i < n; ++i) y_h[i] = yf[i];
+    } else {
+      DBuf<double> x, y(n);
+      x.upload(x_h, ncols, s.st);
+      csr_apply<double, double, double, double, MODE_PLAIN, false>(
+          s.st, d.lanes, n, d.rp, d.ci, d.v64, x.get(), nullptr, y.get(), 1.0);
+      y.download(y_h, n, s.st);
+      CHRONOS_CUDA(cudaStreamSynchronize(s.st));
+    }
+  });
+}
+
+int chronos_amg_setup(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
+                      const double *val_h, int ntv0, const double *TV0_h, chronos_hier **out) {
+  return guard([&] {
+    CHRONOS_REQUIRE(prm && out, CHRONOS_EINVAL, "null argument");
+    CHRONOS_REQUIRE(ntv0 == 0 || TV0_h, CHRONOS_EINVAL, "TV0 missing");
+    HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
+    auto *hh = new chronos_hier();
+    try {
+      hh->h = build_hierarchy(*prm, A, ntv0, TV0_h);
+    } catch (...) {
+      delete hh;
+      throw;
+    }
+    *out = hh;
+  });
+}
+
+int chronos_hier_free(chronos_hier *h) {
+  return guard([&] { delete h; });
+}
+
+int chronos_hier_nlevels(const chronos_hier *h, int *nlev) {
+  return guard([&] {
+    CHRONOS_REQUIRE(h && nlev, CHRONOS_EINVAL, "null argument");
+    *nlev = (int)h->h->levels.size();
+  });
+}
+
+int chronos_hier_level_info(const chronos_hier *h, int level, chronos_level_info *info) {
+  return guard([&] {
+    CHRONOS_REQUIRE(h && info && level >= 0 && level < (int)h->h->levels.size(), CHRONOS_EINVAL,
+                    "bad level");
+    const Level &L = h->h->levels[level];
+    info->n = L.n;
+    info->nnz_A = L.A.nnz;
+    info->nnz_G = L.coarsest ? 0 : L.G.nnz;
+    info->nnz_P = L.coarsest ? 0 : L.P.nnz;
+    info->nc = L.coarsest ? 0 : L.nc;
+    info->omega = L.omega;
+    info->lambda = L.lambda;
+    info->threads_per_row = L.A.lanes;
+  });
+}
+
+int chronos_hier_export(const chronos_hier *h, int level, char which, int *nrows, int *ncols,
+                        int64_t *nnz, int *iat_h, int *ja_h, double *val_h) {
+  return guard([&] {
+    CHRONOS_REQUIRE(h && nrows && ncols && nnz && level >= 0 &&
+                        level < (int)h->h->levels.size(), CHRONOS_EINVAL, "bad argument");
+    const Level &L = h->h->levels[level];
+    const DMat *m = nullptr;
+    if (which == 'A') m = &L.A;
+    else if (which == 'G' && !L.coarsest) m = &L.G;
+    else if (which == 'P' && !L.coarsest) m = &L.P;
+    CHRONOS_REQUIRE(m, CHRONOS_EINVAL, "matrix not available on this level");
+    *nrows = m->nrows;
+    *ncols = m->ncols;
+    *nnz = m->nnz;
+    if (!iat_h || !ja_h || !val_h) return;
+    m->rp.download(iat_h, (size_t)m->nrows + 1, h->h->st);
+    m->ci.download(ja_h, m->nnz, h->h->st);
+    m->v64.download(val_h, m->nnz, h->h->st);
+    CHRONOS_CUDA(cudaStreamSynchronize(h->h->st));
+  });
+}
+
+int chronos_hier_setup_times(const chronos_hier *h, double *t8) {
+  return guard([&] {
+    CHRONOS_REQUIRE(h && t8, CHRONOS_EINVAL, "null argument");
+    for (int i = 0; i < 8; ++i) t8[i] = h->h->times[i];
+  });
+}
+
+int chronos_diag_fix(int n, const int *iat_h, const int *ja_h, double *val_h) {
+  return guard([&] {
+    HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
+    ScopedStream s;
+    DMat d;
+    upload_csr(A, d, false, s.st);
+    auto mv = [&](const double *x, double *y) {
+      csr_apply<double, double, double, double, MODE_PLAIN, false>(s.st, 8, n, d.rp, d.ci, d.v64, x,
+                                                                  nullptr, y, 1.0);
+    };
+    // |lambda|_max of A (eigs(A,1,'lm'), A SPD: the largest eigenvalue)
+    const double lmax = lanczos_lmax(n, mv, 1e-3, 300, s.st);
+    for (int i = 0; i < n; ++i)
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if (A.ci[k] == i && val_h[k] == 1.0) val_h[k] = lmax / 10.0;
+  });
+}
+
+int chronos_vcycle(chronos_hier *hh, const double *b_h, double *x_h, int nrhs) {
+  return guard([&] {
+    CHRONOS_REQUIRE(hh && b_h && x_h && nrhs >= 1, CHRONOS_EINVAL, "bad argument");
+    Hier &h = *hh->h;
+    const int n = h.levels[0].n;
+    DBuf<double> b(n), x(n);
+    for (int c = 0; c < nrhs; ++c) {
+      b.upload(b_h + (size_t)c * n, n, h.st);
+      h.vcycle(b.get(), x.get(), nullptr, nullptr);
+      x.download(x_h + (size_t)c * n, n, h.st);
+    }
+    CHRONOS_CUDA(cudaStreamSynchronize(h.st));
+  });
+}
+
+int chronos_pcg_dev(chronos_hier *hh, const double *b_d, double *x_d, int itmax, double tol,
+                    int *iters, double *resvec_h, int *flag, double *seconds) {
+  return guard([&] {
+    CHRONOS_REQUIRE(hh && b_d && x_d && iters && flag, CHRONOS_EINVAL, "null argument");
+    std::vector<double> rv;
+    int it = 0, fl = 0;
+    try {
+      hh->h->pcg_solve(b_d, x_d, itmax, tol, &it, &fl, resvec_h ? &rv : nullptr, seconds);
+    } catch (const Error &e) {
+      *iters = it;
+      *flag = 1;
+      throw;
+    }
+    *iters = it;
+    *flag = fl;
+    if (resvec_h) std::memcpy(resvec_h, rv.data(), sizeof(double) * rv.size());
+  });
+}
+
+int chronos_pcg(chronos_hier *hh, const double *b_h, double *x_h, int itmax, double tol,
+                int *iters, double *resvec_h, int *flag, double *seconds) {
+  return guard([&] {
+    CHRONOS_REQUIRE(hh && b_h && x_h && iters && flag, CHRONOS_EINVAL, "null argument");
+    Hier &h = *hh->h;
+    const int n = h.levels[0].n;
+    DBuf<double> b, x;
+    b.upload(b_h, n, h.st);
+    x.upload(x_h, n, h.st);
+    std::vector<double> rv;
+    int it = 0, fl = 0;
+    h.pcg_solve(b.get(), x.get(), itmax, tol, &it, &fl, resvec_h ? &rv : nullptr, seconds);
+    x.download(x_h, n, h.st);
+    CHRONOS_CUDA(cudaStreamSynchronize(h.st));
+    *iters = it;
+    *flag = fl;
+    if (resvec_h) std::memcpy(resvec_h, rv.data(), sizeof(double) * rv.size());
+  });
+}
+
+int chronos_pcg_block(chronos_hier *hh, int nrhs, const double *B_h, double *X_h, int itmax,
+                      double tol, int *iters_h, int *flags_h, double *seconds) {
+  return guard([&] {
+    CHRONOS_REQUIRE(hh && B_h && X_h && iters_h && flags_h && nrhs >= 1, CHRONOS_EINVAL,
+                    "bad argument");
+    Hier &h = *hh->h;
+    const int n = h.levels[0].n;
+    DBuf<double> b(n), x(n);
+    double total = 0.0;
+    for (int c = 0; c < nrhs; ++c) {
+      b.upload(B_h + (size_t)c * n, n, h.st);
+      x.upload(X_h + (size_t)c * n, n, h.st);
+      double sec = 0.0;
+      h.pcg_solve(b.get(), x.get(), itmax, tol, &iters_h[c], &flags_h[c], nullptr, &sec);
+      total += sec;
+      x.download(X_h + (size_t)c * n, n, h.st);
+    }
+    CHRONOS_CUDA(cudaStreamSynchronize(h.st));
+    if (seconds) *seconds = total;
+  });
+}
+
+int chronos_sqmr(chronos_hier *hh, const int *iat_h, const int *ja_h, const double *val_h,
+                 const double *b_h, double *x_h, int itmax, double tol, int *iters,
+                 double *relres, int *info) {
+  return guard([&] {
+    CHRONOS_REQUIRE(hh && b_h && x_h && iters && relres && info, CHRONOS_EINVAL, "null argument");
+    Hier &h = *hh->h;
+    cudaStream_t st = h.st;
+    const int n = h.levels[0].n;
+    DMat op;
+    if (iat_h) {
+      upload_csr(from_csr0(n, n, iat_h, ja_h, val_h), op, false, st);
+      autotune_lanes(op, false, st);
+    }
+    auto apply_op = [&](const double *x, double *y) {
+      if (!iat_h) { h.apply_A(x, y); return; }
+      csr_apply<double, double, double, double, MODE_PLAIN, false>(st, op.lanes, n, op.rp, op.ci,
+                                                                  op.v64, x, nullptr, y, 1.0);
+    };
+    DBuf<double> rhs, pnew, r(n), q(n), d(n), vscr(n), u(n), tmp(n), scratch(256);
+    rhs.upload(b_h, n, st);
+    pnew.upload(x_h, n, st);
+    d.zero(st);
+    auto dot = [&](const double *a, const double *b) { return device_dot(n, a, b, scratch.get(), st); };
+    auto lprec = [&](const double *in, double *out) { h.vcycle(in, out, nullptr, nullptr); };
+    // SQMR.m:24-36
+    const double bnorm = std::sqrt(dot(rhs.get(), rhs.get()));
+    apply_op(pnew.get(), tmp.get());
+    device_scale_copy(n, 1.0, rhs.get(), r.get(), st);
+    device_axpby(n, -1.0, tmp.get(), 1.0, r.get(), st);
+    lprec(r.get(), vscr.get());
+    device_scale_copy(n, 1.0, vscr.get(), q.get(), st);
+    double tau = std::sqrt(dot(vscr.get(), vscr.get()));
+    double rho0 = dot(r.get(), q.get());
+    double theta0 = 0.0;
+    int niter = 0, inf = 0;
+    bool exit_test = false;
+    while (!exit_test && niter < itmax) {
+      ++niter;
+      apply_op(q.get(), vscr.get());
+      const double sigma = dot(q.get(), vscr.get());
+      if (std::fabs(sigma) < 1e-20 * rho0) { inf = 10; break; }
+      const double alpha = rho0 / sigma;
+      device_axpby(n, -alpha, vscr.get(), 1.0, r.get(), st);
+      lprec(r.get(), vscr.get());
+      const double theta1 = std::sqrt(dot(vscr.get(), vscr.get())) / tau;
+      const double gamma = 1.0 / std::sqrt(1.0 + theta1 * theta1);
+      tau = tau * theta1 * gamma;
+      // d = d*gamma^2*theta0^2 + gamma^2*alpha*q
+      device_axpby(n, gamma * gamma * alpha, q.get(), gamma * gamma * theta0 * theta0, d.get(), st);
+      theta0 = theta1;
+      device_axpby(n, 1.0, d.get(), 1.0, pnew.get(), st);
+      const double resnorm = std::sqrt(dot(r.get(), r.get())) / bnorm;
+      if (resnorm < tol) {
+        exit_test = true;
+      } else {
+        device_scale_copy(n, 1.0, vscr.get(), u.get(), st);
+        const double rho1 = dot(r.get(), u.get());
+        if (std::fabs(rho0) < 1e-20 * rho1) { inf = 20; break; }
+        const double beta = rho1 / rho0;
+        rho0 = rho1;
+        device_axpby(n, 1.0, u.get(), beta, q.get(), st);
+      }
+    }
+    if (niter >= itmax) inf = 1;
+    apply_op(pnew.get(), tmp.get());
+    device_axpby(n, 1.0, rhs.get(), -1.0, tmp.get(), st);
+    *relres = std::sqrt(dot(tmp.get(), tmp.get())) / bnorm;
+    *iters = niter;
+    *info = inf;
+    pnew.download(x_h, n, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+int chronos_adjoint_grad(chronos_hier *hh, const double *u_h, const double *g_h, int itmax,
+                         double tol, double *lambda_h, double *grad_h, int *iters) {
+  return guard([&] {
+    CHRONOS_REQUIRE(hh && u_h && g_h && lambda_h && grad_h && iters, CHRONOS_EINVAL, "null argument");
+    Hier &h = *hh->h;
+    const int n = h.levels[0].n;
+    const DMat &A = h.levels[0].A;
+    DBuf<double> u, g, lam(n), grad(std::max<int64_t>(A.nnz, 1));
+    u.upload(u_h, n, h.st);
+    g.upload(g_h, n, h.st);
+    lam.zero(h.st);
+    int it = 0, fl = 0;
+    h.pcg_solve(g.get(), lam.get(), itmax, tol, &it, &fl, nullptr, nullptr);
+    adjoint_scatter(n, A.rp, A.ci, lam.get(), u.get(), grad.get(), h.st);
+    lam.download(lambda_h, n, h.st);
+    grad.download(grad_h, A.nnz, h.st);
+    CHRONOS_CUDA(cudaStreamSynchronize(h.st));
+    *iters = it;
+    CHRONOS_REQUIRE(fl == 0, CHRONOS_EBREAKDOWN, "adjoint solve did not converge");
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+// Shared helpers of the chronos_b200 library: status handling, device buffers,
+// warp/block reductions.  sm_100a only.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "errors.h"
+
+namespace chronos {
+
+#define CHRONOS_CUDA(call)                                                        \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      throw ::chronos::Error(CHRONOS_ECUDA, std::string(#call) + ": " +             \
+                                                cudaGetErrorString(e_) + " at " +   \
+                                                __FILE__ + ":" + std::to_string(__LINE__)); \
+    }                                                                               \
+  } while (0)
+
+#define CHRONOS_CHECK_LAUNCH() CHRONOS_CUDA(cudaGetLastError())
+
+// Owning device allocation (cudaMalloc / cudaFree), movable, typed.
+template <typename T>
+class DBuf {
+ public:
+  DBuf() = default;
+  explicit DBuf(size_t n) { alloc(n); }
+  ~DBuf() { release(); }
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  DBuf(DBuf &&o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+  DBuf &operator=(DBuf &&o) noexcept {
+    if (this != &o) { release(); p_ = o.p_; n_ = o.n_; o.p_ = nullptr; o.n_ = 0; }
+    return *this;
+  }
+  void alloc(size_t n) {
+    release();
+    if (n == 0) return;
+    cudaError_t e = cudaMalloc(&p_, n * sizeof(T));
+    if (e != cudaSuccess) {
+      p_ = nullptr;
+      cudaGetLastError();
+      throw Error(CHRONOS_ENOMEM, "cudaMalloc of " + std::to_string(n * sizeof(T)) +
+                                      " bytes failed: " + cudaGetErrorString(e));
+    }
+    n_ = n;
+  }
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  void upload(const T *h, size_t n, cudaStream_t s = 0) {
+    if (n_ < n) alloc(n);
+    if (n) CHRONOS_CUDA(cudaMemcpyAsync(p_, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T> &h, cudaStream_t s = 0) { upload(h.data(), h.size(), s); }
+  void download(T *h, size_t n, cudaStream_t s = 0) const {
+    if (n) CHRONOS_CUDA(cudaMemcpyAsync(h, p_, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+  std::vector<T> to_host(cudaStream_t s = 0) const {
+    std::vector<T> h(n_);
+    download(h.data(), n_, s);
+    CHRONOS_CUDA(cudaStreamSynchronize(s));
+    return h;
+  }
+  void zero(cudaStream_t s = 0) {
+    if (n_) CHRONOS_CUDA(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
+  }
+  T *get() const { return p_; }
+  size_t size() const { return n_; }
+  operator T *() const { return p_; }
+
+ private:
+  T *p_ = nullptr;
+  size_t n_ = 0;
+};
+
+// ---- device helpers ------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over groups of L consecutive lanes (L a power of two <= 32); every lane
+// of the group ends with the group sum.
+template <int L, typename T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic block reduction of one double per thread; result valid in
+// thread 0.  blockDim.x must be a multiple of 32 and <= 1024.
+__device__ __forceinline__ double block_sum(double v, double *smem32) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) smem32[wid] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (wid == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    r = lane < nw ? smem32[lane] : 0.0;
+    r = warp_sum(r);
+  }
+  __syncthreads();
+  return r;
+}
+
+inline int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    CHRONOS_CUDA(cudaGetDevice(&dev));
+    CHRONOS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  }
+  return sms;
+}
+
+inline unsigned ceil_div(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace chronos

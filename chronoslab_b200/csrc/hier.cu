@@ -1,0 +1,819 @@
+// AMG hierarchy on the GPU: setup orchestration (cpt_aspAMG.m), the V-cycle
+// (AMG_Vcycle.m) and the outer PCG_CJ loop (PCG_CJ.m) as one CUDA graph.
+//
+// Setup per level (cpt_aspAMG.m:87-347, filters off):
+//   host  adaptive FSAI pattern search          smoother.m:35 -> afsai_cpp
+//   GPU   FSAI numeric phase (FP64 local solves) cpt_afsai_coef.cpp:440-541
+//   GPU   lambda_max(G A G') by Lanczos -> omega = min(1, 1.9/lambda)   smoother.m:73-81
+//   host  test space qr (tspace NONE), SoC + PMIS, BAMG prolongation
+//   GPU   Galerkin Ac = P'(A P) (FP64, Gustavson order)                   cpt_aspAMG.m:277
+//   GPU   coarsest: dense FP64 Cholesky and inverse                      cpt_aspAMG.m:107-116
+// The stored hierarchy is FP32 (values of A_l, G_l, G_l', P_l, P_l' with FP32
+// accumulation) or FP64; the outer PCG, its dot products, the level-1 operator
+// used by PCG and the coarsest solve stay FP64.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "hier.h"
+#include "spmv.cuh"
+
+namespace chronos {
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+PcgState::~PcgState() {
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+}
+
+Hier::~Hier() {
+  if (st) cudaStreamSynchronize(st);
+  levels.clear();
+  if (pcg.exec) { cudaGraphExecDestroy(pcg.exec); pcg.exec = nullptr; }
+  if (pcg.graph) { cudaGraphDestroy(pcg.graph); pcg.graph = nullptr; }
+  if (st) cudaStreamDestroy(st);
+}
+
+// ---------------------------------------------------------------------------
+// Device matrices
+// ---------------------------------------------------------------------------
+
+void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st) {
+  CHRONOS_REQUIRE(h.nnz() < INT32_MAX, CHRONOS_ENOTSUP, "matrix with 2^31 or more entries");
+  d.nrows = h.nrows;
+  d.ncols = h.ncols;
+  d.nnz = h.nnz();
+  std::vector<int> rp(h.rp.begin(), h.rp.end());
+  d.rp.upload(rp, st);
+  d.ci.upload(h.ci, st);
+  d.v64.upload(h.v, st);
+  if (fp32) {
+    d.v32.alloc(std::max<int64_t>(d.nnz, 1));
+    convert_f64_to_f32(d.nnz, d.v64.get(), d.v32.get(), st);
+  }
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+}
+
+static int heuristic_lanes(const DMat &m) {
+  const double avg = m.nrows ? (double)m.nnz / m.nrows : 1.0;
+  int L = 2;
+  while (L < 32 && L < avg * 0.75) L <<= 1;
+  return L;
+}
+
+void autotune_lanes(DMat &m, bool fp32, cudaStream_t st) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int64_t, int, bool>, int> cache;
+  if (m.nrows <= 0) return;
+  const auto key = std::make_tuple(m.nrows, m.nnz, m.ncols, fp32);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) { m.lanes = it->second; return; }
+  }
+  m.lanes = heuristic_lanes(m);
+  if (m.nnz < 4096) {                      // launch-latency bound: no timing
+    std::lock_guard<std::mutex> lk(mu);
+    cache[key] = m.lanes;
+    return;
+  }
+  DBuf<double> x64(m.ncols), y64(m.nrows);
+  DBuf<float> x32(m.ncols), y32(m.nrows);
+  x64.zero(st);
+  x32.zero(st);
+  cudaEvent_t e0, e1;
+  CHRONOS_CUDA(cudaEventCreate(&e0));
+  CHRONOS_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int bestL = m.lanes;
+  for (int L : {2, 4, 8, 16, 32}) {
+    auto launch = [&]() {
+      if (fp32)
+        csr_apply<float, float, float, float, MODE_PLAIN, false>(st, L, m.nrows, m.rp, m.ci, m.v32,
+                                                               x32.get(), nullptr, y32.get(), 1.0f);
+      else
+        csr_apply<double, double, double, double, MODE_PLAIN, false>(
+            st, L, m.nrows, m.rp, m.ci, m.v64, x64.get(), nullptr, y64.get(), 1.0);
+    };
+    launch();
+    CHRONOS_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < 5; ++r) launch();
+    CHRONOS_CUDA(cudaEventRecord(e1, st));
+    CHRONOS_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) { best = ms; bestL = L; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  m.lanes = bestL;
+  std::lock_guard<std::mutex> lk(mu);
+  cache[key] = bestL;
+}
+
+// ---------------------------------------------------------------------------
+// Lanczos estimate of lambda_max (replaces eigs(...,'la', tol) / 'lm')
+// ---------------------------------------------------------------------------
+
+// Largest eigenvalue of the symmetric tridiagonal (a, b) by Sturm bisection.
+static double tridiag_lmax(const std::vector<double> &a, const std::vector<double> &b) {
+  const int m = (int)a.size();
+  double lo = 1e300, hi = -1e300;
+  for (int i = 0; i < m; ++i) {
+    double r = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i + 1 < m ? std::fabs(b[i]) : 0.0);
+    lo = std::min(lo, a[i] - r);
+    hi = std::max(hi, a[i] + r);
+  }
+  auto count_below = [&](double x) {   // eigenvalues < x
+    int c = 0;
+    double d = 1.0;
+    for (int i = 0; i < m; ++i) {
+      double bb = i > 0 ? b[i - 1] * b[i - 1] : 0.0;
+      d = a[i] - x - (i > 0 ? bb / d : 0.0);
+      if (d == 0.0) d = -1e-300;
+      if (d < 0) ++c;
+    }
+    return c;
+  };
+  for (int it = 0; it < 200 && hi - lo > 1e-15 * std::max(std::fabs(hi), 1e-300); ++it) {
+    double mid = 0.5 * (lo + hi);
+    if (count_below(mid) >= m) hi = mid; else lo = mid;
+  }
+  return hi;
+}
+
+double lanczos_lmax(int n, const std::function<void(const double *, double *)> &mv, double tol,
+                    int maxit, cudaStream_t st) {
+  DBuf<double> v(n), vp(n), w(n), scratch(256);
+  std::vector<double> ones(n, 1.0 / std::sqrt((double)n));
+  v.upload(ones, st);
+  vp.zero(st);
+  std::vector<double> a, b;
+  double theta = 0.0, beta = 0.0;
+  for (int j = 0; j < maxit; ++j) {
+    mv(v.get(), w.get());
+    const double alpha = device_dot(n, w.get(), v.get(), scratch.get(), st);
+    device_axpby(n, -alpha, v.get(), 1.0, w.get(), st);
+    if (j > 0) device_axpby(n, -beta, vp.get(), 1.0, w.get(), st);
+    a.push_back(alpha);
+    beta = std::sqrt(std::max(device_dot(n, w.get(), w.get(), scratch.get(), st), 0.0));
+    const double th = tridiag_lmax(a, b);
+    const bool conv = j > 0 && std::fabs(th - theta) <= tol * std::fabs(th);
+    theta = th;
+    if (conv || beta <= 1e-300 * std::fabs(theta)) break;
+    b.push_back(beta);
+    std::swap(vp, v);                     // vp <- v
+    device_scale_copy(n, 1.0 / beta, w.get(), v.get(), st);
+  }
+  return theta;
+}
+
+// ---------------------------------------------------------------------------
+// Setup
+// ---------------------------------------------------------------------------
+
+static void alloc_vectors(Level &L, int precision, cudaStream_t st) {
+  const size_t n = std::max(L.n, 1);
+  if (precision == CHRONOS_FP32) {
+    L.b32.alloc(n); L.x32.alloc(n); L.r32.alloc(n); L.t32.alloc(n);
+    L.b32.zero(st); L.x32.zero(st); L.r32.zero(st); L.t32.zero(st);
+  } else {
+    L.b64.alloc(n); L.x64.alloc(n); L.r64.alloc(n); L.t64.alloc(n);
+    L.b64.zero(st); L.x64.zero(st); L.r64.zero(st); L.t64.zero(st);
+  }
+}
+
+static HostCSR download_csr(int nrows, int ncols, const DBuf<int> &rp, const DBuf<int> &ci,
+                            const DBuf<double> &v, int64_t nnz, cudaStream_t st) {
+  HostCSR h;
+  h.nrows = nrows;
+  h.ncols = ncols;
+  std::vector<int> r(nrows + 1);
+  rp.download(r.data(), nrows + 1, st);
+  h.ci.resize(nnz);
+  h.v.resize(nnz);
+  ci.download(h.ci.data(), nnz, st);
+  v.download(h.v.data(), nnz, st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  h.rp.assign(r.begin(), r.end());
+  return h;
+}
+
+static void validate_csr(const HostCSR &A) {
+  CHRONOS_REQUIRE(A.nrows > 0 && A.ncols == A.nrows, CHRONOS_EINVAL, "matrix must be square, n > 0");
+  CHRONOS_REQUIRE((int64_t)A.rp.size() == (int64_t)A.nrows + 1 && A.rp[0] == 0, CHRONOS_EINVAL,
+                  "malformed CSR row pointers");
+  for (int i = 0; i < A.nrows; ++i) {
+    CHRONOS_REQUIRE(A.rp[i + 1] >= A.rp[i], CHRONOS_EINVAL, "CSR row pointers must not decrease");
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      CHRONOS_REQUIRE(A.ci[k] >= 0 && A.ci[k] < A.ncols, CHRONOS_EINVAL, "CSR column out of range");
+      CHRONOS_REQUIRE(k == A.rp[i] || A.ci[k] > A.ci[k - 1], CHRONOS_EINVAL,
+                      "CSR columns must be strictly increasing within a row");
+      CHRONOS_REQUIRE(std::isfinite(A.v[k]), CHRONOS_EINVAL, "non-finite matrix entry");
+    }
+  }
+}
+
+std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A0, int ntv0,
+                                      const double *TV0) {
+  const double t_start = now_s();
+  validate_csr(A0);
+  std::string smeth(prm.smoother_method), tmeth(prm.tspace_method), ptype(prm.proltype),
+      pemin(prm.prol_emin);
+  for (auto *s : {&smeth, &tmeth, &ptype, &pemin})
+    for (auto &c : *s) c = (char)toupper(c);
+  CHRONOS_REQUIRE(smeth == "AFSAI_SYM", CHRONOS_ENOTSUP, "smoother " + smeth + " is outside this path");
+  CHRONOS_REQUIRE(tmeth == "NONE", CHRONOS_ENOTSUP, "test-space method " + tmeth + " is outside this path");
+  CHRONOS_REQUIRE(ptype == "BAMG", CHRONOS_ENOTSUP, "prolongation " + ptype + " is outside this path");
+  CHRONOS_REQUIRE(pemin == "NONE", CHRONOS_ENOTSUP, "prolongation post-process " + pemin + " is outside this path");
+  CHRONOS_REQUIRE(prm.nl_agg == 0, CHRONOS_ENOTSUP, "aggressive coarsening is outside this path");
+  CHRONOS_REQUIRE(prm.updateCF == 0, CHRONOS_ENOTSUP, "updateCF != 0 is outside this path");
+  CHRONOS_REQUIRE(prm.filt_wgt >= 100 && prm.filt_tau <= 0, CHRONOS_ENOTSUP,
+                  "prolongation / coarse-operator filtering is outside this path");
+  CHRONOS_REQUIRE(prm.ntv >= 1 && prm.nstep >= 0 && prm.step_size >= 1 &&
+                      prm.nstep * prm.step_size <= 64, CHRONOS_EINVAL,
+                  "bad smoother / test-space sizes (nstep*step_size <= 64)");
+  CHRONOS_REQUIRE(prm.precision == CHRONOS_FP32 || prm.precision == CHRONOS_FP64, CHRONOS_EINVAL,
+                  "precision must be CHRONOS_FP32 or CHRONOS_FP64");
+
+  auto h = std::make_unique<Hier>();
+  h->prm = prm;
+  h->precision = prm.precision;
+  const bool fp32 = prm.precision == CHRONOS_FP32;
+  CHRONOS_CUDA(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  cudaStream_t st = h->st;
+  const int nthreads = prm.nthread > 0 ? prm.nthread : 0;
+  int nth = nthreads;
+  if (nth <= 0) {
+#ifdef _OPENMP
+    nth = omp_get_max_threads();
+#else
+    nth = 1;
+#endif
+  }
+
+  MT19937 rng((uint32_t)(prm.seed ? prm.seed : 5489));
+  int n = A0.nrows;
+  const int ntv = prm.ntv;
+  std::vector<double> TV((size_t)n * ntv, 0.0);          // column-major
+  const int ncopy = std::min(std::max(ntv0, 0), ntv);
+  for (int j = 0; j < ncopy; ++j)
+    std::copy(TV0 + (size_t)j * n, TV0 + (size_t)(j + 1) * n, TV.begin() + (size_t)j * n);
+  for (int j = std::max(ntv0, 0); j < ntv; ++j)           // rand(n, ntv-ntv0), column-major
+    for (int i = 0; i < n; ++i) TV[(size_t)j * n + i] = rng.next_res53();
+  qr_orthonormalize(n, ntv, TV.data());
+
+  HostCSR Al = A0;
+  std::array<double, 8> &T = h->times;
+  for (int level = 1;; ++level) {
+    h->levels.emplace_back();
+    Level &L = h->levels.back();
+    n = Al.nrows;
+    L.n = n;
+    upload_csr(Al, L.A, fp32, st);
+    if (n <= prm.maxCoarseSZ || level >= prm.nLevMax) {
+      const double t0 = now_s();
+      CHRONOS_REQUIRE(n <= 8192, CHRONOS_ENOTSUP, "coarsest level larger than 8192 rows");
+      std::vector<double> dense((size_t)n * n, 0.0);
+      for (int i = 0; i < n; ++i)
+        for (int64_t k = Al.rp[i]; k < Al.rp[i + 1]; ++k) dense[(size_t)Al.ci[k] * n + i] = Al.v[k];
+      DBuf<double> Ld;
+      Ld.upload(dense, st);
+      const int info = dense_cholesky_device(n, Ld.get(), st);
+      CHRONOS_REQUIRE(info == 0, CHRONOS_ENOTSPD,
+                      "coarsest-level Cholesky failed at pivot " + std::to_string(info));
+      L.W.alloc((size_t)n * n);
+      dense_inverse_from_chol(n, Ld.get(), L.W.get(), st);
+      L.coarsest = true;
+      alloc_vectors(L, h->precision, st);
+      T[6] += now_s() - t0;
+      break;
+    }
+    // ---- smoother: adaptive FSAI (host pattern, GPU values) ----------------
+    double t0 = now_s();
+    FsaiResult fr = fsai_adaptive(Al, prm.nstep, prm.step_size, prm.epsilon, nth,
+                                   prm.fsai_fabs == 0);
+    CHRONOS_REQUIRE(fr.posdef, CHRONOS_ENOTSPD,
+                    "matrix deemed indefinite during FSAI (the nonsymmetric fallback is outside this path)");
+    T[0] += now_s() - t0;
+    t0 = now_s();
+    {
+      HostCSR &Gh = fr.G;
+      std::vector<int> rowlen(n);
+      for (int i = 0; i < n; ++i) rowlen[i] = (int)(Gh.rp[i + 1] - Gh.rp[i]);
+      upload_csr(Gh, L.G, false, st);       // pattern (+ host values, overwritten)
+      const int fl = fsai_numeric_device(n, L.A.rp, L.A.ci, L.A.v64, L.G.rp, L.G.ci, L.G.v64,
+                                         rowlen, st);
+      CHRONOS_REQUIRE(fl == 0, CHRONOS_ENOTSPD, "FSAI numeric phase met a non-SPD local system");
+      // NaN-diagonal repair (smoother.m:61-71): row -> 1/sqrt(a_ii) e_i
+      std::vector<double> gv(L.G.nnz);
+      L.G.v64.download(gv.data(), L.G.nnz, st);
+      CHRONOS_CUDA(cudaStreamSynchronize(st));
+      bool fixed = false;
+      for (int i = 0; i < n; ++i) {
+        const int64_t dpos = Gh.rp[i + 1] - 1;
+        if (std::isnan(gv[dpos])) {
+          double aii = 0;
+          for (int64_t k = Al.rp[i]; k < Al.rp[i + 1]; ++k) if (Al.ci[k] == i) aii = Al.v[k];
+          for (int64_t k = Gh.rp[i]; k < dpos; ++k) gv[k] = 0.0;
+          gv[dpos] = 1.0 / std::sqrt(aii);
+          fixed = true;
+        }
+      }
+      if (fixed) L.G.v64.upload(gv, st);
+      std::vector<int64_t> perm;
+      HostCSR Gt = csr_transpose_map(Gh, perm);
+      Gt.v.assign(Gt.ci.size(), 0.0);
+      upload_csr(Gt, L.Gt, false, st);
+      DBuf<int64_t> dperm;
+      dperm.upload(perm, st);
+      gather_values(L.G.nnz, L.G.v64.get(), dperm.get(), L.Gt.v64.get(), st);
+      if (fp32) {
+        L.G.v32.alloc(std::max<int64_t>(L.G.nnz, 1));
+        L.Gt.v32.alloc(std::max<int64_t>(L.Gt.nnz, 1));
+        convert_f64_to_f32(L.G.nnz, L.G.v64.get(), L.G.v32.get(), st);
+        convert_f64_to_f32(L.Gt.nnz, L.Gt.v64.get(), L.Gt.v32.get(), st);
+      }
+      CHRONOS_CUDA(cudaStreamSynchronize(st));
+    }
+    T[1] += now_s() - t0;
+    // ---- omega = min(1, 1.9 / lambda_max(G A G')) ----------------------------
+    t0 = now_s();
+    {
+      DBuf<double> t1(n), t2(n);
+      Level *Lp = &L;
+      auto mv = [&](const double *v, double *w) {
+        csr_apply<double, double, double, double, MODE_PLAIN, false>(
+            st, 8, n, Lp->Gt.rp, Lp->Gt.ci, Lp->Gt.v64, v, nullptr, t1.get(), 1.0);
+        csr_apply<double, double, double, double, MODE_PLAIN, false>(
+            st, 8, n, Lp->A.rp, Lp->A.ci, Lp->A.v64, t1.get(), nullptr, t2.get(), 1.0);
+        csr_apply<double, double, double, double, MODE_PLAIN, false>(
+            st, 8, n, Lp->G.rp, Lp->G.ci, Lp->G.v64, t2.get(), nullptr, w, 1.0);
+      };
+      L.lambda = lanczos_lmax(n, mv, 5e-4, 200, st);
+      L.omega = std::min(1.0, 1.9 / L.lambda);
+    }
+    T[2] += now_s() - t0;
+    // ---- test space, coarsening --------------------------------------------
+    t0 = now_s();
+    qr_orthonormalize(n, ntv, TV.data());
+    HostCSR S = soc_matrix(Al, prm.SoC_type, prm.soc_tau);
+    int nc = 0;
+    std::vector<int> fcn = pmis_split(Al, S, rng, &nc);
+    CHRONOS_REQUIRE(nc > 0 && nc < n, CHRONOS_EINVAL, "coarsening produced no usable coarse level");
+    T[3] += now_s() - t0;
+    // ---- BAMG prolongation -----------------------------------------------------
+    t0 = now_s();
+    std::vector<int> fc0(n);
+    std::vector<int> clist;
+    clist.reserve(nc);
+    for (int i = 0; i < n; ++i) {
+      fc0[i] = fcn[i] > 0 ? fcn[i] - 1 : -1;
+      if (fcn[i] > 0) clist.push_back(i);
+    }
+    std::vector<double> TVr((size_t)n * ntv);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < ntv; ++j) TVr[(size_t)i * ntv + j] = TV[(size_t)j * n + i];
+    BamgParams bp{prm.itmax_vol, prm.dist_min, prm.dist_max, ntv,
+                  prm.prol_np > 0 ? prm.prol_np : nth, prm.maxcond, prm.maxrownrm, prm.tol_vol,
+                  prm.eps_prol};
+    std::vector<int> c_mark;
+    HostCSR Ph = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
+    std::vector<double> TVn((size_t)nc * ntv);
+    for (int j = 0; j < ntv; ++j)
+      for (int c = 0; c < nc; ++c) TVn[(size_t)j * nc + c] = TV[(size_t)j * n + clist[c]];
+    TV.swap(TVn);
+    T[4] += now_s() - t0;
+    // ---- Galerkin on the GPU ---------------------------------------------------
+    t0 = now_s();
+    L.nc = nc;
+    upload_csr(Ph, L.P, fp32, st);
+    HostCSR Pt = csr_transpose(Ph);
+    upload_csr(Pt, L.Pt, fp32, st);
+    DBuf<int> aprp, apci, acrp, acci;
+    DBuf<double> apv, acv;
+    int64_t nnz_ap = 0, nnz_ac = 0;
+    spgemm_device(n, nc, L.A.rp, L.A.ci, L.A.v64, L.P.rp, L.P.ci, L.P.v64, aprp, apci, apv,
+                  &nnz_ap, st);
+    spgemm_device(nc, nc, L.Pt.rp, L.Pt.ci, L.Pt.v64, aprp, apci, apv, acrp, acci, acv, &nnz_ac,
+                  st);
+    HostCSR Ac = download_csr(nc, nc, acrp, acci, acv, nnz_ac, st);
+    T[5] += now_s() - t0;
+    alloc_vectors(L, h->precision, st);
+    Al = std::move(Ac);
+  }
+  // SpMV lane counts
+  for (auto &L : h->levels) {
+    autotune_lanes(L.A, fp32, st);
+    if (!L.coarsest) {
+      autotune_lanes(L.G, fp32, st);
+      autotune_lanes(L.Gt, fp32, st);
+      autotune_lanes(L.P, fp32, st);
+      autotune_lanes(L.Pt, fp32, st);
+    }
+  }
+  // the level-1 FP64 operator of the outer PCG
+  if (fp32) autotune_lanes(h->levels[0].A, false, st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  T[7] = now_s() - t_start;
+  return h;
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle
+// ---------------------------------------------------------------------------
+
+// Deterministic dot of two device vectors into *out (used when the top level
+// is also the coarsest).
+__global__ void k_dot_store(int n, const double *a, const double *b, double *part,
+                            unsigned *ticket, double *out) {
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += a[i] * b[i];
+  double v[1] = {s};
+  grid_reduce<1>(v, part, ticket, StoreScalar{out});
+}
+
+template <typename T, typename BT, typename OT, bool TOP>
+static void vcycle_level(Hier &h, int l, const BT *b, OT *out, const double *dw, double *dot_out) {
+  Level &L = h.levels[l];
+  cudaStream_t st = h.st;
+  const int n = L.n;
+  double *part = h.pcg.part.get();
+  unsigned *tick = h.pcg.tickets.get();
+  if (L.coarsest) {
+    dense_matvec<BT, OT>(n, L.W.get(), b, out, st);
+    if (TOP && dw) {
+      k_dot_store<<<std::min(num_sms() * 4, (int)ceil_div(n, 256)), 256, 0, st>>>(
+          n, (const double *)out, dw, part, tick, dot_out);
+      CHRONOS_CHECK_LAUNCH();
+    }
+    return;
+  }
+  T *x = L.x<T>(), *r = L.r<T>(), *t = L.t<T>();
+  const T w = (T)L.omega;
+  const DMat &A = L.A, &G = L.G, &Gt = L.Gt, &P = L.P, &Pt = L.Pt;
+  // presmooth from x0 = 0: x = w G'(G b)
+  csr_apply<T, BT, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), b, nullptr, t, T(1));
+  csr_apply<T, T, T, T, MODE_SCALE, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, nullptr, x, w);
+  for (int k = 1; k < h.prm.nupre; ++k) {
+    csr_apply<T, T, BT, T, MODE_RESID, false>(st, A.lanes, n, A.rp, A.ci, vals<T>(A), x, b, r, T(1));
+    csr_apply<T, T, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), r, nullptr, t, T(1));
+    csr_apply<T, T, T, T, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, x, w);
+  }
+  // residual and restriction
+  csr_apply<T, T, BT, T, MODE_RESID, false>(st, A.lanes, n, A.rp, A.ci, vals<T>(A), x, b, r, T(1));
+  Level &C = h.levels[l + 1];
+  csr_apply<T, T, T, T, MODE_PLAIN, false>(st, Pt.lanes, L.nc, Pt.rp, Pt.ci, vals<T>(Pt), r, nullptr,
+                                           C.b<T>(), T(1));
+  vcycle_level<T, T, T, false>(h, l + 1, C.b<T>(), C.x<T>(), nullptr, nullptr);
+  // prolongation and correction
+  csr_apply<T, T, T, T, MODE_AXPY, false>(st, P.lanes, n, P.rp, P.ci, vals<T>(P), C.x<T>(), x, x, T(1));
+  // postsmooth
+  const int npost = h.prm.nupost;
+  for (int k = 0; k < npost; ++k) {
+    csr_apply<T, T, BT, T, MODE_RESID, false>(st, A.lanes, n, A.rp, A.ci, vals<T>(A), x, b, r, T(1));
+    csr_apply<T, T, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), r, nullptr, t, T(1));
+    if (k + 1 < npost) {
+      csr_apply<T, T, T, T, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, x, w);
+    } else if (TOP && dw) {
+      csr_apply<T, T, T, OT, MODE_AXPY, true>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, out,
+                                              w, dw, part, tick, dot_out);
+    } else {
+      csr_apply<T, T, T, OT, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, out, w);
+    }
+  }
+  if (npost == 0) {
+    // out = x + 0 * (G' t): copy / convert through the same epilogue
+    if (TOP && dw)
+      csr_apply<T, T, T, OT, MODE_AXPY, true>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, out,
+                                              T(0), dw, part, tick, dot_out);
+    else
+      csr_apply<T, T, T, OT, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, out,
+                                               T(0));
+  }
+}
+
+void Hier::vcycle(const double *b, double *out, const double *dw, double *dot_out) {
+  if (precision == CHRONOS_FP32)
+    vcycle_level<float, double, double, true>(*this, 0, b, out, dw, dot_out);
+  else
+    vcycle_level<double, double, double, true>(*this, 0, b, out, dw, dot_out);
+}
+
+void Hier::apply_A(const double *x, double *y) {
+  const DMat &A = levels[0].A;
+  csr_apply<double, double, double, double, MODE_PLAIN, false>(st, A.lanes, A.nrows, A.rp, A.ci,
+                                                               A.v64, x, nullptr, y, 1.0);
+}
+
+// ---------------------------------------------------------------------------
+// PCG_CJ
+// ---------------------------------------------------------------------------
+
+// p = pres (first iteration) or p = pres + beta p, beta = -(pres'axp)/ptap.
+__global__ void k_pcg_p_update(int n, const double *__restrict__ pres, double *__restrict__ p,
+                               const double *__restrict__ sc) {
+  const bool first = sc[SC_ITER] < 0.5;
+  const double beta = first ? 0.0 : -sc[SC_PRES_AXP] / sc[SC_PTAP];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    p[i] = first ? pres[i] : pres[i] + beta * p[i];
+}
+
+struct FinAlpha {
+  double *sc;
+  __device__ void operator()(const double *t) const {
+    const double ptap = t[0], pres = t[1];
+    sc[SC_PTAP] = ptap;
+    sc[SC_PRES] = pres;
+    if (!(ptap > 0.0) || !isfinite(pres)) {     // breakdown: p'Ap <= 0 or NaN
+      sc[SC_BREAKDOWN] = 1.0;
+      sc[SC_ALPHA] = 0.0;
+    } else {
+      sc[SC_ALPHA] = pres / ptap;
+    }
+  }
+};
+
+// axp = A p (FP64) with ptap = p'axp and p'res.
+template <int L>
+__global__ void __launch_bounds__(kApplyThreads)
+k_pcg_spmv(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+           const double *__restrict__ v, const double *__restrict__ p,
+           const double *__restrict__ res, double *__restrict__ axp, double *part,
+           unsigned *ticket, double *sc) {
+  constexpr int R = 32 / L;
+  const int lane = threadIdx.x & 31, g = lane / L, gl = lane & (L - 1);
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double d0 = 0.0, d1 = 0.0;
+  for (int base = warp * R; base < n; base += nwarps * R) {
+    const int row = base + g;
+    double sum = 0.0, s2 = 0.0;
+    if (row < n) {
+      const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
+      int k = s + gl;
+      for (; k + L < e; k += 2 * L) {
+        sum += __ldg(v + k) * __ldg(p + __ldg(ci + k));
+        s2 += __ldg(v + k + L) * __ldg(p + __ldg(ci + k + L));
+      }
+      if (k < e) sum += __ldg(v + k) * __ldg(p + __ldg(ci + k));
+      sum += s2;
+    }
+    sum = group_sum<L>(sum);
+    if (row < n && gl == 0) {
+      axp[row] = sum;
+      const double pi = p[row];
+      d0 += pi * sum;
+      d1 += pi * res[row];
+    }
+  }
+  double vals2[2] = {d0, d1};
+  grid_reduce<2>(vals2, part, ticket, FinAlpha{sc});
+}
+
+struct FinResidual {
+  double *sc, *resvec;
+  cudaGraphConditionalHandle handle;
+  int use_cond;
+  __device__ void operator()(const double *t) const {
+    const double resiter = sqrt(t[0]) / sc[SC_BNORM];
+    const double it = sc[SC_ITER] + 1.0;
+    sc[SC_ITER] = it;
+    sc[SC_RR] = t[0];
+    sc[SC_RESITER] = resiter;
+    resvec[(int)it] = resiter;
+    const bool stop = resiter < sc[SC_TOL] || it >= sc[SC_ITMAX] || sc[SC_BREAKDOWN] != 0.0 ||
+                      !isfinite(resiter);
+    if (use_cond) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+  }
+};
+
+// x += alpha p; res -= alpha axp; ||res||^2; stopping test of PCG_CJ.m:58-64.
+__global__ void __launch_bounds__(256)
+k_pcg_xr_update(int n, double *__restrict__ x, double *__restrict__ res,
+                const double *__restrict__ p, const double *__restrict__ axp, double *part,
+                unsigned *ticket, double *sc, double *resvec, cudaGraphConditionalHandle handle,
+                int use_cond) {
+  const double alpha = sc[SC_ALPHA];
+  double rr = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    x[i] += alpha * p[i];
+    const double ri = res[i] - alpha * axp[i];
+    res[i] = ri;
+    rr += ri * ri;
+  }
+  double v[1] = {rr};
+  grid_reduce<1>(v, part, ticket, FinResidual{sc, resvec, handle, use_cond});
+}
+
+static int reduce_blocks(int n) {
+  return std::max(1, std::min(num_sms() * 8, (int)ceil_div(n, 256)));
+}
+
+// Captures one PCG_CJ iteration (PCG_CJ.m:36-64) into the current stream capture.
+static void capture_iteration(Hier &h, cudaGraphConditionalHandle handle, int use_cond) {
+  PcgState &s = h.pcg;
+  cudaStream_t st = h.st;
+  const int n = s.n;
+  const int nb = reduce_blocks(n);
+  double *sc = s.sc.get();
+  // pres = M^{-1} res  (with pres'axp for beta)
+  h.vcycle(s.res.get(), s.pres.get(), s.axp.get(), sc + SC_PRES_AXP);
+  k_pcg_p_update<<<nb, 256, 0, st>>>(n, s.pres.get(), s.p.get(), sc);
+  CHRONOS_CHECK_LAUNCH();
+  const DMat &A = h.levels[0].A;
+  const int L = A.lanes;
+  int blocks = std::min(num_sms() * 8, (int)ceil_div(n, kApplyThreads / L));
+  double *part = s.part.get() + 4 * 3 * 2048;
+  unsigned *tk = s.tickets.get();
+#define CHRONOS_PCG_CASE(LL)                                                                \
+  case LL:                                                                                  \
+    k_pcg_spmv<LL><<<blocks, kApplyThreads, 0, st>>>(n, A.rp, A.ci, A.v64, s.p.get(),       \
+                                                    s.res.get(), s.axp.get(), part, tk + 1, sc); \
+    break;
+  switch (L) {
+    CHRONOS_PCG_CASE(2)
+    CHRONOS_PCG_CASE(4)
+    CHRONOS_PCG_CASE(8)
+    CHRONOS_PCG_CASE(16)
+    CHRONOS_PCG_CASE(32)
+    default: throw Error(CHRONOS_EINVAL, "bad lane count");
+  }
+#undef CHRONOS_PCG_CASE
+  CHRONOS_CHECK_LAUNCH();
+  k_pcg_xr_update<<<nb, 256, 0, st>>>(n, s.x.get(), s.res.get(), s.p.get(), s.axp.get(),
+                                       s.part.get() + 8 * 3 * 2048, tk + 2, sc,
+                                       s.resvec.get(), handle, use_cond);
+  CHRONOS_CHECK_LAUNCH();
+}
+
+static void ensure_pcg_state(Hier &h, int itmax) {
+  PcgState &s = h.pcg;
+  const int n = h.levels[0].n;
+  if (s.n != n) {
+    s.n = n;
+    s.x.alloc(n); s.res.alloc(n); s.p.alloc(n); s.axp.alloc(n); s.pres.alloc(n);
+    s.sc.alloc(SC_COUNT);
+    s.part.alloc((size_t)12 * 3 * 2048);
+    s.tickets.alloc(8);
+    s.tickets.zero(h.st);
+    s.axp.zero(h.st);
+    s.p.zero(h.st);
+  }
+  if (s.resvec_cap < itmax + 1) {
+    // resvec is baked into the graph: rebuild it when the buffer moves
+    s.resvec.alloc((size_t)itmax + 1);
+    s.resvec_cap = itmax + 1;
+    if (s.exec) { cudaGraphExecDestroy(s.exec); s.exec = nullptr; }
+    if (s.graph) { cudaGraphDestroy(s.graph); s.graph = nullptr; }
+  }
+}
+
+static void build_pcg_graph(Hier &h) {
+  PcgState &s = h.pcg;
+  cudaStream_t st = h.st;
+  if (s.exec) return;
+  if (h.prm.use_graph) {
+    CHRONOS_CUDA(cudaGraphCreate(&s.graph, 0));
+    cudaGraphConditionalHandle handle;
+    CHRONOS_CUDA(cudaGraphConditionalHandleCreate(&handle, s.graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = handle;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    CHRONOS_CUDA(cudaGraphAddNode(&node, s.graph, nullptr, 0, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    CHRONOS_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeThreadLocal));
+    try {
+      capture_iteration(h, handle, 1);
+    } catch (...) {
+      cudaGraph_t dummy;
+      cudaStreamEndCapture(st, &dummy);
+      throw;
+    }
+    CHRONOS_CUDA(cudaStreamEndCapture(st, &body));
+    CHRONOS_CUDA(cudaGraphInstantiate(&s.exec, s.graph, 0));
+    s.conditional = true;
+  } else {
+    CHRONOS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    try {
+      capture_iteration(h, 0, 0);
+    } catch (...) {
+      cudaGraph_t dummy;
+      cudaStreamEndCapture(st, &dummy);
+      throw;
+    }
+    CHRONOS_CUDA(cudaStreamEndCapture(st, &s.graph));
+    CHRONOS_CUDA(cudaGraphInstantiate(&s.exec, s.graph, 0));
+    s.conditional = false;
+  }
+}
+
+__global__ void k_pcg_init(double *sc, double *resvec, double tol, double itmax) {
+  // sc[SC_BNORM], sc[SC_RR] hold ||b||^2 and ||r0||^2 from the reductions
+  const double bn = sqrt(sc[SC_BNORM]);
+  sc[SC_BNORM] = bn;
+  sc[SC_RESITER] = sqrt(sc[SC_RR]) / bn;
+  resvec[0] = sc[SC_RESITER];
+  sc[SC_ITER] = 0.0;
+  sc[SC_TOL] = tol;
+  sc[SC_ITMAX] = itmax;
+  sc[SC_BREAKDOWN] = 0.0;
+}
+
+void Hier::pcg_solve(const double *b, double *x, int itmax, double tol, int *iters, int *flag,
+                     std::vector<double> *resvec_out, double *seconds) {
+  ensure_pcg_state(*this, std::max(itmax, 1));
+  PcgState &s = pcg;
+  const int n = s.n;
+  cudaEvent_t e0, e1;
+  CHRONOS_CUDA(cudaEventCreate(&e0));
+  CHRONOS_CUDA(cudaEventCreate(&e1));
+  CHRONOS_CUDA(cudaEventRecord(e0, st));
+  // res = b - A x0, ||b||, ||res|| (PCG_CJ.m:11-30)
+  CHRONOS_CUDA(cudaMemcpyAsync(s.x.get(), x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  const DMat &A = levels[0].A;
+  csr_apply<double, double, double, double, MODE_RESID, false>(st, A.lanes, n, A.rp, A.ci, A.v64,
+                                                               s.x.get(), b, s.res.get(), 1.0);
+  const int nb = reduce_blocks(n);
+  double *part = s.part.get();
+  k_dot_store<<<nb, 256, 0, st>>>(n, b, b, part, s.tickets.get() + 3, s.sc.get() + SC_BNORM);
+  CHRONOS_CHECK_LAUNCH();
+  k_dot_store<<<nb, 256, 0, st>>>(n, s.res.get(), s.res.get(), part, s.tickets.get() + 3,
+                                   s.sc.get() + SC_RR);
+  CHRONOS_CHECK_LAUNCH();
+  k_pcg_init<<<1, 1, 0, st>>>(s.sc.get(), s.resvec.get(), tol, (double)itmax);
+  CHRONOS_CHECK_LAUNCH();
+  double sc_h[SC_COUNT];
+  CHRONOS_CUDA(cudaMemcpyAsync(sc_h, s.sc.get(), sizeof(sc_h), cudaMemcpyDeviceToHost, st));
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  int it = 0;
+  if (sc_h[SC_BNORM] == 0.0) {                 // PCG_CJ.m:12-16
+    CHRONOS_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * n, st));
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    *iters = 0;
+    *flag = 0;
+    if (resvec_out) resvec_out->assign(1, 0.0);
+    if (seconds) *seconds = 0.0;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return;
+  }
+  if (itmax > 0) {
+    build_pcg_graph(*this);
+    if (s.conditional) {
+      CHRONOS_CUDA(cudaGraphLaunch(s.exec, st));
+    } else {
+      double *pinned = nullptr;
+      CHRONOS_CUDA(cudaMallocHost(&pinned, sizeof(double) * SC_COUNT));
+      for (int k = 0; k < itmax; ++k) {
+        CHRONOS_CUDA(cudaGraphLaunch(s.exec, st));
+        CHRONOS_CUDA(cudaMemcpyAsync(pinned, s.sc.get(), sizeof(double) * SC_COUNT,
+                                     cudaMemcpyDeviceToHost, st));
+        CHRONOS_CUDA(cudaStreamSynchronize(st));
+        const double r = pinned[SC_RESITER];
+        if (r < tol || pinned[SC_BREAKDOWN] != 0.0 || !std::isfinite(r)) break;
+      }
+      cudaFreeHost(pinned);
+    }
+  }
+  CHRONOS_CUDA(cudaMemcpyAsync(x, s.x.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  CHRONOS_CUDA(cudaEventRecord(e1, st));
+  CHRONOS_CUDA(cudaMemcpyAsync(sc_h, s.sc.get(), sizeof(sc_h), cudaMemcpyDeviceToHost, st));
+  CHRONOS_CUDA(cudaEventSynchronize(e1));
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  it = (int)(sc_h[SC_ITER] + 0.5);
+  *iters = it;
+  const double resiter = sc_h[SC_RESITER];
+  *flag = (resiter > tol || !std::isfinite(resiter)) ? 1 : 0;   // PCG_CJ.m:69-71
+  if (sc_h[SC_BREAKDOWN] != 0.0) *flag = 1;
+  if (resvec_out) {
+    resvec_out->resize(it + 1);
+    s.resvec.download(resvec_out->data(), it + 1, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+  }
+  if (seconds) *seconds = ms * 1e-3;
+  if (sc_h[SC_BREAKDOWN] != 0.0)
+    throw Error(CHRONOS_EBREAKDOWN, "PCG breakdown: p'Ap <= 0 or NaN at iteration " +
+                                        std::to_string(it));
+}
+
+}  // namespace chronos

@@ -1,0 +1,96 @@
+// The AMG hierarchy handle behind chronos_hier: per-level device matrices,
+// work vectors, the PCG state and its CUDA graph.
+#pragma once
+
+#include <array>
+#include <functional>
+#include <memory>
+#include <vector>
+
+#include "host/host.h"
+#include "internal.h"
+
+namespace chronos {
+
+struct Level {
+  int n = 0, nc = 0;
+  bool coarsest = false;
+  DMat A, G, Gt, P, Pt;
+  DBuf<double> W;                  // coarsest: A^{-1} from the Cholesky factor
+  double omega = 1.0, lambda = 0.0;
+  // work vectors (one set per precision in use)
+  DBuf<float> b32, x32, r32, t32;
+  DBuf<double> b64, x64, r64, t64;
+  template <typename T> T *b();
+  template <typename T> T *x();
+  template <typename T> T *r();
+  template <typename T> T *t();
+};
+
+template <> inline float *Level::b<float>() { return b32.get(); }
+template <> inline float *Level::x<float>() { return x32.get(); }
+template <> inline float *Level::r<float>() { return r32.get(); }
+template <> inline float *Level::t<float>() { return t32.get(); }
+template <> inline double *Level::b<double>() { return b64.get(); }
+template <> inline double *Level::x<double>() { return x64.get(); }
+template <> inline double *Level::r<double>() { return r64.get(); }
+template <> inline double *Level::t<double>() { return t64.get(); }
+
+template <typename T> inline const T *vals(const DMat &m);
+template <> inline const float *vals<float>(const DMat &m) { return m.v32.get(); }
+template <> inline const double *vals<double>(const DMat &m) { return m.v64.get(); }
+
+// Device scalars of the PCG recurrence.
+enum PcgScalar {
+  SC_BNORM = 0, SC_PTAP, SC_ALPHA, SC_PRES_AXP, SC_RR, SC_RESITER, SC_ITER, SC_TOL, SC_ITMAX,
+  SC_BREAKDOWN, SC_PRES, SC_COUNT = 16
+};
+
+struct PcgState {
+  int n = 0;
+  DBuf<double> x, res, p, axp, pres, resvec;
+  DBuf<double> sc;                  // SC_COUNT scalars
+  DBuf<double> part;                // block partials (3 per block, several slots)
+  DBuf<unsigned> tickets;           // one ticket per reducing kernel
+  cudaGraphExec_t exec = nullptr;   // the whole solve (device-side loop) or one iteration
+  cudaGraph_t graph = nullptr;
+  bool conditional = false;
+  int resvec_cap = 0;
+  ~PcgState();
+};
+
+struct Hier {
+  chronos_params prm{};
+  int precision = CHRONOS_FP32;
+  std::vector<Level> levels;
+  cudaStream_t st = nullptr;
+  std::array<double, 8> times{};   // setup timings
+  PcgState pcg;
+  ~Hier();
+
+  // one V-cycle: out = M^{-1} b on device FP64 vectors of length n0;
+  // when dw != nullptr also *dot_out = out . dw (deterministic).
+  void vcycle(const double *b, double *out, const double *dw, double *dot_out);
+  // PCG_CJ to tolerance on device vectors; returns iterations, flag.
+  void pcg_solve(const double *b, double *x, int itmax, double tol, int *iters, int *flag,
+                 std::vector<double> *resvec, double *seconds);
+  // y = A x with the level-0 FP64 operator.
+  void apply_A(const double *x, double *y);
+};
+
+std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A,
+                                      int ntv0, const double *TV0);
+
+void params_default(chronos_params *p);
+void params_read(const char *fnames_path, chronos_params *p);
+
+// Upload a host CSR (FP64) to a device matrix, with FP32 values when fp32.
+void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st);
+// SpMV lane count by timing the candidates (cached per shape).
+void autotune_lanes(DMat &m, bool fp32, cudaStream_t st);
+// Largest eigenvalue of the symmetric operator given as a device FP64 matvec,
+// by Lanczos with a unit start vector; relative tolerance tol.
+double lanczos_lmax(int n, const std::function<void(const double *, double *)> &mv, double tol,
+                    int maxit, cudaStream_t st);
+
+}  // namespace chronos

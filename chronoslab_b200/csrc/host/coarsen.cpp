@@ -1,0 +1,286 @@
+// Host coarsening of the solve path: strength of connection, Dirichlet-node
+// marking and the sequential PMIS sweep, restated from the reference's MATLAB
+// (sources/Preconditioner/AMG/coarsen/): coarsen.m:30-76,
+// mark_isolated_nodes.m:1-8, cpt_SoC_dom.m:25-63, cpt_SoC_cla.m:107-159,
+// cpt_PMIS.m:1-102.  Plus the MT19937 stream MATLAB's rng(0) draws from, the
+// thin Householder QR used for qr(TV,0) and CSR transposes.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+
+#include "host.h"
+#include "../errors.h"
+
+namespace chronos {
+
+// ---- MT19937 -----------------------------------------------------------------
+void MT19937::seed_(uint32_t s) {
+  mt_[0] = s;
+  for (int i = 1; i < 624; ++i)
+    mt_[i] = 1812433253u * (mt_[i - 1] ^ (mt_[i - 1] >> 30)) + (uint32_t)i;
+  mti_ = 624;
+}
+
+uint32_t MT19937::next_u32() {
+  static const uint32_t mag01[2] = {0u, 0x9908b0dfu};
+  if (mti_ >= 624) {
+    int k = 0;
+    for (; k < 624 - 397; ++k) {
+      uint32_t y = (mt_[k] & 0x80000000u) | (mt_[k + 1] & 0x7fffffffu);
+      mt_[k] = mt_[k + 397] ^ (y >> 1) ^ mag01[y & 1u];
+    }
+    for (; k < 623; ++k) {
+      uint32_t y = (mt_[k] & 0x80000000u) | (mt_[k + 1] & 0x7fffffffu);
+      mt_[k] = mt_[k + (397 - 624)] ^ (y >> 1) ^ mag01[y & 1u];
+    }
+    uint32_t y = (mt_[623] & 0x80000000u) | (mt_[0] & 0x7fffffffu);
+    mt_[623] = mt_[396] ^ (y >> 1) ^ mag01[y & 1u];
+    mti_ = 0;
+  }
+  uint32_t y = mt_[mti_++];
+  y ^= (y >> 11);
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= (y >> 18);
+  return y;
+}
+
+// ---- CSR transposes ---------------------------------------------------------
+HostCSR csr_transpose_map(const HostCSR &A, std::vector<int64_t> &perm) {
+  HostCSR T;
+  T.nrows = A.ncols;
+  T.ncols = A.nrows;
+  T.rp.assign((size_t)T.nrows + 1, 0);
+  const int64_t nnz = A.nnz();
+  for (int64_t k = 0; k < nnz; ++k) T.rp[(size_t)A.ci[k] + 1]++;
+  for (int i = 0; i < T.nrows; ++i) T.rp[i + 1] += T.rp[i];
+  T.ci.resize(nnz);
+  T.v.resize(nnz);
+  perm.resize(nnz);
+  std::vector<int64_t> pos(T.rp.begin(), T.rp.end() - 1);
+  for (int i = 0; i < A.nrows; ++i)
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+      int64_t d = pos[A.ci[k]]++;
+      T.ci[d] = i;
+      T.v[d] = A.v.empty() ? 0.0 : A.v[k];
+      perm[d] = k;
+    }
+  return T;
+}
+
+HostCSR csr_transpose(const HostCSR &A) {
+  std::vector<int64_t> perm;
+  return csr_transpose_map(A, perm);
+}
+
+// ---- strength of connection ------------------------------------------------
+static std::vector<double> diagonal(const HostCSR &A) {
+  std::vector<double> d(A.nrows, 0.0);
+  for (int i = 0; i < A.nrows; ++i)
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] == i) d[i] = A.v[k];
+  return d;
+}
+
+HostCSR soc_matrix(const HostCSR &A, const char *soc_type, double tau) {
+  const int n = A.nrows;
+  std::string t(soc_type);
+  for (auto &c : t) c = (char)toupper(c);
+  HostCSR S;
+  S.nrows = S.ncols = n;
+  S.rp.assign((size_t)n + 1, 0);
+  std::vector<double> d = diagonal(A);
+  if (t == "DOM") {
+    // cpt_SoC_dom.m:26-47: s_ij = |a_ij| / sqrt(d_i d_j), strong if s_ij > tau.
+    CHRONOS_REQUIRE(tau >= 0, CHRONOS_ENOTSUP, "DOM strength with tau < 0 is outside this path");
+    for (int i = 0; i < n; ++i) {
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        double a = A.v[k];
+        if (a == 0.0) continue;
+        int j = A.ci[k];
+        double s = std::fabs(a) / std::sqrt(d[i] * d[j]);
+        if (s > tau) { S.ci.push_back(j); S.v.push_back(s); }
+      }
+      S.rp[i + 1] = (int64_t)S.ci.size();
+    }
+    return S;
+  }
+  if (t == "CLA") {
+    // cpt_SoC_cla.m:109-159.  Column minimum of the off-diagonal part counts
+    // implicit zeros (MATLAB min over a sparse column).
+    std::vector<double> minc(n, 0.0), maxabs(n, 0.0);
+    std::vector<int64_t> cnt(n, 0);
+    for (int i = 0; i < n; ++i)
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        int j = A.ci[k];
+        double a = A.v[k];
+        if (j == i || a == 0.0) continue;
+        if (cnt[j] == 0) minc[j] = a; else minc[j] = std::min(minc[j], a);
+        maxabs[j] = std::max(maxabs[j], std::fabs(a));
+        cnt[j]++;
+      }
+    bool all_nonneg = true;
+    for (int j = 0; j < n; ++j) {
+      if (cnt[j] < n) minc[j] = std::min(minc[j], 0.0);   // implicit zeros
+      if (minc[j] < 0) all_nonneg = false;
+    }
+    for (int j = 0; j < n; ++j) {
+      if (minc[j] == 0.0) minc[j] = 1.0;
+      if (maxabs[j] == 0.0) maxabs[j] = 1.0;
+    }
+    for (int i = 0; i < n; ++i) {
+      bool have_diag = false;
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        double a = A.v[k];
+        if (a == 0.0) continue;
+        int j = A.ci[k];
+        double s = all_nonneg ? std::fabs(a) / std::max(maxabs[i], maxabs[j])
+                              : a / std::max(minc[i], minc[j]);
+        double val = s > tau ? s : 0.0;
+        if (j == i) { val += 1.0; have_diag = true; }     // S + speye(nn)
+        if (val != 0.0) { S.ci.push_back(j); S.v.push_back(val); }
+      }
+      if (!have_diag) {                                   // diagonal of speye
+        auto pos = std::lower_bound(S.ci.begin() + S.rp[i], S.ci.end(), i) - S.ci.begin();
+        S.ci.insert(S.ci.begin() + pos, i);
+        S.v.insert(S.v.begin() + pos, 1.0);
+      }
+      S.rp[i + 1] = (int64_t)S.ci.size();
+    }
+    return S;
+  }
+  throw Error(CHRONOS_ENOTSUP, "SoC type " + t + " is outside this path (DOM, CLA)");
+}
+
+// ---- PMIS -------------------------------------------------------------------
+std::vector<int> pmis_split(const HostCSR &A, const HostCSR &S, MT19937 &rng, int *nc_out) {
+  const int n = S.nrows;
+  // mark_isolated_nodes.m: columns of A with a single nonzero -> Dirichlet (-2)
+  std::vector<int> colcnt(n, 0);
+  for (int i = 0; i < A.nrows; ++i)
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.v[k] != 0.0) colcnt[A.ci[k]]++;
+  std::vector<int> fc(n, 0);
+  for (int j = 0; j < n; ++j)
+    if (colcnt[j] == 1) fc[j] = -2;
+
+  // S without its diagonal; its transpose gives the columns S(:,inod)
+  HostCSR So;
+  So.nrows = So.ncols = n;
+  So.rp.assign((size_t)n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    for (int64_t k = S.rp[i]; k < S.rp[i + 1]; ++k)
+      if (S.ci[k] != i && S.v[k] != 0.0) { So.ci.push_back(S.ci[k]); So.v.push_back(1.0); }
+    So.rp[i + 1] = (int64_t)So.ci.size();
+  }
+  HostCSR St = csr_transpose(So);                 // row j of St = column j of S
+  // S_sym = |S| + |S'|: union of the patterns of row j of S and of S'
+  std::vector<int64_t> sym_rp((size_t)n + 1, 0);
+  std::vector<int> sym_ci;
+  sym_ci.reserve(So.ci.size() * 2);
+  for (int j = 0; j < n; ++j) {
+    int64_t a = So.rp[j], ae = So.rp[j + 1], b = St.rp[j], be = St.rp[j + 1];
+    while (a < ae || b < be) {
+      int ca = a < ae ? So.ci[a] : INT32_MAX, cb = b < be ? St.ci[b] : INT32_MAX;
+      int c = std::min(ca, cb);
+      sym_ci.push_back(c);
+      if (ca == c) ++a;
+      if (cb == c) ++b;
+    }
+    sym_rp[j + 1] = (int64_t)sym_ci.size();
+  }
+  // nod_weight = sum(S ~= 0, 1)' + rand(nn,1)
+  std::vector<double> w(n), wfree(n);
+  for (int j = 0; j < n; ++j) w[j] = (double)(St.rp[j + 1] - St.rp[j]);
+  for (int j = 0; j < n; ++j) w[j] += rng.next_res53();
+  for (int j = 0; j < n; ++j) {
+    if (fc[j] == -2) fc[j] = -1;
+    wfree[j] = fc[j] == -1 ? -1.0 : w[j];
+  }
+  std::vector<int> list;
+  list.reserve(n);
+  for (int j = 0; j < n; ++j)
+    if (fc[j] == 0) list.push_back(j);
+  int64_t len = (int64_t)list.size();
+  int64_t ind = 0;
+  while (len > 0) {
+    const int inod = list[ind];
+    if (fc[inod] != 0) {
+      list[ind] = list[len - 1];
+      --len;
+    } else {
+      bool is_coarse = true;
+      const double wi = w[inod];
+      for (int64_t k = sym_rp[inod]; k < sym_rp[inod + 1]; ++k)
+        if (wfree[sym_ci[k]] > wi) { is_coarse = false; break; }
+      if (!is_coarse) {
+        ++ind;
+      } else {
+        for (int64_t k = St.rp[inod]; k < St.rp[inod + 1]; ++k) {
+          fc[St.ci[k]] = -1;
+          wfree[St.ci[k]] = -1.0;
+        }
+        fc[inod] = 1;
+        wfree[inod] = -1.0;
+        list[ind] = list[len - 1];
+        --len;
+      }
+    }
+    if (ind > len - 1) ind = 0;
+  }
+  int nc = 0, nf = 0;
+  for (int j = 0; j < n; ++j) {
+    if (fc[j] > 0) fc[j] = ++nc;
+    else fc[j] = -(++nf);
+  }
+  *nc_out = nc;
+  return fc;
+}
+
+// ---- thin QR ------------------------------------------------------------------
+// Householder QR with LAPACK's sign convention (beta = -sign(x1)*||x||); Q is
+// accumulated explicitly into X (n x k, column-major).
+void qr_orthonormalize(int n, int k, double *X) {
+  if (k == 0 || n == 0) return;
+  std::vector<double> V((size_t)n * k, 0.0), tau(k, 0.0);
+  std::vector<double> R(X, X + (size_t)n * k);
+  for (int j = 0; j < k && j < n; ++j) {
+    double *c = &R[(size_t)j * n];
+    double nrm2 = 0;
+    for (int i = j + 1; i < n; ++i) nrm2 += c[i] * c[i];
+    double alpha = c[j];
+    double *v = &V[(size_t)j * n];
+    if (nrm2 == 0.0) { tau[j] = 0.0; v[j] = 1.0; continue; }
+    double beta = -std::copysign(std::sqrt(alpha * alpha + nrm2), alpha);
+    tau[j] = (beta - alpha) / beta;
+    double scal = 1.0 / (alpha - beta);
+    v[j] = 1.0;
+    for (int i = j + 1; i < n; ++i) v[i] = c[i] * scal;
+    c[j] = beta;
+    for (int i = j + 1; i < n; ++i) c[i] = 0.0;
+    for (int jj = j + 1; jj < k; ++jj) {
+      double *cc = &R[(size_t)jj * n];
+      double s = 0;
+      for (int i = j; i < n; ++i) s += v[i] * cc[i];
+      s *= tau[j];
+      for (int i = j; i < n; ++i) cc[i] -= s * v[i];
+    }
+  }
+  // Q = H_0 H_1 ... H_{k-1} applied to the first k columns of I
+  for (int j = 0; j < k; ++j)
+    for (int i = 0; i < n; ++i) X[(size_t)j * n + i] = (i == j) ? 1.0 : 0.0;
+  for (int j = std::min(k, n) - 1; j >= 0; --j) {
+    const double *v = &V[(size_t)j * n];
+    for (int jj = 0; jj < k; ++jj) {
+      double *cc = &X[(size_t)jj * n];
+      double s = 0;
+      for (int i = j; i < n; ++i) s += v[i] * cc[i];
+      s *= tau[j];
+      for (int i = j; i < n; ++i) cc[i] -= s * v[i];
+    }
+  }
+}
+
+}  // namespace chronos

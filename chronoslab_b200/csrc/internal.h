@@ -1,0 +1,61 @@
+// Host-callable launchers shared between the translation units of the
+// library.  Device pointers unless named *_h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+namespace chronos {
+
+// Device CSR, 0-based, int32 row pointers and columns; values in FP64 and,
+// for the FP32 hierarchy, an FP32 copy sharing the pattern.
+struct DMat {
+  int nrows = 0, ncols = 0;
+  int64_t nnz = 0;
+  DBuf<int> rp, ci;
+  DBuf<double> v64;
+  DBuf<float> v32;
+  int lanes = 8;            // SpMV lanes per row (autotuned)
+};
+
+// ---- FSAI numeric (setup_kernels.cu) ------------------------------------------
+// G values on the pattern grp/gci (rows: strictly-lower ascending, diagonal
+// last).  A: 0-based CSR, sorted rows.  Returns the flags word: bit 0 =
+// non-SPD local block or non-positive Schur complement somewhere.
+int fsai_numeric_device(int n, const int *arp, const int *aci, const double *av, const int *grp,
+                        const int *gci, double *gval, const std::vector<int> &rowlen_h,
+                        cudaStream_t st);
+
+// ---- Galerkin (setup_kernels.cu) ---------------------------------------------
+// C = X * Y (X: m x k, Y: k x ncols), Gustavson accumulation order, exact
+// zeros dropped, columns sorted.  Output arrays allocated here.
+void spgemm_device(int m, int ncols, const int *xrp, const int *xci, const double *xv,
+                   const int *yrp, const int *yci, const double *yv, DBuf<int> &crp,
+                   DBuf<int> &cci, DBuf<double> &cv, int64_t *nnz_c, cudaStream_t st);
+
+// ---- dense coarse level (setup_kernels.cu) ----------------------------------
+// In-place lower Cholesky of the n x n column-major A (device); returns 0 or
+// the 1-based index of the first non-positive pivot.
+int dense_cholesky_device(int n, double *A, cudaStream_t st);
+// W = A^{-1} = L^{-T} L^{-1} from the lower factor L (column-major).  W is
+// symmetric (row- and column-major alike).
+void dense_inverse_from_chol(int n, const double *L, double *W, cudaStream_t st);
+// x = W b (W FP64 row-major n x n).
+template <typename TI, typename TO>
+void dense_matvec(int n, const double *W, const TI *b, TO *x, cudaStream_t st);
+
+// ---- vector helpers (setup_kernels.cu) ---------------------------------------
+void gather_values(int64_t nnz, const double *src, const int64_t *perm, double *dst,
+                   cudaStream_t st);
+void convert_f64_to_f32(int64_t n, const double *src, float *dst, cudaStream_t st);
+double device_dot(int n, const double *a, const double *b, double *scratch, cudaStream_t st);
+void device_axpby(int n, double a, const double *x, double b, double *y, cudaStream_t st);
+void device_scale_copy(int n, double a, const double *x, double *y, cudaStream_t st);
+// grad[k] = -lambda[row(k)] * u[col(k)]
+void adjoint_scatter(int n, const int *rp, const int *ci, const double *lambda, const double *u,
+                     double *grad, cudaStream_t st);
+
+}  // namespace chronos

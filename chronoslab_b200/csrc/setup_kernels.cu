@@ -1,0 +1,600 @@
+// Setup-phase kernels of the solve path (sm_100a):
+//  * FSAI numeric phase: one warp per row gathers the local SPD system
+//    A[P,P], -A[P,i] of its pattern, factors it in shared memory (FP64
+//    Cholesky), solves, and scales the row by 1/sqrt(a_ii - A_iP A_PP^-1 A_Pi)
+//    (cpt_afsai_coef.cpp:440-541).  Rows are bucketed by local size so each
+//    bucket runs with the shared-memory tile that fits it.
+//  * Galerkin product P'*(A*P) (cpt_aspAMG.m:277) as two row-wise sparse
+//    products with per-row hash tables: symbolic count, then numeric
+//    accumulation in Gustavson order (each output entry summed in the order
+//    of the left factor's row, products and sums rounded separately), exact
+//    zeros dropped, rows sorted.
+//  * Coarsest level: dense FP64 Cholesky, inverse from the factor, dense
+//    matvec apply (AMG_Vcycle.m:9-10).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <numeric>
+
+#include "internal.h"
+
+namespace chronos {
+
+// =============================================================================
+// FSAI numeric
+// =============================================================================
+
+// Position of column c in the sorted row [k, ke) of aci, or -1.
+__device__ __forceinline__ int find_col(const int *aci, int k, int ke, int c) {
+  int lo = k, hi = ke - 1;
+  while (lo <= hi) {
+    int mid = (lo + hi) >> 1;
+    int v = aci[mid];
+    if (v == c) return mid;
+    if (v < c) lo = mid + 1; else hi = mid - 1;
+  }
+  return -1;
+}
+
+template <int MMAX>
+__global__ void k_fsai_numeric(int nb, const int *__restrict__ rows, const int *__restrict__ arp,
+                               const int *__restrict__ aci, const double *__restrict__ av,
+                               const int *__restrict__ grp, const int *__restrict__ gci,
+                               double *__restrict__ gval, int *flags) {
+  extern __shared__ double smem[];
+  constexpr int STRIDE = MMAX * MMAX + 3 * MMAX;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int wglob = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (wglob >= nb) return;                      // warp-uniform exit
+  double *M = smem + (size_t)wib * STRIDE;      // row-major lower: M[j*MMAX + l], l <= j
+  double *rhs = M + MMAX * MMAX;                // -A[i,P] (kept for the Schur term)
+  double *y = rhs + MMAX;                       // solution
+  const int i = rows[wglob];
+  const int gs = grp[i], ge = grp[i + 1];
+  const int m = ge - gs - 1;                    // strictly-lower entries
+  const int *P = gci + gs;
+  const int ai = arp[i], aie = arp[i + 1];
+  // Gather: column c (owned by lane c mod 32) from row P[c], entries P[j], j >= c.
+  for (int c = lane; c < m; c += 32) {
+    const int r = P[c];
+    int k = arp[r];
+    const int ke = arp[r + 1];
+    // first entry with column >= r (binary search)
+    int lo = k, hi = ke;
+    while (lo < hi) { int mid = (lo + hi) >> 1; if (aci[mid] < r) lo = mid + 1; else hi = mid; }
+    k = lo;
+    for (int j = c; j < m; ++j) {
+      const int pj = P[j];
+      while (k < ke && aci[k] < pj) ++k;
+      M[j * MMAX + c] = (k < ke && aci[k] == pj) ? av[k] : 0.0;
+    }
+    const int pos = find_col(aci, ai, aie, r);
+    rhs[c] = pos >= 0 ? -av[pos] : 0.0;
+  }
+  double aii = 0.0;
+  bool have_diag = false;
+  {
+    const int pos = find_col(aci, ai, aie, i);
+    if (pos >= 0) { aii = av[pos]; have_diag = true; }
+  }
+  __syncwarp();
+  bool spd = true;
+  // Right-looking Cholesky; lane j owns rows j, j+32.
+  for (int k = 0; k < m; ++k) {
+    double d = M[k * MMAX + k];
+    if (!(d > 0.0)) { spd = false; break; }     // warp-uniform (all lanes read the same d)
+    d = sqrt(d);
+    __syncwarp();
+    for (int j = k + 1 + lane; j < m; j += 32) M[j * MMAX + k] /= d;
+    if (lane == 0) M[k * MMAX + k] = d;
+    __syncwarp();
+    for (int j = k + 1 + lane; j < m; j += 32) {
+      const double ljk = M[j * MMAX + k];
+      for (int l = k + 1; l <= j; ++l) M[j * MMAX + l] -= ljk * M[l * MMAX + k];
+    }
+    __syncwarp();
+  }
+  double scal = 0.0;
+  if (spd) {
+    for (int j = lane; j < m; j += 32) y[j] = rhs[j];
+    __syncwarp();
+    for (int k = 0; k < m; ++k) {               // L z = rhs
+      const double zk = y[k] / M[k * MMAX + k];
+      __syncwarp();
+      if (lane == 0) y[k] = zk;
+      for (int j = k + 1 + lane; j < m; j += 32) y[j] -= M[j * MMAX + k] * zk;
+      __syncwarp();
+    }
+    for (int k = m - 1; k >= 0; --k) {          // L^T y = z
+      const double yk = y[k] / M[k * MMAX + k];
+      __syncwarp();
+      if (lane == 0) y[k] = yk;
+      for (int j = lane; j < k; j += 32) y[j] -= M[k * MMAX + j] * yk;
+      __syncwarp();
+    }
+    double part = 0.0;
+    for (int j = lane; j < m; j += 32) part += rhs[j] * y[j];
+    part = warp_sum(part);
+    scal = aii - part;
+  }
+  bool ok = spd && have_diag && scal > 0.0;
+  if (!ok) {
+    if (lane == 0) atomicOr(flags, 1);
+    scal = 1.0;
+    if (!spd)                                    // keep a defined row: diagonal scaling only
+      for (int j = lane; j < m; j += 32) y[j] = 0.0;
+    __syncwarp();
+  }
+  const double s = 1.0 / sqrt(scal);
+  for (int j = lane; j < m; j += 32) gval[gs + j] = s * y[j];
+  if (lane == 0) gval[gs + m] = s;
+}
+
+int fsai_numeric_device(int n, const int *arp, const int *aci, const double *av, const int *grp,
+                        const int *gci, double *gval, const std::vector<int> &rowlen_h,
+                        cudaStream_t st) {
+  // Bucket rows by local system size m = rowlen - 1.
+  std::vector<int> b16, b32, b64;
+  for (int i = 0; i < n; ++i) {
+    const int m = rowlen_h[i] - 1;
+    if (m <= 16) b16.push_back(i);
+    else if (m <= 32) b32.push_back(i);
+    else if (m <= 64) b64.push_back(i);
+    else throw Error(CHRONOS_ENOTSUP, "FSAI local system larger than 64 (nstep*step_size)");
+  }
+  DBuf<int> flags(1);
+  flags.zero(st);
+  DBuf<int> d16, d32, d64;
+  auto run = [&](auto kern, const std::vector<int> &rows, DBuf<int> &drows, int mmax, int warps) {
+    if (rows.empty()) return;
+    drows.upload(rows, st);
+    const size_t sm = (size_t)warps * (mmax * mmax + 3 * mmax) * sizeof(double);
+    CHRONOS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const unsigned blocks = ceil_div((int64_t)rows.size(), warps);
+    kern<<<blocks, warps * 32, sm, st>>>((int)rows.size(), drows.get(), arp, aci, av, grp, gci,
+                                         gval, flags.get());
+    CHRONOS_CHECK_LAUNCH();
+  };
+  run(k_fsai_numeric<16>, b16, d16, 16, 8);
+  run(k_fsai_numeric<32>, b32, d32, 32, 4);
+  run(k_fsai_numeric<64>, b64, d64, 64, 2);
+  int fl = 0;
+  CHRONOS_CUDA(cudaMemcpyAsync(&fl, flags.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  return fl;
+}
+
+// =============================================================================
+// Sparse product C = X * Y with per-row hash tables in global memory
+// =============================================================================
+
+__global__ void k_spgemm_products(int m, const int *xrp, const int *xci, const int *yrp,
+                                  int64_t *prod) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  int64_t s = 0;
+  for (int k = xrp[i]; k < xrp[i + 1]; ++k) {
+    const int j = xci[k];
+    s += yrp[j + 1] - yrp[j];
+  }
+  prod[i] = s;
+}
+
+__device__ __forceinline__ unsigned hash_slot(int key, unsigned mask) {
+  return ((unsigned)key * 2654435761u) & mask;
+}
+
+// Inserts key into the open-addressing table (keys initialised to -1);
+// returns the slot and whether this call created it.
+__device__ __forceinline__ unsigned hash_insert(int *keys, unsigned mask, int key, bool *fresh) {
+  unsigned s = hash_slot(key, mask);
+  while (true) {
+    int cur = keys[s];
+    if (cur == key) { *fresh = false; return s; }
+    if (cur == -1) {
+      int prev = atomicCAS(keys + s, -1, key);
+      if (prev == -1) { *fresh = true; return s; }
+      if (prev == key) { *fresh = false; return s; }
+    }
+    s = (s + 1) & mask;
+  }
+}
+
+// Symbolic: unique columns per row (warp per row, rows [r0, r1)).
+__global__ void k_spgemm_symbolic(int r0, int r1, const int *xrp, const int *xci, const int *yrp,
+                                  const int *yci, const int64_t *toff, const unsigned *tcap,
+                                  int *keys, int *cnt) {
+  const int lane = threadIdx.x & 31;
+  const int i = r0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (i >= r1) return;
+  int *tk = keys + toff[i - r0];
+  const unsigned cap = tcap[i - r0], mask = cap - 1;
+  for (unsigned s = lane; s < cap; s += 32) tk[s] = -1;
+  __syncwarp();
+  int mine = 0;
+  for (int k = xrp[i]; k < xrp[i + 1]; ++k) {
+    const int j = xci[k];
+    for (int kk = yrp[j] + lane; kk < yrp[j + 1]; kk += 32) {
+      bool fresh;
+      hash_insert(tk, mask, yci[kk], &fresh);
+      mine += fresh;
+    }
+  }
+  mine = warp_sum(mine);
+  if (lane == 0) cnt[i] = mine;
+}
+
+// Numeric: accumulate in the order of row i of X (products rounded, then
+// added), emit the nonzero entries unsorted into [crp_sym[i], ...); cnt_out[i]
+// = number emitted.
+__global__ void k_spgemm_numeric(int r0, int r1, const int *xrp, const int *xci, const double *xv,
+                                 const int *yrp, const int *yci, const double *yv,
+                                 const int64_t *toff, const unsigned *tcap, int *keys,
+                                 double *vals, const int64_t *crp_sym, int *cci, double *cv,
+                                 int *cnt_out) {
+  const int lane = threadIdx.x & 31;
+  const int i = r0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (i >= r1) return;
+  int *tk = keys + toff[i - r0];
+  double *tv = vals + toff[i - r0];
+  const unsigned cap = tcap[i - r0], mask = cap - 1;
+  for (unsigned s = lane; s < cap; s += 32) { tk[s] = -1; tv[s] = 0.0; }
+  __syncwarp();
+  for (int k = xrp[i]; k < xrp[i + 1]; ++k) {
+    const int j = xci[k];
+    const double a = xv[k];
+    for (int kk = yrp[j] + lane; kk < yrp[j + 1]; kk += 32) {
+      bool fresh;
+      const unsigned s = hash_insert(tk, mask, yci[kk], &fresh);
+      tv[s] = __dadd_rn(tv[s], __dmul_rn(a, yv[kk]));
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  int64_t base = crp_sym[i];
+  int emitted = 0;
+  for (unsigned s0 = 0; s0 < cap; s0 += 32) {
+    const unsigned s = s0 + lane;
+    bool keep = false;
+    int key = -1;
+    double val = 0.0;
+    if (s < cap) {
+      key = tk[s];
+      val = tv[s];
+      keep = key != -1 && val != 0.0;
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      const int off = __popc(bal & ((1u << lane) - 1u));
+      cci[base + emitted + off] = key;
+      cv[base + emitted + off] = val;
+    }
+    emitted += __popc(bal);
+  }
+  if (lane == 0) cnt_out[i] = emitted;
+}
+
+__global__ void k_compact_rows(int m, const int64_t *src_rp, const int *cnt, const int *crp,
+                               const int *sci, const double *sv, int *dci, double *dv) {
+  const int i = blockIdx.x;
+  if (i >= m) return;
+  const int64_t s = src_rp[i];
+  const int d = crp[i], c = cnt[i];
+  for (int k = threadIdx.x; k < c; k += blockDim.x) {
+    dci[d + k] = sci[s + k];
+    dv[d + k] = sv[s + k];
+  }
+}
+
+static unsigned next_pow2(uint64_t v) {
+  uint64_t p = 32;
+  while (p < v) p <<= 1;
+  return (unsigned)p;
+}
+
+void spgemm_device(int m, int ncols, const int *xrp, const int *xci, const double *xv,
+                   const int *yrp, const int *yci, const double *yv, DBuf<int> &crp,
+                   DBuf<int> &cci, DBuf<double> &cv, int64_t *nnz_c, cudaStream_t st) {
+  crp.alloc((size_t)m + 1);
+  if (m == 0) {
+    crp.zero(st);
+    *nnz_c = 0;
+    return;
+  }
+  DBuf<int64_t> dprod(m);
+  k_spgemm_products<<<ceil_div(m, 256), 256, 0, st>>>(m, xrp, xci, yrp, dprod.get());
+  CHRONOS_CHECK_LAUNCH();
+  std::vector<int64_t> prod = dprod.to_host(st);
+  std::vector<unsigned> cap(m);
+  const uint64_t colcap = (uint64_t)2 * (uint64_t)std::max(ncols, 1);
+  for (int i = 0; i < m; ++i) cap[i] = next_pow2(std::min<uint64_t>(2 * (uint64_t)prod[i] + 1, colcap));
+  // Chunks of rows whose tables fit the slot budget.
+  const uint64_t budget = (uint64_t)1 << 24;     // 16M slots (192 MB with values)
+  std::vector<int> bounds{0};
+  {
+    uint64_t acc = 0;
+    for (int i = 0; i < m; ++i) {
+      if (acc + cap[i] > budget && i > bounds.back()) { bounds.push_back(i); acc = 0; }
+      acc += cap[i];
+    }
+    bounds.push_back(m);
+  }
+  uint64_t maxchunk = 0;
+  for (size_t c = 0; c + 1 < bounds.size(); ++c) {
+    uint64_t acc = 0;
+    for (int i = bounds[c]; i < bounds[c + 1]; ++i) acc += cap[i];
+    maxchunk = std::max(maxchunk, acc);
+  }
+  DBuf<int> keys(maxchunk);
+  DBuf<double> vals(maxchunk);
+  DBuf<int64_t> toff(m);
+  DBuf<unsigned> tcap(m);
+  std::vector<int64_t> toff_h(m);
+  for (size_t c = 0; c + 1 < bounds.size(); ++c) {
+    int64_t acc = 0;
+    for (int i = bounds[c]; i < bounds[c + 1]; ++i) { toff_h[i] = acc; acc += cap[i]; }
+  }
+  toff.upload(toff_h, st);
+  tcap.upload(cap.data(), m, st);
+  DBuf<int> cnt(m);
+  for (size_t c = 0; c + 1 < bounds.size(); ++c) {
+    const int r0 = bounds[c], r1 = bounds[c + 1];
+    k_spgemm_symbolic<<<ceil_div((int64_t)(r1 - r0) * 32, 256), 256, 0, st>>>(
+        r0, r1, xrp, xci, yrp, yci, toff.get() + r0, tcap.get() + r0, keys.get(), cnt.get());
+    CHRONOS_CHECK_LAUNCH();
+  }
+  std::vector<int> cnt_h = cnt.to_host(st);
+  std::vector<int64_t> rps(m + 1, 0);
+  for (int i = 0; i < m; ++i) rps[i + 1] = rps[i] + cnt_h[i];
+  DBuf<int64_t> drps(m + 1);
+  drps.upload(rps, st);
+  DBuf<int> sci(std::max<int64_t>(rps[m], 1));
+  DBuf<double> sv(std::max<int64_t>(rps[m], 1));
+  DBuf<int> cnt2(m);
+  for (size_t c = 0; c + 1 < bounds.size(); ++c) {
+    const int r0 = bounds[c], r1 = bounds[c + 1];
+    k_spgemm_numeric<<<ceil_div((int64_t)(r1 - r0) * 32, 256), 256, 0, st>>>(
+        r0, r1, xrp, xci, xv, yrp, yci, yv, toff.get() + r0, tcap.get() + r0, keys.get(),
+        vals.get(), drps.get(), sci.get(), sv.get(), cnt2.get());
+    CHRONOS_CHECK_LAUNCH();
+  }
+  std::vector<int> cnt2_h = cnt2.to_host(st);
+  // Sort every row segment [rps[i], rps[i]+cnt2[i]) by column.
+  {
+    DBuf<int64_t> seg_end(m);
+    std::vector<int64_t> se(m);
+    for (int i = 0; i < m; ++i) se[i] = rps[i] + cnt2_h[i];
+    seg_end.upload(se, st);
+    const int64_t total = rps[m];
+    DBuf<int> sci2(std::max<int64_t>(total, 1));
+    DBuf<double> sv2(std::max<int64_t>(total, 1));
+    size_t tmp_bytes = 0;
+    CHRONOS_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, tmp_bytes, sci.get(), sci2.get(),
+                                                     sv.get(), sv2.get(), total, m, drps.get(),
+                                                     seg_end.get(), st));
+    DBuf<unsigned char> tmp(std::max<size_t>(tmp_bytes, 1));
+    CHRONOS_CUDA(cub::DeviceSegmentedSort::SortPairs(tmp.get(), tmp_bytes, sci.get(), sci2.get(),
+                                                     sv.get(), sv2.get(), total, m, drps.get(),
+                                                     seg_end.get(), st));
+    sci = std::move(sci2);
+    sv = std::move(sv2);
+  }
+  std::vector<int> crp_h(m + 1, 0);
+  for (int i = 0; i < m; ++i) {
+    const int64_t t = (int64_t)crp_h[i] + cnt2_h[i];
+    CHRONOS_REQUIRE(t < INT32_MAX, CHRONOS_ENOTSUP, "sparse product exceeds 2^31 entries");
+    crp_h[i + 1] = (int)t;
+  }
+  crp.upload(crp_h, st);
+  const int64_t nnz = crp_h[m];
+  cci.alloc(std::max<int64_t>(nnz, 1));
+  cv.alloc(std::max<int64_t>(nnz, 1));
+  k_compact_rows<<<m, 128, 0, st>>>(m, drps.get(), cnt2.get(), crp.get(), sci.get(), sv.get(),
+                                    cci.get(), cv.get());
+  CHRONOS_CHECK_LAUNCH();
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  *nnz_c = nnz;
+}
+
+// =============================================================================
+// Dense coarse level
+// =============================================================================
+
+// Single-block right-looking Cholesky on an n x n column-major matrix.
+__global__ void __launch_bounds__(1024) k_dense_cholesky(int n, double *A, int *info) {
+  __shared__ int bad;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  if (tid == 0) { bad = 0; *info = 0; }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    if (tid == 0) {
+      const double d = A[(size_t)k * n + k];
+      if (!(d > 0.0)) bad = k + 1;
+      else A[(size_t)k * n + k] = sqrt(d);
+    }
+    __syncthreads();
+    if (bad) break;
+    const double dk = A[(size_t)k * n + k];
+    for (int i = k + 1 + tid; i < n; i += blockDim.x) A[(size_t)k * n + i] /= dk;
+    __syncthreads();
+    for (int j = k + 1 + wid; j < n; j += nw) {
+      const double ljk = A[(size_t)k * n + j];
+      for (int i = j + lane; i < n; i += 32) A[(size_t)j * n + i] -= A[(size_t)k * n + i] * ljk;
+    }
+    __syncthreads();
+  }
+  if (tid == 0) *info = bad;
+  // zero the strict upper triangle
+  for (int j = 1 + wid; j < n; j += nw)
+    for (int i = lane; i < j; i += 32) A[(size_t)j * n + i] = 0.0;
+}
+
+int dense_cholesky_device(int n, double *A, cudaStream_t st) {
+  DBuf<int> info(1);
+  k_dense_cholesky<<<1, 1024, 0, st>>>(n, A, info.get());
+  CHRONOS_CHECK_LAUNCH();
+  int h = 0;
+  CHRONOS_CUDA(cudaMemcpyAsync(&h, info.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  return h;
+}
+
+// Column j of L^{-1} by forward substitution (one block per column).
+__global__ void k_tri_inverse(int n, const double *L, double *X) {
+  extern __shared__ double xs[];
+  const int j = blockIdx.x;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) xs[i] = (i == j) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int k = j; k < n; ++k) {
+    const double xk = xs[k] / L[(size_t)k * n + k];
+    __syncthreads();
+    if (threadIdx.x == 0) xs[k] = xk;
+    for (int i = k + 1 + threadIdx.x; i < n; i += blockDim.x) xs[i] -= L[(size_t)k * n + i] * xk;
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) X[(size_t)j * n + i] = xs[i];
+}
+
+// W = X^T X with X = L^{-1} lower (column-major); 16x16 tiles.
+__global__ void k_gram(int n, const double *X, double *W) {
+  __shared__ double a[16][17], b[16][17];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int i = blockIdx.y * 16 + ty, j = blockIdx.x * 16 + tx;
+  double s = 0.0;
+  const int kstart = max(blockIdx.y * 16, blockIdx.x * 16);
+  for (int k0 = (kstart / 16) * 16; k0 < n; k0 += 16) {
+    const int ka = k0 + tx, kb = k0 + ty;
+    const int ci = blockIdx.y * 16 + ty, cj = blockIdx.x * 16 + tx;
+    a[ty][tx] = (ci < n && ka < n) ? X[(size_t)ci * n + ka] : 0.0;   // X[ka][ci]
+    b[ty][tx] = (cj < n && kb < n) ? X[(size_t)cj * n + kb] : 0.0;   // X[kb][cj]
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) s += a[ty][kk] * b[kk][tx];
+    __syncthreads();
+  }
+  if (i < n && j < n) W[(size_t)i * n + j] = s;
+}
+
+void dense_inverse_from_chol(int n, const double *L, double *W, cudaStream_t st) {
+  DBuf<double> X((size_t)n * n);
+  const size_t sm = (size_t)n * sizeof(double);
+  CHRONOS_REQUIRE(sm <= 200 * 1024, CHRONOS_ENOTSUP, "coarsest level too large for the dense solve");
+  if (sm > 48 * 1024)
+    CHRONOS_CUDA(cudaFuncSetAttribute(k_tri_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_tri_inverse<<<n, 256, sm, st>>>(n, L, X.get());
+  CHRONOS_CHECK_LAUNCH();
+  dim3 grid(ceil_div(n, 16), ceil_div(n, 16)), blk(16, 16);
+  k_gram<<<grid, blk, 0, st>>>(n, X.get(), W);
+  CHRONOS_CHECK_LAUNCH();
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+}
+
+template <typename TI, typename TO>
+__global__ void k_dense_matvec(int n, const double *__restrict__ W, const TI *__restrict__ b,
+                               TO *__restrict__ x) {
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  const double *w = W + (size_t)row * n;
+  double s = 0.0;
+  for (int j = lane; j < n; j += 32) s += w[j] * (double)b[j];
+  s = warp_sum(s);
+  if (lane == 0) x[row] = (TO)s;
+}
+
+template <typename TI, typename TO>
+void dense_matvec(int n, const double *W, const TI *b, TO *x, cudaStream_t st) {
+  k_dense_matvec<TI, TO><<<ceil_div((int64_t)n * 32, 256), 256, 0, st>>>(n, W, b, x);
+  CHRONOS_CHECK_LAUNCH();
+}
+template void dense_matvec<float, float>(int, const double *, const float *, float *, cudaStream_t);
+template void dense_matvec<double, double>(int, const double *, const double *, double *, cudaStream_t);
+
+// =============================================================================
+// Vector helpers
+// =============================================================================
+
+__global__ void k_gather(int64_t nnz, const double *src, const int64_t *perm, double *dst) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz;
+       k += (int64_t)gridDim.x * blockDim.x)
+    dst[k] = src[perm[k]];
+}
+
+void gather_values(int64_t nnz, const double *src, const int64_t *perm, double *dst,
+                   cudaStream_t st) {
+  if (nnz <= 0) return;
+  k_gather<<<std::min<int64_t>(ceil_div(nnz, 256), 4096), 256, 0, st>>>(nnz, src, perm, dst);
+  CHRONOS_CHECK_LAUNCH();
+}
+
+__global__ void k_f64_to_f32(int64_t n, const double *s, float *d) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x)
+    d[k] = (float)s[k];
+}
+
+void convert_f64_to_f32(int64_t n, const double *src, float *dst, cudaStream_t st) {
+  if (n <= 0) return;
+  k_f64_to_f32<<<std::min<int64_t>(ceil_div(n, 256), 4096), 256, 0, st>>>(n, src, dst);
+  CHRONOS_CHECK_LAUNCH();
+}
+
+__global__ void k_dot_partial(int n, const double *a, const double *b, double *part) {
+  __shared__ double red[32];
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += a[i] * b[i];
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+double device_dot(int n, const double *a, const double *b, double *scratch, cudaStream_t st) {
+  const int blocks = 256;
+  k_dot_partial<<<blocks, 256, 0, st>>>(n, a, b, scratch);
+  CHRONOS_CHECK_LAUNCH();
+  double h[256];
+  CHRONOS_CUDA(cudaMemcpyAsync(h, scratch, sizeof(h), cudaMemcpyDeviceToHost, st));
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  double s = 0.0;
+  for (int i = 0; i < blocks; ++i) s += h[i];
+  return s;
+}
+
+__global__ void k_axpby(int n, double a, const double *x, double b, double *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = a * x[i] + b * y[i];
+}
+
+void device_axpby(int n, double a, const double *x, double b, double *y, cudaStream_t st) {
+  k_axpby<<<std::min<int64_t>(ceil_div(n, 256), 4096), 256, 0, st>>>(n, a, x, b, y);
+  CHRONOS_CHECK_LAUNCH();
+}
+
+__global__ void k_scale_copy(int n, double a, const double *x, double *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = a * x[i];
+}
+
+void device_scale_copy(int n, double a, const double *x, double *y, cudaStream_t st) {
+  k_scale_copy<<<std::min<int64_t>(ceil_div(n, 256), 4096), 256, 0, st>>>(n, a, x, y);
+  CHRONOS_CHECK_LAUNCH();
+}
+
+// One warp per row: grad[k] = -lambda_i * u_{col(k)} over the row's entries.
+__global__ void k_adjoint_scatter(int n, const int *rp, const int *ci, const double *lam,
+                                  const double *u, double *grad) {
+  const int lane = threadIdx.x & 31;
+  const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (row >= n) return;
+  const double li = -lam[row];
+  for (int k = rp[row] + lane; k < rp[row + 1]; k += 32) grad[k] = li * u[ci[k]];
+}
+
+void adjoint_scatter(int n, const int *rp, const int *ci, const double *lambda, const double *u,
+                     double *grad, cudaStream_t st) {
+  if (n <= 0) return;
+  k_adjoint_scatter<<<ceil_div((int64_t)n * 32, 256), 256, 0, st>>>(n, rp, ci, lambda, u, grad);
+  CHRONOS_CHECK_LAUNCH();
+}
+
+}  // namespace chronos

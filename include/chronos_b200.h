@@ -1,0 +1,261 @@
+/*
+ * chronos_b200.h -- C ABI of the B200 (sm_100a) AMG-preconditioned SPD solve path.
+ *
+ * Drop-in boundary for ChronosLab's solve path.  Every entry point returns an
+ * int status: 0 = ok, negative = error (CHRONOS_E*); the message of the last
+ * error on the calling thread is available from chronos_last_error().  No C++
+ * exception crosses this boundary.
+ *
+ * Ownership: input pointers are borrowed and never freed by the library; the
+ * library owns everything a handle (chronos_hier, chronos_galerkin_plan) holds
+ * until the matching *_free call.  One handle is used by one host thread at a
+ * time and on one CUDA stream.  Pointers named *_h are host memory; *_d are
+ * device memory of the current device.
+ *
+ * Reference interfaces replaced (paths inside the ChronosLab project):
+ *   chronos_fsai_compute   <- SYM_aFSAI_compute MEX
+ *                             (sources/Preconditioner/AMG/smoother/MEX_SYM_AFSAI/
+ *                              SYM_aFSAI_compute.cpp:15-20,57-149; compute_local_fsai.h:8-11)
+ *   chronos_fsai_numeric   <- numeric half of the same MEX (cpt_afsai_coef.cpp:440-541)
+ *   chronos_amg_setup      <- cpt_aspAMG(param,A,TV0)   (aspAMG/cpt_aspAMG.m:1,54; called at
+ *                             Drivers/driver_AMG/aspAMG_main.m:175, utils/computeAMG.m:46)
+ *   chronos_vcycle         <- AMG_Vcycle(hrc,A,b)       (aspAMG/AMG_Vcycle.m:1-54)
+ *   chronos_pcg            <- PCG_CJ(prodM,prodA,b,x0,itmax,tol) (LinearSolver/PCG_CJ.m:1-73;
+ *                             called at aspAMG_main.m:199-202)
+ *   chronos_sqmr           <- SQMR(Afun,rhs,tol,itmax,lprec,rprec) (LinearSolver/SQMR.m:1-108;
+ *                             called at Tests/CubeBAMG_NONE.m:28)
+ *   chronos_galerkin_*     <- Anext = Pf'*(A*Pf)        (aspAMG/cpt_aspAMG.m:277)
+ *   chronos_dense_chol     <- [L,p,S] = chol(A,'lower') (aspAMG/cpt_aspAMG.m:109) and the
+ *                             coarsest solve S*(L'\(L\(S'*b))) (AMG_Vcycle.m:9-10)
+ *   chronos_params_read    <- readDefaultParams.m / aspAMG_main.m:17-59 and read_*.m
+ */
+#ifndef CHRONOS_B200_H
+#define CHRONOS_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define CHRONOS_OK            0
+#define CHRONOS_EINVAL       -1   /* bad argument, malformed CSR, size limit */
+#define CHRONOS_ECUDA        -2   /* CUDA runtime error */
+#define CHRONOS_ENOMEM       -3   /* host or device allocation failed */
+#define CHRONOS_ENOTSPD      -4   /* non-SPD block / Cholesky breakdown */
+#define CHRONOS_EBREAKDOWN   -5   /* Krylov breakdown (p'Ap <= 0, NaN) */
+#define CHRONOS_EIO          -6   /* parameter or data file error */
+#define CHRONOS_ENOTSUP      -7   /* option outside this solve path */
+
+/* ---- precision of the stored hierarchy -------------------------------- */
+#define CHRONOS_FP64 0            /* all-FP64 GPU path */
+#define CHRONOS_FP32 1            /* FP32 hierarchy, FP32 accumulate; FP64 outer solve */
+
+/* ---- parameters: the positional parm_* files of the reference ----------- */
+typedef struct chronos_params {
+  /* parm_AMG (read_amg.m) */
+  int nLevMax, maxCoarseSZ;
+  /* parm_SMOOTH (read_smoother.m:73-79) */
+  int nthread, nupre, nupost, nstep, step_size;
+  double epsilon;
+  char smoother_method[32];       /* AFSAI_SYM on this path */
+  /* parm_TSPACE (read_tspace.m) */
+  int ntv, tspace_itmax;
+  double tspace_tol;
+  char tspace_method[32];         /* NONE on this path */
+  int init_approx;
+  /* parm_COARSEN (read_coarsen.m:177-179) */
+  char SoC_type[16];              /* DOM or CLA */
+  double soc_tau;
+  int nl_agg;
+  /* parm_PROLONG (read_prolong.m; the BAMG lines) */
+  char proltype[16];              /* BAMG */
+  char prol_emin[16];             /* NONE */
+  int prol_np, itmax_vol;
+  double tol_vol;
+  int dist_min, dist_max;
+  double maxcond, maxrownrm, eps_prol;
+  int updateCF;
+  /* parm_FILTER (read_filter.m) */
+  int filt_np;
+  double filt_wgt, filt_tol, filt_tau;
+  int min_patt;
+  /* parm_GENERAL (read_general.m:4-11) */
+  int ascii_input;
+  char rhs_build[16];
+  int symmetric;
+  char solv_method[16];
+  int itmax;
+  double tol;
+  int restart;
+  /* build options (no counterpart in the parameter files) */
+  int precision;                  /* CHRONOS_FP32 or CHRONOS_FP64 */
+  int use_graph;                  /* 1: whole solve as one CUDA graph with a device-side loop */
+  uint64_t seed;                  /* MT19937 seed of MATLAB's rng(0) stream: 5489 */
+  int fsai_fabs;                  /* 0 (default): FSAI candidate ranking and exit test compare
+                                     magnitudes as the reference's g++ build does, through C's
+                                     int abs (truncation toward zero); 1: through fabs */
+} chronos_params;
+
+/* Reference regression-test parameters (Tests/parm_*): DOM 0.01, BAMG/NONE,
+ * AFSAI_SYM 15/1/1e-3, ntv 6, V(1,1), nLevMax 10, maxCoarseSZ 1000. */
+void chronos_params_default(chronos_params *p);
+/* Reads an aspAMG.fnames file (first 7 lines name parm_AMG, parm_SMOOTH,
+ * parm_TSPACE, parm_COARSEN, parm_PROLONG, parm_FILTER, parm_GENERAL, relative
+ * to the fnames file) into p; fields not in the files keep their value. */
+int chronos_params_read(const char *fnames_path, chronos_params *p);
+
+/* Copies the last error message of this thread into buf (NUL-terminated). */
+int chronos_last_error(char *buf, int len);
+/* Library version string. */
+const char *chronos_version(void);
+
+/* ---- FSAI ------------------------------------------------------------- */
+/* Drop-in for SYM_aFSAI_compute: same argument meaning (1-based CSR, int64 row
+ * pointers, int32 columns, nrows_M - nrows = trailing-block shift).  Pattern by
+ * the adaptive Kaporin search on the host; values by the GPU numeric kernel
+ * (FP64).  ja_G/coef_G must hold nrows*(1+n_step*step_size) entries.  Each row
+ * lists its strictly-lower entries ascending, then the diagonal.  Non-SPD is a
+ * flag (is_posdef = 0), not an error, as in the MEX. */
+int chronos_fsai_compute(int nthread, int n_step, int step_size, double tau, double eps,
+                         int nrows, int nrows_M, int64_t nterm_M,
+                         const int64_t *iat_M_h, const int *ja_M_h, const double *coef_M_h,
+                         int64_t *nterm_G, int64_t *iat_G_h, int *ja_G_h, double *coef_G_h,
+                         int *is_posdef);
+/* Numeric phase only: G values on a given pattern (1-based CSR of G, each row
+ * strictly-lower ascending then the diagonal).  A is 1-based CSR (int64 iat,
+ * int32 ja).  One dense SPD solve per row on the GPU, FP64. */
+int chronos_fsai_numeric(int n, const int64_t *iat_A_h, const int *ja_A_h, const double *val_A_h,
+                         const int64_t *iat_G_h, const int *ja_G_h, double *val_G_h,
+                         int *is_posdef);
+
+/* ---- host-side setup pieces (no GPU) ------------------------------------ */
+/* Result handle for a CSR produced by the library (0-based, FP64). */
+typedef struct chronos_csr chronos_csr;
+int chronos_csr_info(const chronos_csr *m, int *nrows, int *ncols, int64_t *nnz);
+int chronos_csr_fetch(const chronos_csr *m, int *iat_h, int *ja_h, double *val_h);
+int chronos_csr_free(chronos_csr *m);
+
+/* Symbolic half of SYM_aFSAI_compute on the host (cpt_afsai_coef.cpp:316-543):
+ * the adaptive pattern with the host FP64 values of the final local solves.
+ * A: 0-based CSR, sorted rows.  G rows: strictly-lower ascending, then the
+ * diagonal.  fsai_fabs as in chronos_params. */
+int chronos_fsai_pattern(int n, const int *iat_h, const int *ja_h, const double *val_h,
+                         int nstep, int step_size, double eps, int nthread, int fsai_fabs,
+                         int *is_posdef, chronos_csr **G);
+/* coarsen.m on the host: strength of connection (prm->SoC_type, prm->soc_tau)
+ * and the PMIS C/F splitting with the MT19937 stream of prm->seed advanced by
+ * rng_skip draws first.  fcnode_h[n]: coarse k -> k (1..nc), fine -> -(1..nf),
+ * as the reference numbers them.  S (may be NULL) receives the strength matrix. */
+int chronos_coarsen(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
+                    const double *val_h, uint64_t rng_skip, int *fcnode_h, int *nc,
+                    chronos_csr **S);
+/* cpt_ProlMEX_BAMG on the host: BAMG prolongation (n x nc) from the strength
+ * pattern S, fcnode as returned by chronos_coarsen, and the test space TV
+ * (n x ntv, column-major).  c_mark_h[n] (may be NULL) flags rows not
+ * interpolated to eps_prol. */
+int chronos_bamg(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
+                 const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
+                 chronos_csr **P);
+
+/* ---- Galerkin product P'*(A*P) on the GPU (0-based CSR, FP64) --------- */
+typedef struct chronos_galerkin_plan chronos_galerkin_plan;
+/* Symbolic + numeric phase; returns the nnz of Ac (exact zeros dropped, as
+ * MATLAB's sparse product does).  Each output entry is accumulated in the same
+ * order as a row-wise Gustavson product, so values and pattern are bitwise
+ * reproducible. */
+int chronos_galerkin_compute(int n, int nc,
+                             const int *iat_A_h, const int *ja_A_h, const double *val_A_h,
+                             const int *iat_P_h, const int *ja_P_h, const double *val_P_h,
+                             int64_t *nnz_Ac, chronos_galerkin_plan **plan);
+/* Copies Ac (row pointers nc+1, sorted columns, values) to host buffers. */
+int chronos_galerkin_fetch(chronos_galerkin_plan *plan, int *iat_Ac_h, int *ja_Ac_h,
+                           double *val_Ac_h);
+int chronos_galerkin_free(chronos_galerkin_plan *plan);
+
+/* ---- Dense Cholesky of the coarsest level (FP64, GPU) ------------------- */
+/* A_h: n x n column-major SPD.  On success L_h (n x n column-major) holds the
+ * lower factor with zeros above the diagonal.  Returns CHRONOS_ENOTSPD on a
+ * non-positive pivot. */
+int chronos_dense_chol(int n, const double *A_h, double *L_h);
+
+/* ---- CSR SpMV on the GPU (parity helper) ------------------------------- */
+/* y = A x, 0-based CSR, values stored in `precision` and accumulated in it. */
+int chronos_spmv(int n, int ncols, const int *iat_h, const int *ja_h, const double *val_h,
+                 const double *x_h, double *y_h, int precision);
+
+/* ---- AMG hierarchy ------------------------------------------------------ */
+typedef struct chronos_hier chronos_hier;
+
+typedef struct chronos_level_info {
+  int n;                /* rows */
+  int64_t nnz_A, nnz_G, nnz_P;
+  int nc;               /* columns of P (0 on the coarsest level) */
+  double omega, lambda; /* smoother damping and lambda_max(G A G') */
+  int threads_per_row;  /* SpMV lanes per row chosen by the autotuner for A */
+} chronos_level_info;
+
+/* Builds the hierarchy of A (0-based CSR, FP64, host memory) with the test
+ * space TV0 (n x ntv0, column-major; may be NULL with ntv0 = 0).  Coarsening
+ * (SoC + PMIS), C/F splitting and the BAMG prolongation run on the host as in
+ * the reference; FSAI values, lambda_max, the Galerkin products and the
+ * coarse Cholesky run on the GPU.  prm->precision selects the stored
+ * precision.  A diagonal entry equal to 1 is NOT rewritten here (the
+ * computeAMG.m:5-10 Dirichlet fix is the caller's, see chronos_diag_fix). */
+int chronos_amg_setup(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
+                      const double *val_h, int ntv0, const double *TV0_h, chronos_hier **out);
+int chronos_hier_free(chronos_hier *h);
+int chronos_hier_nlevels(const chronos_hier *h, int *nlev);
+int chronos_hier_level_info(const chronos_hier *h, int level, chronos_level_info *info);
+/* Exports level `level` (0-based) matrix `which` ('A', 'G' or 'P') as 0-based
+ * CSR in FP64.  Call with null arrays to get the sizes in *nrows / *nnz. */
+int chronos_hier_export(const chronos_hier *h, int level, char which, int *nrows, int *ncols,
+                        int64_t *nnz, int *iat_h, int *ja_h, double *val_h);
+/* Setup timings in seconds: [fsai_pattern, fsai_numeric, omega, coarsen, prolong,
+ * galerkin, coarse_factor, total]. */
+int chronos_hier_setup_times(const chronos_hier *h, double *t8);
+
+/* computeAMG.m:5-10: diagonal entries equal to 1 become lambda_max(A)/10
+ * (lambda_max by a GPU Lanczos run).  Updates val_h in place. */
+int chronos_diag_fix(int n, const int *iat_h, const int *ja_h, double *val_h);
+
+/* One V(nupre,nupost) cycle x = M^{-1} b (x0 absent), host vectors, FP64 in/out.
+ * nrhs columns, column-major (leading dimension n). */
+int chronos_vcycle(chronos_hier *h, const double *b_h, double *x_h, int nrhs);
+
+/* PCG_CJ on the level-1 operator with the V-cycle preconditioner, x0 = x_h on
+ * input.  resvec_h (itmax+1 entries, may be NULL) receives ||r_k||/||b||.
+ * flag = 1 when not converged (PCG_CJ.m:69-71).  seconds (may be NULL)
+ * receives the device time of the solve (CUDA events, copies excluded). */
+int chronos_pcg(chronos_hier *h, const double *b_h, double *x_h, int itmax, double tol,
+                int *iters, double *resvec_h, int *flag, double *seconds);
+/* Same on device vectors (b_d, x_d: n FP64), the hot path without copies. */
+int chronos_pcg_dev(chronos_hier *h, const double *b_d, double *x_d, int itmax, double tol,
+                    int *iters, double *resvec_h, int *flag, double *seconds);
+/* Block of nrhs independent right-hand sides (column-major n x nrhs) solved
+ * together: one SpMM V-cycle per iteration, per-column PCG_CJ recurrences and
+ * stopping tests.  iters_h[nrhs], flags_h[nrhs]. */
+int chronos_pcg_block(chronos_hier *h, int nrhs, const double *B_h, double *X_h, int itmax,
+                      double tol, int *iters_h, int *flags_h, double *seconds);
+
+/* SQMR (SQMR.m) with the V-cycle as left preconditioner and identity right.
+ * The operator is the 0-based FP64 CSR (iat_h, ja_h, val_h) of the hierarchy's
+ * size, or the level-1 operator when iat_h is NULL (the reference's tests
+ * apply the unmodified A while the preconditioner was built from the
+ * Dirichlet-fixed one, Tests/CubeBAMG_NONE.m:19,28). */
+int chronos_sqmr(chronos_hier *h, const int *iat_h, const int *ja_h, const double *val_h,
+                 const double *b_h, double *x_h, int itmax, double tol, int *iters,
+                 double *relres, int *info);
+
+/* ---- Adjoint ------------------------------------------------------------ */
+/* For J(u) with u = A^{-1} b and dJ/du = g: solves A lambda = g with the same
+ * hierarchy (A is SPD so A^T = A) and returns dJ/dA on A's pattern,
+ * grad_h[k] = -lambda[row(k)] * u[col(k)] (nnz_A entries), plus lambda_h. */
+int chronos_adjoint_grad(chronos_hier *h, const double *u_h, const double *g_h, int itmax,
+                         double tol, double *lambda_h, double *grad_h, int *iters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHRONOS_B200_H */

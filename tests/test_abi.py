@@ -1,0 +1,65 @@
+"""The C ABI library loads without a GPU and exports every declared symbol."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import chronoslab_b200 as cb
+from chronoslab_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        src = open(os.path.join(ROOT, "include", h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"^\s*(?:int|void|const char \*)\s*(chronos_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert len(names) >= 30
+    for name in names:
+        assert hasattr(lib, name), name
+    assert set(names) == set(_lib.SIGNATURES), "ctypes table out of sync with the header"
+
+
+def test_params_struct_layout_matches(lib):
+    p = cb.params()
+    assert p.nLevMax == 10 and p.maxCoarseSZ == 1000 and p.nstep == 15 and p.step_size == 1
+    assert p.epsilon == 1e-3 and p.SoC_type == b"DOM" and p.soc_tau == 0.01
+    assert p.proltype == b"BAMG" and p.maxrownrm == 5.0 and p.eps_prol == 1e-10
+    assert p.precision == cb.CHRONOS_FP32 and p.seed == 5489 and p.fsai_fabs == 0
+    assert p.tol == 1e-8 and p.itmax == 15000
+
+
+def test_last_error_and_status(lib):
+    with pytest.raises(cb.ChronosError) as e:
+        cb.readDefaultParams("/nonexistent/aspAMG.fnames")
+    assert e.value.code == -6 and "cannot open" in str(e.value)
+
+
+def test_bad_csr_rejected(lib):
+    import scipy.sparse as sp
+    A = sp.csr_matrix(np.eye(3))
+    # columns out of order are rejected by the host validation, before any GPU use
+    bad = sp.csr_matrix((np.ones(2), np.array([1, 0]), np.array([0, 2, 2, 2])), shape=(3, 3))
+    bad.has_sorted_indices = True          # lie to skip scipy's sort
+    ip = bad.indptr.astype(np.int32)
+    ix = bad.indices.astype(np.int32)
+    dv = bad.data.astype(np.float64)
+    h = ctypes.c_void_p()
+    ok = ctypes.c_int()
+    code = lib.chronos_fsai_pattern(3, ip.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                    ix.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                    dv.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                    15, 1, 1e-3, 1, 0, ctypes.byref(ok), ctypes.byref(h))
+    assert code == -1 and "increasing" in _lib.last_error()
+    assert cb.version().startswith("chronos_b200")

@@ -1,0 +1,151 @@
+"""GPU hierarchy, V-cycle and Krylov parity against the oracle, through the C ABI."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+import scipy.sparse.linalg  # noqa: F401
+
+from conftest import rowwise_close
+import chronoslab_b200 as cb
+from chronoslab_b200 import problems as PB
+from oracle import amg_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def oracle_from_gpu(h):
+    """Oracle hierarchy built from the GPU hierarchy's own level matrices."""
+    parts = []
+    for l in range(h.nlevels):
+        info = h.level_info(l)
+        p = {"A": h.export(l, "A")}
+        if l < h.nlevels - 1:
+            p.update(G=h.export(l, "G"), P=h.export(l, "P"), omega=info["omega"])
+        parts.append(p)
+    return O.hierarchy_from_parts(parts)
+
+
+@pytest.fixture(scope="module")
+def elast():
+    A, X = PB.elasticity_q1(10, return_coords=True)
+    return A, PB.rbm_test_space(X), PB.elasticity_rhs(A, X, seed=0)
+
+
+@pytest.fixture(scope="module")
+def poisson():
+    A = PB.poisson7(20)
+    return A, None, PB.uniform_rhs(A.shape[0], seed=1)
+
+
+@pytest.mark.parametrize("prec,tol", [(cb.CHRONOS_FP64, 1e-12), (cb.CHRONOS_FP32, 2e-5)])
+@pytest.mark.parametrize("case", ["elast", "poisson"])
+def test_vcycle_parity(lib, case, prec, tol, request):
+    A, TV, b = request.getfixturevalue(case)
+    ntv = 6 if TV is not None else 1
+    with cb.Hierarchy(A, TV, cb.params(precision=prec, ntv=ntv)) as h:
+        assert h.nlevels >= 2
+        Ho = oracle_from_gpu(h)
+        x = h.vcycle(b)
+        xo = O.amg_vcycle(Ho, b)
+        assert rel(x, xo) <= tol
+
+
+@pytest.mark.parametrize("case", ["elast", "poisson"])
+def test_pcg_iterations_fp64(lib, case, request):
+    A, TV, b = request.getfixturevalue(case)
+    ntv = 6 if TV is not None else 1
+    with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP64, ntv=ntv)) as h:
+        Ho = oracle_from_gpu(h)
+        x, it, rv, flag, _ = h.pcg(b, itmax=500, tol=1e-8)
+        xo, ito, rvo, flago = O.pcg_cj(lambda r: O.amg_vcycle(Ho, r), lambda v: A @ v, b,
+                                       np.zeros_like(b), 500, 1e-8)
+        assert flag == 0 and flago == 0
+        assert abs(it - ito) <= 1
+        assert rv.shape == (it + 1,)
+        assert np.allclose(rv[:min(it, ito)], rvo[:min(it, ito)], rtol=1e-6, atol=0)
+        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= 1e-8
+
+
+@pytest.mark.parametrize("case", ["elast", "poisson"])
+def test_pcg_fp32_hierarchy(lib, case, request):
+    """FP32 hierarchy + FP64 outer PCG reaches the FP64 true residual and agrees
+    with the FP64 oracle solve."""
+    A, TV, b = request.getfixturevalue(case)
+    ntv = 6 if TV is not None else 1
+    with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32, ntv=ntv)) as h32, \
+            cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP64, ntv=ntv)) as h64:
+        x32, it32, _, f32, _ = h32.pcg(b, itmax=500, tol=1e-8)
+        x64, it64, _, f64, _ = h64.pcg(b, itmax=500, tol=1e-8)
+        assert f32 == 0 and f64 == 0
+        assert np.linalg.norm(b - A @ x32) / np.linalg.norm(b) <= 1e-8
+        assert abs(it32 - it64) <= 2
+        xs = sp.linalg.spsolve(A.tocsc(), b)
+        assert rel(x32, xs) <= 1e-6
+
+
+def test_graph_loop_matches_host_loop(lib, elast):
+    A, TV, b = elast
+    out = []
+    for g in (1, 0):
+        with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32, use_graph=g)) as h:
+            x, it, rv, flag, _ = h.pcg(b, itmax=500, tol=1e-8)
+            out.append((x, it, rv))
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])          # deterministic reductions
+
+
+def test_pcg_repeatable_and_x0(lib, poisson):
+    A, _, b = poisson
+    with cb.Hierarchy(A, None, cb.params(ntv=1)) as h:
+        x1, it1, _, _, _ = h.pcg(b, itmax=500, tol=1e-8)
+        x2, it2, _, _, _ = h.pcg(b, itmax=500, tol=1e-8)
+        assert it1 == it2 and np.array_equal(x1, x2)
+        # warm start at the solution: PCG_CJ always takes one iteration
+        x3, it3, rv3, flag3, _ = h.pcg(b, x0=x1, itmax=500, tol=1e-8)
+        assert it3 == 1 and flag3 == 0
+        # zero right-hand side returns zero, no iterations (PCG_CJ.m:12-16)
+        x4, it4, _, flag4, _ = h.pcg(np.zeros_like(b), itmax=500, tol=1e-8)
+        assert it4 == 0 and flag4 == 0 and not np.any(x4)
+        # itmax reached -> flag 1 (PCG_CJ.m:69-71)
+        _, it5, _, flag5, _ = h.pcg(b, itmax=2, tol=1e-14)
+        assert it5 == 2 and flag5 == 1
+
+
+def test_cubo_end_to_end_pinned(lib, cubo, cubo_ref):
+    """The reference's pinned regression: SQMR to 1e-6 on Cubo_4820 with the
+    Tests/parm_* settings takes 43 iterations, tolerance max(5%, 2)
+    (Tests/CubeBAMG_NONE.m:3,34)."""
+    A, Af, TV0 = cubo["A"], cubo["Af"], cubo["TV0"]
+    ref_it = cubo_ref["info"]["reference_sqmr_iterations"]
+    with cb.Hierarchy(Af, TV0, cb.params(precision=cb.CHRONOS_FP64)) as h:
+        assert h.level_info(0)["nnz_G"] == cubo_ref["info"]["nnz_G_level1"]
+        assert h.level_info(0)["nc"] == cubo_ref["info"]["nc_level1"]
+        # SQMR's operator is the unmodified A, the preconditioner uses Af
+        x, info, relres, niter = h.sqmr(np.ones(A.shape[0]), 1e-6, 100, A=A)
+        assert info == 0
+        assert abs(niter - cubo_ref["info"]["oracle_sqmr_iterations"]) <= 1
+        assert not (abs(ref_it / niter - 1) > 0.05 and abs(ref_it - niter) > 2)
+        x, it, _, flag, _ = h.pcg(np.ones(A.shape[0]), itmax=200, tol=1e-8)
+        assert flag == 0
+        assert abs(it - cubo_ref["info"]["oracle_pcg_iterations_1e-8"]) <= 1
+
+
+def test_setup_components_match_golden(lib, cubo, cubo_ref):
+    with cb.Hierarchy(cubo["Af"], cubo["TV0"], cb.params(precision=cb.CHRONOS_FP64)) as h:
+        G = h.export(0, "G")
+        Gref = cubo_ref["G"]
+        assert np.array_equal(G.indptr, Gref.indptr) and np.array_equal(G.indices, Gref.indices)
+        assert rowwise_close(G, Gref, 1e-10)
+        P = h.export(0, "P")
+        D = (P - cubo_ref["P"]).tocsr()
+        bad_rows = np.unique(D.nonzero()[0][np.abs(D.data) > 1e-10])
+        assert bad_rows.size <= 0.001 * P.shape[0]
+        # the coarse operator is the Galerkin product of the exported P
+        Ac = h.export(1, "A")
+        ref = (P.T @ (cubo["Af"] @ P)).tocsr()
+        assert rel(Ac.toarray(), ref.toarray()) <= 1e-13
+        info = h.level_info(0)
+        assert 0.0 < info["omega"] <= 1.0
