@@ -1,0 +1,404 @@
+"""Benchmark of the AMG-preconditioned PCG solve path on B200.
+
+Workload: 3D linear elasticity, trilinear hex (Q1) elements on the unit cube,
+ne^3 elements (default 80^3: 1,574,640 DOF, ~81 nnz/row), E = 1, nu = 0.3,
+clamped at z = 0; BAMG prolongation with the six rigid-body modes as test
+space, adaptive FSAI smoother, V(1,1); right-hand side = unit body force plus
+seeded N(0, 0.01) noise; x0 = 0; PCG_CJ to relative residual 1e-8.
+
+One step = one full PCG solve to 1e-8 on inputs resident in HBM.  `value` is
+the FP32-hierarchy solve time (FP64 outer PCG), lower is better; the all-FP64
+GPU path is timed in the same run (`fp64_ms`).  `e2e` is the same solve through
+the public C ABI call with host buffers (host->device copy of b and x0 and the
+device->host copy of x inside the timed region).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
+
+Multi-GPU: a single solve does not shard (dependent SpMVs and global dot
+products), so N GPUs run N independent replicas (different right-hand-side
+seeds), weak scaling; `value` is the slowest rank's time per solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "PCG time-to-1e-8 rel-res, FP32-hierarchy vs FP64 GPU; V-cycle HBM GB/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["product", "reference"], default="product")
+    ap.add_argument("--ne", type=int, default=80, help="elements per cube edge")
+    ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--itmax", type=int, default=1000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-solve", choices=["fp32", "fp64"], default=None,
+                    help="for ncu --profile-from-start off: build one hierarchy, warm up, "
+                         "then bracket exactly one solve with the profiler range and exit")
+    return ap.parse_args()
+
+
+def run_profile_solve(args):
+    import torch
+    import chronoslab_b200 as cb
+    A, TV, b = build_problem(args.ne, seed=0)
+    prec = cb.CHRONOS_FP32 if args.profile_solve == "fp32" else cb.CHRONOS_FP64
+    # ncu cannot profile the kernel nodes of a graph holding a conditional
+    # node: the profiled solve runs the same per-iteration graph from a host
+    # loop (use_graph = 0), kernel for kernel the same work
+    h = cb.Hierarchy(A, TV, cb.params(precision=prec, use_graph=0))
+    dev = torch.device("cuda", 0)
+    bd = torch.from_numpy(b).to(dev)
+    x = torch.zeros(A.shape[0], dtype=torch.float64, device=dev)
+    h.pcg_dev(bd.data_ptr(), x.data_ptr(), args.itmax, args.tol)
+    x.zero_()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    it, flag, sec = h.pcg_dev(bd.data_ptr(), x.data_ptr(), args.itmax, args.tol)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile_solve": args.profile_solve, "ne": args.ne, "iterations": it,
+                      "flag": flag, "ms": sec * 1e3, "levels": [h.level_info(l)
+                                                                for l in range(h.nlevels)]}))
+    h.close()
+    return 0
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = max(smax, float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_from_profiles(name):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(name)
+    except (OSError, ValueError):
+        return None
+
+
+def build_problem(ne, seed):
+    from chronoslab_b200 import problems as PB
+    A, X = PB.elasticity_q1(ne, return_coords=True)
+    TV = PB.rbm_test_space(X)
+    b = PB.elasticity_rhs(A, X, seed=seed)
+    return A, TV, b
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's CPU implementation of the path
+# ---------------------------------------------------------------------------
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    import numpy as np
+    from oracle import amg_oracle as O
+    from oracle import c_oracle as CO
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref (the reference's FSAI/BAMG C++) was not built"}))
+        return 0
+    A, TV, b = build_problem(args.ne, seed=0)
+    threads = cpu_threads()
+    prm = O.default_params(threads)
+    t0 = time.perf_counter()
+    H = CO.reference_hierarchy(A, TV, prm)
+    setup_s = time.perf_counter() - t0
+    CH = CO.CHierarchy(H, threads=threads)
+    for _ in range(args.warmup):
+        CH.pcg(b, itmax=args.itmax, tol=args.tol)
+    times, its = [], []
+    x = None
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        x, it, rv, flag = CH.pcg(b, itmax=args.itmax, tol=args.tol)
+        times.append((time.perf_counter() - t) * 1e3)
+        its.append(it)
+    ms = sum(times) / len(times)
+    relres = float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": ms, "unit": "ms",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Q1 elasticity, body force + N(0,0.01) noise)",
+        "config": {"workload": f"Q1 elasticity {args.ne}^3 elements, {A.shape[0]} DOF, "
+                               f"{A.nnz} nnz, PCG_CJ + AMG V(1,1) to {args.tol}",
+                   "solver": "FP64 PCG_CJ + V-cycle, C/OpenMP restatement of the MATLAB path; "
+                             "hierarchy from the reference's own FSAI and BAMG C++"},
+        "iterations": its[-1], "true_relres": relres, "setup_s": setup_s,
+        "cpu_baseline": {"value": ms, "unit": "ms", "cores": threads, "kind": "reference",
+                         "sample": "one full PCG_CJ solve to 1e-8 per step"},
+        "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# product arm
+# ---------------------------------------------------------------------------
+
+def run_product(args, world, rank, local):
+    import numpy as np
+    import torch
+    import chronoslab_b200 as cb
+
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                 device_id=torch.device("cuda", 0))
+        dist = tdist
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+
+    A, TV, b = build_problem(args.ne, seed=rank)
+    n = A.shape[0]
+    h32 = cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32))
+    h64 = cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP64))
+    setup32, setup64 = h32.setup_times(), h64.setup_times()
+
+    bd = torch.from_numpy(b).to(dev)
+    x32 = torch.zeros(n, dtype=torch.float64, device=dev)
+    x64 = torch.zeros(n, dtype=torch.float64, device=dev)
+
+    def solve(h, x):
+        x.zero_()
+        torch.cuda.synchronize()
+        return h.pcg_dev(bd.data_ptr(), x.data_ptr(), args.itmax, args.tol)
+
+    for _ in range(args.warmup):
+        solve(h32, x32)
+        solve(h64, x64)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    barrier()
+    with clocks:
+        t32, t64, it32, it64 = [], [], [], []
+        for _ in range(args.steps):
+            it, flag, sec = solve(h32, x32)
+            assert flag == 0, "FP32-hierarchy PCG did not converge"
+            t32.append(sec * 1e3)
+            it32.append(it)
+        for _ in range(args.steps):
+            it, flag, sec = solve(h64, x64)
+            assert flag == 0, "FP64 PCG did not converge"
+            t64.append(sec * 1e3)
+            it64.append(it)
+    barrier()
+    ms32 = sum(t32) / len(t32)
+    ms64 = sum(t64) / len(t64)
+    if dist:
+        tt = torch.tensor([ms32, ms64], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms32, ms64 = tt.tolist()
+
+    # end to end through the public call with host buffers
+    e2e = []
+    xh = np.zeros(n)
+    barrier()
+    for _ in range(max(2, args.steps // 2)):
+        t = time.perf_counter()
+        xh, it, rv, flag, _ = h32.pcg(b, np.zeros(n), args.itmax, args.tol)
+        e2e.append((time.perf_counter() - t) * 1e3)
+    e2e_ms = sum(e2e) / len(e2e)
+    if dist:
+        tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = tt.item()
+
+    x32h = x32.cpu().numpy()
+    x64h = x64.cpu().numpy()
+    bn = np.linalg.norm(b)
+    relres32 = float(np.linalg.norm(b - A @ x32h) / bn)
+    relres64 = float(np.linalg.norm(b - A @ x64h) / bn)
+
+    prof = h32.profile(reps=20)
+    prof64 = h64.profile(reps=20)
+    peak, peak_kind = peaks()
+    achieved = prof["top_apply_bytes"] / (prof["top_apply_ms"] * 1e-3) / 1e9
+    vgbs32 = prof["vcycle_bytes"] / (prof["vcycle_ms"] * 1e-3) / 1e9
+    vgbs64 = prof64["vcycle_bytes"] / (prof64["vcycle_ms"] * 1e-3) / 1e9
+    it_gbs = prof["iteration_bytes"] * it32[-1] / (ms32 * 1e-3) / 1e9
+
+    levels = [h32.level_info(l) for l in range(h32.nlevels)]
+
+    cpu = None
+    rel_err_oracle = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import amg_oracle as O
+        from oracle import c_oracle as CO
+        parts = []
+        for l in range(h64.nlevels):
+            p = {"A": h64.export(l, "A")}
+            if l < h64.nlevels - 1:
+                p.update(G=h64.export(l, "G"), P=h64.export(l, "P"),
+                         omega=h64.level_info(l)["omega"])
+            parts.append(p)
+        threads = cpu_threads()
+        CH = CO.CHierarchy(O.hierarchy_from_parts(parts), threads=threads)
+        t = time.perf_counter()
+        xo, ito, _, flo = CH.pcg(b, itmax=args.itmax, tol=args.tol)
+        cpu_ms = (time.perf_counter() - t) * 1e3
+        rel_err_oracle = float(np.linalg.norm(x32h - xo) / np.linalg.norm(xo))
+        cpu = {"value": cpu_ms, "unit": "ms", "cores": threads, "kind": "port",
+               "sample": f"one full FP64 PCG_CJ solve to {args.tol} of the same system "
+                         f"({ito} iterations) with the oracle's C/OpenMP V-cycle on the "
+                         f"GPU hierarchy's FP64 level matrices"}
+
+    launches = (prof["kernels_per_iteration"] * it32[-1] + prof["kernels_per_solve"]) * args.steps \
+        + (prof64["kernels_per_iteration"] * it64[-1] + prof64["kernels_per_solve"]) * args.steps
+
+    out = {
+        "metric": METRIC, "value": ms32, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms32, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 hierarchy / f64 outer",
+        "data": "synthetic (seeded Q1 elasticity, body force + N(0,0.01) noise)",
+        "config": {
+            "workload": f"Q1 elasticity {args.ne}^3 elements, {n} DOF, {A.nnz} nnz, "
+                        f"BAMG + aFSAI V(1,1), PCG_CJ to {args.tol}",
+            "levels": [L["n"] for L in levels],
+            "l2": "inputs larger than L2 (level-1 operator alone is "
+                  f"{A.nnz * 12 / 1e9:.2f} GB in FP64)",
+            "parallelism": f"{world} independent replica(s), one per GPU",
+        },
+        "fp64_ms": ms64,
+        "speedup_fp32_vs_fp64": ms64 / ms32,
+        "iterations": {"fp32": it32[-1], "fp64": it64[-1]},
+        "true_relres": {"fp32": relres32, "fp64": relres64},
+        "rel_err_vs_fp64_oracle": rel_err_oracle,
+        "vcycle_hbm_gbs": {"fp32": vgbs32, "fp64": vgbs64},
+        "pcg_iteration_hbm_gbs": it_gbs,
+        "setup_s": {"fp32": setup32["total"], "fp64": setup64["total"]},
+        "roofline": {"bound": "hbm", "kernel": "level-1 residual r = b - A x (FP32 CSR)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic_from_profiles("top_apply"),
+                     "algorithmic_bytes": prof["top_apply_bytes"],
+                     "launch_ms": prof["top_apply_ms"]},
+        "clocks": clocks.summary(),
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 2 * n * 8,
+                "d2h_bytes_per_step": n * 8},
+        "gpu_launches": launches,
+    }
+    if cpu:
+        out["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(out))
+    h32.close()
+    h64.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_env()
+    if world > 1:
+        # one device per rank: both CUDA runtimes in the process (torch's and
+        # the library's) then see the same single device
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+    if args.profile_solve:
+        return run_profile_solve(args)
+    return run_product(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

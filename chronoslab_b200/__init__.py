@@ -307,7 +307,7 @@ class Hierarchy:
         check(self._lib.chronos_hier_level_info(self._h, level, C.byref(info)))
         return {"n": info.n, "nnz_A": info.nnz_A, "nnz_G": info.nnz_G, "nnz_P": info.nnz_P,
                 "nc": info.nc, "omega": info.omega, "lambda": info.lambda_,
-                "threads_per_row": info.threads_per_row}
+                "threads_per_row": info.threads_per_row, "block_rows": info.block_rows}
 
     def export(self, level, which):
         nr, ncl, nnz = C.c_int(), C.c_int(), C.c_int64()
@@ -327,6 +327,13 @@ class Hierarchy:
         keys = ["fsai_pattern", "fsai_numeric", "omega", "coarsen", "prolong", "galerkin",
                 "coarse_factor", "total"]
         return dict(zip(keys, t.tolist()))
+
+    def profile(self, reps=20):
+        """CUDA-event timings (ms) and algorithmic bytes of the hot kernels."""
+        from ._lib import chronos_profile
+        p = chronos_profile()
+        check(self._lib.chronos_hier_profile(self._h, reps, C.byref(p)))
+        return {k: getattr(p, k) for k, _ in chronos_profile._fields_}
 
     def vcycle(self, b):
         b = np.asarray(b, dtype=np.float64)

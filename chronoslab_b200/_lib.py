@@ -42,14 +42,23 @@ class chronos_params(C.Structure):
         ("solv_method", C.c_char * 16), ("itmax", C.c_int), ("tol", C.c_double),
         ("restart", C.c_int),
         ("precision", C.c_int), ("use_graph", C.c_int), ("seed", C.c_uint64),
-        ("fsai_fabs", C.c_int),
+        ("fsai_fabs", C.c_int), ("use_bsr", C.c_int),
     ]
 
 
 class chronos_level_info(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz_A", C.c_int64), ("nnz_G", C.c_int64),
                 ("nnz_P", C.c_int64), ("nc", C.c_int), ("omega", C.c_double),
-                ("lambda_", C.c_double), ("threads_per_row", C.c_int)]
+                ("lambda_", C.c_double), ("threads_per_row", C.c_int),
+                ("block_rows", C.c_int)]
+
+
+class chronos_profile(C.Structure):
+    _fields_ = [("vcycle_ms", C.c_double), ("vcycle_bytes", C.c_double),
+                ("top_apply_ms", C.c_double), ("top_apply_bytes", C.c_double),
+                ("outer_spmv_ms", C.c_double), ("outer_spmv_bytes", C.c_double),
+                ("iteration_bytes", C.c_double), ("kernels_per_iteration", C.c_int),
+                ("kernels_per_solve", C.c_int)]
 
 
 _i = C.c_int
@@ -88,6 +97,7 @@ SIGNATURES = {
     "chronos_hier_level_info": [_vp, _i, C.POINTER(chronos_level_info)],
     "chronos_hier_export": [_vp, _i, C.c_char, _pi, _pi, _pi64, _pi, _pi, _pd],
     "chronos_hier_setup_times": [_vp, _pd],
+    "chronos_hier_profile": [_vp, _i, C.POINTER(chronos_profile)],
     "chronos_diag_fix": [_i, _pi, _pi, _pd],
     "chronos_vcycle": [_vp, _pd, _pd, _i],
     "chronos_pcg": [_vp, _pd, _pd, _i, _d, _pi, _pd, _pi, _pd],

@@ -421,7 +421,8 @@ int chronos_hier_level_info(const chronos_hier *h, int level, chronos_level_info
     info->nc = L.coarsest ? 0 : L.nc;
     info->omega = L.omega;
     info->lambda = L.lambda;
-    info->threads_per_row = L.A.lanes;
+    info->threads_per_row = L.A.nb > 0 ? 1 : L.A.lanes;   // block form: a thread per block row
+    info->block_rows = L.A.nb;
   });
 }
 
@@ -451,6 +452,13 @@ int chronos_hier_setup_times(const chronos_hier *h, double *t8) {
   return guard([&] {
     CHRONOS_REQUIRE(h && t8, CHRONOS_EINVAL, "null argument");
     for (int i = 0; i < 8; ++i) t8[i] = h->h->times[i];
+  });
+}
+
+int chronos_hier_profile(chronos_hier *hh, int reps, chronos_profile *out) {
+  return guard([&] {
+    CHRONOS_REQUIRE(hh && out, CHRONOS_EINVAL, "null argument");
+    hh->h->profile(reps, out);
   });
 }
 

@@ -18,6 +18,9 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <cstdio>
+#include <cstdlib>
+#include <sys/stat.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -71,54 +74,268 @@ static int heuristic_lanes(const DMat &m) {
   return L;
 }
 
-void autotune_lanes(DMat &m, bool fp32, cudaStream_t st) {
-  static std::mutex mu;
-  static std::map<std::tuple<int, int64_t, int, bool>, int> cache;
-  if (m.nrows <= 0) return;
-  const auto key = std::make_tuple(m.nrows, m.nnz, m.ncols, fp32);
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    auto it = cache.find(key);
-    if (it != cache.end()) { m.lanes = it->second; return; }
+// Autotuner of the lanes per row (CSR) or per block row (BSR3): times each
+// candidate on the matrix itself and keeps the fastest.  Decisions are cached
+// per matrix signature (format, rows, entries, columns, precision) in memory
+// and in a text file (CHRONOS_TUNE_CACHE, default ~/.cache/chronos_b200_tune.txt)
+// so later processes on the machine -- a profiler run included -- reuse them.
+namespace {
+using TuneKey = std::tuple<char, int, int64_t, int, bool>;
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+bool g_tune_loaded = false;
+
+std::string tune_path() {
+  if (const char *p = std::getenv("CHRONOS_TUNE_CACHE")) return p;
+  const char *home = std::getenv("HOME");
+  return std::string(home ? home : "/tmp") + "/.cache/chronos_b200_tune.txt";
+}
+
+void tune_load_locked() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  FILE *f = std::fopen(tune_path().c_str(), "r");
+  if (!f) return;
+  char kind;
+  int nr, nc, fp, L;
+  long long nnz;
+  while (std::fscanf(f, " %c %d %lld %d %d %d", &kind, &nr, &nnz, &nc, &fp, &L) == 6)
+    g_tune[TuneKey(kind, nr, (int64_t)nnz, nc, fp != 0)] = L;
+  std::fclose(f);
+}
+
+void tune_store_locked(const TuneKey &k, int L) {
+  g_tune[k] = L;
+  const std::string path = tune_path();
+  const auto slash = path.find_last_of('/');
+  if (slash != std::string::npos) {
+    const std::string dir = path.substr(0, slash);
+    // create the directory without a shell
+    for (size_t i = 1; i <= dir.size(); ++i)
+      if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
   }
-  m.lanes = heuristic_lanes(m);
-  if (m.nnz < 4096) {                      // launch-latency bound: no timing
-    std::lock_guard<std::mutex> lk(mu);
-    cache[key] = m.lanes;
-    return;
+  if (FILE *f = std::fopen(path.c_str(), "a")) {
+    std::fprintf(f, "%c %d %lld %d %d %d\n", std::get<0>(k), std::get<1>(k),
+                 (long long)std::get<2>(k), std::get<3>(k), std::get<4>(k) ? 1 : 0, L);
+    std::fclose(f);
   }
-  DBuf<double> x64(m.ncols), y64(m.nrows);
-  DBuf<float> x32(m.ncols), y32(m.nrows);
-  x64.zero(st);
-  x32.zero(st);
+}
+
+template <typename Launch>
+int time_candidates(const std::vector<int> &cands, Launch launch, cudaStream_t st) {
   cudaEvent_t e0, e1;
   CHRONOS_CUDA(cudaEventCreate(&e0));
   CHRONOS_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
-  int bestL = m.lanes;
-  for (int L : {2, 4, 8, 16, 32}) {
-    auto launch = [&]() {
-      if (fp32)
-        csr_apply<float, float, float, float, MODE_PLAIN, false>(st, L, m.nrows, m.rp, m.ci, m.v32,
-                                                               x32.get(), nullptr, y32.get(), 1.0f);
-      else
-        csr_apply<double, double, double, double, MODE_PLAIN, false>(
-            st, L, m.nrows, m.rp, m.ci, m.v64, x64.get(), nullptr, y64.get(), 1.0);
-    };
-    launch();
-    CHRONOS_CUDA(cudaEventRecord(e0, st));
-    for (int r = 0; r < 5; ++r) launch();
-    CHRONOS_CUDA(cudaEventRecord(e1, st));
-    CHRONOS_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best) { best = ms; bestL = L; }
+  int bestL = cands.front();
+  for (int L : cands) {
+    launch(L);
+    float tmin = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+      CHRONOS_CUDA(cudaEventRecord(e0, st));
+      for (int q = 0; q < 4; ++q) launch(L);
+      CHRONOS_CUDA(cudaEventRecord(e1, st));
+      CHRONOS_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      tmin = std::min(tmin, ms);
+    }
+    if (tmin < best) { best = tmin; bestL = L; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  m.lanes = bestL;
-  std::lock_guard<std::mutex> lk(mu);
-  cache[key] = bestL;
+  return bestL;
+}
+}  // namespace
+
+void autotune_lanes(DMat &m, bool fp32, cudaStream_t st) {
+  if (m.nrows <= 0) return;
+  const TuneKey key('C', m.nrows, m.nnz, m.ncols, fp32);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) m.lanes = it->second;
+    else m.lanes = -1;
+  }
+  if (m.lanes < 0) {
+    m.lanes = heuristic_lanes(m);
+    if (m.nnz >= 4096) {                    // below: launch-latency bound, keep the heuristic
+      DBuf<double> x64(m.ncols), y64(m.nrows);
+      DBuf<float> x32(m.ncols), y32(m.nrows);
+      x64.zero(st);
+      x32.zero(st);
+      m.lanes = time_candidates({1, 2, 4, 8, 16, 32}, [&](int L) {
+        if (fp32)
+          csr_apply<float, float, float, float, MODE_PLAIN, false>(st, L, m.nrows, m.rp, m.ci, m.v32,
+                                                                 x32.get(), nullptr, y32.get(), 1.0f);
+        else
+          csr_apply<double, double, double, double, MODE_PLAIN, false>(
+              st, L, m.nrows, m.rp, m.ci, m.v64, x64.get(), nullptr, y64.get(), 1.0);
+      }, st);
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_store_locked(key, m.lanes);
+  }
+}
+
+// Sliced 3x3 block form of a CSR matrix whose row triples share a pattern of
+// whole, aligned 3x3 blocks (structural zeros included).  Returns false
+// otherwise.  Layout as k_sell3_apply reads it.
+// Block lengths of the 3x3 block form, or empty when A has none.
+static std::vector<int> block_row_lengths(const HostCSR &A) {
+  if (A.nrows % 3 != 0 || A.ncols % 3 != 0 || A.nrows == 0) return {};
+  const int nb = A.nrows / 3;
+  std::vector<int> blen(nb);
+  for (int I = 0; I < nb; ++I) {
+    const int64_t len = A.rp[3 * I + 1] - A.rp[3 * I];
+    if (len % 3 != 0) return {};
+    for (int r = 1; r < 3; ++r)
+      if (A.rp[3 * I + r + 1] - A.rp[3 * I + r] != len) return {};
+    const int64_t s0 = A.rp[3 * I];
+    for (int64_t k = 0; k < len; k += 3) {
+      const int c = A.ci[s0 + k];
+      if (c % 3 != 0) return {};
+      for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc)
+          if (A.ci[A.rp[3 * I + r] + k + cc] != c + cc) return {};
+    }
+    blen[I] = (int)(len / 3);
+  }
+  return blen;
+}
+
+// Layout for T threads per block row: chunks of C = 32/T block rows, each
+// padded to its longest row rounded up to a multiple of T; slot j of row l
+// at off_c + (j/T)*32 + (j%T)*C + l; chw = padded width / T.
+static bool build_sell3(const HostCSR &A, const std::vector<int> &blen, int T,
+                        std::vector<int> &choff, std::vector<int> &chw, std::vector<int> &sci,
+                        std::vector<double> &planes) {
+  const int nb = (int)blen.size();
+  const int C = 32 / T;
+  const int nchunk = (nb + C - 1) / C;
+  choff.assign((size_t)nchunk + 1, 0);
+  chw.assign(nchunk, 0);
+  for (int c = 0; c < nchunk; ++c) {
+    int w = 0;
+    for (int l = 0; l < C && C * c + l < nb; ++l) w = std::max(w, blen[C * c + l]);
+    w = (w + T - 1) / T;
+    chw[c] = w;
+    const int64_t next = (int64_t)choff[c] + 32LL * w;
+    if (next >= INT32_MAX) return false;
+    choff[c + 1] = (int)next;
+  }
+  const int64_t nslots = choff[nchunk];
+  sci.assign(nslots, 0);
+  planes.assign((size_t)9 * nslots, 0.0);
+  for (int I = 0; I < nb; ++I) {
+    const int c = I / C, l = I % C;
+    const int64_t s0 = A.rp[3 * I];
+    for (int j = 0; j < blen[I]; ++j) {
+      const int64_t slot = choff[c] + 32LL * (j / T) + (int64_t)(j % T) * C + l;
+      sci[slot] = A.ci[s0 + 3 * j] / 3;
+      for (int r = 0; r < 3; ++r)
+        for (int cc = 0; cc < 3; ++cc)
+          planes[(size_t)(3 * r + cc) * nslots + slot] = A.v[A.rp[3 * I + r] + 3 * j + cc];
+    }
+  }
+  return true;
+}
+
+static void upload_sell3(const HostCSR &A, const std::vector<int> &blen, int T, DMat &d,
+                         bool fp32, cudaStream_t st) {
+  std::vector<int> choff, chw, sci;
+  std::vector<double> planes;
+  if (!build_sell3(A, blen, T, choff, chw, sci, planes)) return;
+  d.nb = A.nrows / 3;
+  d.sell_T = T;
+  d.nchunk = (int)chw.size();
+  d.nnzb = 0;
+  for (int l : blen) d.nnzb += l;
+  d.nslots = choff.back();
+  d.choff.upload(choff, st);
+  d.chw.upload(chw, st);
+  d.sci.upload(sci, st);
+  d.bv64.upload(planes, st);
+  if (fp32) {
+    d.bv32.alloc(planes.size());
+    convert_f64_to_f32((int64_t)planes.size(), d.bv64.get(), d.bv32.get(), st);
+  }
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+}
+
+// Attaches the sliced block form with the fastest threads-per-block-row
+// (timed in the precision the V-cycle uses; cached like the CSR lanes).
+static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) {
+  const std::vector<int> blen = block_row_lengths(A);
+  if (blen.empty()) return;
+  const TuneKey key('S', (int)blen.size(), A.nnz(), A.ncols, fp32);
+  int T = -1;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) T = it->second;
+  }
+  if (T < 0) {
+    DBuf<double> x64(A.ncols), y64(A.nrows);
+    DBuf<float> x32(A.ncols), y32(A.nrows);
+    x64.zero(st);
+    x32.zero(st);
+    float best = 1e30f;
+    cudaEvent_t e0, e1;
+    CHRONOS_CUDA(cudaEventCreate(&e0));
+    CHRONOS_CUDA(cudaEventCreate(&e1));
+    for (int t : {1, 2, 4}) {
+      DMat probe;
+      upload_sell3(A, blen, t, probe, fp32, st);
+      auto launch = [&] {
+        if (fp32)
+          sell3_apply<float, float, float, float, MODE_PLAIN, false>(
+              st, t, probe.nb, probe.nchunk, probe.choff, probe.chw, probe.sci, probe.bv32.get(),
+              probe.nslots, x32.get(), (const float *)nullptr, y32.get(), 1.0f);
+        else
+          sell3_apply<double, double, double, double, MODE_PLAIN, false>(
+              st, t, probe.nb, probe.nchunk, probe.choff, probe.chw, probe.sci, probe.bv64.get(),
+              probe.nslots, x64.get(), (const double *)nullptr, y64.get(), 1.0);
+      };
+      launch();
+      float tmin = 1e30f;
+      for (int r = 0; r < 3; ++r) {
+        CHRONOS_CUDA(cudaEventRecord(e0, st));
+        for (int q = 0; q < 4; ++q) launch();
+        CHRONOS_CUDA(cudaEventRecord(e1, st));
+        CHRONOS_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        tmin = std::min(tmin, ms);
+      }
+      if (tmin < best) { best = tmin; T = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_store_locked(key, T);
+  }
+  upload_sell3(A, blen, T, d, fp32, st);
+}
+
+template <typename T> inline const T *bvals(const DMat &m);
+template <> inline const float *bvals<float>(const DMat &m) { return m.bv32.get(); }
+template <> inline const double *bvals<double>(const DMat &m) { return m.bv64.get(); }
+
+// Operator apply through the block form when the matrix has one.
+template <typename T, typename XT, typename ZT, typename YT, int MODE, bool DOT>
+static void op_apply(cudaStream_t st, const DMat &A, const XT *x, const ZT *z, YT *y, T alpha,
+                     const double *dw = nullptr, double *part = nullptr, unsigned *tick = nullptr,
+                     double *dot_out = nullptr) {
+  if (A.nb > 0)
+    sell3_apply<T, XT, ZT, YT, MODE, DOT>(st, A.sell_T, A.nb, A.nchunk, A.choff, A.chw, A.sci,
+                                          bvals<T>(A), A.nslots, x, z, y, alpha, dw, part, tick,
+                                          dot_out);
+  else
+    csr_apply<T, XT, ZT, YT, MODE, DOT>(st, A.lanes, A.nrows, A.rp, A.ci, vals<T>(A), x, z, y,
+                                        alpha, dw, part, tick, dot_out);
 }
 
 // ---------------------------------------------------------------------------
@@ -281,6 +498,7 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
     n = Al.nrows;
     L.n = n;
     upload_csr(Al, L.A, fp32, st);
+    if (prm.use_bsr) attach_sell3(Al, L.A, fp32, st);
     if (n <= prm.maxCoarseSZ || level >= prm.nLevMax) {
       const double t0 = now_s();
       CHRONOS_REQUIRE(n <= 8192, CHRONOS_ENOTSUP, "coarsest level larger than 8192 rows");
@@ -467,12 +685,12 @@ static void vcycle_level(Hier &h, int l, const BT *b, OT *out, const double *dw,
   csr_apply<T, BT, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), b, nullptr, t, T(1));
   csr_apply<T, T, T, T, MODE_SCALE, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, nullptr, x, w);
   for (int k = 1; k < h.prm.nupre; ++k) {
-    csr_apply<T, T, BT, T, MODE_RESID, false>(st, A.lanes, n, A.rp, A.ci, vals<T>(A), x, b, r, T(1));
+    op_apply<T, T, BT, T, MODE_RESID, false>(st, A, x, b, r, T(1));
     csr_apply<T, T, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), r, nullptr, t, T(1));
     csr_apply<T, T, T, T, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, x, w);
   }
   // residual and restriction
-  csr_apply<T, T, BT, T, MODE_RESID, false>(st, A.lanes, n, A.rp, A.ci, vals<T>(A), x, b, r, T(1));
+  op_apply<T, T, BT, T, MODE_RESID, false>(st, A, x, b, r, T(1));
   Level &C = h.levels[l + 1];
   csr_apply<T, T, T, T, MODE_PLAIN, false>(st, Pt.lanes, L.nc, Pt.rp, Pt.ci, vals<T>(Pt), r, nullptr,
                                            C.b<T>(), T(1));
@@ -482,7 +700,7 @@ static void vcycle_level(Hier &h, int l, const BT *b, OT *out, const double *dw,
   // postsmooth
   const int npost = h.prm.nupost;
   for (int k = 0; k < npost; ++k) {
-    csr_apply<T, T, BT, T, MODE_RESID, false>(st, A.lanes, n, A.rp, A.ci, vals<T>(A), x, b, r, T(1));
+    op_apply<T, T, BT, T, MODE_RESID, false>(st, A, x, b, r, T(1));
     csr_apply<T, T, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), r, nullptr, t, T(1));
     if (k + 1 < npost) {
       csr_apply<T, T, T, T, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, x, w);
@@ -512,9 +730,8 @@ void Hier::vcycle(const double *b, double *out, const double *dw, double *dot_ou
 }
 
 void Hier::apply_A(const double *x, double *y) {
-  const DMat &A = levels[0].A;
-  csr_apply<double, double, double, double, MODE_PLAIN, false>(st, A.lanes, A.nrows, A.rp, A.ci,
-                                                               A.v64, x, nullptr, y, 1.0);
+  op_apply<double, double, double, double, MODE_PLAIN, false>(st, levels[0].A, x,
+                                                              (const double *)nullptr, y, 1.0);
 }
 
 // ---------------------------------------------------------------------------
@@ -582,6 +799,94 @@ k_pcg_spmv(int n, const int *__restrict__ rp, const int *__restrict__ ci,
   grid_reduce<2>(vals2, part, ticket, FinAlpha{sc});
 }
 
+// The same on the sliced 3x3 block form (see k_sell3_apply).
+template <int T>
+__global__ void __launch_bounds__(kApplyThreads)
+k_pcg_spmv_sell3(int nb, int nchunk, const int *__restrict__ choff, const int *__restrict__ chw,
+                 const int *__restrict__ sci, const double *__restrict__ V, int64_t nslots,
+                 const double *__restrict__ p, const double *__restrict__ res,
+                 double *__restrict__ axp, double *part, unsigned *ticket, double *sc) {
+  constexpr int C = 32 / T;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double d0 = 0.0, d1 = 0.0;
+  for (int c = warp; c < nchunk; c += nwarps) {
+    const int off = __ldg(choff + c) + lane, w = __ldg(chw + c);
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+#pragma unroll 2
+    for (int j = 0; j < w; ++j) {
+      const int k = off + 32 * j;
+      const int col = 3 * __ldg(sci + k);
+      const double xa = __ldg(p + col), xb = __ldg(p + col + 1), xc = __ldg(p + col + 2);
+      s0 += __ldg(V + k) * xa + __ldg(V + nslots + k) * xb + __ldg(V + 2 * nslots + k) * xc;
+      s1 += __ldg(V + 3 * nslots + k) * xa + __ldg(V + 4 * nslots + k) * xb +
+            __ldg(V + 5 * nslots + k) * xc;
+      s2 += __ldg(V + 6 * nslots + k) * xa + __ldg(V + 7 * nslots + k) * xb +
+            __ldg(V + 8 * nslots + k) * xc;
+    }
+    if (T > 1) {
+      s0 = slot_sum<T>(s0);
+      s1 = slot_sum<T>(s1);
+      s2 = slot_sum<T>(s2);
+    }
+    const int br = C * c + (lane & (C - 1));
+    if (lane < C && br < nb) {
+      const double s[3] = {s0, s1, s2};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const int row = 3 * br + r;
+        axp[row] = s[r];
+        const double pi = p[row];
+        d0 += pi * s[r];
+        d1 += pi * res[row];
+      }
+    }
+  }
+  double vals2[2] = {d0, d1};
+  grid_reduce<2>(vals2, part, ticket, FinAlpha{sc});
+}
+
+// axp = A p with ptap and p'res, through the block form when A has one.
+static void launch_pcg_spmv(cudaStream_t st, const DMat &A, const double *p, const double *res,
+                            double *axp, double *part, unsigned *tick, double *sc) {
+  if (A.nb > 0) {
+    const int blocks = std::min(num_sms() * 8, (int)ceil_div(A.nchunk, kApplyThreads / 32));
+#define CHRONOS_PCGS_CASE(TT)                                                                  \
+  case TT:                                                                                     \
+    k_pcg_spmv_sell3<TT><<<blocks, kApplyThreads, 0, st>>>(A.nb, A.nchunk, A.choff, A.chw,     \
+                                                           A.sci, A.bv64.get(), A.nslots, p,   \
+                                                           res, axp, part, tick, sc);          \
+    break;
+    switch (A.sell_T) {
+      CHRONOS_PCGS_CASE(1)
+      CHRONOS_PCGS_CASE(2)
+      CHRONOS_PCGS_CASE(4)
+      default: throw Error(CHRONOS_EINVAL, "bad threads per block row");
+    }
+#undef CHRONOS_PCGS_CASE
+  } else {
+    const int n = A.nrows;
+    const int L = std::max(A.lanes, 2);
+    const int blocks = std::min(num_sms() * 8, (int)ceil_div(n, kApplyThreads / L));
+#define CHRONOS_PCG_CASE(LL)                                                                   \
+  case LL:                                                                                     \
+    k_pcg_spmv<LL><<<blocks, kApplyThreads, 0, st>>>(n, A.rp, A.ci, A.v64, p, res, axp, part,  \
+                                                    tick, sc);                                 \
+    break;
+    switch (L) {
+      CHRONOS_PCG_CASE(2)
+      CHRONOS_PCG_CASE(4)
+      CHRONOS_PCG_CASE(8)
+      CHRONOS_PCG_CASE(16)
+      CHRONOS_PCG_CASE(32)
+      default: throw Error(CHRONOS_EINVAL, "bad lane count");
+    }
+#undef CHRONOS_PCG_CASE
+  }
+  CHRONOS_CHECK_LAUNCH();
+}
+
 struct FinResidual {
   double *sc, *resvec;
   cudaGraphConditionalHandle handle;
@@ -632,26 +937,9 @@ static void capture_iteration(Hier &h, cudaGraphConditionalHandle handle, int us
   h.vcycle(s.res.get(), s.pres.get(), s.axp.get(), sc + SC_PRES_AXP);
   k_pcg_p_update<<<nb, 256, 0, st>>>(n, s.pres.get(), s.p.get(), sc);
   CHRONOS_CHECK_LAUNCH();
-  const DMat &A = h.levels[0].A;
-  const int L = A.lanes;
-  int blocks = std::min(num_sms() * 8, (int)ceil_div(n, kApplyThreads / L));
-  double *part = s.part.get() + 4 * 3 * 2048;
   unsigned *tk = s.tickets.get();
-#define CHRONOS_PCG_CASE(LL)                                                                \
-  case LL:                                                                                  \
-    k_pcg_spmv<LL><<<blocks, kApplyThreads, 0, st>>>(n, A.rp, A.ci, A.v64, s.p.get(),       \
-                                                    s.res.get(), s.axp.get(), part, tk + 1, sc); \
-    break;
-  switch (L) {
-    CHRONOS_PCG_CASE(2)
-    CHRONOS_PCG_CASE(4)
-    CHRONOS_PCG_CASE(8)
-    CHRONOS_PCG_CASE(16)
-    CHRONOS_PCG_CASE(32)
-    default: throw Error(CHRONOS_EINVAL, "bad lane count");
-  }
-#undef CHRONOS_PCG_CASE
-  CHRONOS_CHECK_LAUNCH();
+  launch_pcg_spmv(st, h.levels[0].A, s.p.get(), s.res.get(), s.axp.get(),
+                  s.part.get() + 4 * 3 * 2048, tk + 1, sc);
   k_pcg_xr_update<<<nb, 256, 0, st>>>(n, s.x.get(), s.res.get(), s.p.get(), s.axp.get(),
                                        s.part.get() + 8 * 3 * 2048, tk + 2, sc,
                                        s.resvec.get(), handle, use_cond);
@@ -746,9 +1034,8 @@ void Hier::pcg_solve(const double *b, double *x, int itmax, double tol, int *ite
   CHRONOS_CUDA(cudaEventRecord(e0, st));
   // res = b - A x0, ||b||, ||res|| (PCG_CJ.m:11-30)
   CHRONOS_CUDA(cudaMemcpyAsync(s.x.get(), x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  const DMat &A = levels[0].A;
-  csr_apply<double, double, double, double, MODE_RESID, false>(st, A.lanes, n, A.rp, A.ci, A.v64,
-                                                               s.x.get(), b, s.res.get(), 1.0);
+  op_apply<double, double, double, double, MODE_RESID, false>(st, levels[0].A, s.x.get(), b,
+                                                              s.res.get(), 1.0);
   const int nb = reduce_blocks(n);
   double *part = s.part.get();
   k_dot_store<<<nb, 256, 0, st>>>(n, b, b, part, s.tickets.get() + 3, s.sc.get() + SC_BNORM);
@@ -814,6 +1101,113 @@ void Hier::pcg_solve(const double *b, double *x, int itmax, double tol, int *ite
   if (sc_h[SC_BREAKDOWN] != 0.0)
     throw Error(CHRONOS_EBREAKDOWN, "PCG breakdown: p'Ap <= 0 or NaN at iteration " +
                                         std::to_string(it));
+}
+
+// ---------------------------------------------------------------------------
+// Profiling: algorithmic bytes and CUDA-event timings of the hot kernels
+// ---------------------------------------------------------------------------
+
+// Compulsory traffic of one CSR apply of M (values s bytes, int32 indices):
+// nnz*(s+4) + (rows+1)*4 + x (ncols*sx) + y (rows*sy) + extra row vectors.
+static double apply_bytes(const DMat &M, double s, double sx, double sy, double extra_per_row) {
+  // block form: 9 values + one block-column index per 3x3 block (true blocks:
+  // the chunk padding is not algorithmic traffic)
+  const double mat = M.nb > 0 ? (double)M.nnzb * (9.0 * s + 4.0) + (M.nchunk + 1.0) * 8.0
+                              : (double)M.nnz * (s + 4.0) + (M.nrows + 1.0) * 4.0;
+  return mat + M.ncols * sx + M.nrows * (sy + extra_per_row);
+}
+
+static double vcycle_bytes_level(const Hier &h, int l, double s, double sb, double sout, bool top) {
+  const Level &L = h.levels[l];
+  const int n = L.n;
+  if (L.coarsest) return (double)n * n * 8.0 + n * (sb + sout);
+  double b = 0.0;
+  b += apply_bytes(L.G, s, sb, s, 0.0);                     // t = G b
+  b += apply_bytes(L.Gt, s, s, s, 0.0);                     // x = w G' t
+  for (int k = 1; k < h.prm.nupre; ++k)
+    b += apply_bytes(L.A, s, s, s, sb) + apply_bytes(L.G, s, s, s, 0.0) +
+         apply_bytes(L.Gt, s, s, s, s);
+  b += apply_bytes(L.A, s, s, s, sb);                       // r = b - A x
+  b += apply_bytes(L.Pt, s, s, s, 0.0);                     // b_c = P' r
+  b += vcycle_bytes_level(h, l + 1, s, s, s, false);
+  b += apply_bytes(L.P, s, s, s, s);                        // x = x + P x_c
+  for (int k = 0; k < h.prm.nupost; ++k) {
+    const bool last = k + 1 == h.prm.nupost;
+    b += apply_bytes(L.A, s, s, s, sb);                     // r = b - A x
+    b += apply_bytes(L.G, s, s, s, 0.0);                    // t = G r
+    b += apply_bytes(L.Gt, s, s, last ? sout : s, s + (top && last ? 8.0 : 0.0));
+  }
+  return b;
+}
+
+static int vcycle_kernels(const Hier &h) {
+  int k = 0;
+  for (const auto &L : h.levels) {
+    if (L.coarsest) { k += 1; break; }
+    k += 2 + 3 * (h.prm.nupre - 1) + 2 + 1 + 3 * h.prm.nupost + (h.prm.nupost == 0 ? 1 : 0);
+  }
+  if (h.levels[0].coarsest) k += 1;                         // the separate dot
+  return k;
+}
+
+void Hier::profile(int reps, chronos_profile *out) {
+  reps = std::max(reps, 1);
+  const int n = levels[0].n;
+  const bool fp32 = precision == CHRONOS_FP32;
+  const double s = fp32 ? 4.0 : 8.0;
+  ensure_pcg_state(*this, 16);
+  PcgState &ps = pcg;
+  DBuf<double> b(n), x(n), w(n);
+  std::vector<double> hb(n);
+  for (int i = 0; i < n; ++i) hb[i] = std::sin(0.37 * i + 1.0);
+  b.upload(hb, st);
+  w.upload(hb, st);
+  cudaEvent_t e0, e1;
+  CHRONOS_CUDA(cudaEventCreate(&e0));
+  CHRONOS_CUDA(cudaEventCreate(&e1));
+  auto time_it = [&](const std::function<void()> &f) {
+    f();
+    CHRONOS_CUDA(cudaEventRecord(e0, st));
+    for (int r = 0; r < reps; ++r) f();
+    CHRONOS_CUDA(cudaEventRecord(e1, st));
+    CHRONOS_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    return (double)ms / reps;
+  };
+  out->vcycle_ms = time_it([&] { vcycle(b.get(), x.get(), w.get(), ps.sc.get() + SC_PRES_AXP); });
+  out->vcycle_bytes = vcycle_bytes_level(*this, 0, s, 8.0, 8.0, true);
+  const Level &L0 = levels[0];
+  const DMat &A = L0.A;
+  if (!L0.coarsest) {
+    out->top_apply_ms = time_it([&] {
+      if (fp32)
+        op_apply<float, float, double, float, MODE_RESID, false>(st, A, L0.x32.get(), b.get(),
+                                                                L0.r32.get(), 1.0f);
+      else
+        op_apply<double, double, double, double, MODE_RESID, false>(st, A, L0.x64.get(), b.get(),
+                                                                   L0.r64.get(), 1.0);
+    });
+    out->top_apply_bytes = apply_bytes(A, s, s, s, 8.0);
+  } else {
+    out->top_apply_ms = 0.0;
+    out->top_apply_bytes = 0.0;
+  }
+  // outer FP64 SpMV with its two dots, as captured in the PCG iteration
+  double *part = ps.part.get() + 4 * 3 * 2048;
+  CHRONOS_CUDA(cudaMemcpyAsync(ps.p.get(), b.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  CHRONOS_CUDA(cudaMemcpyAsync(ps.res.get(), b.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  out->outer_spmv_ms = time_it([&] {
+    launch_pcg_spmv(st, A, ps.p.get(), ps.res.get(), ps.axp.get(), part, ps.tickets.get() + 1,
+                    ps.sc.get());
+  });
+  out->outer_spmv_bytes = apply_bytes(A, 8.0, 8.0, 8.0, 16.0);
+  out->iteration_bytes = out->vcycle_bytes + out->outer_spmv_bytes + 3.0 * n * 8 + 6.0 * n * 8;
+  out->kernels_per_iteration = vcycle_kernels(*this) + 3;
+  out->kernels_per_solve = 4;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
 }
 
 }  // namespace chronos

@@ -76,6 +76,8 @@ struct Hier {
                  std::vector<double> *resvec, double *seconds);
   // y = A x with the level-0 FP64 operator.
   void apply_A(const double *x, double *y);
+  // timings and algorithmic bytes of the hot kernels
+  void profile(int reps, chronos_profile *out);
 };
 
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A,

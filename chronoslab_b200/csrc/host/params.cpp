@@ -96,6 +96,8 @@ void params_default(chronos_params *p) {
   p->precision = CHRONOS_FP32;
   p->use_graph = 1;
   p->seed = 5489;
+  p->fsai_fabs = 0;
+  p->use_bsr = 1;
 }
 
 void params_read(const char *fnames_path, chronos_params *p) {

@@ -19,6 +19,17 @@ struct DMat {
   DBuf<double> v64;
   DBuf<float> v32;
   int lanes = 8;            // SpMV lanes per row (autotuned)
+  // Optional sliced 3x3 block form of the same matrix (chunks of 32 block
+  // rows, slot-major, plane-major values), used when every row triple shares
+  // a pattern of whole aligned 3x3 blocks.
+  int nb = 0;               // block rows (0: no block form)
+  int sell_T = 1;           // threads per block row (1, 2, 4; autotuned)
+  int nchunk = 0;
+  int64_t nnzb = 0;         // true blocks
+  int64_t nslots = 0;       // stored slots (blocks + padding)
+  DBuf<int> choff, chw, sci;
+  DBuf<double> bv64;
+  DBuf<float> bv32;
 };
 
 // ---- FSAI numeric (setup_kernels.cu) ------------------------------------------

@@ -83,48 +83,152 @@ struct StoreScalar {
   __device__ void operator()(const double *t) const { *dst = t[0]; }
 };
 
+template <typename VT, int MODE, typename ZT>
+__device__ __forceinline__ VT apply_epilogue(VT sum, VT alpha, const ZT *z, int row) {
+  if (MODE == MODE_PLAIN) return sum;
+  if (MODE == MODE_SCALE) return alpha * sum;
+  if (MODE == MODE_RESID) return (VT)z[row] - sum;
+  return (VT)z[row] + alpha * sum;
+}
+
 template <typename VT, typename XT, typename ZT, typename YT, int L, int MODE, bool DOT>
 __global__ void __launch_bounds__(kApplyThreads)
 k_csr_apply(int n, const int *__restrict__ rp, const int *__restrict__ ci,
             const VT *__restrict__ v, const XT *__restrict__ x, const ZT *z, YT *y, VT alpha,
             const double *__restrict__ dw, double *part, unsigned *ticket, double *dot_out) {
-  constexpr int R = 32 / L;                       // rows per warp step
+  // Each lane group holds two rows in flight (rows base+g and base+R+g) so
+  // short rows, whose cost is the dependent chain row pointer -> column ->
+  // x gather, overlap two chains per thread.
+  constexpr int R = 32 / L;                       // groups per warp
   const int lane = threadIdx.x & 31;
   const int g = lane / L, gl = lane & (L - 1);
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double dacc = 0.0;
-  for (int base = warp * R; base < n; base += nwarps * R) {
-    const int row = base + g;
-    VT sum = VT(0);
-    if (row < n) {
-      const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
-      int k = s + gl;
-      // two independent accumulators keep more loads in flight
-      VT s2 = VT(0);
-      for (; k + L < e; k += 2 * L) {
-        sum += __ldg(v + k) * (VT)__ldg(x + __ldg(ci + k));
-        s2 += __ldg(v + k + L) * (VT)__ldg(x + __ldg(ci + k + L));
-      }
-      if (k < e) sum += __ldg(v + k) * (VT)__ldg(x + __ldg(ci + k));
-      sum += s2;
+  for (int base = warp * 2 * R; base < n; base += nwarps * 2 * R) {
+    const int r0 = base + g, r1 = base + R + g;
+    int k0 = 0, e0 = 0, k1 = 0, e1 = 0;
+    if (r0 < n) { k0 = __ldg(rp + r0) + gl; e0 = __ldg(rp + r0 + 1); }
+    if (r1 < n) { k1 = __ldg(rp + r1) + gl; e1 = __ldg(rp + r1 + 1); }
+    VT a0 = VT(0), a1 = VT(0);
+    while (k0 < e0 || k1 < e1) {
+      if (k0 < e0) { a0 += __ldg(v + k0) * (VT)__ldg(x + __ldg(ci + k0)); k0 += L; }
+      if (k1 < e1) { a1 += __ldg(v + k1) * (VT)__ldg(x + __ldg(ci + k1)); k1 += L; }
     }
-    sum = group_sum<L>(sum);
-    if (row < n && gl == 0) {
-      VT r;
-      if (MODE == MODE_PLAIN) r = sum;
-      else if (MODE == MODE_SCALE) r = alpha * sum;
-      else if (MODE == MODE_RESID) r = (VT)z[row] - sum;
-      else r = (VT)z[row] + alpha * sum;
-      const YT out = (YT)r;
-      y[row] = out;
-      if (DOT) dacc += (double)out * dw[row];
+    a0 = group_sum<L>(a0);
+    a1 = group_sum<L>(a1);
+    if (gl == 0) {
+      if (r0 < n) {
+        const YT out = (YT)apply_epilogue<VT, MODE>(a0, alpha, z, r0);
+        y[r0] = out;
+        if (DOT) dacc += (double)out * dw[r0];
+      }
+      if (r1 < n) {
+        const YT out = (YT)apply_epilogue<VT, MODE>(a1, alpha, z, r1);
+        y[r1] = out;
+        if (DOT) dacc += (double)out * dw[r1];
+      }
     }
   }
   if (DOT) {
     double vals[1] = {dacc};
     grid_reduce<1>(vals, part, ticket, StoreScalar{dot_out});
   }
+}
+
+// Sliced 3x3 block apply (SELL-32 over 3x3 blocks) for operators assembled
+// from 3x3 node blocks (3 DOF per node).  Block rows are grouped in chunks of
+// 32; chunk c is padded to its longest block row w_c and stored slot-major:
+// slot j of the chunk's 32 rows is contiguous, so thread `lane` of the warp
+// owning the chunk reads block (row 32c+lane, slot j) with every load of the
+// warp coalesced.  Values are plane-major (V[e * nslots + k], e = 3*r + c):
+// nine coalesced 4- or 8-byte loads per block, one 4-byte column index per
+// nine values (0.44 index bytes per entry), no cross-lane reduction; padding
+// slots hold zeros and column 0.  The three row results go through the same
+// fused epilogues as the CSR kernel.
+// T threads share a block row (T = 1, 2, 4): a chunk holds C = 32/T block
+// rows and slot j of row l sits at off_c + (j/T)*32 + (j%T)*C + l, so lane
+// p*C + l walks slots j = p, p+T, ... with the same coalesced warp loads, and
+// the T partial sums meet through warp shuffles.  chw holds w_c / T.
+template <int T, typename VT>
+__device__ __forceinline__ VT slot_sum(VT v) {
+  constexpr int C = 32 / T;
+#pragma unroll
+  for (int o = C; o < 32; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <typename VT, typename XT, typename ZT, typename YT, int T, int MODE, bool DOT>
+__global__ void __launch_bounds__(kApplyThreads)
+k_sell3_apply(int nb, int nchunk, const int *__restrict__ choff, const int *__restrict__ chw,
+              const int *__restrict__ sci, const VT *__restrict__ V, int64_t nslots,
+              const XT *__restrict__ x, const ZT *z, YT *y, VT alpha,
+              const double *__restrict__ dw, double *part, unsigned *ticket, double *dot_out) {
+  constexpr int C = 32 / T;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double dacc = 0.0;
+  for (int c = warp; c < nchunk; c += nwarps) {
+    const int off = __ldg(choff + c) + lane, w = __ldg(chw + c);
+    VT s0 = VT(0), s1 = VT(0), s2 = VT(0);
+#pragma unroll 2
+    for (int j = 0; j < w; ++j) {
+      const int k = off + 32 * j;
+      const int col = 3 * __ldg(sci + k);
+      const VT xa = (VT)__ldg(x + col), xb = (VT)__ldg(x + col + 1), xc = (VT)__ldg(x + col + 2);
+      s0 += __ldg(V + k) * xa + __ldg(V + nslots + k) * xb + __ldg(V + 2 * nslots + k) * xc;
+      s1 += __ldg(V + 3 * nslots + k) * xa + __ldg(V + 4 * nslots + k) * xb +
+            __ldg(V + 5 * nslots + k) * xc;
+      s2 += __ldg(V + 6 * nslots + k) * xa + __ldg(V + 7 * nslots + k) * xb +
+            __ldg(V + 8 * nslots + k) * xc;
+    }
+    if (T > 1) {
+      s0 = slot_sum<T>(s0);
+      s1 = slot_sum<T>(s1);
+      s2 = slot_sum<T>(s2);
+    }
+    const int br = C * c + (lane & (C - 1));
+    if (lane < C && br < nb) {
+      const VT s[3] = {s0, s1, s2};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const int row = 3 * br + r;
+        const YT out = (YT)apply_epilogue<VT, MODE>(s[r], alpha, z, row);
+        y[row] = out;
+        if (DOT) dacc += (double)out * dw[row];
+      }
+    }
+  }
+  if (DOT) {
+    double vals[1] = {dacc};
+    grid_reduce<1>(vals, part, ticket, StoreScalar{dot_out});
+  }
+}
+
+template <typename VT, typename XT, typename ZT, typename YT, int MODE, bool DOT>
+void sell3_apply(cudaStream_t st, int T, int nb, int nchunk, const int *choff, const int *chw,
+                 const int *sci, const VT *V, int64_t nslots, const XT *x, const ZT *z, YT *y,
+                 VT alpha, const double *dw = nullptr, double *part = nullptr,
+                 unsigned *ticket = nullptr, double *dot_out = nullptr) {
+  if (nb <= 0) return;
+  int blocks = (int)ceil_div(nchunk, kApplyThreads / 32);
+  const int cap = num_sms() * 8;
+  if (blocks > cap) blocks = cap;
+#define CHRONOS_SELL_CASE(TT)                                                                  \
+  case TT:                                                                                     \
+    k_sell3_apply<VT, XT, ZT, YT, TT, MODE, DOT><<<blocks, kApplyThreads, 0, st>>>(            \
+        nb, nchunk, choff, chw, sci, V, nslots, x, z, y, alpha, dw, part, ticket, dot_out);    \
+    break;
+  switch (T) {
+    CHRONOS_SELL_CASE(1)
+    CHRONOS_SELL_CASE(2)
+    CHRONOS_SELL_CASE(4)
+    default:
+      throw Error(CHRONOS_EINVAL, "sell3_apply: threads per block row must be 1, 2 or 4");
+  }
+#undef CHRONOS_SELL_CASE
+  CHRONOS_CHECK_LAUNCH();
 }
 
 // Launch helper: persistent grid of blocks_per_sm * #SMs blocks (or fewer
@@ -135,7 +239,7 @@ void csr_apply(cudaStream_t st, int L, int n, const int *rp, const int *ci, cons
                double *part = nullptr, unsigned *ticket = nullptr, double *dot_out = nullptr,
                int max_blocks = 0) {
   if (n <= 0) return;
-  const int rows_per_block = kApplyThreads / L;
+  const int rows_per_block = 2 * kApplyThreads / L;
   int blocks = (int)ceil_div(n, rows_per_block);
   const int cap = max_blocks > 0 ? max_blocks : num_sms() * 8;
   if (blocks > cap) blocks = cap;
@@ -145,13 +249,14 @@ void csr_apply(cudaStream_t st, int L, int n, const int *rp, const int *ci, cons
         n, rp, ci, v, x, z, y, alpha, dw, part, ticket, dot_out);                         \
     break;
   switch (L) {
+    CHRONOS_APPLY_CASE(1)
     CHRONOS_APPLY_CASE(2)
     CHRONOS_APPLY_CASE(4)
     CHRONOS_APPLY_CASE(8)
     CHRONOS_APPLY_CASE(16)
     CHRONOS_APPLY_CASE(32)
     default:
-      throw Error(CHRONOS_EINVAL, "csr_apply: lanes per row must be 2,4,8,16 or 32");
+      throw Error(CHRONOS_EINVAL, "csr_apply: lanes per row must be 1,2,4,8,16 or 32");
   }
 #undef CHRONOS_APPLY_CASE
   CHRONOS_CHECK_LAUNCH();

@@ -96,6 +96,8 @@ typedef struct chronos_params {
   int fsai_fabs;                  /* 0 (default): FSAI candidate ranking and exit test compare
                                      magnitudes as the reference's g++ build does, through C's
                                      int abs (truncation toward zero); 1: through fabs */
+  int use_bsr;                    /* 1 (default): apply the level-1 operator in 3x3 block form
+                                     when its pattern is made of whole aligned 3x3 blocks */
 } chronos_params;
 
 /* Reference regression-test parameters (Tests/parm_*): DOM 0.01, BAMG/NONE,
@@ -194,6 +196,7 @@ typedef struct chronos_level_info {
   int nc;               /* columns of P (0 on the coarsest level) */
   double omega, lambda; /* smoother damping and lambda_max(G A G') */
   int threads_per_row;  /* SpMV lanes per row chosen by the autotuner for A */
+  int block_rows;       /* > 0: A is applied in 3x3 block form with this many block rows */
 } chronos_level_info;
 
 /* Builds the hierarchy of A (0-based CSR, FP64, host memory) with the test
@@ -215,6 +218,20 @@ int chronos_hier_export(const chronos_hier *h, int level, char which, int *nrows
 /* Setup timings in seconds: [fsai_pattern, fsai_numeric, omega, coarsen, prolong,
  * galerkin, coarse_factor, total]. */
 int chronos_hier_setup_times(const chronos_hier *h, double *t8);
+
+/* Kernel timings of a built hierarchy (CUDA events on its stream, `reps`
+ * launches each after one warm-up) and the algorithmic bytes each moves:
+ * values + column indices + row pointers once, every vector read or written
+ * once (the compulsory traffic of a CSR apply). */
+typedef struct chronos_profile {
+  double vcycle_ms, vcycle_bytes;          /* one V-cycle, FP64 in/out */
+  double top_apply_ms, top_apply_bytes;    /* level-1 residual b - A x in the stored precision */
+  double outer_spmv_ms, outer_spmv_bytes;  /* the PCG's FP64 A p with its two dot products */
+  double iteration_bytes;                  /* one PCG_CJ iteration in total */
+  int kernels_per_iteration;               /* kernel launches of one PCG iteration */
+  int kernels_per_solve;                   /* launches outside the loop, per solve */
+} chronos_profile;
+int chronos_hier_profile(chronos_hier *h, int reps, chronos_profile *out);
 
 /* computeAMG.m:5-10: diagonal entries equal to 1 become lambda_max(A)/10
  * (lambda_max by a GPU Lanczos run).  Updates val_h in place. */

@@ -86,6 +86,27 @@ def test_pcg_fp32_hierarchy(lib, case, request):
         assert rel(x32, xs) <= 1e-6
 
 
+@pytest.mark.parametrize("prec,tol", [(cb.CHRONOS_FP64, 1e-12), (cb.CHRONOS_FP32, 2e-5)])
+def test_block_form_matches_csr(lib, elast, prec, tol):
+    """The 3x3 block form of the level-1 operator gives the CSR results."""
+    A, TV, b = elast
+    with cb.Hierarchy(A, TV, cb.params(precision=prec, use_bsr=1)) as hb, \
+            cb.Hierarchy(A, TV, cb.params(precision=prec, use_bsr=0)) as hc:
+        assert hb.level_info(0)["block_rows"] == A.shape[0] // 3
+        assert hc.level_info(0)["block_rows"] == 0
+        assert rel(hb.vcycle(b), hc.vcycle(b)) <= tol
+        xb, itb, _, fb, _ = hb.pcg(b, itmax=500, tol=1e-8)
+        xc, itc, _, fc, _ = hc.pcg(b, itmax=500, tol=1e-8)
+        assert fb == 0 and fc == 0 and abs(itb - itc) <= 1
+        assert np.linalg.norm(b - A @ xb) / np.linalg.norm(b) <= 1e-8
+
+
+def test_block_form_not_used_without_blocks(lib, poisson):
+    A, _, b = poisson
+    with cb.Hierarchy(A, None, cb.params(ntv=1)) as h:
+        assert h.level_info(0)["block_rows"] == 0
+
+
 def test_graph_loop_matches_host_loop(lib, elast):
     A, TV, b = elast
     out = []
@@ -142,7 +163,16 @@ def test_setup_components_match_golden(lib, cubo, cubo_ref):
         P = h.export(0, "P")
         D = (P - cubo_ref["P"]).tocsr()
         bad_rows = np.unique(D.nonzero()[0][np.abs(D.data) > 1e-10])
-        assert bad_rows.size <= 0.001 * P.shape[0]
+        # The hierarchy orthonormalises TV twice (cpt_aspAMG.m:46 and tspace
+        # NONE), our Householder QR rounding differs from LAPACK's, and the
+        # Cubo rigid-body test space puts many BAMG rows on a knife edge (row
+        # norm at maxrownrm, maxVol ties): a few rows pick another, equally
+        # exact, interpolation set.  Same inputs: test_host's BAMG check.
+        assert bad_rows.size <= 0.01 * P.shape[0]
+        TVc = cubo["TV0"][np.flatnonzero(cubo_ref["fcnode"] > 0)]
+        ok = cubo_ref["c_mark"] == 0
+        err = np.linalg.norm(P @ TVc - cubo["TV0"], axis=1)
+        assert np.all(err[ok] <= 1e-8 * np.linalg.norm(cubo["TV0"], axis=1)[ok] + 1e-14)
         # the coarse operator is the Galerkin product of the exported P
         Ac = h.export(1, "A")
         ref = (P.T @ (cubo["Af"] @ P)).tocsr()
