@@ -86,6 +86,7 @@ SIGNATURES = {
     "chronos_fsai_compute": [_i, _i, _i, _d, _d, _i, _i, _i64, _pi64, _pi, _pd, _pi64, _pi64,
                              _pi, _pd, _pi],
     "chronos_fsai_numeric": [_i, _pi64, _pi, _pd, _pi64, _pi, _pd, _pi],
+    "chronos_fsai_numeric_noalloc": [_i, _vp, _vp, _vp, _vp, _vp, _vp, _pi, _vp],
     "chronos_galerkin_compute": [_i, _i, _pi, _pi, _pd, _pi, _pi, _pd, _pi64, _pp],
     "chronos_galerkin_fetch": [_vp, _pi, _pi, _pd],
     "chronos_galerkin_free": [_vp],

@@ -14,6 +14,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <mutex>
 #include <numeric>
 
 #include "internal.h"
@@ -597,4 +598,105 @@ void adjoint_scatter(int n, const int *rp, const int *ci, const double *lambda, 
   CHRONOS_CHECK_LAUNCH();
 }
 
+// =============================================================================
+// FSAI numeric phase without allocation (chronos_fsai_numeric_noalloc)
+// =============================================================================
+//
+// Same kernels as fsai_numeric_device, but the scratch they need -- the three
+// row-bucket lists and the flag word -- lives in one file-scope device array
+// instead of cudaMalloc'd buffers.  The array is a fixed 12 MiB + 256 B per
+// device that loads the library, held until the process exits.  Every call
+// shares it: calls that overlap on the GPU (two streams, two host threads)
+// race on it and must be serialised by the caller.
+
+constexpr int kNoAllocMaxRows = 1 << 20;
+constexpr int kNoAllocHeader = 64;            // ints: [0..2] bucket counts, [3] flags
+static __device__ __align__(256) int g_fsai_noalloc_scratch[kNoAllocHeader + 3 * kNoAllocMaxRows];
+
+// In host code g_fsai_noalloc_scratch names a host-side stand-in, not a device
+// address: the device address is looked up once per device with
+// cudaGetSymbolAddress (with that device current) and cached here.
+static int *g_noalloc_addr[64] = {nullptr};
+static std::mutex g_noalloc_mu;
+
+static int *noalloc_scratch_address() {
+  int dev = 0;
+  CHRONOS_CUDA(cudaGetDevice(&dev));
+  CHRONOS_REQUIRE(dev >= 0 && dev < 64, CHRONOS_EINVAL, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    CHRONOS_CUDA(cudaGetSymbolAddress(&p, g_fsai_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<int *>(p);
+  }
+  return g_noalloc_addr[dev];
+}
+
+// Sorts rows into the 16 / 32 / 64 buckets of fsai_numeric_device; a row
+// longer than 64 strictly-lower entries sets flag bit 1.
+__global__ void k_fsai_bucket_rows(int n, const int *__restrict__ grp, int *scratch) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int m = grp[i + 1] - grp[i] - 1;
+  int b;
+  if (m <= 16) b = 0;
+  else if (m <= 32) b = 1;
+  else if (m <= 64) b = 2;
+  else { atomicOr(scratch + 3, 2); return; }
+  const int pos = atomicAdd(scratch + b, 1);
+  scratch[kNoAllocHeader + b * kNoAllocMaxRows + pos] = i;
+}
+
+int fsai_numeric_noalloc(int n, const int *arp, const int *aci, const double *av, const int *grp,
+                         const int *gci, double *gval, cudaStream_t st) {
+  CHRONOS_REQUIRE(n > 0 && n <= kNoAllocMaxRows, CHRONOS_EINVAL,
+                  "chronos_fsai_numeric_noalloc: n must be in [1, 1048576] (its static scratch "
+                  "holds 1048576 rows)");
+  int *scr = noalloc_scratch_address();
+  // the previous call's contents remain: clear the counts and the flag word
+  CHRONOS_CUDA(cudaMemsetAsync(scr, 0, kNoAllocHeader * sizeof(int), st));
+  k_fsai_bucket_rows<<<ceil_div(n, 256), 256, 0, st>>>(n, grp, scr);
+  CHRONOS_CHECK_LAUNCH();
+  int hdr[4] = {0, 0, 0, 0};
+  CHRONOS_CUDA(cudaMemcpyAsync(hdr, scr, sizeof(hdr), cudaMemcpyDeviceToHost, st));
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  CHRONOS_REQUIRE(!(hdr[3] & 2), CHRONOS_ENOTSUP,
+                  "FSAI local system larger than 64 (nstep*step_size)");
+  auto run = [&](auto kern, int cnt, int bucket, int mmax, int warps) {
+    if (cnt == 0) return;
+    const size_t sm = (size_t)warps * (mmax * mmax + 3 * mmax) * sizeof(double);
+    CHRONOS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<ceil_div(cnt, warps), warps * 32, sm, st>>>(
+        cnt, scr + kNoAllocHeader + bucket * kNoAllocMaxRows, arp, aci, av, grp, gci, gval, scr + 3);
+    CHRONOS_CHECK_LAUNCH();
+  };
+  run(k_fsai_numeric<16>, hdr[0], 0, 16, 8);
+  run(k_fsai_numeric<32>, hdr[1], 1, 32, 4);
+  run(k_fsai_numeric<64>, hdr[2], 2, 64, 2);
+  int fl = 0;
+  CHRONOS_CUDA(cudaMemcpyAsync(&fl, scr + 3, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  return fl;
+}
+
 }  // namespace chronos
+
+extern "C" int chronos_fsai_numeric_noalloc(int n, const int *iat_A_d, const int *ja_A_d,
+                                            const double *val_A_d, const int *iat_G_d,
+                                            const int *ja_G_d, double *val_G_d, int *is_posdef,
+                                            void *stream) {
+  try {
+    CHRONOS_REQUIRE(iat_A_d && ja_A_d && val_A_d && iat_G_d && ja_G_d && val_G_d && is_posdef,
+                    CHRONOS_EINVAL, "null argument");
+    const int fl = chronos::fsai_numeric_noalloc(n, iat_A_d, ja_A_d, val_A_d, iat_G_d, ja_G_d,
+                                                 val_G_d, static_cast<cudaStream_t>(stream));
+    *is_posdef = (fl & 1) ? 0 : 1;
+    return CHRONOS_OK;
+  } catch (const chronos::Error &e) {
+    chronos::set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception &e) {
+    chronos::set_last_error(e.what());
+    return CHRONOS_EINVAL;
+  }
+}

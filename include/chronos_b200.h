@@ -132,6 +132,28 @@ int chronos_fsai_numeric(int n, const int64_t *iat_A_h, const int *ja_A_h, const
                          const int64_t *iat_G_h, const int *ja_G_h, double *val_G_h,
                          int *is_posdef);
 
+/* FSAI numeric phase that allocates nothing.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot let a library
+ * call cudaMalloc or cudaFree: hosts that own all device memory through their
+ * own pool (a framework's caching allocator, a MATLAB gpuArray host, an
+ * embedded or real-time host that reserves memory up front) and callers whose
+ * other streams must not be stalled by the device-wide synchronisation that
+ * cudaFree implies.  Same result as chronos_fsai_numeric, but every pointer is
+ * device memory the caller owns: A and the pattern of G as 0-based CSR with
+ * int32 row pointers and columns (G rows: strictly-lower columns ascending,
+ * then the diagonal), val_G_d receives the values; is_posdef is host memory.
+ * Work is queued on `stream` (a cudaStream_t; NULL for the legacy default
+ * stream) and the call returns after it completes.
+ * Scratch: a fixed 12 MiB + 256 B array in device memory, part of the
+ * library's module, held on every GPU that loads the library until the
+ * process exits; n is limited to 1048576 rows (larger n returns
+ * CHRONOS_EINVAL).  The first call on a device looks up the array's device
+ * address for that device.  All calls share the array: calls that overlap on
+ * the GPU race on it and must be serialised by the caller. */
+int chronos_fsai_numeric_noalloc(int n, const int *iat_A_d, const int *ja_A_d,
+                                 const double *val_A_d, const int *iat_G_d, const int *ja_G_d,
+                                 double *val_G_d, int *is_posdef, void *stream);
+
 /* ---- host-side setup pieces (no GPU) ------------------------------------ */
 /* Result handle for a CSR produced by the library (0-based, FP64). */
 typedef struct chronos_csr chronos_csr;
