@@ -541,17 +541,15 @@ int chronos_pcg_block(chronos_hier *hh, int nrhs, const double *B_h, double *X_h
                     "bad argument");
     Hier &h = *hh->h;
     const int n = h.levels[0].n;
-    DBuf<double> b(n), x(n);
     double total = 0.0;
-    for (int c = 0; c < nrhs; ++c) {
-      b.upload(B_h + (size_t)c * n, n, h.st);
-      x.upload(X_h + (size_t)c * n, n, h.st);
+    // chunks of at most 16 columns, each one SpMM block solve
+    for (int c0 = 0; c0 < nrhs; c0 += 16) {
+      const int m = std::min(16, nrhs - c0);
       double sec = 0.0;
-      h.pcg_solve(b.get(), x.get(), itmax, tol, &iters_h[c], &flags_h[c], nullptr, &sec);
+      h.pcg_block(m, B_h + (size_t)c0 * n, X_h + (size_t)c0 * n, itmax, tol, iters_h + c0,
+                  flags_h + c0, &sec);
       total += sec;
-      x.download(X_h + (size_t)c * n, n, h.st);
     }
-    CHRONOS_CUDA(cudaStreamSynchronize(h.st));
     if (seconds) *seconds = total;
   });
 }

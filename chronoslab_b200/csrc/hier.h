@@ -59,6 +59,8 @@ struct PcgState {
   ~PcgState();
 };
 
+struct BlockState;   // block-of-right-hand-sides solve state (block.cu)
+
 struct Hier {
   chronos_params prm{};
   int precision = CHRONOS_FP32;
@@ -78,6 +80,10 @@ struct Hier {
   void apply_A(const double *x, double *y);
   // timings and algorithmic bytes of the hot kernels
   void profile(int reps, chronos_profile *out);
+  // nrhs <= 16 columns (column-major host blocks) solved together
+  void pcg_block(int nrhs, const double *B_h, double *X_h, int itmax, double tol, int *iters,
+                 int *flags, double *seconds);
+  std::shared_ptr<BlockState> block;
 };
 
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A,
