@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--itmax", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["c2", "c3", "c4"], default="c2",
+                    help="c2: elasticity (default, the headline); c3: diffusion 128^3 with a "
+                         "block of 16 right-hand sides; c4: 64 batched problems")
     ap.add_argument("--profile-solve", choices=["fp32", "fp64"], default=None,
                     help="for ncu --profile-from-start off: build one hierarchy, warm up, "
                          "then bracket exactly one solve with the profiler range and exit")
@@ -386,6 +389,80 @@ def run_product(args, world, rank, local):
     return 0
 
 
+def run_block_or_batch(args):
+    """C3 (block of 16 right-hand sides, SpMM V-cycles) or C4 (64 independent
+    problems of uneven sizes, queued together); FP32 hierarchy vs FP64."""
+    import numpy as np
+    import chronoslab_b200 as cb
+    from chronoslab_b200 import problems as PB
+    out = {"metric": METRIC, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 hierarchy / f64 outer",
+           "data": "synthetic (seeded)"}
+    res = {}
+    if args.workload == "c3":
+        ne = 128 if args.ne == 80 else args.ne
+        A, _ = PB.diffusion7(ne, sigma=2.0, corr_len=8.0, zaniso=0.01, seed=0)
+        B = PB.uniform_rhs(A.shape[0], seed=1, ncols=16)
+        ones = np.ones(A.shape[0])
+        for prec, name in ((cb.CHRONOS_FP32, "fp32"), (cb.CHRONOS_FP64, "fp64")):
+            with cb.Hierarchy(A, ones, cb.params(precision=prec, ntv=1)) as h:
+                for _ in range(args.warmup):
+                    h.pcg_block(B, itmax=args.itmax, tol=args.tol)
+                ts = []
+                for _ in range(args.steps):
+                    X, its, fl, sec = h.pcg_block(B, itmax=args.itmax, tol=args.tol)
+                    assert np.all(fl == 0)
+                    ts.append(sec * 1e3)
+                one = []
+                for _ in range(2):
+                    x, it, _, f, sec1 = h.pcg(B[:, 0], itmax=args.itmax, tol=args.tol)
+                    one.append(sec1 * 1e3)
+                relres = max(np.linalg.norm(B[:, j] - A @ X[:, j]) / np.linalg.norm(B[:, j])
+                             for j in range(16))
+                res[name] = {"ms": sum(ts) / len(ts), "iters": its.tolist(),
+                             "single_rhs_ms": min(one), "true_relres_max": relres,
+                             "levels": [h.level_info(l)["n"] for l in range(h.nlevels)]}
+        out["config"] = {"workload": f"log-normal diffusion {ne}^3 ({A.shape[0]} rows, {A.nnz} "
+                                     "nnz), block of 16 RHS, SpMM V-cycles, PCG_CJ to "
+                                     f"{args.tol} per column"}
+    else:
+        rng = np.random.default_rng(0)
+        edges = rng.integers(16, 65, 64)
+        As, bs = [], []
+        for p, e in enumerate(edges):
+            if p % 2 == 0:
+                A = PB.poisson7(int(e))
+            else:
+                A, _ = PB.diffusion7(int(e), sigma=2.0, corr_len=8.0, zaniso=0.01, seed=p)
+            As.append(A)
+            bs.append(PB.uniform_rhs(A.shape[0], seed=1000 + p))
+        for prec, name in ((cb.CHRONOS_FP32, "fp32"), (cb.CHRONOS_FP64, "fp64")):
+            t0 = time.perf_counter()
+            with cb.Batch(As, cb.params(precision=prec, ntv=1, nstep=15, step_size=4)) as Bt:
+                setup = time.perf_counter() - t0
+                for _ in range(args.warmup):
+                    Bt.solve(bs, itmax=args.itmax, tol=args.tol)
+                ts = []
+                for _ in range(args.steps):
+                    xs, its, fl, sec = Bt.solve(bs, itmax=args.itmax, tol=args.tol)
+                    assert np.all(fl == 0)
+                    ts.append(sec * 1e3)
+                res[name] = {"ms": sum(ts) / len(ts), "setup_s": setup,
+                             "iters_min_max": [int(its.min()), int(its.max())]}
+        out["config"] = {"workload": "64 independent problems (Poisson / log-normal diffusion, "
+                                     f"edge U[16,64]: {min(A.shape[0] for A in As)} to "
+                                     f"{max(A.shape[0] for A in As)} rows), FSAI 15 steps x 4, "
+                                     "batch solve, PCG_CJ to 1e-8 each"}
+    out["value"] = res["fp32"]["ms"]
+    out["ms_per_step"] = res["fp32"]["ms"]
+    out["fp64_ms"] = res["fp64"]["ms"]
+    out["speedup_fp32_vs_fp64"] = res["fp64"]["ms"] / res["fp32"]["ms"]
+    out["detail"] = res
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     world, rank, local = dist_env()
@@ -397,6 +474,8 @@ def main():
         return run_reference(args, world, rank)
     if args.profile_solve:
         return run_profile_solve(args)
+    if args.workload != "c2":
+        return run_block_or_batch(args)
     return run_product(args, world, rank, local)
 
 

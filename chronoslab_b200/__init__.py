@@ -22,7 +22,8 @@ from ._lib import (CHRONOS_FP32, CHRONOS_FP64, ChronosError, chronos_level_info,
                    check, last_error, load)
 
 __all__ = [
-    "CHRONOS_FP32", "CHRONOS_FP64", "ChronosError", "Hierarchy", "params", "readDefaultParams",
+    "CHRONOS_FP32", "CHRONOS_FP64", "ChronosError", "Hierarchy", "Batch", "params",
+    "readDefaultParams",
     "cpt_aspAMG", "AMG_Vcycle", "PCG_CJ", "SQMR", "SYM_aFSAI_compute", "afsai_cpp",
     "fsai_numeric", "fsai_pattern", "coarsen", "bamg", "galerkin", "dense_chol", "spmv",
     "diag_fix", "version",
@@ -398,6 +399,66 @@ class Hierarchy:
         check(self._lib.chronos_adjoint_grad(self._h, _pd(u), _pd(g), itmax, tol, _pd(lam),
                                              _pd(grad), C.byref(it)))
         return lam, grad[:A0["nnz_A"]], it.value
+
+
+class Batch:
+    """Independent problems of uneven sizes (chronos_batch): one hierarchy per
+    problem, all solves queued together (one conditional-graph launch each,
+    own stream, largest first)."""
+
+    def __init__(self, As, prm=None):
+        self._lib = load()
+        self.prm = prm or params(ntv=1)
+        mats = [_csr(A) for A in As]
+        self.ns = [m[0] for m in mats]
+        self._keep = mats
+        npb = len(mats)
+        n = np.array(self.ns, dtype=np.int32)
+        P = C.c_void_p * npb
+        iat = P(*[m[1].ctypes.data for m in mats])
+        ja = P(*[m[2].ctypes.data for m in mats])
+        val = P(*[m[3].ctypes.data for m in mats])
+        h = C.c_void_p()
+        check(self._lib.chronos_batch_setup(C.byref(self.prm), npb, _pi(n), iat, ja, val,
+                                            C.byref(h)))
+        self._h = h
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.chronos_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def nlevels(self, p):
+        nl, n0 = C.c_int(), C.c_int()
+        check(self._lib.chronos_batch_info(self._h, p, C.byref(nl), C.byref(n0)))
+        return nl.value
+
+    def solve(self, bs, itmax=1000, tol=1e-8):
+        """Returns (xs, iters, flags, seconds)."""
+        npb = len(self.ns)
+        bs = [np.ascontiguousarray(b, dtype=np.float64) for b in bs]
+        xs = [np.zeros(n) for n in self.ns]
+        P = C.c_void_p * npb
+        its = np.zeros(npb, np.int32)
+        fl = np.zeros(npb, np.int32)
+        sec = C.c_double()
+        check(self._lib.chronos_batch_solve(self._h, P(*[b.ctypes.data for b in bs]),
+                                            P(*[x.ctypes.data for x in xs]), itmax, tol, _pi(its),
+                                            _pi(fl), C.byref(sec)))
+        return xs, its, fl, sec.value
 
 
 def cpt_aspAMG(param, A, TV0=None):

@@ -104,7 +104,11 @@ SIGNATURES = {
     "chronos_pcg": [_vp, _pd, _pd, _i, _d, _pi, _pd, _pi, _pd],
     "chronos_pcg_dev": [_vp, _vp, _vp, _i, _d, _pi, _pd, _pi, _pd],
     "chronos_pcg_block": [_vp, _i, _pd, _pd, _i, _d, _pi, _pi, _pd],
-    "chronos_sqmr": [_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _pi, _pd, _pi],
+    "chronos_batch_setup": [C.POINTER(chronos_params), _i, _pi, _pp, _pp, _pp, _pp],
+    "chronos_batch_solve": [_vp, _pp, _pp, _i, _d, _pi, _pi, _pd],
+    "chronos_batch_info": [_vp, _i, _pi, _pi],
+    "chronos_batch_free": [_vp],
+    "chronos_sqmr":[_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _pi, _pd, _pi],
     "chronos_adjoint_grad": [_vp, _pd, _pd, _i, _d, _pd, _pd, _pi],
 }
 _RESTYPE = {"chronos_params_default": None, "chronos_version": C.c_char_p}

@@ -27,7 +27,7 @@ class AMGSolve(torch.autograd.Function):
         n = indptr.size - 1
         A = sp.csr_matrix((values.detach().cpu().numpy().astype(np.float64), indices, indptr),
                           shape=(n, n))
-        h = Hierarchy(A, None, prm)
+        h = Hierarchy(A, np.ones(n), prm)          # constant near-null vector
         u, it, rv, flag, _ = h.pcg(b.detach().cpu().numpy().astype(np.float64), itmax=itmax,
                                    tol=tol)
         if flag != 0:

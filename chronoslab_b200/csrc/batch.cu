@@ -1,0 +1,150 @@
+// Batch of independent SPD problems of uneven sizes: one hierarchy per
+// problem (each exactly what a single chronos_amg_setup builds), and a batch
+// solve that queues every problem's whole PCG_CJ -- one conditional-graph
+// launch each -- on its own stream with no host synchronisation in between,
+// largest problems first, so the small problems' short kernels overlap with
+// the large ones' on the GPU.
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "hier.h"
+
+namespace chronos {
+
+struct Batch {
+  std::vector<std::unique_ptr<Hier>> h;
+  std::vector<int> order;           // largest level-1 operator first
+};
+
+}  // namespace chronos
+
+using namespace chronos;
+
+struct chronos_batch {
+  Batch b;
+};
+
+template <typename F>
+static int batch_guard(F &&f) {
+  try {
+    f();
+    return CHRONOS_OK;
+  } catch (const Error &e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    set_last_error("host allocation failed");
+    return CHRONOS_ENOMEM;
+  } catch (const std::exception &e) {
+    set_last_error(e.what());
+    return CHRONOS_EINVAL;
+  }
+}
+
+extern "C" {
+
+int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
+                        const int *const *iat_h, const int *const *ja_h,
+                        const double *const *val_h, chronos_batch **out) {
+  return batch_guard([&] {
+    CHRONOS_REQUIRE(prm && n && iat_h && ja_h && val_h && out && nprob > 0, CHRONOS_EINVAL,
+                    "bad argument");
+    CHRONOS_REQUIRE(prm->use_graph, CHRONOS_EINVAL, "batched solves need use_graph = 1");
+    auto bt = std::make_unique<chronos_batch>();
+    for (int p = 0; p < nprob; ++p) {
+      CHRONOS_REQUIRE(n[p] > 0 && iat_h[p] && iat_h[p][0] == 0, CHRONOS_EINVAL,
+                      "problem " + std::to_string(p) + ": 0-based CSR expected");
+      HostCSR A;
+      A.nrows = A.ncols = n[p];
+      A.rp.assign(iat_h[p], iat_h[p] + n[p] + 1);
+      A.ci.assign(ja_h[p], ja_h[p] + A.rp[n[p]]);
+      A.v.assign(val_h[p], val_h[p] + A.rp[n[p]]);
+      // scalar problems: the constant vector as TV0 (as aspAMG_main.m:92-95 for
+      // a .mat without a test space), padded with random columns if ntv > 1
+      std::vector<double> ones(n[p], 1.0);
+      bt->b.h.push_back(build_hierarchy(*prm, A, 1, ones.data()));
+    }
+    bt->b.order.resize(nprob);
+    std::iota(bt->b.order.begin(), bt->b.order.end(), 0);
+    std::stable_sort(bt->b.order.begin(), bt->b.order.end(), [&](int a, int c) {
+      return bt->b.h[a]->levels[0].A.nnz > bt->b.h[c]->levels[0].A.nnz;
+    });
+    *out = bt.release();
+  });
+}
+
+int chronos_batch_solve(chronos_batch *bt, const double *const *b_h, double *const *x_h,
+                        int itmax, double tol, int *iters, int *flags, double *seconds) {
+  return batch_guard([&] {
+    CHRONOS_REQUIRE(bt && b_h && x_h && iters && flags, CHRONOS_EINVAL, "null argument");
+    Batch &B = bt->b;
+    const int np = (int)B.h.size();
+    std::vector<DBuf<double>> bd(np), xd(np);
+    std::vector<char> zero(np, 0);
+    for (int p = 0; p < np; ++p) {
+      Hier &h = *B.h[p];
+      const int n = h.levels[0].n;
+      double s = 0.0;
+      for (int i = 0; i < n; ++i) s += b_h[p][i] * b_h[p][i];
+      zero[p] = s == 0.0;
+      bd[p].upload(b_h[p], n, h.st);
+      xd[p].upload(x_h[p], n, h.st);
+      CHRONOS_CUDA(cudaStreamSynchronize(h.st));
+    }
+    cudaStream_t fork;
+    CHRONOS_CUDA(cudaStreamCreateWithFlags(&fork, cudaStreamNonBlocking));
+    cudaEvent_t start;
+    std::vector<cudaEvent_t> done(np);
+    CHRONOS_CUDA(cudaEventCreate(&start));
+    for (auto &e : done) CHRONOS_CUDA(cudaEventCreate(&e));
+    CHRONOS_CUDA(cudaEventRecord(start, fork));
+    for (int p : B.order) {
+      Hier &h = *B.h[p];
+      CHRONOS_CUDA(cudaStreamWaitEvent(h.st, start, 0));
+      if (!zero[p]) h.pcg_enqueue(bd[p].get(), xd[p].get(), itmax, tol);
+      CHRONOS_CUDA(cudaEventRecord(done[p], h.st));
+    }
+    float ms = 0.f;
+    for (int p = 0; p < np; ++p) {
+      CHRONOS_CUDA(cudaEventSynchronize(done[p]));
+      float t = 0.f;
+      CHRONOS_CUDA(cudaEventElapsedTime(&t, start, done[p]));
+      ms = std::max(ms, t);
+    }
+    for (int p = 0; p < np; ++p) {
+      Hier &h = *B.h[p];
+      const int n = h.levels[0].n;
+      if (zero[p]) {                       // PCG_CJ.m:12-16
+        std::fill(x_h[p], x_h[p] + n, 0.0);
+        iters[p] = 0;
+        flags[p] = 0;
+        continue;
+      }
+      xd[p].download(x_h[p], n, h.st);
+      CHRONOS_CUDA(cudaStreamSynchronize(h.st));
+      h.pcg_collect(tol, &iters[p], &flags[p]);
+    }
+    cudaEventDestroy(start);
+    for (auto &e : done) cudaEventDestroy(e);
+    cudaStreamDestroy(fork);
+    if (seconds) *seconds = ms * 1e-3;
+  });
+}
+
+int chronos_batch_info(const chronos_batch *bt, int p, int *nlev, int *n0) {
+  return batch_guard([&] {
+    CHRONOS_REQUIRE(bt && nlev && n0 && p >= 0 && p < (int)bt->b.h.size(), CHRONOS_EINVAL,
+                    "bad argument");
+    *nlev = (int)bt->b.h[p]->levels.size();
+    *n0 = bt->b.h[p]->levels[0].n;
+  });
+}
+
+int chronos_batch_free(chronos_batch *bt) {
+  return batch_guard([&] { delete bt; });
+}
+
+}  // extern "C"

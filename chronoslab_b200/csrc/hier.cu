@@ -37,6 +37,7 @@ static double now_s() {
 PcgState::~PcgState() {
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
+  if (sc_pinned) cudaFreeHost(sc_pinned);
 }
 
 Hier::~Hier() {
@@ -1101,6 +1102,44 @@ void Hier::pcg_solve(const double *b, double *x, int itmax, double tol, int *ite
   if (sc_h[SC_BREAKDOWN] != 0.0)
     throw Error(CHRONOS_EBREAKDOWN, "PCG breakdown: p'Ap <= 0 or NaN at iteration " +
                                         std::to_string(it));
+}
+
+// The whole solve queued on st with no host synchronisation: initial
+// residual, the conditional-graph loop, the copy of x and of the scalars to a
+// pinned host buffer.  b must not be zero (the caller checks ||b||: PCG_CJ.m
+// returns x = 0 without iterating then).  pcg_collect reads the outcome once
+// st has drained.
+void Hier::pcg_enqueue(const double *b, double *x, int itmax, double tol) {
+  CHRONOS_REQUIRE(prm.use_graph, CHRONOS_EINVAL, "queued solves need use_graph = 1");
+  ensure_pcg_state(*this, std::max(itmax, 1));
+  build_pcg_graph(*this);
+  PcgState &s = pcg;
+  const int n = s.n;
+  if (!s.sc_pinned) CHRONOS_CUDA(cudaMallocHost(&s.sc_pinned, sizeof(double) * SC_COUNT));
+  CHRONOS_CUDA(cudaMemcpyAsync(s.x.get(), x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  op_apply<double, double, double, double, MODE_RESID, false>(st, levels[0].A, s.x.get(), b,
+                                                              s.res.get(), 1.0);
+  const int nb = reduce_blocks(n);
+  k_dot_store<<<nb, 256, 0, st>>>(n, b, b, s.part.get(), s.tickets.get() + 3,
+                                   s.sc.get() + SC_BNORM);
+  CHRONOS_CHECK_LAUNCH();
+  k_dot_store<<<nb, 256, 0, st>>>(n, s.res.get(), s.res.get(), s.part.get(), s.tickets.get() + 3,
+                                   s.sc.get() + SC_RR);
+  CHRONOS_CHECK_LAUNCH();
+  k_pcg_init<<<1, 1, 0, st>>>(s.sc.get(), s.resvec.get(), tol, (double)itmax);
+  CHRONOS_CHECK_LAUNCH();
+  if (itmax > 0) CHRONOS_CUDA(cudaGraphLaunch(s.exec, st));
+  CHRONOS_CUDA(cudaMemcpyAsync(x, s.x.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  CHRONOS_CUDA(cudaMemcpyAsync(s.sc_pinned, s.sc.get(), sizeof(double) * SC_COUNT,
+                               cudaMemcpyDeviceToHost, st));
+}
+
+void Hier::pcg_collect(double tol, int *iters, int *flag) const {
+  const double *sc = pcg.sc_pinned;
+  CHRONOS_REQUIRE(sc, CHRONOS_EINVAL, "no queued solve to collect");
+  *iters = (int)(sc[SC_ITER] + 0.5);
+  const double r = sc[SC_RESITER];
+  *flag = (r > tol || !std::isfinite(r) || sc[SC_BREAKDOWN] != 0.0) ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------

@@ -56,6 +56,7 @@ struct PcgState {
   cudaGraph_t graph = nullptr;
   bool conditional = false;
   int resvec_cap = 0;
+  double *sc_pinned = nullptr;      // pinned copy of the scalars for queued solves
   ~PcgState();
 };
 
@@ -76,6 +77,10 @@ struct Hier {
   // PCG_CJ to tolerance on device vectors; returns iterations, flag.
   void pcg_solve(const double *b, double *x, int itmax, double tol, int *iters, int *flag,
                  std::vector<double> *resvec, double *seconds);
+  // the same solve queued on st without host synchronisation (b != 0), and
+  // its outcome once st has drained
+  void pcg_enqueue(const double *b, double *x, int itmax, double tol);
+  void pcg_collect(double tol, int *iters, int *flag) const;
   // y = A x with the level-0 FP64 operator.
   void apply_A(const double *x, double *y);
   // timings and algorithmic bytes of the hot kernels

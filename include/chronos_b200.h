@@ -278,6 +278,24 @@ int chronos_pcg_dev(chronos_hier *h, const double *b_d, double *x_d, int itmax, 
 int chronos_pcg_block(chronos_hier *h, int nrhs, const double *B_h, double *X_h, int itmax,
                       double tol, int *iters_h, int *flags_h, double *seconds);
 
+/* ---- Batch of independent problems of uneven sizes ---------------------- */
+/* One hierarchy per problem (each what chronos_amg_setup builds for it with
+ * the constant vector as TV0, padded to ntv columns as the reference does).  No
+ * counterpart call in the reference, which solves one system per driver run
+ * (aspAMG_main.m:175,199-202); each problem of the batch is that run. */
+typedef struct chronos_batch chronos_batch;
+int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
+                        const int *const *iat_h, const int *const *ja_h,
+                        const double *const *val_h, chronos_batch **out);
+/* PCG_CJ on every problem (x0 = x_h[p] on input), all queued before any
+ * result is read: per problem one conditional-graph launch on its own stream,
+ * largest first.  iters[p], flags[p] as chronos_pcg; seconds = device time
+ * from the first launch to the last problem's completion. */
+int chronos_batch_solve(chronos_batch *b, const double *const *b_h, double *const *x_h,
+                        int itmax, double tol, int *iters, int *flags, double *seconds);
+int chronos_batch_info(const chronos_batch *b, int p, int *nlevels, int *n0);
+int chronos_batch_free(chronos_batch *b);
+
 /* SQMR (SQMR.m) with the V-cycle as left preconditioner and identity right.
  * The operator is the 0-based FP64 CSR (iat_h, ja_h, val_h) of the hierarchy's
  * size, or the level-1 operator when iat_h is NULL (the reference's tests

@@ -21,7 +21,7 @@ def diffusion():
 @pytest.mark.parametrize("prec", [cb.CHRONOS_FP64, cb.CHRONOS_FP32])
 def test_block_matches_columns(lib, diffusion, prec):
     A, B = diffusion
-    with cb.Hierarchy(A, None, cb.params(precision=prec, ntv=1)) as h:
+    with cb.Hierarchy(A, np.ones(A.shape[0]),cb.params(precision=prec, ntv=1)) as h:
         X, its, flags, sec = h.pcg_block(B, itmax=1000, tol=1e-8)
         assert np.all(flags == 0)
         for j in range(B.shape[1]):
@@ -33,7 +33,7 @@ def test_block_matches_columns(lib, diffusion, prec):
 
 def test_block_iterations_match_oracle(lib, diffusion):
     A, B = diffusion
-    with cb.Hierarchy(A, None, cb.params(precision=cb.CHRONOS_FP64, ntv=1)) as h:
+    with cb.Hierarchy(A, np.ones(A.shape[0]),cb.params(precision=cb.CHRONOS_FP64, ntv=1)) as h:
         parts = []
         for l in range(h.nlevels):
             p = {"A": h.export(l, "A")}
@@ -52,7 +52,7 @@ def test_block_padding_and_zero_columns(lib, diffusion):
     A, B = diffusion
     B5 = B[:, :5].copy()
     B5[:, 2] = 0.0
-    with cb.Hierarchy(A, None, cb.params(ntv=1)) as h:
+    with cb.Hierarchy(A, np.ones(A.shape[0]),cb.params(ntv=1)) as h:
         X, its, flags, _ = h.pcg_block(B5, itmax=1000, tol=1e-8)
         assert X.shape == B5.shape
         assert its[2] == 0 and flags[2] == 0 and not np.any(X[:, 2])

@@ -37,14 +37,14 @@ def elast():
 @pytest.fixture(scope="module")
 def poisson():
     A = PB.poisson7(20)
-    return A, None, PB.uniform_rhs(A.shape[0], seed=1)
+    return A, np.ones((A.shape[0], 1)), PB.uniform_rhs(A.shape[0], seed=1)
 
 
 @pytest.mark.parametrize("prec,tol", [(cb.CHRONOS_FP64, 1e-12), (cb.CHRONOS_FP32, 2e-5)])
 @pytest.mark.parametrize("case", ["elast", "poisson"])
 def test_vcycle_parity(lib, case, prec, tol, request):
     A, TV, b = request.getfixturevalue(case)
-    ntv = 6 if TV is not None else 1
+    ntv = TV.shape[1]
     with cb.Hierarchy(A, TV, cb.params(precision=prec, ntv=ntv)) as h:
         assert h.nlevels >= 2
         Ho = oracle_from_gpu(h)
@@ -56,7 +56,7 @@ def test_vcycle_parity(lib, case, prec, tol, request):
 @pytest.mark.parametrize("case", ["elast", "poisson"])
 def test_pcg_iterations_fp64(lib, case, request):
     A, TV, b = request.getfixturevalue(case)
-    ntv = 6 if TV is not None else 1
+    ntv = TV.shape[1]
     with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP64, ntv=ntv)) as h:
         Ho = oracle_from_gpu(h)
         x, it, rv, flag, _ = h.pcg(b, itmax=500, tol=1e-8)
@@ -74,7 +74,7 @@ def test_pcg_fp32_hierarchy(lib, case, request):
     """FP32 hierarchy + FP64 outer PCG reaches the FP64 true residual and agrees
     with the FP64 oracle solve."""
     A, TV, b = request.getfixturevalue(case)
-    ntv = 6 if TV is not None else 1
+    ntv = TV.shape[1]
     with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32, ntv=ntv)) as h32, \
             cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP64, ntv=ntv)) as h64:
         x32, it32, _, f32, _ = h32.pcg(b, itmax=500, tol=1e-8)
@@ -103,7 +103,7 @@ def test_block_form_matches_csr(lib, elast, prec, tol):
 
 def test_block_form_not_used_without_blocks(lib, poisson):
     A, _, b = poisson
-    with cb.Hierarchy(A, None, cb.params(ntv=1)) as h:
+    with cb.Hierarchy(A, np.ones(A.shape[0]), cb.params(ntv=1)) as h:
         assert h.level_info(0)["block_rows"] == 0
 
 
@@ -120,7 +120,7 @@ def test_graph_loop_matches_host_loop(lib, elast):
 
 def test_pcg_repeatable_and_x0(lib, poisson):
     A, _, b = poisson
-    with cb.Hierarchy(A, None, cb.params(ntv=1)) as h:
+    with cb.Hierarchy(A, np.ones(A.shape[0]), cb.params(ntv=1)) as h:
         x1, it1, _, _, _ = h.pcg(b, itmax=500, tol=1e-8)
         x2, it2, _, _, _ = h.pcg(b, itmax=500, tol=1e-8)
         assert it1 == it2 and np.array_equal(x1, x2)
