@@ -24,57 +24,115 @@ template <int K> struct StoreK {
   }
 };
 
-template <typename VT, typename XT, typename ZT, typename YT, int K, int MODE, bool DOT>
+// VEC consecutive elements as one 8- or 16-byte access (aligned: K is a
+// multiple of VEC and every block starts on a 256-byte boundary).
+template <typename T, int VEC> struct Vec;
+template <> struct Vec<float, 4> {
+  __device__ static void ld(const float *p, float (&o)[4]) {
+    const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+    o[0] = t.x; o[1] = t.y; o[2] = t.z; o[3] = t.w;
+  }
+  __device__ static void st(float *p, const float (&o)[4]) {
+    *reinterpret_cast<float4 *>(p) = make_float4(o[0], o[1], o[2], o[3]);
+  }
+};
+template <> struct Vec<float, 2> {
+  __device__ static void ld(const float *p, float (&o)[2]) {
+    const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+    o[0] = t.x; o[1] = t.y;
+  }
+  __device__ static void st(float *p, const float (&o)[2]) {
+    *reinterpret_cast<float2 *>(p) = make_float2(o[0], o[1]);
+  }
+};
+template <> struct Vec<double, 2> {
+  __device__ static void ld(const double *p, double (&o)[2]) {
+    const double2 t = __ldg(reinterpret_cast<const double2 *>(p));
+    o[0] = t.x; o[1] = t.y;
+  }
+  __device__ static void st(double *p, const double (&o)[2]) {
+    *reinterpret_cast<double2 *>(p) = make_double2(o[0], o[1]);
+  }
+};
+
+// Lanes own VEC consecutive right-hand-side columns of one row: K/VEC lanes
+// per row, 32*VEC/K rows per warp; each stored value and column index is
+// fetched once per row group and applied to K columns.
+template <typename VT, typename XT, typename ZT, typename YT, int K, int VEC, int MODE, bool DOT>
 __global__ void __launch_bounds__(kApplyThreads)
 k_csr_spmm(int n, const int *__restrict__ rp, const int *__restrict__ ci,
            const VT *__restrict__ v, const XT *__restrict__ X, const ZT *Z, YT *Y, VT alpha,
            const double *__restrict__ DW, double *part, unsigned *ticket, double *dot_out) {
-  constexpr int R = 32 / K;
-  const int lane = threadIdx.x & 31, g = lane / K, j = lane % K;
+  constexpr int LPR = K / VEC;
+  constexpr int R = 32 / LPR;
+  const int lane = threadIdx.x & 31, g = lane / LPR, j0 = (lane % LPR) * VEC;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  double dacc = 0.0;
+  double dacc[VEC];
+#pragma unroll
+  for (int e = 0; e < VEC; ++e) dacc[e] = 0.0;
   for (int base = warp * R; base < n; base += nwarps * R) {
     const int row = base + g;
     if (row < n) {
-      VT s = VT(0), s2 = VT(0);
-      int k = __ldg(rp + row);
-      const int e = __ldg(rp + row + 1);
-      for (; k + 1 < e; k += 2) {
-        s += __ldg(v + k) * (VT)__ldg(X + (size_t)__ldg(ci + k) * K + j);
-        s2 += __ldg(v + k + 1) * (VT)__ldg(X + (size_t)__ldg(ci + k + 1) * K + j);
+      VT s[VEC];
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) s[e] = VT(0);
+      const int e1 = __ldg(rp + row + 1);
+      for (int k = __ldg(rp + row); k < e1; ++k) {
+        const VT a = __ldg(v + k);
+        XT xv[VEC];
+        Vec<XT, VEC>::ld(X + (size_t)__ldg(ci + k) * K + j0, xv);
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) s[e] += a * (VT)xv[e];
       }
-      if (k < e) s += __ldg(v + k) * (VT)__ldg(X + (size_t)__ldg(ci + k) * K + j);
-      s += s2;
-      const size_t o = (size_t)row * K + j;
-      VT r;
-      if (MODE == MODE_PLAIN) r = s;
-      else if (MODE == MODE_SCALE) r = alpha * s;
-      else if (MODE == MODE_RESID) r = (VT)Z[o] - s;
-      else r = (VT)Z[o] + alpha * s;
-      const YT out = (YT)r;
-      Y[o] = out;
-      if (DOT) dacc += (double)out * DW[o];
+      const size_t o = (size_t)row * K + j0;
+      ZT zv[VEC];
+      if (MODE == MODE_RESID || MODE == MODE_AXPY) Vec<ZT, VEC>::ld(Z + o, zv);
+      YT out[VEC];
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) {
+        VT r;
+        if (MODE == MODE_PLAIN) r = s[e];
+        else if (MODE == MODE_SCALE) r = alpha * s[e];
+        else if (MODE == MODE_RESID) r = (VT)zv[e] - s[e];
+        else r = (VT)zv[e] + alpha * s[e];
+        out[e] = (YT)r;
+        if (DOT) dacc[e] += (double)out[e] * DW[o + e];
+      }
+      Vec<YT, VEC>::st(Y + o, out);
     }
   }
   if (DOT) {
     double vals[K];
 #pragma unroll
-    for (int q = 0; q < K; ++q) vals[q] = (q == j) ? dacc : 0.0;
+    for (int q = 0; q < K; ++q) vals[q] = 0.0;
+#pragma unroll
+    for (int e = 0; e < VEC; ++e)
+#pragma unroll
+      for (int q = 0; q < K; ++q)
+        if (q == j0 + e) vals[q] = dacc[e];
     grid_reduce<K>(vals, part, ticket, StoreK<K>{dot_out});
   }
 }
+
+// 16-byte accesses when every operand is FP32 (VEC 4), else VEC 2.
+template <typename XT, typename ZT, typename YT, int K>
+struct SpmmVec {
+  static constexpr int v4 = (sizeof(XT) == 4 && sizeof(YT) == 4 && sizeof(ZT) == 4) ? 4 : 2;
+  static constexpr int value = v4 > K ? K : v4;
+};
 
 template <typename VT, typename XT, typename ZT, typename YT, int K, int MODE, bool DOT>
 static void spmm(cudaStream_t st, const DMat &M, const VT *vals, const XT *X, const ZT *Z, YT *Y,
                  VT alpha, const double *DW = nullptr, double *part = nullptr,
                  unsigned *tick = nullptr, double *dot_out = nullptr) {
+  constexpr int VEC = SpmmVec<XT, ZT, YT, K>::value;
   const int n = M.nrows;
   if (n <= 0) return;
-  const int rows_per_block = kApplyThreads / K;
+  const int rows_per_block = kApplyThreads * VEC / K;
   int blocks = (int)ceil_div(n, rows_per_block);
   blocks = std::min(blocks, num_sms() * 8);
-  k_csr_spmm<VT, XT, ZT, YT, K, MODE, DOT><<<blocks, kApplyThreads, 0, st>>>(
+  k_csr_spmm<VT, XT, ZT, YT, K, VEC, MODE, DOT><<<blocks, kApplyThreads, 0, st>>>(
       n, M.rp, M.ci, vals, X, Z, Y, alpha, DW, part, tick, dot_out);
   CHRONOS_CHECK_LAUNCH();
 }
@@ -217,28 +275,40 @@ k_bpcg_spmm(int n, const int *__restrict__ rp, const int *__restrict__ ci,
             const double *__restrict__ v, const double *__restrict__ p,
             const double *__restrict__ res, double *__restrict__ axp, double *part,
             unsigned *ticket, double *sc) {
-  constexpr int R = 32 / K;
-  const int lane = threadIdx.x & 31, g = lane / K, j = lane % K;
+  constexpr int LPR = K / 2;                      // two columns per lane (double2)
+  constexpr int R = 32 / LPR;
+  const int lane = threadIdx.x & 31, g = lane / LPR, j0 = (lane % LPR) * 2;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  double d0 = 0.0, d1 = 0.0;
+  double d0[2] = {0.0, 0.0}, d1[2] = {0.0, 0.0};
   for (int base = warp * R; base < n; base += nwarps * R) {
     const int row = base + g;
     if (row < n) {
-      double s = 0.0;
-      for (int k = __ldg(rp + row); k < __ldg(rp + row + 1); ++k)
-        s += __ldg(v + k) * __ldg(p + (size_t)__ldg(ci + k) * K + j);
-      const size_t o = (size_t)row * K + j;
-      axp[o] = s;
-      d0 += p[o] * s;
-      d1 += p[o] * res[o];
+      double s[2] = {0.0, 0.0};
+      const int e1 = __ldg(rp + row + 1);
+      for (int k = __ldg(rp + row); k < e1; ++k) {
+        const double a = __ldg(v + k);
+        double pv[2];
+        Vec<double, 2>::ld(p + (size_t)__ldg(ci + k) * K + j0, pv);
+        s[0] += a * pv[0];
+        s[1] += a * pv[1];
+      }
+      const size_t o = (size_t)row * K + j0;
+      Vec<double, 2>::st(axp + o, s);
+      double po[2], ro[2];
+      Vec<double, 2>::ld(p + o, po);
+      Vec<double, 2>::ld(res + o, ro);
+      for (int e = 0; e < 2; ++e) {
+        d0[e] += po[e] * s[e];
+        d1[e] += po[e] * ro[e];
+      }
     }
   }
   double vals[2 * K];
 #pragma unroll
   for (int q = 0; q < K; ++q) {
-    vals[q] = (q == j) ? d0 : 0.0;
-    vals[K + q] = (q == j) ? d1 : 0.0;
+    vals[q] = (q == j0) ? d0[0] : (q == j0 + 1) ? d0[1] : 0.0;
+    vals[K + q] = (q == j0) ? d1[0] : (q == j0 + 1) ? d1[1] : 0.0;
   }
   grid_reduce<2 * K>(vals, part, ticket, FinAlphaBlock<K>{sc});
 }
@@ -350,7 +420,7 @@ static void capture_block_iteration(Hier &h, BlockState &s, cudaGraphConditional
   k_bpcg_p_update<K><<<nb, 256, 0, st>>>(n, s.pres.get(), s.p.get(), sc);
   CHRONOS_CHECK_LAUNCH();
   const DMat &A = h.levels[0].A;
-  const int blocks = std::min(num_sms() * 8, (int)ceil_div(n, kApplyThreads / K));
+  const int blocks = std::min(num_sms() * 8, (int)ceil_div(n, kApplyThreads * 2 / K));
   k_bpcg_spmm<K><<<blocks, kApplyThreads, 0, st>>>(n, A.rp, A.ci, A.v64, s.p.get(), s.res.get(),
                                                    s.axp.get(), s.part.get() + 2 * K * 2048,
                                                    tk + 1, sc);

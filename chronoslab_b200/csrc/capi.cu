@@ -520,7 +520,9 @@ int chronos_pcg(chronos_hier *hh, const double *b_h, double *x_h, int itmax, dou
     CHRONOS_REQUIRE(hh && b_h && x_h && iters && flag, CHRONOS_EINVAL, "null argument");
     Hier &h = *hh->h;
     const int n = h.levels[0].n;
-    DBuf<double> b, x;
+    // staging buffers live with the handle: no allocation per call
+    if (h.stage_b.size() < (size_t)n) { h.stage_b.alloc(n); h.stage_x.alloc(n); }
+    DBuf<double> &b = h.stage_b, &x = h.stage_x;
     b.upload(b_h, n, h.st);
     x.upload(x_h, n, h.st);
     std::vector<double> rv;

@@ -89,6 +89,7 @@ struct Hier {
   void pcg_block(int nrhs, const double *B_h, double *X_h, int itmax, double tol, int *iters,
                  int *flags, double *seconds);
   std::shared_ptr<BlockState> block;
+  DBuf<double> stage_b, stage_x;    // host-buffer entry points' device staging
 };
 
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A,
