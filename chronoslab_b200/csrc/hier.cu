@@ -57,23 +57,64 @@ void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st) {
   d.nrows = h.nrows;
   d.ncols = h.ncols;
   d.nnz = h.nnz();
-  std::vector<int> rp(h.rp.begin(), h.rp.end());
-  d.rp.upload(rp, st);
+  d.rp_h.assign(h.rp.begin(), h.rp.end());
+  d.rp.upload(d.rp_h, st);
   d.ci.upload(h.ci, st);
   d.v64.upload(h.v, st);
   if (fp32) {
     d.v32.alloc(std::max<int64_t>(d.nnz, 1));
     convert_f64_to_f32(d.nnz, d.v64.get(), d.v32.get(), st);
   }
-  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  // 16-bit column offsets when every row spans fewer than 65536 columns
+  std::vector<int> base(std::max(h.nrows, 1), 0);
+  bool fits = h.nrows > 0;
+  for (int i = 0; i < h.nrows && fits; ++i) {
+    if (h.rp[i] == h.rp[i + 1]) continue;
+    int lo = h.ci[h.rp[i]], hi = lo;
+    for (int64_t k = h.rp[i] + 1; k < h.rp[i + 1]; ++k) {
+      lo = std::min(lo, h.ci[k]);
+      hi = std::max(hi, h.ci[k]);
+    }
+    base[i] = lo;
+    fits = hi - lo <= 0xffff;
+  }
+  d.idx16 = fits;
+  if (fits) {
+    std::vector<uint16_t> off(std::max<int64_t>(d.nnz, 1), 0);
+    for (int i = 0; i < h.nrows; ++i)
+      for (int64_t k = h.rp[i]; k < h.rp[i + 1]; ++k) off[k] = (uint16_t)(h.ci[k] - base[i]);
+    d.cbase.upload(base, st);
+    d.c16.upload(off, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+  } else {
+    d.cbase.release();
+    d.c16.release();
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+  }
+  set_lanes(d, heuristic_lanes(d), st);
 }
 
-static int heuristic_lanes(const DMat &m) {
+int heuristic_lanes(const DMat &m) {
   const double avg = m.nrows ? (double)m.nnz / m.nrows : 1.0;
   int L = 2;
   while (L < 32 && L < avg * 0.75) L <<= 1;
   return L;
 }
+
+void set_lanes(DMat &m, int L, cudaStream_t st) {
+  m.lanes = L;
+  m.lthresh = long_row_threshold(L);
+  std::vector<int> rows;
+  if (m.lthresh < 0x7fffffff)
+    for (int i = 0; i < m.nrows; ++i)
+      if (m.rp_h[i + 1] - m.rp_h[i] > m.lthresh) rows.push_back(i);
+  m.nlong = (int)rows.size();
+  if (m.nlong) {
+    m.longrows.upload(rows, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+  }
+}
+
 
 // Autotuner of the lanes per row (CSR) or per block row (BSR3): times each
 // candidate on the matrix itself and keeps the fastest.  Decisions are cached
@@ -122,62 +163,61 @@ void tune_store_locked(const TuneKey &k, int L) {
   }
 }
 
-template <typename Launch>
-int time_candidates(const std::vector<int> &cands, Launch launch, cudaStream_t st) {
-  cudaEvent_t e0, e1;
-  CHRONOS_CUDA(cudaEventCreate(&e0));
-  CHRONOS_CUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  int bestL = cands.front();
-  for (int L : cands) {
-    launch(L);
-    float tmin = 1e30f;
-    for (int r = 0; r < 3; ++r) {
-      CHRONOS_CUDA(cudaEventRecord(e0, st));
-      for (int q = 0; q < 4; ++q) launch(L);
-      CHRONOS_CUDA(cudaEventRecord(e1, st));
-      CHRONOS_CUDA(cudaEventSynchronize(e1));
-      float ms = 0;
-      CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-      tmin = std::min(tmin, ms);
-    }
-    if (tmin < best) { best = tmin; bestL = L; }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  return bestL;
-}
 }  // namespace
 
 void autotune_lanes(DMat &m, bool fp32, cudaStream_t st) {
   if (m.nrows <= 0) return;
-  const TuneKey key('C', m.nrows, m.nnz, m.ncols, fp32);
+  // 'H': the hybrid CSR kernel (k_csrh_apply); the index width is part of the shape
+  const TuneKey key(m.idx16 ? 'h' : 'H', m.nrows, m.nnz, m.ncols, fp32);
+  int L = -1;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     tune_load_locked();
     auto it = g_tune.find(key);
-    if (it != g_tune.end()) m.lanes = it->second;
-    else m.lanes = -1;
+    if (it != g_tune.end()) L = it->second;
   }
-  if (m.lanes < 0) {
-    m.lanes = heuristic_lanes(m);
+  if (L < 0) {
+    L = heuristic_lanes(m);
     if (m.nnz >= 4096) {                    // below: launch-latency bound, keep the heuristic
       DBuf<double> x64(m.ncols), y64(m.nrows);
       DBuf<float> x32(m.ncols), y32(m.nrows);
       x64.zero(st);
       x32.zero(st);
-      m.lanes = time_candidates({1, 2, 4, 8, 16, 32}, [&](int L) {
-        if (fp32)
-          csr_apply<float, float, float, float, MODE_PLAIN, false>(st, L, m.nrows, m.rp, m.ci, m.v32,
-                                                                 x32.get(), nullptr, y32.get(), 1.0f);
-        else
-          csr_apply<double, double, double, double, MODE_PLAIN, false>(
-              st, L, m.nrows, m.rp, m.ci, m.v64, x64.get(), nullptr, y64.get(), 1.0);
-      }, st);
+      cudaEvent_t e0, e1;
+      CHRONOS_CUDA(cudaEventCreate(&e0));
+      CHRONOS_CUDA(cudaEventCreate(&e1));
+      float best = 1e30f;
+      for (int cand : {1, 2, 4, 8, 16, 32}) {
+        set_lanes(m, cand, st);
+        auto launch = [&] {
+          if (fp32)
+            mat_apply<float, float, float, float, MODE_PLAIN, false>(st, m, m.v32.get(), x32.get(),
+                                                                    (const float *)nullptr,
+                                                                    y32.get(), 1.0f);
+          else
+            mat_apply<double, double, double, double, MODE_PLAIN, false>(
+                st, m, m.v64.get(), x64.get(), (const double *)nullptr, y64.get(), 1.0);
+        };
+        launch();
+        float tmin = 1e30f;
+        for (int r = 0; r < 3; ++r) {
+          CHRONOS_CUDA(cudaEventRecord(e0, st));
+          for (int q = 0; q < 4; ++q) launch();
+          CHRONOS_CUDA(cudaEventRecord(e1, st));
+          CHRONOS_CUDA(cudaEventSynchronize(e1));
+          float ms = 0;
+          CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+          tmin = std::min(tmin, ms);
+        }
+        if (tmin < best) { best = tmin; L = cand; }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
     }
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    tune_store_locked(key, m.lanes);
+    tune_store_locked(key, L);
   }
+  set_lanes(m, L, st);
 }
 
 // Sliced 3x3 block form of a CSR matrix whose row triples share a pattern of
@@ -335,8 +375,8 @@ static void op_apply(cudaStream_t st, const DMat &A, const XT *x, const ZT *z, Y
                                           bvals<T>(A), A.nslots, x, z, y, alpha, dw, part, tick,
                                           dot_out);
   else
-    csr_apply<T, XT, ZT, YT, MODE, DOT>(st, A.lanes, A.nrows, A.rp, A.ci, vals<T>(A), x, z, y,
-                                        alpha, dw, part, tick, dot_out);
+    mat_apply<T, XT, ZT, YT, MODE, DOT>(st, A, vals<T>(A), x, z, y, alpha, dw, part, tick,
+                                        dot_out);
 }
 
 // ---------------------------------------------------------------------------
@@ -683,42 +723,42 @@ static void vcycle_level(Hier &h, int l, const BT *b, OT *out, const double *dw,
   const T w = (T)L.omega;
   const DMat &A = L.A, &G = L.G, &Gt = L.Gt, &P = L.P, &Pt = L.Pt;
   // presmooth from x0 = 0: x = w G'(G b)
-  csr_apply<T, BT, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), b, nullptr, t, T(1));
-  csr_apply<T, T, T, T, MODE_SCALE, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, nullptr, x, w);
+  mat_apply<T, BT, T, T, MODE_PLAIN, false>(st, G, vals<T>(G), b, nullptr, t, T(1));
+  mat_apply<T, T, T, T, MODE_SCALE, false>(st, Gt, vals<T>(Gt), t, nullptr, x, w);
   for (int k = 1; k < h.prm.nupre; ++k) {
     op_apply<T, T, BT, T, MODE_RESID, false>(st, A, x, b, r, T(1));
-    csr_apply<T, T, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), r, nullptr, t, T(1));
-    csr_apply<T, T, T, T, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, x, w);
+    mat_apply<T, T, T, T, MODE_PLAIN, false>(st, G, vals<T>(G), r, nullptr, t, T(1));
+    mat_apply<T, T, T, T, MODE_AXPY, false>(st, Gt, vals<T>(Gt), t, x, x, w);
   }
   // residual and restriction
   op_apply<T, T, BT, T, MODE_RESID, false>(st, A, x, b, r, T(1));
   Level &C = h.levels[l + 1];
-  csr_apply<T, T, T, T, MODE_PLAIN, false>(st, Pt.lanes, L.nc, Pt.rp, Pt.ci, vals<T>(Pt), r, nullptr,
+  mat_apply<T, T, T, T, MODE_PLAIN, false>(st, Pt, vals<T>(Pt), r, nullptr,
                                            C.b<T>(), T(1));
   vcycle_level<T, T, T, false>(h, l + 1, C.b<T>(), C.x<T>(), nullptr, nullptr);
   // prolongation and correction
-  csr_apply<T, T, T, T, MODE_AXPY, false>(st, P.lanes, n, P.rp, P.ci, vals<T>(P), C.x<T>(), x, x, T(1));
+  mat_apply<T, T, T, T, MODE_AXPY, false>(st, P, vals<T>(P), C.x<T>(), x, x, T(1));
   // postsmooth
   const int npost = h.prm.nupost;
   for (int k = 0; k < npost; ++k) {
     op_apply<T, T, BT, T, MODE_RESID, false>(st, A, x, b, r, T(1));
-    csr_apply<T, T, T, T, MODE_PLAIN, false>(st, G.lanes, n, G.rp, G.ci, vals<T>(G), r, nullptr, t, T(1));
+    mat_apply<T, T, T, T, MODE_PLAIN, false>(st, G, vals<T>(G), r, nullptr, t, T(1));
     if (k + 1 < npost) {
-      csr_apply<T, T, T, T, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, x, w);
+      mat_apply<T, T, T, T, MODE_AXPY, false>(st, Gt, vals<T>(Gt), t, x, x, w);
     } else if (TOP && dw) {
-      csr_apply<T, T, T, OT, MODE_AXPY, true>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, out,
+      mat_apply<T, T, T, OT, MODE_AXPY, true>(st, Gt, vals<T>(Gt), t, x, out,
                                               w, dw, part, tick, dot_out);
     } else {
-      csr_apply<T, T, T, OT, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, out, w);
+      mat_apply<T, T, T, OT, MODE_AXPY, false>(st, Gt, vals<T>(Gt), t, x, out, w);
     }
   }
   if (npost == 0) {
     // out = x + 0 * (G' t): copy / convert through the same epilogue
     if (TOP && dw)
-      csr_apply<T, T, T, OT, MODE_AXPY, true>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, out,
+      mat_apply<T, T, T, OT, MODE_AXPY, true>(st, Gt, vals<T>(Gt), t, x, out,
                                               T(0), dw, part, tick, dot_out);
     else
-      csr_apply<T, T, T, OT, MODE_AXPY, false>(st, Gt.lanes, n, Gt.rp, Gt.ci, vals<T>(Gt), t, x, out,
+      mat_apply<T, T, T, OT, MODE_AXPY, false>(st, Gt, vals<T>(Gt), t, x, out,
                                                T(0));
   }
 }

@@ -102,6 +102,10 @@ void params_read(const char *fnames_path, chronos_params *p);
 void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st);
 // SpMV lane count by timing the candidates (cached per shape).
 void autotune_lanes(DMat &m, bool fp32, cudaStream_t st);
+// Lanes per row from the mean row length; setting the lanes also rebuilds the
+// matrix's long-row list.
+int heuristic_lanes(const DMat &m);
+void set_lanes(DMat &m, int L, cudaStream_t st);
 // Largest eigenvalue of the symmetric operator given as a device FP64 matvec,
 // by Lanczos with a unit start vector; relative tolerance tol.
 double lanczos_lmax(int n, const std::function<void(const double *, double *)> &mv, double tol,

@@ -19,6 +19,17 @@ struct DMat {
   DBuf<double> v64;
   DBuf<float> v32;
   int lanes = 8;            // SpMV lanes per row (autotuned)
+  std::vector<int> rp_h;    // host copy of the row pointers (long-row lists)
+  // 16-bit column offsets from a per-row base (the row's smallest column),
+  // present when every row spans fewer than 65536 columns: 2 index bytes per
+  // entry plus 4 per row instead of 4 per entry.
+  bool idx16 = false;
+  DBuf<int> cbase;
+  DBuf<uint16_t> c16;
+  // Rows longer than lthresh are applied by whole warps (listed in
+  // longrows); the others by groups of `lanes` lanes.
+  int lthresh = 0x7fffffff, nlong = 0;
+  DBuf<int> longrows;
   // Optional sliced 3x3 block form of the same matrix (chunks of 32 block
   // rows, slot-major, plane-major values), used when every row triple shares
   // a pattern of whole aligned 3x3 blocks.

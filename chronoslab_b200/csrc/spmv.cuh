@@ -16,7 +16,10 @@
 // conversions at the ends of the V-cycle into its first and last kernels.
 #pragma once
 
+#include <algorithm>
+
 #include "common.cuh"
+#include "internal.h"
 
 namespace chronos {
 
@@ -228,6 +231,156 @@ void sell3_apply(cudaStream_t st, int T, int nb, int nchunk, const int *choff, c
       throw Error(CHRONOS_EINVAL, "sell3_apply: threads per block row must be 1, 2 or 4");
   }
 #undef CHRONOS_SELL_CASE
+  CHRONOS_CHECK_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// Hybrid CSR apply of the V-cycle operators (G, G', P, P' and the CSR levels
+// of A).  Differences from k_csr_apply:
+//  * each lane issues the loads of up to kRowUnroll entries (values, column
+//    indices, then the x gathers) before it uses any of them, so the
+//    dependent chain row pointer -> column -> x is paid once per kRowUnroll
+//    entries instead of once per entry;
+//  * rows longer than lthresh (listed in longrows) are skipped by the
+//    L-lane groups and applied by whole warps in a second range of blocks of
+//    the same launch, so a few long rows (the transposed FSAI factor's
+//    popular columns) no longer serialise a short-row warp;
+//  * optional 16-bit column offsets from a per-row base.
+// Each row's entries are summed in a fixed order (lane-strided partial sums,
+// then a shuffle tree), so results are deterministic.
+constexpr int kRowUnroll = 4;
+
+template <typename VT, typename XT, int L, bool I16>
+__device__ __forceinline__ VT csr_row_dot(int k, int e, int cb, const int *__restrict__ ci,
+                                          const uint16_t *__restrict__ c16,
+                                          const VT *__restrict__ v, const XT *__restrict__ x) {
+  constexpr int U = kRowUnroll;
+  VT acc = VT(0);
+  for (; k + (U - 1) * L < e; k += U * L) {
+    int c[U];
+    VT a[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      c[u] = I16 ? cb + (int)__ldg(c16 + k + u * L) : __ldg(ci + k + u * L);
+      a[u] = __ldg(v + k + u * L);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) acc += a[u] * (VT)__ldg(x + c[u]);
+  }
+  // the fewer than U entries left to this lane
+  int c[U - 1];
+  VT a[U - 1];
+#pragma unroll
+  for (int u = 0; u < U - 1; ++u) {
+    const int kk = k + u * L;
+    c[u] = -1;
+    a[u] = VT(0);
+    if (kk < e) {
+      c[u] = I16 ? cb + (int)__ldg(c16 + kk) : __ldg(ci + kk);
+      a[u] = __ldg(v + kk);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < U - 1; ++u)
+    if (c[u] >= 0) acc += a[u] * (VT)__ldg(x + c[u]);
+  return acc;
+}
+
+template <typename VT, typename XT, typename ZT, typename YT, int L, int MODE, bool DOT, bool I16>
+__global__ void __launch_bounds__(kApplyThreads)
+k_csrh_apply(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+             const int *__restrict__ cbase, const uint16_t *__restrict__ c16,
+             const VT *__restrict__ v, const XT *__restrict__ x, const ZT *z, YT *y, VT alpha,
+             int short_blocks, int lthresh, const int *__restrict__ longrows, int nlong,
+             const double *__restrict__ dw, double *part, unsigned *ticket, double *dot_out) {
+  const int lane = threadIdx.x & 31;
+  double dacc = 0.0;
+  if ((int)blockIdx.x < short_blocks) {
+    constexpr int R = 32 / L;                      // row groups per warp
+    const int g = lane / L, gl = lane & (L - 1);
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (short_blocks * blockDim.x) >> 5;
+    for (int base = warp * R; base < n; base += nwarps * R) {   // warp-uniform trip count
+      const int row = base + g;
+      VT a = VT(0);
+      bool live = false;
+      if (row < n) {
+        const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
+        if (e - s <= lthresh) {
+          live = true;
+          a = csr_row_dot<VT, XT, L, I16>(s + gl, e, I16 ? __ldg(cbase + row) : 0, ci, c16, v, x);
+        }
+      }
+      a = group_sum<L>(a);
+      if (live && gl == 0) {
+        const YT out = (YT)apply_epilogue<VT, MODE>(a, alpha, z, row);
+        y[row] = out;
+        if (DOT) dacc += (double)out * dw[row];
+      }
+    }
+  } else {
+    const int warp = ((blockIdx.x - short_blocks) * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = ((gridDim.x - short_blocks) * blockDim.x) >> 5;
+    for (int i = warp; i < nlong; i += nwarps) {
+      const int row = __ldg(longrows + i);
+      const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
+      VT a = csr_row_dot<VT, XT, 32, I16>(s + lane, e, I16 ? __ldg(cbase + row) : 0, ci, c16, v,
+                                          x);
+      a = warp_sum(a);
+      if (lane == 0) {
+        const YT out = (YT)apply_epilogue<VT, MODE>(a, alpha, z, row);
+        y[row] = out;
+        if (DOT) dacc += (double)out * dw[row];
+      }
+    }
+  }
+  if (DOT) {
+    double vals[1] = {dacc};
+    grid_reduce<1>(vals, part, ticket, StoreScalar{dot_out});
+  }
+}
+
+// Long-row threshold for `lanes`-lane groups: rows longer than 16 entries per
+// lane go to whole warps.
+inline int long_row_threshold(int lanes) { return lanes >= 32 ? 0x7fffffff : 16 * lanes; }
+
+// Apply of a device matrix through k_csrh_apply with its tuned lanes, long-row
+// list and index width.  At most num_sms()*8 blocks (the reduction partial
+// buffers hold 2048 per slot).
+template <typename VT, typename XT, typename ZT, typename YT, int MODE, bool DOT>
+void mat_apply(cudaStream_t st, const DMat &M, const VT *v, const XT *x, const ZT *z, YT *y,
+               VT alpha, const double *dw = nullptr, double *part = nullptr,
+               unsigned *ticket = nullptr, double *dot_out = nullptr) {
+  const int n = M.nrows;
+  if (n <= 0) return;
+  const int L = M.lanes;
+  const int cap = num_sms() * 8;
+  const int wpb = kApplyThreads / 32;
+  int lb = M.nlong > 0 ? (int)std::min<int64_t>(ceil_div(M.nlong, wpb), cap / 4) : 0;
+  int sb = (int)std::min<int64_t>(ceil_div(n, kApplyThreads / L), cap - lb);
+  const int grid = sb + lb;
+#define CHRONOS_H_CASE(LL)                                                                    \
+  case LL:                                                                                    \
+    if (M.idx16)                                                                              \
+      k_csrh_apply<VT, XT, ZT, YT, LL, MODE, DOT, true><<<grid, kApplyThreads, 0, st>>>(      \
+          n, M.rp, M.ci, M.cbase, M.c16, v, x, z, y, alpha, sb, M.lthresh, M.longrows,        \
+          M.nlong, dw, part, ticket, dot_out);                                                \
+    else                                                                                      \
+      k_csrh_apply<VT, XT, ZT, YT, LL, MODE, DOT, false><<<grid, kApplyThreads, 0, st>>>(     \
+          n, M.rp, M.ci, M.cbase, M.c16, v, x, z, y, alpha, sb, M.lthresh, M.longrows,        \
+          M.nlong, dw, part, ticket, dot_out);                                                \
+    break;
+  switch (L) {
+    CHRONOS_H_CASE(1)
+    CHRONOS_H_CASE(2)
+    CHRONOS_H_CASE(4)
+    CHRONOS_H_CASE(8)
+    CHRONOS_H_CASE(16)
+    CHRONOS_H_CASE(32)
+    default:
+      throw Error(CHRONOS_EINVAL, "mat_apply: lanes per row must be 1,2,4,8,16 or 32");
+  }
+#undef CHRONOS_H_CASE
   CHRONOS_CHECK_LAUNCH();
 }
 
