@@ -42,7 +42,8 @@ class chronos_params(C.Structure):
         ("solv_method", C.c_char * 16), ("itmax", C.c_int), ("tol", C.c_double),
         ("restart", C.c_int),
         ("precision", C.c_int), ("use_graph", C.c_int), ("seed", C.c_uint64),
-        ("fsai_fabs", C.c_int), ("use_bsr", C.c_int),
+        ("fsai_fabs", C.c_int), ("use_bsr", C.c_int), ("exact_outer", C.c_int),
+        ("replace_ratio", C.c_double),
     ]
 
 

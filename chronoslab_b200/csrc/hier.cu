@@ -803,48 +803,91 @@ struct FinAlpha {
   }
 };
 
-// axp = A p (FP64) with ptap = p'axp and p'res.
-template <int L>
+// axp = A p with ptap = p'axp and p'res, accumulated in FP64; the stored
+// values VT are the FP64 operator (exact PCG_CJ arithmetic) or the FP32 copy
+// of the hierarchy (with true-residual replacement, see FinResidual).  Rows
+// as in k_csrh_apply: L-lane groups, long rows on whole warps.
+template <typename VT, int L, bool I16>
 __global__ void __launch_bounds__(kApplyThreads)
 k_pcg_spmv(int n, const int *__restrict__ rp, const int *__restrict__ ci,
-           const double *__restrict__ v, const double *__restrict__ p,
-           const double *__restrict__ res, double *__restrict__ axp, double *part,
+           const int *__restrict__ cbase, const uint16_t *__restrict__ c16,
+           const VT *__restrict__ v, const double *__restrict__ p,
+           const double *__restrict__ res, double *__restrict__ axp, int short_blocks,
+           int lthresh, const int *__restrict__ longrows, int nlong, double *part,
            unsigned *ticket, double *sc) {
-  constexpr int R = 32 / L;
-  const int lane = threadIdx.x & 31, g = lane / L, gl = lane & (L - 1);
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int lane = threadIdx.x & 31;
   double d0 = 0.0, d1 = 0.0;
-  for (int base = warp * R; base < n; base += nwarps * R) {
-    const int row = base + g;
-    double sum = 0.0, s2 = 0.0;
-    if (row < n) {
-      const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
-      int k = s + gl;
-      for (; k + L < e; k += 2 * L) {
-        sum += __ldg(v + k) * __ldg(p + __ldg(ci + k));
-        s2 += __ldg(v + k + L) * __ldg(p + __ldg(ci + k + L));
+  if ((int)blockIdx.x < short_blocks) {
+    constexpr int R = 32 / L;
+    const int g = lane / L, gl = lane & (L - 1);
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (short_blocks * blockDim.x) >> 5;
+    for (int base = warp * R; base < n; base += nwarps * R) {
+      const int row = base + g;
+      double a = 0.0;
+      bool live = false;
+      if (row < n) {
+        const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
+        if (e - s <= lthresh) {
+          live = true;
+          a = csr_row_dot<double, VT, double, L, I16>(s + gl, e, I16 ? __ldg(cbase + row) : 0,
+                                                      ci, c16, v, p);
+        }
       }
-      if (k < e) sum += __ldg(v + k) * __ldg(p + __ldg(ci + k));
-      sum += s2;
+      a = group_sum<L>(a);
+      if (live && gl == 0) {
+        axp[row] = a;
+        const double pi = p[row];
+        d0 += pi * a;
+        d1 += pi * res[row];
+      }
     }
-    sum = group_sum<L>(sum);
-    if (row < n && gl == 0) {
-      axp[row] = sum;
-      const double pi = p[row];
-      d0 += pi * sum;
-      d1 += pi * res[row];
+  } else {
+    const int warp = ((blockIdx.x - short_blocks) * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = ((gridDim.x - short_blocks) * blockDim.x) >> 5;
+    for (int i = warp; i < nlong; i += nwarps) {
+      const int row = __ldg(longrows + i);
+      const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
+      double a = csr_row_dot<double, VT, double, 32, I16>(
+          s + lane, e, I16 ? __ldg(cbase + row) : 0, ci, c16, v, p);
+      a = warp_sum(a);
+      if (lane == 0) {
+        axp[row] = a;
+        const double pi = p[row];
+        d0 += pi * a;
+        d1 += pi * res[row];
+      }
     }
   }
   double vals2[2] = {d0, d1};
   grid_reduce<2>(vals2, part, ticket, FinAlpha{sc});
 }
 
+// The three row sums of one block row of the sliced 3x3 block form (lane's
+// slots; the T partial sums are combined by the caller), accumulated in AT.
+template <typename AT, typename VT, typename XT>
+__device__ __forceinline__ void sell3_rows(int off, int w, const int *__restrict__ sci,
+                                           const VT *__restrict__ V, int64_t nslots,
+                                           const XT *__restrict__ x, AT &s0, AT &s1, AT &s2) {
+#pragma unroll 2
+  for (int j = 0; j < w; ++j) {
+    const int k = off + 32 * j;
+    const int col = 3 * __ldg(sci + k);
+    const AT xa = (AT)__ldg(x + col), xb = (AT)__ldg(x + col + 1), xc = (AT)__ldg(x + col + 2);
+    s0 += (AT)__ldg(V + k) * xa + (AT)__ldg(V + nslots + k) * xb +
+          (AT)__ldg(V + 2 * nslots + k) * xc;
+    s1 += (AT)__ldg(V + 3 * nslots + k) * xa + (AT)__ldg(V + 4 * nslots + k) * xb +
+          (AT)__ldg(V + 5 * nslots + k) * xc;
+    s2 += (AT)__ldg(V + 6 * nslots + k) * xa + (AT)__ldg(V + 7 * nslots + k) * xb +
+          (AT)__ldg(V + 8 * nslots + k) * xc;
+  }
+}
+
 // The same on the sliced 3x3 block form (see k_sell3_apply).
-template <int T>
+template <typename VT, int T>
 __global__ void __launch_bounds__(kApplyThreads)
 k_pcg_spmv_sell3(int nb, int nchunk, const int *__restrict__ choff, const int *__restrict__ chw,
-                 const int *__restrict__ sci, const double *__restrict__ V, int64_t nslots,
+                 const int *__restrict__ sci, const VT *__restrict__ V, int64_t nslots,
                  const double *__restrict__ p, const double *__restrict__ res,
                  double *__restrict__ axp, double *part, unsigned *ticket, double *sc) {
   constexpr int C = 32 / T;
@@ -853,19 +896,9 @@ k_pcg_spmv_sell3(int nb, int nchunk, const int *__restrict__ choff, const int *_
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   double d0 = 0.0, d1 = 0.0;
   for (int c = warp; c < nchunk; c += nwarps) {
-    const int off = __ldg(choff + c) + lane, w = __ldg(chw + c);
     double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-#pragma unroll 2
-    for (int j = 0; j < w; ++j) {
-      const int k = off + 32 * j;
-      const int col = 3 * __ldg(sci + k);
-      const double xa = __ldg(p + col), xb = __ldg(p + col + 1), xc = __ldg(p + col + 2);
-      s0 += __ldg(V + k) * xa + __ldg(V + nslots + k) * xb + __ldg(V + 2 * nslots + k) * xc;
-      s1 += __ldg(V + 3 * nslots + k) * xa + __ldg(V + 4 * nslots + k) * xb +
-            __ldg(V + 5 * nslots + k) * xc;
-      s2 += __ldg(V + 6 * nslots + k) * xa + __ldg(V + 7 * nslots + k) * xb +
-            __ldg(V + 8 * nslots + k) * xc;
-    }
+    sell3_rows<double, VT, double>(__ldg(choff + c) + lane, __ldg(chw + c), sci, V, nslots, p,
+                                   s0, s1, s2);
     if (T > 1) {
       s0 = slot_sum<T>(s0);
       s1 = slot_sum<T>(s1);
@@ -888,16 +921,36 @@ k_pcg_spmv_sell3(int nb, int nchunk, const int *__restrict__ choff, const int *_
   grid_reduce<2>(vals2, part, ticket, FinAlpha{sc});
 }
 
-// axp = A p with ptap and p'res, through the block form when A has one.
-static void launch_pcg_spmv(cudaStream_t st, const DMat &A, const double *p, const double *res,
-                            double *axp, double *part, unsigned *tick, double *sc) {
+static int pcg_grid(const DMat &A, int *short_blocks) {
+  const int cap = num_sms() * 8;
   if (A.nb > 0) {
-    const int blocks = std::min(num_sms() * 8, (int)ceil_div(A.nchunk, kApplyThreads / 32));
+    *short_blocks = 0;
+    return std::min(cap, (int)ceil_div(A.nchunk, kApplyThreads / 32));
+  }
+  const int lb = A.nlong > 0 ? std::min<int>(ceil_div(A.nlong, kApplyThreads / 32), cap / 4) : 0;
+  const int sb = std::min<int>(ceil_div(A.nrows, kApplyThreads / A.lanes), cap - lb);
+  *short_blocks = sb;
+  return sb + lb;
+}
+
+// axp = A p with ptap and p'res, through the block form when A has one; FP32
+// stored values when fp32vals (the FP32 hierarchy's copy), FP64 otherwise.
+static void launch_pcg_spmv(cudaStream_t st, const DMat &A, bool fp32vals, const double *p,
+                            const double *res, double *axp, double *part, unsigned *tick,
+                            double *sc) {
+  int sb = 0;
+  const int grid = pcg_grid(A, &sb);
+  if (A.nb > 0) {
 #define CHRONOS_PCGS_CASE(TT)                                                                  \
   case TT:                                                                                     \
-    k_pcg_spmv_sell3<TT><<<blocks, kApplyThreads, 0, st>>>(A.nb, A.nchunk, A.choff, A.chw,     \
-                                                           A.sci, A.bv64.get(), A.nslots, p,   \
-                                                           res, axp, part, tick, sc);          \
+    if (fp32vals)                                                                              \
+      k_pcg_spmv_sell3<float, TT><<<grid, kApplyThreads, 0, st>>>(                             \
+          A.nb, A.nchunk, A.choff, A.chw, A.sci, A.bv32.get(), A.nslots, p, res, axp, part,    \
+          tick, sc);                                                                           \
+    else                                                                                       \
+      k_pcg_spmv_sell3<double, TT><<<grid, kApplyThreads, 0, st>>>(                            \
+          A.nb, A.nchunk, A.choff, A.chw, A.sci, A.bv64.get(), A.nslots, p, res, axp, part,    \
+          tick, sc);                                                                           \
     break;
     switch (A.sell_T) {
       CHRONOS_PCGS_CASE(1)
@@ -907,15 +960,22 @@ static void launch_pcg_spmv(cudaStream_t st, const DMat &A, const double *p, con
     }
 #undef CHRONOS_PCGS_CASE
   } else {
-    const int n = A.nrows;
-    const int L = std::max(A.lanes, 2);
-    const int blocks = std::min(num_sms() * 8, (int)ceil_div(n, kApplyThreads / L));
+#define CHRONOS_PCG_LAUNCH(VT, VALS, LL, I16)                                                  \
+  k_pcg_spmv<VT, LL, I16><<<grid, kApplyThreads, 0, st>>>(                                     \
+      A.nrows, A.rp, A.ci, A.cbase, A.c16, VALS, p, res, axp, sb, A.lthresh, A.longrows,       \
+      A.nlong, part, tick, sc)
 #define CHRONOS_PCG_CASE(LL)                                                                   \
   case LL:                                                                                     \
-    k_pcg_spmv<LL><<<blocks, kApplyThreads, 0, st>>>(n, A.rp, A.ci, A.v64, p, res, axp, part,  \
-                                                    tick, sc);                                 \
+    if (fp32vals) {                                                                            \
+      if (A.idx16) CHRONOS_PCG_LAUNCH(float, A.v32.get(), LL, true);                           \
+      else CHRONOS_PCG_LAUNCH(float, A.v32.get(), LL, false);                                  \
+    } else {                                                                                   \
+      if (A.idx16) CHRONOS_PCG_LAUNCH(double, A.v64.get(), LL, true);                          \
+      else CHRONOS_PCG_LAUNCH(double, A.v64.get(), LL, false);                                 \
+    }                                                                                          \
     break;
-    switch (L) {
+    switch (A.lanes) {
+      CHRONOS_PCG_CASE(1)
       CHRONOS_PCG_CASE(2)
       CHRONOS_PCG_CASE(4)
       CHRONOS_PCG_CASE(8)
@@ -924,23 +984,41 @@ static void launch_pcg_spmv(cudaStream_t st, const DMat &A, const double *p, con
       default: throw Error(CHRONOS_EINVAL, "bad lane count");
     }
 #undef CHRONOS_PCG_CASE
+#undef CHRONOS_PCG_LAUNCH
   }
   CHRONOS_CHECK_LAUNCH();
 }
 
+// End of an iteration's x/res update (PCG_CJ.m:58-64).  Exact mode: the
+// recursive residual decides the stop.  Replacement mode (outer operator
+// from stored FP32 values): the recursive residual is replaced by the FP64
+// true residual (k_pcg_replace) when it has fallen below replace_ratio times
+// its largest value since the last replacement, when it passes the
+// tolerance, and at itmax; the stop is then decided on the true residual.
 struct FinResidual {
   double *sc, *resvec;
   cudaGraphConditionalHandle handle;
-  int use_cond;
+  int use_cond, mixed;
   __device__ void operator()(const double *t) const {
-    const double resiter = sqrt(t[0]) / sc[SC_BNORM];
+    const double rn = sqrt(t[0]);
+    const double resiter = rn / sc[SC_BNORM];
     const double it = sc[SC_ITER] + 1.0;
     sc[SC_ITER] = it;
     sc[SC_RR] = t[0];
     sc[SC_RESITER] = resiter;
     resvec[(int)it] = resiter;
-    const bool stop = resiter < sc[SC_TOL] || it >= sc[SC_ITMAX] || sc[SC_BREAKDOWN] != 0.0 ||
-                      !isfinite(resiter);
+    const bool bad = sc[SC_BREAKDOWN] != 0.0 || !isfinite(resiter);
+    bool stop;
+    if (mixed) {
+      const double rmax = fmax(sc[SC_RMAX], rn);
+      sc[SC_RMAX] = rmax;
+      const bool rep = !bad && (rn < sc[SC_RATIO] * rmax || resiter < sc[SC_TOL] ||
+                                it >= sc[SC_ITMAX]);
+      sc[SC_REPLACE] = rep ? 1.0 : 0.0;
+      stop = bad;                      // otherwise k_pcg_replace decides when it runs
+    } else {
+      stop = resiter < sc[SC_TOL] || it >= sc[SC_ITMAX] || bad;
+    }
     if (use_cond) cudaGraphSetConditional(handle, stop ? 0u : 1u);
   }
 };
@@ -950,7 +1028,7 @@ __global__ void __launch_bounds__(256)
 k_pcg_xr_update(int n, double *__restrict__ x, double *__restrict__ res,
                 const double *__restrict__ p, const double *__restrict__ axp, double *part,
                 unsigned *ticket, double *sc, double *resvec, cudaGraphConditionalHandle handle,
-                int use_cond) {
+                int use_cond, int mixed) {
   const double alpha = sc[SC_ALPHA];
   double rr = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -960,11 +1038,178 @@ k_pcg_xr_update(int n, double *__restrict__ x, double *__restrict__ res,
     rr += ri * ri;
   }
   double v[1] = {rr};
-  grid_reduce<1>(v, part, ticket, FinResidual{sc, resvec, handle, use_cond});
+  grid_reduce<1>(v, part, ticket, FinResidual{sc, resvec, handle, use_cond, mixed});
+}
+
+// Stop decision on the true residual after a replacement.
+struct FinReplace {
+  double *sc, *resvec;
+  cudaGraphConditionalHandle handle;
+  int use_cond;
+  __device__ void operator()(const double *t) const {
+    const double rn = sqrt(t[0]);
+    const double resiter = rn / sc[SC_BNORM];
+    const double it = sc[SC_ITER];
+    sc[SC_RR] = t[0];
+    sc[SC_RESITER] = resiter;
+    sc[SC_RMAX] = rn;
+    resvec[(int)it] = resiter;
+    const bool stop = resiter < sc[SC_TOL] || it >= sc[SC_ITMAX] || !isfinite(resiter);
+    if (use_cond) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+  }
+};
+
+// res = b - A x with the FP64 operator and ||res||^2, only when the previous
+// kernel flagged a replacement (every block reads the same flag, so the grid
+// returns as a whole otherwise).
+template <int L, bool I16>
+__global__ void __launch_bounds__(kApplyThreads)
+k_pcg_replace(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+              const int *__restrict__ cbase, const uint16_t *__restrict__ c16,
+              const double *__restrict__ v, const double *__restrict__ x,
+              const double *__restrict__ b, double *__restrict__ res, int short_blocks,
+              int lthresh, const int *__restrict__ longrows, int nlong, double *part,
+              unsigned *ticket, double *sc, double *resvec, cudaGraphConditionalHandle handle,
+              int use_cond) {
+  if (sc[SC_REPLACE] == 0.0) return;
+  const int lane = threadIdx.x & 31;
+  double rr = 0.0;
+  if ((int)blockIdx.x < short_blocks) {
+    constexpr int R = 32 / L;
+    const int g = lane / L, gl = lane & (L - 1);
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (short_blocks * blockDim.x) >> 5;
+    for (int base = warp * R; base < n; base += nwarps * R) {
+      const int row = base + g;
+      double a = 0.0;
+      bool live = false;
+      if (row < n) {
+        const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
+        if (e - s <= lthresh) {
+          live = true;
+          a = csr_row_dot<double, double, double, L, I16>(
+              s + gl, e, I16 ? __ldg(cbase + row) : 0, ci, c16, v, x);
+        }
+      }
+      a = group_sum<L>(a);
+      if (live && gl == 0) {
+        const double r = b[row] - a;
+        res[row] = r;
+        rr += r * r;
+      }
+    }
+  } else {
+    const int warp = ((blockIdx.x - short_blocks) * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = ((gridDim.x - short_blocks) * blockDim.x) >> 5;
+    for (int i = warp; i < nlong; i += nwarps) {
+      const int row = __ldg(longrows + i);
+      const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
+      double a = csr_row_dot<double, double, double, 32, I16>(
+          s + lane, e, I16 ? __ldg(cbase + row) : 0, ci, c16, v, x);
+      a = warp_sum(a);
+      if (lane == 0) {
+        const double r = b[row] - a;
+        res[row] = r;
+        rr += r * r;
+      }
+    }
+  }
+  double vals[1] = {rr};
+  grid_reduce<1>(vals, part, ticket, FinReplace{sc, resvec, handle, use_cond});
+}
+
+template <int T>
+__global__ void __launch_bounds__(kApplyThreads)
+k_pcg_replace_sell3(int nb, int nchunk, const int *__restrict__ choff,
+                    const int *__restrict__ chw, const int *__restrict__ sci,
+                    const double *__restrict__ V, int64_t nslots, const double *__restrict__ x,
+                    const double *__restrict__ b, double *__restrict__ res, double *part,
+                    unsigned *ticket, double *sc, double *resvec,
+                    cudaGraphConditionalHandle handle, int use_cond) {
+  if (sc[SC_REPLACE] == 0.0) return;
+  constexpr int C = 32 / T;
+  const int lane = threadIdx.x & 31;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double rr = 0.0;
+  for (int c = warp; c < nchunk; c += nwarps) {
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    sell3_rows<double, double, double>(__ldg(choff + c) + lane, __ldg(chw + c), sci, V, nslots,
+                                       x, s0, s1, s2);
+    if (T > 1) {
+      s0 = slot_sum<T>(s0);
+      s1 = slot_sum<T>(s1);
+      s2 = slot_sum<T>(s2);
+    }
+    const int br = C * c + (lane & (C - 1));
+    if (lane < C && br < nb) {
+      const double s[3] = {s0, s1, s2};
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const int row = 3 * br + r;
+        const double rv = b[row] - s[r];
+        res[row] = rv;
+        rr += rv * rv;
+      }
+    }
+  }
+  double vals[1] = {rr};
+  grid_reduce<1>(vals, part, ticket, FinReplace{sc, resvec, handle, use_cond});
+}
+
+static void launch_pcg_replace(cudaStream_t st, const DMat &A, const double *x, const double *b,
+                               double *res, double *part, unsigned *tick, double *sc,
+                               double *resvec, cudaGraphConditionalHandle handle, int use_cond) {
+  int sb = 0;
+  const int grid = pcg_grid(A, &sb);
+  if (A.nb > 0) {
+#define CHRONOS_REP3_CASE(TT)                                                                  \
+  case TT:                                                                                     \
+    k_pcg_replace_sell3<TT><<<grid, kApplyThreads, 0, st>>>(                                   \
+        A.nb, A.nchunk, A.choff, A.chw, A.sci, A.bv64.get(), A.nslots, x, b, res, part, tick,  \
+        sc, resvec, handle, use_cond);                                                         \
+    break;
+    switch (A.sell_T) {
+      CHRONOS_REP3_CASE(1)
+      CHRONOS_REP3_CASE(2)
+      CHRONOS_REP3_CASE(4)
+      default: throw Error(CHRONOS_EINVAL, "bad threads per block row");
+    }
+#undef CHRONOS_REP3_CASE
+  } else {
+#define CHRONOS_REP_CASE(LL)                                                                   \
+  case LL:                                                                                     \
+    if (A.idx16)                                                                               \
+      k_pcg_replace<LL, true><<<grid, kApplyThreads, 0, st>>>(                                 \
+          A.nrows, A.rp, A.ci, A.cbase, A.c16, A.v64.get(), x, b, res, sb, A.lthresh,          \
+          A.longrows, A.nlong, part, tick, sc, resvec, handle, use_cond);                      \
+    else                                                                                       \
+      k_pcg_replace<LL, false><<<grid, kApplyThreads, 0, st>>>(                                \
+          A.nrows, A.rp, A.ci, A.cbase, A.c16, A.v64.get(), x, b, res, sb, A.lthresh,          \
+          A.longrows, A.nlong, part, tick, sc, resvec, handle, use_cond);                      \
+    break;
+    switch (A.lanes) {
+      CHRONOS_REP_CASE(1)
+      CHRONOS_REP_CASE(2)
+      CHRONOS_REP_CASE(4)
+      CHRONOS_REP_CASE(8)
+      CHRONOS_REP_CASE(16)
+      CHRONOS_REP_CASE(32)
+      default: throw Error(CHRONOS_EINVAL, "bad lane count");
+    }
+#undef CHRONOS_REP_CASE
+  }
+  CHRONOS_CHECK_LAUNCH();
 }
 
 static int reduce_blocks(int n) {
   return std::max(1, std::min(num_sms() * 8, (int)ceil_div(n, 256)));
+}
+
+// True when the outer PCG applies the stored FP32 values with true-residual
+// replacement (FP32 hierarchy, exact_outer = 0).
+static bool mixed_outer(const Hier &h) {
+  return h.precision == CHRONOS_FP32 && !h.prm.exact_outer;
 }
 
 // Captures one PCG_CJ iteration (PCG_CJ.m:36-64) into the current stream capture.
@@ -973,18 +1218,23 @@ static void capture_iteration(Hier &h, cudaGraphConditionalHandle handle, int us
   cudaStream_t st = h.st;
   const int n = s.n;
   const int nb = reduce_blocks(n);
+  const bool mixed = mixed_outer(h);
   double *sc = s.sc.get();
   // pres = M^{-1} res  (with pres'axp for beta)
   h.vcycle(s.res.get(), s.pres.get(), s.axp.get(), sc + SC_PRES_AXP);
   k_pcg_p_update<<<nb, 256, 0, st>>>(n, s.pres.get(), s.p.get(), sc);
   CHRONOS_CHECK_LAUNCH();
   unsigned *tk = s.tickets.get();
-  launch_pcg_spmv(st, h.levels[0].A, s.p.get(), s.res.get(), s.axp.get(),
+  launch_pcg_spmv(st, h.levels[0].A, mixed, s.p.get(), s.res.get(), s.axp.get(),
                   s.part.get() + 4 * 3 * 2048, tk + 1, sc);
   k_pcg_xr_update<<<nb, 256, 0, st>>>(n, s.x.get(), s.res.get(), s.p.get(), s.axp.get(),
                                        s.part.get() + 8 * 3 * 2048, tk + 2, sc,
-                                       s.resvec.get(), handle, use_cond);
+                                       s.resvec.get(), handle, use_cond, mixed ? 1 : 0);
   CHRONOS_CHECK_LAUNCH();
+  if (mixed)
+    launch_pcg_replace(st, h.levels[0].A, s.x.get(), s.b.get(), s.res.get(),
+                       s.part.get() + 10 * 3 * 2048, tk + 4, sc, s.resvec.get(), handle,
+                       use_cond);
 }
 
 static void ensure_pcg_state(Hier &h, int itmax) {
@@ -992,7 +1242,7 @@ static void ensure_pcg_state(Hier &h, int itmax) {
   const int n = h.levels[0].n;
   if (s.n != n) {
     s.n = n;
-    s.x.alloc(n); s.res.alloc(n); s.p.alloc(n); s.axp.alloc(n); s.pres.alloc(n);
+    s.x.alloc(n); s.res.alloc(n); s.p.alloc(n); s.axp.alloc(n); s.pres.alloc(n); s.b.alloc(n);
     s.sc.alloc(SC_COUNT);
     s.part.alloc((size_t)12 * 3 * 2048);
     s.tickets.alloc(8);
@@ -1052,11 +1302,19 @@ static void build_pcg_graph(Hier &h) {
   }
 }
 
-__global__ void k_pcg_init(double *sc, double *resvec, double tol, double itmax) {
+static double replace_ratio(const Hier &h) {
+  const double r = h.prm.replace_ratio;
+  return (r > 0.0 && r < 1.0) ? r : 0.01;
+}
+
+__global__ void k_pcg_init(double *sc, double *resvec, double tol, double itmax, double ratio) {
   // sc[SC_BNORM], sc[SC_RR] hold ||b||^2 and ||r0||^2 from the reductions
   const double bn = sqrt(sc[SC_BNORM]);
   sc[SC_BNORM] = bn;
   sc[SC_RESITER] = sqrt(sc[SC_RR]) / bn;
+  sc[SC_RMAX] = sqrt(sc[SC_RR]);
+  sc[SC_REPLACE] = 0.0;
+  sc[SC_RATIO] = ratio;
   resvec[0] = sc[SC_RESITER];
   sc[SC_ITER] = 0.0;
   sc[SC_TOL] = tol;
@@ -1075,6 +1333,8 @@ void Hier::pcg_solve(const double *b, double *x, int itmax, double tol, int *ite
   CHRONOS_CUDA(cudaEventRecord(e0, st));
   // res = b - A x0, ||b||, ||res|| (PCG_CJ.m:11-30)
   CHRONOS_CUDA(cudaMemcpyAsync(s.x.get(), x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  if (mixed_outer(*this))
+    CHRONOS_CUDA(cudaMemcpyAsync(s.b.get(), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   op_apply<double, double, double, double, MODE_RESID, false>(st, levels[0].A, s.x.get(), b,
                                                               s.res.get(), 1.0);
   const int nb = reduce_blocks(n);
@@ -1084,7 +1344,8 @@ void Hier::pcg_solve(const double *b, double *x, int itmax, double tol, int *ite
   k_dot_store<<<nb, 256, 0, st>>>(n, s.res.get(), s.res.get(), part, s.tickets.get() + 3,
                                    s.sc.get() + SC_RR);
   CHRONOS_CHECK_LAUNCH();
-  k_pcg_init<<<1, 1, 0, st>>>(s.sc.get(), s.resvec.get(), tol, (double)itmax);
+  k_pcg_init<<<1, 1, 0, st>>>(s.sc.get(), s.resvec.get(), tol, (double)itmax,
+                              replace_ratio(*this));
   CHRONOS_CHECK_LAUNCH();
   double sc_h[SC_COUNT];
   CHRONOS_CUDA(cudaMemcpyAsync(sc_h, s.sc.get(), sizeof(sc_h), cudaMemcpyDeviceToHost, st));
@@ -1157,6 +1418,8 @@ void Hier::pcg_enqueue(const double *b, double *x, int itmax, double tol) {
   const int n = s.n;
   if (!s.sc_pinned) CHRONOS_CUDA(cudaMallocHost(&s.sc_pinned, sizeof(double) * SC_COUNT));
   CHRONOS_CUDA(cudaMemcpyAsync(s.x.get(), x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  if (mixed_outer(*this))
+    CHRONOS_CUDA(cudaMemcpyAsync(s.b.get(), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   op_apply<double, double, double, double, MODE_RESID, false>(st, levels[0].A, s.x.get(), b,
                                                               s.res.get(), 1.0);
   const int nb = reduce_blocks(n);
@@ -1166,7 +1429,8 @@ void Hier::pcg_enqueue(const double *b, double *x, int itmax, double tol) {
   k_dot_store<<<nb, 256, 0, st>>>(n, s.res.get(), s.res.get(), s.part.get(), s.tickets.get() + 3,
                                    s.sc.get() + SC_RR);
   CHRONOS_CHECK_LAUNCH();
-  k_pcg_init<<<1, 1, 0, st>>>(s.sc.get(), s.resvec.get(), tol, (double)itmax);
+  k_pcg_init<<<1, 1, 0, st>>>(s.sc.get(), s.resvec.get(), tol, (double)itmax,
+                              replace_ratio(*this));
   CHRONOS_CHECK_LAUNCH();
   if (itmax > 0) CHRONOS_CUDA(cudaGraphLaunch(s.exec, st));
   CHRONOS_CUDA(cudaMemcpyAsync(x, s.x.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
@@ -1191,8 +1455,10 @@ void Hier::pcg_collect(double tol, int *iters, int *flag) const {
 static double apply_bytes(const DMat &M, double s, double sx, double sy, double extra_per_row) {
   // block form: 9 values + one block-column index per 3x3 block (true blocks:
   // the chunk padding is not algorithmic traffic)
-  const double mat = M.nb > 0 ? (double)M.nnzb * (9.0 * s + 4.0) + (M.nchunk + 1.0) * 8.0
-                              : (double)M.nnz * (s + 4.0) + (M.nrows + 1.0) * 4.0;
+  // CSR: 4-byte columns, or 2-byte offsets plus a 4-byte base per row
+  const double mat = M.nb > 0    ? (double)M.nnzb * (9.0 * s + 4.0) + (M.nchunk + 1.0) * 8.0
+                     : M.idx16 ? (double)M.nnz * (s + 2.0) + (M.nrows + 1.0) * 4.0 + M.nrows * 4.0
+                               : (double)M.nnz * (s + 4.0) + (M.nrows + 1.0) * 4.0;
   return mat + M.ncols * sx + M.nrows * (sy + extra_per_row);
 }
 
@@ -1272,17 +1538,18 @@ void Hier::profile(int reps, chronos_profile *out) {
     out->top_apply_ms = 0.0;
     out->top_apply_bytes = 0.0;
   }
-  // outer FP64 SpMV with its two dots, as captured in the PCG iteration
+  // outer SpMV with its two dots, as captured in the PCG iteration (stored
+  // FP32 values with FP64 accumulation, or FP64 values)
   double *part = ps.part.get() + 4 * 3 * 2048;
   CHRONOS_CUDA(cudaMemcpyAsync(ps.p.get(), b.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   CHRONOS_CUDA(cudaMemcpyAsync(ps.res.get(), b.get(), sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   out->outer_spmv_ms = time_it([&] {
-    launch_pcg_spmv(st, A, ps.p.get(), ps.res.get(), ps.axp.get(), part, ps.tickets.get() + 1,
-                    ps.sc.get());
+    launch_pcg_spmv(st, A, mixed_outer(*this), ps.p.get(), ps.res.get(), ps.axp.get(), part,
+                    ps.tickets.get() + 1, ps.sc.get());
   });
-  out->outer_spmv_bytes = apply_bytes(A, 8.0, 8.0, 8.0, 16.0);
+  out->outer_spmv_bytes = apply_bytes(A, mixed_outer(*this) ? 4.0 : 8.0, 8.0, 8.0, 16.0);
   out->iteration_bytes = out->vcycle_bytes + out->outer_spmv_bytes + 3.0 * n * 8 + 6.0 * n * 8;
-  out->kernels_per_iteration = vcycle_kernels(*this) + 3;
+  out->kernels_per_iteration = vcycle_kernels(*this) + 3 + (mixed_outer(*this) ? 1 : 0);
   out->kernels_per_solve = 4;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

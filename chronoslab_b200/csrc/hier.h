@@ -43,12 +43,13 @@ template <> inline const double *vals<double>(const DMat &m) { return m.v64.get(
 // Device scalars of the PCG recurrence.
 enum PcgScalar {
   SC_BNORM = 0, SC_PTAP, SC_ALPHA, SC_PRES_AXP, SC_RR, SC_RESITER, SC_ITER, SC_TOL, SC_ITMAX,
-  SC_BREAKDOWN, SC_PRES, SC_COUNT = 16
+  SC_BREAKDOWN, SC_PRES, SC_RMAX, SC_REPLACE, SC_RATIO, SC_COUNT = 16
 };
 
 struct PcgState {
   int n = 0;
   DBuf<double> x, res, p, axp, pres, resvec;
+  DBuf<double> b;                   // copy of the right-hand side (true-residual replacement)
   DBuf<double> sc;                  // SC_COUNT scalars
   DBuf<double> part;                // block partials (3 per block, several slots)
   DBuf<unsigned> tickets;           // one ticket per reducing kernel

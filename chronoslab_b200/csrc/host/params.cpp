@@ -98,6 +98,8 @@ void params_default(chronos_params *p) {
   p->seed = 5489;
   p->fsai_fabs = 0;
   p->use_bsr = 1;
+  p->exact_outer = 0;
+  p->replace_ratio = 0.01;
 }
 
 void params_read(const char *fnames_path, chronos_params *p) {

@@ -250,12 +250,13 @@ void sell3_apply(cudaStream_t st, int T, int nb, int nchunk, const int *choff, c
 // then a shuffle tree), so results are deterministic.
 constexpr int kRowUnroll = 4;
 
-template <typename VT, typename XT, int L, bool I16>
-__device__ __forceinline__ VT csr_row_dot(int k, int e, int cb, const int *__restrict__ ci,
+// Partial sum of lane entries k, k+L, ... < e of one row, accumulated in AT.
+template <typename AT, typename VT, typename XT, int L, bool I16>
+__device__ __forceinline__ AT csr_row_dot(int k, int e, int cb, const int *__restrict__ ci,
                                           const uint16_t *__restrict__ c16,
                                           const VT *__restrict__ v, const XT *__restrict__ x) {
   constexpr int U = kRowUnroll;
-  VT acc = VT(0);
+  AT acc = AT(0);
   for (; k + (U - 1) * L < e; k += U * L) {
     int c[U];
     VT a[U];
@@ -265,7 +266,7 @@ __device__ __forceinline__ VT csr_row_dot(int k, int e, int cb, const int *__res
       a[u] = __ldg(v + k + u * L);
     }
 #pragma unroll
-    for (int u = 0; u < U; ++u) acc += a[u] * (VT)__ldg(x + c[u]);
+    for (int u = 0; u < U; ++u) acc += (AT)a[u] * (AT)__ldg(x + c[u]);
   }
   // the fewer than U entries left to this lane
   int c[U - 1];
@@ -282,7 +283,7 @@ __device__ __forceinline__ VT csr_row_dot(int k, int e, int cb, const int *__res
   }
 #pragma unroll
   for (int u = 0; u < U - 1; ++u)
-    if (c[u] >= 0) acc += a[u] * (VT)__ldg(x + c[u]);
+    if (c[u] >= 0) acc += (AT)a[u] * (AT)__ldg(x + c[u]);
   return acc;
 }
 
@@ -308,7 +309,8 @@ k_csrh_apply(int n, const int *__restrict__ rp, const int *__restrict__ ci,
         const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
         if (e - s <= lthresh) {
           live = true;
-          a = csr_row_dot<VT, XT, L, I16>(s + gl, e, I16 ? __ldg(cbase + row) : 0, ci, c16, v, x);
+          a = csr_row_dot<VT, VT, XT, L, I16>(s + gl, e, I16 ? __ldg(cbase + row) : 0, ci, c16, v,
+                                              x);
         }
       }
       a = group_sum<L>(a);
@@ -324,8 +326,8 @@ k_csrh_apply(int n, const int *__restrict__ rp, const int *__restrict__ ci,
     for (int i = warp; i < nlong; i += nwarps) {
       const int row = __ldg(longrows + i);
       const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
-      VT a = csr_row_dot<VT, XT, 32, I16>(s + lane, e, I16 ? __ldg(cbase + row) : 0, ci, c16, v,
-                                          x);
+      VT a = csr_row_dot<VT, VT, XT, 32, I16>(s + lane, e, I16 ? __ldg(cbase + row) : 0, ci, c16,
+                                              v, x);
       a = warp_sum(a);
       if (lane == 0) {
         const YT out = (YT)apply_epilogue<VT, MODE>(a, alpha, z, row);

@@ -98,6 +98,15 @@ typedef struct chronos_params {
                                      int abs (truncation toward zero); 1: through fabs */
   int use_bsr;                    /* 1 (default): apply the level-1 operator in 3x3 block form
                                      when its pattern is made of whole aligned 3x3 blocks */
+  int exact_outer;                /* 1: the outer PCG applies the level-1 operator with its FP64
+                                     values (PCG_CJ's arithmetic exactly).  0 (default): with
+                                     the hierarchy's stored values (FP32 for CHRONOS_FP32)
+                                     accumulated in FP64, the recursive residual being replaced
+                                     by the FP64 true residual b - A x whenever it has fallen
+                                     by replace_ratio since the last replacement and before
+                                     every stop; the returned relative residual is then the
+                                     true one.  No effect for CHRONOS_FP64 hierarchies. */
+  double replace_ratio;           /* 0.01 (default), in (0, 1) */
 } chronos_params;
 
 /* Reference regression-test parameters (Tests/parm_*): DOM 0.01, BAMG/NONE,
@@ -248,7 +257,7 @@ int chronos_hier_setup_times(const chronos_hier *h, double *t8);
 typedef struct chronos_profile {
   double vcycle_ms, vcycle_bytes;          /* one V-cycle, FP64 in/out */
   double top_apply_ms, top_apply_bytes;    /* level-1 residual b - A x in the stored precision */
-  double outer_spmv_ms, outer_spmv_bytes;  /* the PCG's FP64 A p with its two dot products */
+  double outer_spmv_ms, outer_spmv_bytes;  /* the PCG's A p (FP64 accumulation) with its two dots */
   double iteration_bytes;                  /* one PCG_CJ iteration in total */
   int kernels_per_iteration;               /* kernel launches of one PCG iteration */
   int kernels_per_solve;                   /* launches outside the loop, per solve */

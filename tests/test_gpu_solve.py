@@ -179,3 +179,41 @@ def test_setup_components_match_golden(lib, cubo, cubo_ref):
         assert rel(Ac.toarray(), ref.toarray()) <= 1e-13
         info = h.level_info(0)
         assert 0.0 < info["omega"] <= 1.0
+
+
+@pytest.mark.parametrize("ratio", [0.01, 0.5])
+@pytest.mark.parametrize("case", ["elast", "poisson"])
+def test_outer_fp32_values_with_replacement(lib, case, ratio, request):
+    """FP32 hierarchy, outer A p from the stored FP32 level-1 values with FP64
+    accumulation and FP64 true-residual replacement (the default) against the
+    FP64 outer operator on the same hierarchy: iterations within 1, the true
+    residual below the tolerance, the same solution, and the last residual
+    reported is the true one."""
+    A, TV, b = request.getfixturevalue(case)
+    ntv = TV.shape[1]
+    with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32, ntv=ntv,
+                                       replace_ratio=ratio)) as hm, \
+            cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32, ntv=ntv,
+                                          exact_outer=1)) as he:
+        xm, itm, rvm, fm, _ = hm.pcg(b, itmax=500, tol=1e-8)
+        xe, ite, rve, fe, _ = he.pcg(b, itmax=500, tol=1e-8)
+        assert fm == 0 and fe == 0
+        assert abs(itm - ite) <= 1
+        true_m = np.linalg.norm(b - A @ xm) / np.linalg.norm(b)
+        assert true_m <= 1e-8
+        assert rvm[-1] == pytest.approx(true_m, rel=1e-6)
+        assert rel(xm, xe) <= 1e-7
+
+
+def test_outer_replacement_itmax_and_warm_start(lib, elast):
+    A, TV, b = elast
+    with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32)) as h:
+        # itmax reached: flag 1, the final residual is the true one
+        x, it, rv, flag, _ = h.pcg(b, itmax=3, tol=1e-14)
+        assert it == 3 and flag == 1
+        true = np.linalg.norm(b - A @ x) / np.linalg.norm(b)
+        assert rv[-1] == pytest.approx(true, rel=1e-6)
+        # warm start at the solution: one iteration
+        xs, _, _, _, _ = h.pcg(b, itmax=500, tol=1e-8)
+        x3, it3, _, flag3, _ = h.pcg(b, x0=xs, itmax=500, tol=1e-8)
+        assert it3 == 1 and flag3 == 0
