@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -114,6 +115,44 @@ __device__ __forceinline__ double block_sum(double v, double *smem32) {
   }
   __syncthreads();
   return r;
+}
+
+// ---- programmatic dependent launch ------------------------------------------
+// Kernels of the solve loop begin with pdl_begin(): griddepcontrol.wait
+// returns once the preceding kernel of the stream has completed and its
+// writes are visible (a no-op for a kernel launched without the attribute),
+// then griddepcontrol.launch_dependents lets the next kernel's blocks be
+// scheduled while this one drains.  Nothing is read or written before the
+// wait, so the order of memory effects is the plain stream order.
+__device__ __forceinline__ void pdl_begin() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" :::);
+}
+
+// Programmatic dependent launch is on unless CHRONOS_PDL=0 in the environment.
+inline bool pdl_enabled() {
+  static const int on = [] {
+    const char *e = std::getenv("CHRONOS_PDL");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return on != 0;
+}
+
+// Launch of a kernel that begins with pdl_begin(), with the programmatic
+// stream serialization attribute when enabled.
+template <typename... KArgs, typename... Args>
+void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  CHRONOS_CUDA(cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...));
 }
 
 inline int num_sms() {

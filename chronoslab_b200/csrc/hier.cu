@@ -305,12 +305,19 @@ static void upload_sell3(const HostCSR &A, const std::vector<int> &blen, int T, 
   CHRONOS_CUDA(cudaStreamSynchronize(st));
 }
 
-// Attaches the sliced block form with the fastest threads-per-block-row
-// (timed in the precision the V-cycle uses; cached like the CSR lanes).
+static void launch_pcg_spmv(cudaStream_t st, const DMat &A, bool fp32vals, const double *p,
+                            const double *res, double *axp, double *part, unsigned *tick,
+                            double *sc);
+
+// Attaches the sliced block form with the fastest threads-per-block-row.
+// The layout serves the V-cycle's residuals (two per cycle, hierarchy
+// precision) and the outer PCG's A p (FP64 accumulation, stored FP32 values
+// in FP32 hierarchies), so a candidate is timed on that mix: two residual
+// applies and one outer product.  Cached like the CSR lanes.
 static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) {
   const std::vector<int> blen = block_row_lengths(A);
   if (blen.empty()) return;
-  const TuneKey key('S', (int)blen.size(), A.nnz(), A.ncols, fp32);
+  const TuneKey key('B', (int)blen.size(), A.nnz(), A.ncols, fp32);
   int T = -1;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -319,10 +326,14 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
     if (it != g_tune.end()) T = it->second;
   }
   if (T < 0) {
-    DBuf<double> x64(A.ncols), y64(A.nrows);
+    DBuf<double> x64(A.ncols), y64(A.nrows), p64(A.ncols), q64(A.nrows), part(3 * 2048),
+        sc(SC_COUNT);
     DBuf<float> x32(A.ncols), y32(A.nrows);
+    DBuf<unsigned> tick(1);
     x64.zero(st);
     x32.zero(st);
+    p64.zero(st);
+    tick.zero(st);
     float best = 1e30f;
     cudaEvent_t e0, e1;
     CHRONOS_CUDA(cudaEventCreate(&e0));
@@ -331,14 +342,20 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
       DMat probe;
       upload_sell3(A, blen, t, probe, fp32, st);
       auto launch = [&] {
-        if (fp32)
-          sell3_apply<float, float, float, float, MODE_PLAIN, false>(
-              st, t, probe.nb, probe.nchunk, probe.choff, probe.chw, probe.sci, probe.bv32.get(),
-              probe.nslots, x32.get(), (const float *)nullptr, y32.get(), 1.0f);
-        else
-          sell3_apply<double, double, double, double, MODE_PLAIN, false>(
-              st, t, probe.nb, probe.nchunk, probe.choff, probe.chw, probe.sci, probe.bv64.get(),
-              probe.nslots, x64.get(), (const double *)nullptr, y64.get(), 1.0);
+        for (int k = 0; k < 2; ++k) {
+          if (fp32)
+            sell3_apply<float, float, float, float, MODE_PLAIN, false>(
+                st, t, probe.nb, probe.nchunk, probe.choff, probe.chw, probe.sci,
+                probe.bv32.get(), probe.nslots, x32.get(), (const float *)nullptr, y32.get(),
+                1.0f);
+          else
+            sell3_apply<double, double, double, double, MODE_PLAIN, false>(
+                st, t, probe.nb, probe.nchunk, probe.choff, probe.chw, probe.sci,
+                probe.bv64.get(), probe.nslots, x64.get(), (const double *)nullptr, y64.get(),
+                1.0);
+        }
+        launch_pcg_spmv(st, probe, fp32, p64.get(), p64.get(), q64.get(), part.get(),
+                        tick.get(), sc.get());
       };
       launch();
       float tmin = 1e30f;
@@ -351,6 +368,9 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
         CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         tmin = std::min(tmin, ms);
       }
+      if (std::getenv("CHRONOS_TUNE_VERBOSE"))
+        std::fprintf(stderr, "chronos tune: block form T=%d  %.4f ms per residual pair + outer\n",
+                     t, tmin / 4);
       if (tmin < best) { best = tmin; T = t; }
     }
     cudaEventDestroy(e0);
@@ -696,6 +716,7 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
 // is also the coarsest).
 __global__ void k_dot_store(int n, const double *a, const double *b, double *part,
                             unsigned *ticket, double *out) {
+  pdl_begin();
   double s = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     s += a[i] * b[i];
@@ -713,8 +734,8 @@ static void vcycle_level(Hier &h, int l, const BT *b, OT *out, const double *dw,
   if (L.coarsest) {
     dense_matvec<BT, OT>(n, L.W.get(), b, out, st);
     if (TOP && dw) {
-      k_dot_store<<<std::min(num_sms() * 4, (int)ceil_div(n, 256)), 256, 0, st>>>(
-          n, (const double *)out, dw, part, tick, dot_out);
+      launch_pdl(k_dot_store, std::min(num_sms() * 4, (int)ceil_div(n, 256)), 256, st, n,
+                 (const double *)out, dw, part, tick, dot_out);
       CHRONOS_CHECK_LAUNCH();
     }
     return;
@@ -782,6 +803,7 @@ void Hier::apply_A(const double *x, double *y) {
 // p = pres (first iteration) or p = pres + beta p, beta = -(pres'axp)/ptap.
 __global__ void k_pcg_p_update(int n, const double *__restrict__ pres, double *__restrict__ p,
                                const double *__restrict__ sc) {
+  pdl_begin();
   const bool first = sc[SC_ITER] < 0.5;
   const double beta = first ? 0.0 : -sc[SC_PRES_AXP] / sc[SC_PTAP];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
@@ -815,6 +837,7 @@ k_pcg_spmv(int n, const int *__restrict__ rp, const int *__restrict__ ci,
            const double *__restrict__ res, double *__restrict__ axp, int short_blocks,
            int lthresh, const int *__restrict__ longrows, int nlong, double *part,
            unsigned *ticket, double *sc) {
+  pdl_begin();
   const int lane = threadIdx.x & 31;
   double d0 = 0.0, d1 = 0.0;
   if ((int)blockIdx.x < short_blocks) {
@@ -890,6 +913,7 @@ k_pcg_spmv_sell3(int nb, int nchunk, const int *__restrict__ choff, const int *_
                  const int *__restrict__ sci, const VT *__restrict__ V, int64_t nslots,
                  const double *__restrict__ p, const double *__restrict__ res,
                  double *__restrict__ axp, double *part, unsigned *ticket, double *sc) {
+  pdl_begin();
   constexpr int C = 32 / T;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -944,13 +968,13 @@ static void launch_pcg_spmv(cudaStream_t st, const DMat &A, bool fp32vals, const
 #define CHRONOS_PCGS_CASE(TT)                                                                  \
   case TT:                                                                                     \
     if (fp32vals)                                                                              \
-      k_pcg_spmv_sell3<float, TT><<<grid, kApplyThreads, 0, st>>>(                             \
-          A.nb, A.nchunk, A.choff, A.chw, A.sci, A.bv32.get(), A.nslots, p, res, axp, part,    \
-          tick, sc);                                                                           \
+      launch_pdl(k_pcg_spmv_sell3<float, TT>, grid, kApplyThreads, st, A.nb, A.nchunk,         \
+                 A.choff.get(), A.chw.get(), A.sci.get(), A.bv32.get(), A.nslots, p, res, axp, \
+                 part, tick, sc);                                                              \
     else                                                                                       \
-      k_pcg_spmv_sell3<double, TT><<<grid, kApplyThreads, 0, st>>>(                            \
-          A.nb, A.nchunk, A.choff, A.chw, A.sci, A.bv64.get(), A.nslots, p, res, axp, part,    \
-          tick, sc);                                                                           \
+      launch_pdl(k_pcg_spmv_sell3<double, TT>, grid, kApplyThreads, st, A.nb, A.nchunk,        \
+                 A.choff.get(), A.chw.get(), A.sci.get(), A.bv64.get(), A.nslots, p, res, axp, \
+                 part, tick, sc);                                                              \
     break;
     switch (A.sell_T) {
       CHRONOS_PCGS_CASE(1)
@@ -961,9 +985,9 @@ static void launch_pcg_spmv(cudaStream_t st, const DMat &A, bool fp32vals, const
 #undef CHRONOS_PCGS_CASE
   } else {
 #define CHRONOS_PCG_LAUNCH(VT, VALS, LL, I16)                                                  \
-  k_pcg_spmv<VT, LL, I16><<<grid, kApplyThreads, 0, st>>>(                                     \
-      A.nrows, A.rp, A.ci, A.cbase, A.c16, VALS, p, res, axp, sb, A.lthresh, A.longrows,       \
-      A.nlong, part, tick, sc)
+  launch_pdl(k_pcg_spmv<VT, LL, I16>, grid, kApplyThreads, st, A.nrows, A.rp.get(), A.ci.get(),  \
+             A.cbase.get(), A.c16.get(), VALS, p, res, axp, sb, A.lthresh, A.longrows.get(),    \
+             A.nlong, part, tick, sc)
 #define CHRONOS_PCG_CASE(LL)                                                                   \
   case LL:                                                                                     \
     if (fp32vals) {                                                                            \
@@ -1029,6 +1053,7 @@ k_pcg_xr_update(int n, double *__restrict__ x, double *__restrict__ res,
                 const double *__restrict__ p, const double *__restrict__ axp, double *part,
                 unsigned *ticket, double *sc, double *resvec, cudaGraphConditionalHandle handle,
                 int use_cond, int mixed) {
+  pdl_begin();
   const double alpha = sc[SC_ALPHA];
   double rr = 0.0;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1071,6 +1096,7 @@ k_pcg_replace(int n, const int *__restrict__ rp, const int *__restrict__ ci,
               int lthresh, const int *__restrict__ longrows, int nlong, double *part,
               unsigned *ticket, double *sc, double *resvec, cudaGraphConditionalHandle handle,
               int use_cond) {
+  pdl_begin();
   if (sc[SC_REPLACE] == 0.0) return;
   const int lane = threadIdx.x & 31;
   double rr = 0.0;
@@ -1126,6 +1152,7 @@ k_pcg_replace_sell3(int nb, int nchunk, const int *__restrict__ choff,
                     const double *__restrict__ b, double *__restrict__ res, double *part,
                     unsigned *ticket, double *sc, double *resvec,
                     cudaGraphConditionalHandle handle, int use_cond) {
+  pdl_begin();
   if (sc[SC_REPLACE] == 0.0) return;
   constexpr int C = 32 / T;
   const int lane = threadIdx.x & 31;
@@ -1165,9 +1192,9 @@ static void launch_pcg_replace(cudaStream_t st, const DMat &A, const double *x, 
   if (A.nb > 0) {
 #define CHRONOS_REP3_CASE(TT)                                                                  \
   case TT:                                                                                     \
-    k_pcg_replace_sell3<TT><<<grid, kApplyThreads, 0, st>>>(                                   \
-        A.nb, A.nchunk, A.choff, A.chw, A.sci, A.bv64.get(), A.nslots, x, b, res, part, tick,  \
-        sc, resvec, handle, use_cond);                                                         \
+    launch_pdl(k_pcg_replace_sell3<TT>, grid, kApplyThreads, st, A.nb, A.nchunk,               \
+               A.choff.get(), A.chw.get(), A.sci.get(), A.bv64.get(), A.nslots, x, b, res, part, \
+               tick, sc, resvec, handle, use_cond);                                            \
     break;
     switch (A.sell_T) {
       CHRONOS_REP3_CASE(1)
@@ -1180,13 +1207,13 @@ static void launch_pcg_replace(cudaStream_t st, const DMat &A, const double *x, 
 #define CHRONOS_REP_CASE(LL)                                                                   \
   case LL:                                                                                     \
     if (A.idx16)                                                                               \
-      k_pcg_replace<LL, true><<<grid, kApplyThreads, 0, st>>>(                                 \
-          A.nrows, A.rp, A.ci, A.cbase, A.c16, A.v64.get(), x, b, res, sb, A.lthresh,          \
-          A.longrows, A.nlong, part, tick, sc, resvec, handle, use_cond);                      \
+      launch_pdl(k_pcg_replace<LL, true>, grid, kApplyThreads, st, A.nrows, A.rp.get(),        \
+                 A.ci.get(), A.cbase.get(), A.c16.get(), A.v64.get(), x, b, res, sb, A.lthresh,\
+                 A.longrows.get(), A.nlong, part, tick, sc, resvec, handle, use_cond);         \
     else                                                                                       \
-      k_pcg_replace<LL, false><<<grid, kApplyThreads, 0, st>>>(                                \
-          A.nrows, A.rp, A.ci, A.cbase, A.c16, A.v64.get(), x, b, res, sb, A.lthresh,          \
-          A.longrows, A.nlong, part, tick, sc, resvec, handle, use_cond);                      \
+      launch_pdl(k_pcg_replace<LL, false>, grid, kApplyThreads, st, A.nrows, A.rp.get(),       \
+                 A.ci.get(), A.cbase.get(), A.c16.get(), A.v64.get(), x, b, res, sb, A.lthresh,\
+                 A.longrows.get(), A.nlong, part, tick, sc, resvec, handle, use_cond);         \
     break;
     switch (A.lanes) {
       CHRONOS_REP_CASE(1)
@@ -1222,14 +1249,15 @@ static void capture_iteration(Hier &h, cudaGraphConditionalHandle handle, int us
   double *sc = s.sc.get();
   // pres = M^{-1} res  (with pres'axp for beta)
   h.vcycle(s.res.get(), s.pres.get(), s.axp.get(), sc + SC_PRES_AXP);
-  k_pcg_p_update<<<nb, 256, 0, st>>>(n, s.pres.get(), s.p.get(), sc);
+  launch_pdl(k_pcg_p_update, nb, 256, st, n, (const double *)s.pres.get(), s.p.get(),
+             (const double *)sc);
   CHRONOS_CHECK_LAUNCH();
   unsigned *tk = s.tickets.get();
   launch_pcg_spmv(st, h.levels[0].A, mixed, s.p.get(), s.res.get(), s.axp.get(),
                   s.part.get() + 4 * 3 * 2048, tk + 1, sc);
-  k_pcg_xr_update<<<nb, 256, 0, st>>>(n, s.x.get(), s.res.get(), s.p.get(), s.axp.get(),
-                                       s.part.get() + 8 * 3 * 2048, tk + 2, sc,
-                                       s.resvec.get(), handle, use_cond, mixed ? 1 : 0);
+  launch_pdl(k_pcg_xr_update, nb, 256, st, n, s.x.get(), s.res.get(), (const double *)s.p.get(),
+             (const double *)s.axp.get(), s.part.get() + 8 * 3 * 2048, tk + 2, sc,
+             s.resvec.get(), handle, use_cond, mixed ? 1 : 0);
   CHRONOS_CHECK_LAUNCH();
   if (mixed)
     launch_pcg_replace(st, h.levels[0].A, s.x.get(), s.b.get(), s.res.get(),

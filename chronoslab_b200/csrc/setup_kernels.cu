@@ -493,6 +493,7 @@ void dense_inverse_from_chol(int n, const double *L, double *W, cudaStream_t st)
 template <typename TI, typename TO>
 __global__ void k_dense_matvec(int n, const double *__restrict__ W, const TI *__restrict__ b,
                                TO *__restrict__ x) {
+  pdl_begin();
   const int lane = threadIdx.x & 31;
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (row >= n) return;
@@ -505,7 +506,7 @@ __global__ void k_dense_matvec(int n, const double *__restrict__ W, const TI *__
 
 template <typename TI, typename TO>
 void dense_matvec(int n, const double *W, const TI *b, TO *x, cudaStream_t st) {
-  k_dense_matvec<TI, TO><<<ceil_div((int64_t)n * 32, 256), 256, 0, st>>>(n, W, b, x);
+  launch_pdl(k_dense_matvec<TI, TO>, ceil_div((int64_t)n * 32, 256), 256, st, n, W, b, x);
   CHRONOS_CHECK_LAUNCH();
 }
 template void dense_matvec<float, float>(int, const double *, const float *, float *, cudaStream_t);

@@ -167,6 +167,7 @@ k_sell3_apply(int nb, int nchunk, const int *__restrict__ choff, const int *__re
               const int *__restrict__ sci, const VT *__restrict__ V, int64_t nslots,
               const XT *__restrict__ x, const ZT *z, YT *y, VT alpha,
               const double *__restrict__ dw, double *part, unsigned *ticket, double *dot_out) {
+  pdl_begin();
   constexpr int C = 32 / T;
   const int lane = threadIdx.x & 31;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -220,8 +221,8 @@ void sell3_apply(cudaStream_t st, int T, int nb, int nchunk, const int *choff, c
   if (blocks > cap) blocks = cap;
 #define CHRONOS_SELL_CASE(TT)                                                                  \
   case TT:                                                                                     \
-    k_sell3_apply<VT, XT, ZT, YT, TT, MODE, DOT><<<blocks, kApplyThreads, 0, st>>>(            \
-        nb, nchunk, choff, chw, sci, V, nslots, x, z, y, alpha, dw, part, ticket, dot_out);    \
+    launch_pdl(k_sell3_apply<VT, XT, ZT, YT, TT, MODE, DOT>, blocks, kApplyThreads, st, nb,    \
+               nchunk, choff, chw, sci, V, nslots, x, z, y, alpha, dw, part, ticket, dot_out); \
     break;
   switch (T) {
     CHRONOS_SELL_CASE(1)
@@ -294,6 +295,7 @@ k_csrh_apply(int n, const int *__restrict__ rp, const int *__restrict__ ci,
              const VT *__restrict__ v, const XT *__restrict__ x, const ZT *z, YT *y, VT alpha,
              int short_blocks, int lthresh, const int *__restrict__ longrows, int nlong,
              const double *__restrict__ dw, double *part, unsigned *ticket, double *dot_out) {
+  pdl_begin();
   const int lane = threadIdx.x & 31;
   double dacc = 0.0;
   if ((int)blockIdx.x < short_blocks) {
@@ -364,13 +366,13 @@ void mat_apply(cudaStream_t st, const DMat &M, const VT *v, const XT *x, const Z
 #define CHRONOS_H_CASE(LL)                                                                    \
   case LL:                                                                                    \
     if (M.idx16)                                                                              \
-      k_csrh_apply<VT, XT, ZT, YT, LL, MODE, DOT, true><<<grid, kApplyThreads, 0, st>>>(      \
-          n, M.rp, M.ci, M.cbase, M.c16, v, x, z, y, alpha, sb, M.lthresh, M.longrows,        \
-          M.nlong, dw, part, ticket, dot_out);                                                \
+      launch_pdl(k_csrh_apply<VT, XT, ZT, YT, LL, MODE, DOT, true>, grid, kApplyThreads, st, \
+                 n, M.rp.get(), M.ci.get(), M.cbase.get(), M.c16.get(), v, x, z, y, alpha, sb, \
+                 M.lthresh, M.longrows.get(), M.nlong, dw, part, ticket, dot_out);             \
     else                                                                                      \
-      k_csrh_apply<VT, XT, ZT, YT, LL, MODE, DOT, false><<<grid, kApplyThreads, 0, st>>>(     \
-          n, M.rp, M.ci, M.cbase, M.c16, v, x, z, y, alpha, sb, M.lthresh, M.longrows,        \
-          M.nlong, dw, part, ticket, dot_out);                                                \
+      launch_pdl(k_csrh_apply<VT, XT, ZT, YT, LL, MODE, DOT, false>, grid, kApplyThreads, st,\
+                 n, M.rp.get(), M.ci.get(), M.cbase.get(), M.c16.get(), v, x, z, y, alpha, sb, \
+                 M.lthresh, M.longrows.get(), M.nlong, dw, part, ticket, dot_out);             \
     break;
   switch (L) {
     CHRONOS_H_CASE(1)
