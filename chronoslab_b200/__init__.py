@@ -308,7 +308,8 @@ class Hierarchy:
         check(self._lib.chronos_hier_level_info(self._h, level, C.byref(info)))
         return {"n": info.n, "nnz_A": info.nnz_A, "nnz_G": info.nnz_G, "nnz_P": info.nnz_P,
                 "nc": info.nc, "omega": info.omega, "lambda": info.lambda_,
-                "threads_per_row": info.threads_per_row, "block_rows": info.block_rows}
+                "threads_per_row": info.threads_per_row, "block_rows": info.block_rows,
+                "sell_mask": info.sell_mask}
 
     def export(self, level, which):
         nr, ncl, nnz = C.c_int(), C.c_int(), C.c_int64()

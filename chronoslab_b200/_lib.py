@@ -43,7 +43,7 @@ class chronos_params(C.Structure):
         ("restart", C.c_int),
         ("precision", C.c_int), ("use_graph", C.c_int), ("seed", C.c_uint64),
         ("fsai_fabs", C.c_int), ("use_bsr", C.c_int), ("exact_outer", C.c_int),
-        ("replace_ratio", C.c_double),
+        ("replace_ratio", C.c_double), ("spmv_format", C.c_int),
     ]
 
 
@@ -51,7 +51,7 @@ class chronos_level_info(C.Structure):
     _fields_ = [("n", C.c_int), ("nnz_A", C.c_int64), ("nnz_G", C.c_int64),
                 ("nnz_P", C.c_int64), ("nc", C.c_int), ("omega", C.c_double),
                 ("lambda_", C.c_double), ("threads_per_row", C.c_int),
-                ("block_rows", C.c_int)]
+                ("block_rows", C.c_int), ("sell_mask", C.c_int)]
 
 
 class chronos_profile(C.Structure):

@@ -423,6 +423,8 @@ int chronos_hier_level_info(const chronos_hier *h, int level, chronos_level_info
     info->lambda = L.lambda;
     info->threads_per_row = L.A.nb > 0 ? 1 : L.A.lanes;   // block form: a thread per block row
     info->block_rows = L.A.nb;
+    info->sell_mask = (L.A.use_sell ? 1 : 0) | (L.G.use_sell ? 2 : 0) | (L.Gt.use_sell ? 4 : 0) |
+                      (L.P.use_sell ? 8 : 0) | (L.Pt.use_sell ? 16 : 0);
   });
 }
 

@@ -101,18 +101,108 @@ int heuristic_lanes(const DMat &m) {
   return L;
 }
 
-void set_lanes(DMat &m, int L, cudaStream_t st) {
-  m.lanes = L;
-  m.lthresh = long_row_threshold(L);
+// Rows longer than thresh go to the warp path (both apply forms read the list).
+static void set_long_rows(DMat &m, int thresh, cudaStream_t st) {
+  m.lthresh = thresh;
   std::vector<int> rows;
-  if (m.lthresh < 0x7fffffff)
+  if (thresh < 0x7fffffff)
     for (int i = 0; i < m.nrows; ++i)
-      if (m.rp_h[i + 1] - m.rp_h[i] > m.lthresh) rows.push_back(i);
+      if (m.rp_h[i + 1] - m.rp_h[i] > thresh) rows.push_back(i);
   m.nlong = (int)rows.size();
   if (m.nlong) {
     m.longrows.upload(rows, st);
     CHRONOS_CUDA(cudaStreamSynchronize(st));
   }
+}
+
+void set_lanes(DMat &m, int L, cudaStream_t st) {
+  m.lanes = L;
+  set_long_rows(m, long_row_threshold(L), st);
+}
+
+// Bytes written between timed launches of the autotuners (more than L2).
+constexpr size_t kL2FlushBytes = 256u << 20;
+
+// Rows longer than this are left out of the sliced ELL chunks.
+constexpr int kSellLongRow = 32;
+
+// Builds the sliced ELL form (DMat::use_sell) from the matrix's final values.
+// Returns false (nothing attached) when the slot count does not fit int32.
+static bool build_sell(DMat &m, bool fp32, cudaStream_t st) {
+  const int n = m.nrows;
+  const std::vector<int> ci = m.ci.to_host(st);
+  const std::vector<double> v = m.v64.to_host(st);
+  auto len = [&](int i) { return m.rp_h[i + 1] - m.rp_h[i]; };
+  // chunks in row order (output accesses stay coalesced); the padding to each
+  // chunk's longest row is part of what the autotuner times
+  std::vector<int> order;
+  order.reserve(n);
+  for (int i = 0; i < n; ++i)
+    if (len(i) <= kSellLongRow) order.push_back(i);
+  const int nch = (int)((order.size() + 31) / 32);
+  std::vector<int> choff(nch + 1, 0), chw(nch, 0), cbase(nch, 0), perm((size_t)nch * 32, -1);
+  int64_t tot = 0;
+  bool fits16 = true;
+  for (int c = 0; c < nch; ++c) {
+    int w = 0, lo = 0x7fffffff, hi = -1;
+    for (int l = 0; l < 32 && 32 * (size_t)c + l < order.size(); ++l) {
+      const int row = order[32 * (size_t)c + l];
+      perm[32 * (size_t)c + l] = row;
+      w = std::max(w, len(row));
+      for (int k = m.rp_h[row]; k < m.rp_h[row + 1]; ++k) {
+        lo = std::min(lo, ci[k]);
+        hi = std::max(hi, ci[k]);
+      }
+    }
+    cbase[c] = hi >= 0 ? lo : 0;
+    if (hi >= 0 && hi - lo > 0xffff) fits16 = false;
+    choff[c] = (int)tot;
+    chw[c] = w;
+    tot += 32LL * w;
+    if (tot >= INT32_MAX) return false;
+  }
+  choff[nch] = (int)tot;
+  std::vector<double> sv(std::max<int64_t>(tot, 1), 0.0);
+  std::vector<int> sci;
+  std::vector<uint16_t> s16;
+  if (fits16) s16.assign(std::max<int64_t>(tot, 1), 0);
+  else sci.assign(std::max<int64_t>(tot, 1), 0);
+  for (int c = 0; c < nch; ++c)
+    for (int l = 0; l < 32; ++l) {
+      const int row = perm[32 * (size_t)c + l];
+      if (row < 0) continue;
+      for (int j = 0; j < len(row); ++j) {
+        const int64_t k = choff[c] + 32LL * j + l;
+        const int e = m.rp_h[row] + j;
+        sv[k] = v[e];
+        if (fits16) s16[k] = (uint16_t)(ci[e] - cbase[c]);
+        else sci[k] = ci[e];
+      }
+    }
+  m.s_nchunk = nch;
+  m.sell16 = fits16;
+  m.s_choff.upload(choff, st);
+  m.s_chw.upload(chw, st);
+  m.s_cbase.upload(cbase, st);
+  m.s_perm.upload(perm, st);
+  if (fits16) { m.s_c16.upload(s16, st); m.s_ci.release(); }
+  else { m.s_ci.upload(sci, st); m.s_c16.release(); }
+  m.s_v64.upload(sv, st);
+  if (fp32) {
+    m.s_v32.alloc(sv.size());
+    convert_f64_to_f32((int64_t)sv.size(), m.s_v64.get(), m.s_v32.get(), st);
+  }
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  return true;
+}
+
+static void drop_sell(DMat &m) {
+  m.use_sell = false;
+  m.s_nchunk = 0;
+  for (auto *b : {&m.s_choff, &m.s_chw, &m.s_cbase, &m.s_perm, &m.s_ci}) b->release();
+  m.s_c16.release();
+  m.s_v64.release();
+  m.s_v32.release();
 }
 
 
@@ -165,9 +255,11 @@ void tune_store_locked(const TuneKey &k, int L) {
 
 }  // namespace
 
-void autotune_lanes(DMat &m, bool fp32, cudaStream_t st) {
+void autotune_lanes(DMat &m, bool fp32, cudaStream_t st, int format) {
   if (m.nrows <= 0) return;
-  // 'H': the hybrid CSR kernel (k_csrh_apply); the index width is part of the shape
+  // 'H': the hybrid CSR kernel (k_csrh_apply); the index width is part of the
+  // shape.  A cached value >= 100 means the sliced ELL form with lanes - 100
+  // for the CSR paths.
   const TuneKey key(m.idx16 ? 'h' : 'H', m.nrows, m.nnz, m.ncols, fp32);
   int L = -1;
   {
@@ -176,6 +268,7 @@ void autotune_lanes(DMat &m, bool fp32, cudaStream_t st) {
     auto it = g_tune.find(key);
     if (it != g_tune.end()) L = it->second;
   }
+  const bool verbose = std::getenv("CHRONOS_TUNE_VERBOSE") != nullptr;
   if (L < 0) {
     L = heuristic_lanes(m);
     if (m.nnz >= 4096) {                    // below: launch-latency bound, keep the heuristic
@@ -186,30 +279,51 @@ void autotune_lanes(DMat &m, bool fp32, cudaStream_t st) {
       cudaEvent_t e0, e1;
       CHRONOS_CUDA(cudaEventCreate(&e0));
       CHRONOS_CUDA(cudaEventCreate(&e1));
-      float best = 1e30f;
-      for (int cand : {1, 2, 4, 8, 16, 32}) {
-        set_lanes(m, cand, st);
-        auto launch = [&] {
-          if (fp32)
-            mat_apply<float, float, float, float, MODE_PLAIN, false>(st, m, m.v32.get(), x32.get(),
-                                                                    (const float *)nullptr,
-                                                                    y32.get(), 1.0f);
-          else
-            mat_apply<double, double, double, double, MODE_PLAIN, false>(
-                st, m, m.v64.get(), x64.get(), (const double *)nullptr, y64.get(), 1.0);
-        };
+      auto launch = [&] {
+        if (fp32)
+          mat_apply<float, float, float, float, MODE_PLAIN, false>(st, m, m.v32.get(), x32.get(),
+                                                                  (const float *)nullptr,
+                                                                  y32.get(), 1.0f);
+        else
+          mat_apply<double, double, double, double, MODE_PLAIN, false>(
+              st, m, m.v64.get(), x64.get(), (const double *)nullptr, y64.get(), 1.0);
+      };
+      // In the V-cycle an operator is read after larger ones have passed
+      // through L2, so each timed launch starts from a flushed L2.
+      DBuf<char> flush(kL2FlushBytes);
+      auto time_it = [&] {
         launch();
         float tmin = 1e30f;
-        for (int r = 0; r < 3; ++r) {
+        for (int r = 0; r < 5; ++r) {
+          CHRONOS_CUDA(cudaMemsetAsync(flush.get(), r, kL2FlushBytes, st));
           CHRONOS_CUDA(cudaEventRecord(e0, st));
-          for (int q = 0; q < 4; ++q) launch();
+          launch();
           CHRONOS_CUDA(cudaEventRecord(e1, st));
           CHRONOS_CUDA(cudaEventSynchronize(e1));
           float ms = 0;
           CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
           tmin = std::min(tmin, ms);
         }
-        if (tmin < best) { best = tmin; L = cand; }
+        return tmin * 4;          // per four launches, as reported below
+      };
+      float best = 1e30f;
+      for (int cand : {1, 2, 4, 8, 16, 32}) {
+        set_lanes(m, cand, st);
+        const float t = time_it();
+        if (verbose)
+          std::fprintf(stderr, "chronos tune: csr %d x %d (%lld) lanes %d  %.4f ms\n", m.nrows,
+                       m.ncols, (long long)m.nnz, cand, t / 4);
+        if (t < best) { best = t; L = cand; }
+      }
+      if (format == 0 && (double)m.nnz <= 16.0 * m.nrows && build_sell(m, fp32, st)) {
+        m.use_sell = true;
+        set_long_rows(m, kSellLongRow, st);
+        const float t = time_it();
+        if (verbose)
+          std::fprintf(stderr, "chronos tune: csr %d x %d (%lld) sliced ELL  %.4f ms\n",
+                       m.nrows, m.ncols, (long long)m.nnz, t / 4);
+        if (t < best) L += 100;
+        drop_sell(m);
       }
       cudaEventDestroy(e0);
       cudaEventDestroy(e1);
@@ -217,7 +331,15 @@ void autotune_lanes(DMat &m, bool fp32, cudaStream_t st) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     tune_store_locked(key, L);
   }
-  set_lanes(m, L, st);
+  if (format == 1 && L >= 100) L -= 100;
+  if (format == 2 && L < 100 && (double)m.nnz <= 16.0 * m.nrows) L += 100;
+  if (L >= 100 && build_sell(m, fp32, st)) {
+    m.use_sell = true;
+    m.lanes = L - 100;
+    set_long_rows(m, kSellLongRow, st);
+  } else {
+    set_lanes(m, L >= 100 ? L - 100 : L, st);
+  }
 }
 
 // Sliced 3x3 block form of a CSR matrix whose row triples share a pattern of
@@ -330,6 +452,7 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
         sc(SC_COUNT);
     DBuf<float> x32(A.ncols), y32(A.nrows);
     DBuf<unsigned> tick(1);
+    DBuf<char> flush(kL2FlushBytes);
     x64.zero(st);
     x32.zero(st);
     p64.zero(st);
@@ -360,13 +483,14 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
       launch();
       float tmin = 1e30f;
       for (int r = 0; r < 3; ++r) {
+        CHRONOS_CUDA(cudaMemsetAsync(flush.get(), r, kL2FlushBytes, st));
         CHRONOS_CUDA(cudaEventRecord(e0, st));
-        for (int q = 0; q < 4; ++q) launch();
+        launch();
         CHRONOS_CUDA(cudaEventRecord(e1, st));
         CHRONOS_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        tmin = std::min(tmin, ms);
+        tmin = std::min(tmin, 4 * ms);
       }
       if (std::getenv("CHRONOS_TUNE_VERBOSE"))
         std::fprintf(stderr, "chronos tune: block form T=%d  %.4f ms per residual pair + outer\n",
@@ -693,16 +817,17 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
   }
   // SpMV lane counts
   for (auto &L : h->levels) {
-    autotune_lanes(L.A, fp32, st);
+    const int fmt = prm.spmv_format;
+    autotune_lanes(L.A, fp32, st, fmt);
     if (!L.coarsest) {
-      autotune_lanes(L.G, fp32, st);
-      autotune_lanes(L.Gt, fp32, st);
-      autotune_lanes(L.P, fp32, st);
-      autotune_lanes(L.Pt, fp32, st);
+      autotune_lanes(L.G, fp32, st, fmt);
+      autotune_lanes(L.Gt, fp32, st, fmt);
+      autotune_lanes(L.P, fp32, st, fmt);
+      autotune_lanes(L.Pt, fp32, st, fmt);
     }
   }
   // the level-1 FP64 operator of the outer PCG
-  if (fp32) autotune_lanes(h->levels[0].A, false, st);
+  if (fp32 && prm.exact_outer) autotune_lanes(h->levels[0].A, false, st);
   CHRONOS_CUDA(cudaStreamSynchronize(st));
   T[7] = now_s() - t_start;
   return h;

@@ -102,7 +102,9 @@ void params_read(const char *fnames_path, chronos_params *p);
 // Upload a host CSR (FP64) to a device matrix, with FP32 values when fp32.
 void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st);
 // SpMV lane count by timing the candidates (cached per shape).
-void autotune_lanes(DMat &m, bool fp32, cudaStream_t st);
+// format: 0 tuned (row-grouped CSR or sliced ELL), 1 CSR only, 2 sliced ELL
+// whenever the rows average at most 16 entries.
+void autotune_lanes(DMat &m, bool fp32, cudaStream_t st, int format = 0);
 // Lanes per row from the mean row length; setting the lanes also rebuilds the
 // matrix's long-row list.
 int heuristic_lanes(const DMat &m);

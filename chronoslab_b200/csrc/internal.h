@@ -30,6 +30,20 @@ struct DMat {
   // longrows); the others by groups of `lanes` lanes.
   int lthresh = 0x7fffffff, nlong = 0;
   DBuf<int> longrows;
+  // Sliced ELL form for short rows (use_sell; chosen by the autotuner):
+  // chunks of 32 rows taken in the order s_perm (row order, the long rows
+  // left out; -1 pads the last chunk), slot-major
+  // (slot j of chunk row l at s_choff[c] + 32 j + l), chunk widths s_chw;
+  // columns as 16-bit offsets from the chunk's smallest column (s_cbase) when
+  // every chunk spans fewer than 65536 columns (sell16), else int32 (s_ci);
+  // padding slots hold value 0 and offset 0.  Rows longer than lthresh stay
+  // on the warp path (longrows).
+  bool use_sell = false, sell16 = false;
+  int s_nchunk = 0;
+  DBuf<int> s_choff, s_chw, s_cbase, s_perm, s_ci;
+  DBuf<uint16_t> s_c16;
+  DBuf<double> s_v64;
+  DBuf<float> s_v32;
   // Optional sliced 3x3 block form of the same matrix (chunks of 32 block
   // rows, slot-major, plane-major values), used when every row triple shares
   // a pattern of whole aligned 3x3 blocks.

@@ -344,6 +344,96 @@ k_csrh_apply(int n, const int *__restrict__ rp, const int *__restrict__ ci,
   }
 }
 
+// Sliced ELL apply (see DMat::use_sell): a warp per chunk of 32 rows, lane l
+// owns chunk row l and walks its slots with coalesced 128-byte (values) and
+// 64-byte (16-bit offsets) warp loads, four slots' loads in flight before
+// the gathers; each row's entries are summed in CSR order.  Rows longer than
+// the threshold are applied by whole warps from the CSR arrays in a second
+// range of blocks.
+template <typename VT, typename XT, typename ZT, typename YT, int MODE, bool DOT, bool I16>
+__global__ void __launch_bounds__(kApplyThreads)
+k_sell_apply(int nchunk, const int *__restrict__ choff, const int *__restrict__ chw,
+             const int *__restrict__ cbase, const int *__restrict__ perm,
+             const int *__restrict__ sci, const uint16_t *__restrict__ sc16,
+             const VT *__restrict__ sv, const int *__restrict__ rp, const int *__restrict__ ci,
+             const VT *__restrict__ v, const XT *__restrict__ x, const ZT *z, YT *y, VT alpha,
+             int short_blocks, const int *__restrict__ longrows, int nlong,
+             const double *__restrict__ dw, double *part, unsigned *ticket, double *dot_out) {
+  pdl_begin();
+  const int lane = threadIdx.x & 31;
+  double dacc = 0.0;
+  if ((int)blockIdx.x < short_blocks) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (short_blocks * blockDim.x) >> 5;
+    for (int c = warp; c < nchunk; c += nwarps) {
+      const int off = __ldg(choff + c) + lane, w = __ldg(chw + c);
+      const int cb = I16 ? __ldg(cbase + c) : 0;
+      const int row = __ldg(perm + 32 * c + lane);
+      VT acc = VT(0);
+      int j = 0;
+      for (; j + 3 < w; j += 4) {
+        int col[4];
+        VT a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int k = off + 32 * (j + u);
+          col[u] = I16 ? cb + (int)__ldg(sc16 + k) : __ldg(sci + k);
+          a[u] = __ldg(sv + k);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc += a[u] * (VT)__ldg(x + col[u]);
+      }
+      {
+        int col[3];
+        VT a[3];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          col[u] = -1;
+          a[u] = VT(0);
+          if (j + u < w) {
+            const int k = off + 32 * (j + u);
+            col[u] = I16 ? cb + (int)__ldg(sc16 + k) : __ldg(sci + k);
+            a[u] = __ldg(sv + k);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+          if (col[u] >= 0) acc += a[u] * (VT)__ldg(x + col[u]);
+      }
+      if (row >= 0) {
+        const YT out = (YT)apply_epilogue<VT, MODE>(acc, alpha, z, row);
+        y[row] = out;
+        if (DOT) dacc += (double)out * dw[row];
+      }
+    }
+  } else {
+    const int warp = ((blockIdx.x - short_blocks) * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = ((gridDim.x - short_blocks) * blockDim.x) >> 5;
+    for (int i = warp; i < nlong; i += nwarps) {
+      const int row = __ldg(longrows + i);
+      const int s = __ldg(rp + row), e = __ldg(rp + row + 1);
+      VT a = csr_row_dot<VT, VT, XT, 32, false>(s + lane, e, 0, ci, nullptr, v, x);
+      a = warp_sum(a);
+      if (lane == 0) {
+        const YT out = (YT)apply_epilogue<VT, MODE>(a, alpha, z, row);
+        y[row] = out;
+        if (DOT) dacc += (double)out * dw[row];
+      }
+    }
+  }
+  if (DOT) {
+    double vals[1] = {dacc};
+    grid_reduce<1>(vals, part, ticket, StoreScalar{dot_out});
+  }
+}
+
+template <typename VT> inline const VT *sell_vals(const DMat &m);
+template <> inline const float *sell_vals<float>(const DMat &m) { return m.s_v32.get(); }
+template <> inline const double *sell_vals<double>(const DMat &m) { return m.s_v64.get(); }
+template <typename VT> inline const VT *csr_vals(const DMat &m);
+template <> inline const float *csr_vals<float>(const DMat &m) { return m.v32.get(); }
+template <> inline const double *csr_vals<double>(const DMat &m) { return m.v64.get(); }
+
 // Long-row threshold for `lanes`-lane groups: rows longer than 16 entries per
 // lane go to whole warps.
 inline int long_row_threshold(int lanes) { return lanes >= 32 ? 0x7fffffff : 16 * lanes; }
@@ -361,6 +451,21 @@ void mat_apply(cudaStream_t st, const DMat &M, const VT *v, const XT *x, const Z
   const int cap = num_sms() * 8;
   const int wpb = kApplyThreads / 32;
   int lb = M.nlong > 0 ? (int)std::min<int64_t>(ceil_div(M.nlong, wpb), cap / 4) : 0;
+  if (M.use_sell) {
+    const int sb = (int)std::min<int64_t>(ceil_div(M.s_nchunk, wpb), cap - lb);
+    const VT *sv = sell_vals<VT>(M), *cv = csr_vals<VT>(M);
+    if (M.sell16)
+      launch_pdl(k_sell_apply<VT, XT, ZT, YT, MODE, DOT, true>, sb + lb, kApplyThreads, st,
+                 M.s_nchunk, M.s_choff.get(), M.s_chw.get(), M.s_cbase.get(), M.s_perm.get(),
+                 M.s_ci.get(), M.s_c16.get(), sv, M.rp.get(), M.ci.get(), cv, x, z, y, alpha, sb,
+                 M.longrows.get(), M.nlong, dw, part, ticket, dot_out);
+    else
+      launch_pdl(k_sell_apply<VT, XT, ZT, YT, MODE, DOT, false>, sb + lb, kApplyThreads, st,
+                 M.s_nchunk, M.s_choff.get(), M.s_chw.get(), M.s_cbase.get(), M.s_perm.get(),
+                 M.s_ci.get(), M.s_c16.get(), sv, M.rp.get(), M.ci.get(), cv, x, z, y, alpha, sb,
+                 M.longrows.get(), M.nlong, dw, part, ticket, dot_out);
+    return;
+  }
   int sb = (int)std::min<int64_t>(ceil_div(n, kApplyThreads / L), cap - lb);
   const int grid = sb + lb;
 #define CHRONOS_H_CASE(LL)                                                                    \

@@ -107,6 +107,10 @@ typedef struct chronos_params {
                                      every stop; the returned relative residual is then the
                                      true one.  No effect for CHRONOS_FP64 hierarchies. */
   double replace_ratio;           /* 0.01 (default), in (0, 1) */
+  int spmv_format;                /* storage of the V-cycle's CSR operators: 0 (default) the
+                                     autotuner's choice per operator; 1 row-grouped CSR only;
+                                     2 sliced ELL for every operator averaging at most 16
+                                     entries per row */
 } chronos_params;
 
 /* Reference regression-test parameters (Tests/parm_*): DOM 0.01, BAMG/NONE,
@@ -228,6 +232,7 @@ typedef struct chronos_level_info {
   double omega, lambda; /* smoother damping and lambda_max(G A G') */
   int threads_per_row;  /* SpMV lanes per row chosen by the autotuner for A */
   int block_rows;       /* > 0: A is applied in 3x3 block form with this many block rows */
+  int sell_mask;        /* bits 0-4: A, G, G', P, P' applied in sliced ELL form */
 } chronos_level_info;
 
 /* Builds the hierarchy of A (0-based CSR, FP64, host memory) with the test

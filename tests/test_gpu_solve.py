@@ -217,3 +217,23 @@ def test_outer_replacement_itmax_and_warm_start(lib, elast):
         xs, _, _, _, _ = h.pcg(b, itmax=500, tol=1e-8)
         x3, it3, _, flag3, _ = h.pcg(b, x0=xs, itmax=500, tol=1e-8)
         assert it3 == 1 and flag3 == 0
+
+
+@pytest.mark.parametrize("prec,tol", [(cb.CHRONOS_FP64, 1e-12), (cb.CHRONOS_FP32, 2e-5)])
+@pytest.mark.parametrize("case", ["elast", "poisson"])
+def test_sliced_ell_matches_csr(lib, case, prec, tol, request):
+    """The sliced ELL form of the short-row operators (G, G', P and the
+    7-point A) gives the row-grouped CSR results."""
+    A, TV, b = request.getfixturevalue(case)
+    ntv = TV.shape[1]
+    with cb.Hierarchy(A, TV, cb.params(precision=prec, ntv=ntv, spmv_format=2)) as he, \
+            cb.Hierarchy(A, TV, cb.params(precision=prec, ntv=ntv, spmv_format=1)) as hc:
+        assert he.level_info(0)["sell_mask"] & 0b01110       # G, G', P at level 1
+        assert hc.level_info(0)["sell_mask"] == 0
+        if case == "poisson":
+            assert he.level_info(0)["sell_mask"] & 1         # the 7-point operator itself
+        assert rel(he.vcycle(b), hc.vcycle(b)) <= tol
+        xe, ite, _, fe, _ = he.pcg(b, itmax=500, tol=1e-8)
+        xc, itc, _, fc, _ = hc.pcg(b, itmax=500, tol=1e-8)
+        assert fe == 0 and fc == 0 and abs(ite - itc) <= 1
+        assert np.linalg.norm(b - A @ xe) / np.linalg.norm(b) <= 1e-8
