@@ -105,9 +105,13 @@ int heuristic_lanes(const DMat &m) {
 static void set_long_rows(DMat &m, int thresh, cudaStream_t st) {
   m.lthresh = thresh;
   std::vector<int> rows;
+  m.nnz_long = 0;
   if (thresh < 0x7fffffff)
     for (int i = 0; i < m.nrows; ++i)
-      if (m.rp_h[i + 1] - m.rp_h[i] > thresh) rows.push_back(i);
+      if (m.rp_h[i + 1] - m.rp_h[i] > thresh) {
+        rows.push_back(i);
+        m.nnz_long += m.rp_h[i + 1] - m.rp_h[i];
+      }
   m.nlong = (int)rows.size();
   if (m.nlong) {
     m.longrows.upload(rows, st);
@@ -1076,7 +1080,7 @@ static int pcg_grid(const DMat &A, int *short_blocks) {
     *short_blocks = 0;
     return std::min(cap, (int)ceil_div(A.nchunk, kApplyThreads / 32));
   }
-  const int lb = A.nlong > 0 ? std::min<int>(ceil_div(A.nlong, kApplyThreads / 32), cap / 4) : 0;
+  const int lb = long_blocks(A, cap);
   const int sb = std::min<int>(ceil_div(A.nrows, kApplyThreads / A.lanes), cap - lb);
   *short_blocks = sb;
   return sb + lb;

@@ -29,6 +29,7 @@ struct DMat {
   // Rows longer than lthresh are applied by whole warps (listed in
   // longrows); the others by groups of `lanes` lanes.
   int lthresh = 0x7fffffff, nlong = 0;
+  int64_t nnz_long = 0;     // entries in the long rows
   DBuf<int> longrows;
   // Sliced ELL form for short rows (use_sell; chosen by the autotuner):
   // chunks of 32 rows taken in the order s_perm (row order, the long rows

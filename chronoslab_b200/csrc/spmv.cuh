@@ -17,6 +17,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cmath>
 
 #include "common.cuh"
 #include "internal.h"
@@ -438,6 +439,20 @@ template <> inline const double *csr_vals<double>(const DMat &m) { return m.v64.
 // lane go to whole warps.
 inline int long_row_threshold(int lanes) { return lanes >= 32 ? 0x7fffffff : 16 * lanes; }
 
+// Blocks of a grid of `cap` given to the long rows: their share of the
+// entries (at least one warp per 8 long rows' worth, at most half the grid,
+// never more than one warp per long row).
+inline int long_blocks(const DMat &M, int cap) {
+  if (M.nlong <= 0) return 0;
+  const int wpb = kApplyThreads / 32;
+  const double share = M.nnz > 0 ? (double)M.nnz_long / (double)M.nnz : 0.0;
+  int lb = (int)std::ceil(share * cap);
+  lb = std::max(lb, (int)std::min<int64_t>(ceil_div(M.nlong, 8 * wpb), cap / 4));
+  lb = std::min(lb, cap / 2);
+  lb = std::min<int64_t>(lb, ceil_div(M.nlong, wpb));
+  return std::max(lb, 1);
+}
+
 // Apply of a device matrix through k_csrh_apply with its tuned lanes, long-row
 // list and index width.  At most num_sms()*8 blocks (the reduction partial
 // buffers hold 2048 per slot).
@@ -450,7 +465,7 @@ void mat_apply(cudaStream_t st, const DMat &M, const VT *v, const XT *x, const Z
   const int L = M.lanes;
   const int cap = num_sms() * 8;
   const int wpb = kApplyThreads / 32;
-  int lb = M.nlong > 0 ? (int)std::min<int64_t>(ceil_div(M.nlong, wpb), cap / 4) : 0;
+  const int lb = long_blocks(M, cap);
   if (M.use_sell) {
     const int sb = (int)std::min<int64_t>(ceil_div(M.s_nchunk, wpb), cap - lb);
     const VT *sv = sell_vals<VT>(M), *cv = csr_vals<VT>(M);
