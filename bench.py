@@ -57,6 +57,8 @@ def parse():
 def run_profile_solve(args):
     import torch
     import chronoslab_b200 as cb
+    if args.workload == "c3":
+        return run_profile_block(args)
     A, TV, b = build_problem(args.ne, seed=0)
     prec = cb.CHRONOS_FP32 if args.profile_solve == "fp32" else cb.CHRONOS_FP64
     # ncu cannot profile the kernel nodes of a graph holding a conditional
@@ -77,6 +79,30 @@ def run_profile_solve(args):
                       "flag": flag, "ms": sec * 1e3, "levels": [h.level_info(l)
                                                                 for l in range(h.nlevels)]}))
     h.close()
+    return 0
+
+
+def run_profile_block(args):
+    """One block solve of the c3 workload (16 right-hand sides) bracketed by
+    the profiler range, its iterations launched from a host loop."""
+    import numpy as np
+    import torch
+    import chronoslab_b200 as cb
+    from chronoslab_b200 import problems as PB
+    ne = 128 if args.ne == 80 else args.ne
+    A, _ = PB.diffusion7(ne, sigma=2.0, corr_len=8.0, zaniso=0.01, seed=0)
+    B = PB.uniform_rhs(A.shape[0], seed=1, ncols=16)
+    prec = cb.CHRONOS_FP32 if args.profile_solve == "fp32" else cb.CHRONOS_FP64
+    with cb.Hierarchy(A, np.ones(A.shape[0]), cb.params(precision=prec, ntv=1, use_graph=0)) as h:
+        h.pcg_block(B, itmax=args.itmax, tol=args.tol)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        X, its, fl, sec = h.pcg_block(B, itmax=args.itmax, tol=args.tol)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_solve": args.profile_solve, "workload": "c3", "ne": ne,
+                          "iterations": its.tolist(), "ms": sec * 1e3,
+                          "levels": [h.level_info(l) for l in range(h.nlevels)]}))
     return 0
 
 

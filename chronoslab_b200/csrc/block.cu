@@ -78,7 +78,21 @@ k_csr_spmm(int n, const int *__restrict__ rp, const int *__restrict__ ci,
 #pragma unroll
       for (int e = 0; e < VEC; ++e) s[e] = VT(0);
       const int e1 = __ldg(rp + row + 1);
-      for (int k = __ldg(rp + row); k < e1; ++k) {
+      int k = __ldg(rp + row);
+      for (; k + 3 < e1; k += 4) {            // four entries' loads in flight
+        int c[4];
+        VT a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) { c[u] = __ldg(ci + k + u); a[u] = __ldg(v + k + u); }
+        XT xv[4][VEC];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) Vec<XT, VEC>::ld(X + (size_t)c[u] * K + j0, xv[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) s[e] += a[u] * (VT)xv[u][e];
+      }
+      for (; k < e1; ++k) {
         const VT a = __ldg(v + k);
         XT xv[VEC];
         Vec<XT, VEC>::ld(X + (size_t)__ldg(ci + k) * K + j0, xv);
@@ -103,15 +117,10 @@ k_csr_spmm(int n, const int *__restrict__ rp, const int *__restrict__ ci,
     }
   }
   if (DOT) {
-    double vals[K];
+    double vals[1][VEC];
 #pragma unroll
-    for (int q = 0; q < K; ++q) vals[q] = 0.0;
-#pragma unroll
-    for (int e = 0; e < VEC; ++e)
-#pragma unroll
-      for (int q = 0; q < K; ++q)
-        if (q == j0 + e) vals[q] = dacc[e];
-    grid_reduce<K>(vals, part, ticket, StoreK<K>{dot_out});
+    for (int e = 0; e < VEC; ++e) vals[0][e] = dacc[e];
+    grid_reduce_cols<K, VEC, 1>(vals, part, ticket, StoreK<K>{dot_out});
   }
 }
 
@@ -286,12 +295,38 @@ k_bpcg_spmm(int n, const int *__restrict__ rp, const int *__restrict__ ci,
     if (row < n) {
       double s[2] = {0.0, 0.0};
       const int e1 = __ldg(rp + row + 1);
-      for (int k = __ldg(rp + row); k < e1; ++k) {
-        const double a = __ldg(v + k);
-        double pv[2];
-        Vec<double, 2>::ld(p + (size_t)__ldg(ci + k) * K + j0, pv);
-        s[0] += a * pv[0];
-        s[1] += a * pv[1];
+      int k = __ldg(rp + row);
+      for (; k + 3 < e1; k += 4) {            // four entries' loads in flight
+        int c[4];
+        double a[4], pv[4][2];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) { c[u] = __ldg(ci + k + u); a[u] = __ldg(v + k + u); }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) Vec<double, 2>::ld(p + (size_t)c[u] * K + j0, pv[u]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          s[0] += a[u] * pv[u][0];
+          s[1] += a[u] * pv[u][1];
+        }
+      }
+      if (k < e1) {                            // the last 1..3 entries, loads predicated
+        int c[3];
+        double a[3], pv[3][2];
+#pragma unroll
+        for (int u = 0; u < 3; ++u) {
+          c[u] = -1;
+          a[u] = 0.0;
+          if (k + u < e1) { c[u] = __ldg(ci + k + u); a[u] = __ldg(v + k + u); }
+        }
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+          if (c[u] >= 0) Vec<double, 2>::ld(p + (size_t)c[u] * K + j0, pv[u]);
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+          if (c[u] >= 0) {
+            s[0] += a[u] * pv[u][0];
+            s[1] += a[u] * pv[u][1];
+          }
       }
       const size_t o = (size_t)row * K + j0;
       Vec<double, 2>::st(axp + o, s);
@@ -304,13 +339,8 @@ k_bpcg_spmm(int n, const int *__restrict__ rp, const int *__restrict__ ci,
       }
     }
   }
-  double vals[2 * K];
-#pragma unroll
-  for (int q = 0; q < K; ++q) {
-    vals[q] = (q == j0) ? d0[0] : (q == j0 + 1) ? d0[1] : 0.0;
-    vals[K + q] = (q == j0) ? d1[0] : (q == j0 + 1) ? d1[1] : 0.0;
-  }
-  grid_reduce<2 * K>(vals, part, ticket, FinAlphaBlock<K>{sc});
+  double vals[2][2] = {{d0[0], d0[1]}, {d1[0], d1[1]}};
+  grid_reduce_cols<K, 2, 2>(vals, part, ticket, FinAlphaBlock<K>{sc});
 }
 
 template <int K> struct FinResidualBlock {
@@ -357,10 +387,8 @@ k_bpcg_xr_update(int n, double *__restrict__ x, double *__restrict__ res,
     }
     rr += ri * ri;
   }
-  double vals[K];
-#pragma unroll
-  for (int q = 0; q < K; ++q) vals[q] = (q == j) ? rr : 0.0;
-  grid_reduce<K>(vals, part, ticket, FinResidualBlock<K>{sc, handle, use_cond});
+  double vals[1][1] = {{rr}};
+  grid_reduce_cols<K, 1, 1>(vals, part, ticket, FinResidualBlock<K>{sc, handle, use_cond});
 }
 
 // ||B(:,j)||^2 and ||R(:,j)||^2 into sc (BNORM, RESITER hold squares until init)
@@ -373,10 +401,8 @@ k_bnorm2(int n, const double *__restrict__ B, double *part, unsigned *ticket, do
   for (size_t o = blockIdx.x * (size_t)blockDim.x + threadIdx.x; o < total;
        o += (size_t)gridDim.x * blockDim.x)
     s += B[o] * B[o];
-  double vals[K];
-#pragma unroll
-  for (int q = 0; q < K; ++q) vals[q] = (q == j) ? s : 0.0;
-  grid_reduce<K>(vals, part, ticket, StoreK<K>{dst});
+  double vals[1][1] = {{s}};
+  grid_reduce_cols<K, 1, 1>(vals, part, ticket, StoreK<K>{dst});
 }
 
 template <int K>
@@ -488,7 +514,32 @@ static void block_solve(Hier &h, const double *B_h, double *X_h, int itmax, doub
   CHRONOS_CHECK_LAUNCH();
   k_bpcg_init<K><<<1, 1, 0, st>>>(s.sc.get(), b2.get(), r2.get(), tol, (double)itmax);
   CHRONOS_CHECK_LAUNCH();
-  if (itmax > 0) {
+  if (itmax > 0 && !h.prm.use_graph) {
+    // one iteration per graph launch from a host loop (profilers cannot see
+    // the kernel nodes of a graph holding a conditional node); same kernels
+    if (!s.exec) {
+      CHRONOS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        capture_block_iteration<K>(h, s, 0, 0);
+      } catch (...) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(st, &dummy);
+        throw;
+      }
+      CHRONOS_CUDA(cudaStreamEndCapture(st, &s.graph));
+      CHRONOS_CUDA(cudaGraphInstantiate(&s.exec, s.graph, 0));
+    }
+    double act_h[K];
+    for (int k = 0; k < itmax; ++k) {
+      CHRONOS_CUDA(cudaMemcpyAsync(act_h, s.sc.get() + bs_off(BS_ACTIVE, K), sizeof(act_h),
+                                   cudaMemcpyDeviceToHost, st));
+      CHRONOS_CUDA(cudaStreamSynchronize(st));
+      bool any = false;
+      for (int j = 0; j < K; ++j) any |= act_h[j] != 0.0;
+      if (!any) break;
+      CHRONOS_CUDA(cudaGraphLaunch(s.exec, st));
+    }
+  } else if (itmax > 0) {
     if (!s.exec) {
       CHRONOS_CUDA(cudaGraphCreate(&s.graph, 0));
       cudaGraphConditionalHandle handle;

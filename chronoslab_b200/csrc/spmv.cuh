@@ -82,6 +82,65 @@ __device__ __forceinline__ void grid_reduce(double (&v)[K], double *part, unsign
   }
 }
 
+// Deterministic grid reduction of NQ quantities of K columns (block
+// right-hand sides).  Lane l owns columns (l % (K/VEC))*VEC .. +VEC-1 and
+// v[q][e] is its partial of quantity q for the e-th of them; lanes owning the
+// same columns are combined by shuffles, warps through shared memory, blocks
+// by the last block to arrive (fixed orders throughout).  fin receives the
+// NQ*K totals, quantity-major (t[q*K + j]).  K*NQ <= 32, K/VEC <= 32.
+template <int K, int VEC, int NQ, typename Fin>
+__device__ __forceinline__ void grid_reduce_cols(double (&v)[NQ][VEC], double *part,
+                                                 unsigned *ticket, Fin fin) {
+  constexpr int LPR = K / VEC;       // lanes per column set
+  constexpr int NC = NQ * K;
+  static_assert(NC <= 32 && LPR <= 32, "grid_reduce_cols: K*NQ <= 32");
+  __shared__ double red[32][NC];
+  __shared__ double tot[NC];
+  __shared__ bool last;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NQ; ++q)
+#pragma unroll
+    for (int e = 0; e < VEC; ++e)
+#pragma unroll
+      for (int o = LPR; o < 32; o <<= 1) v[q][e] += __shfl_xor_sync(0xffffffffu, v[q][e], o);
+  if (lane < LPR)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) red[wid][q * K + lane * VEC + e] = v[q][e];
+  __syncthreads();
+  if ((int)threadIdx.x < NC) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += red[w][threadIdx.x];
+    part[(size_t)blockIdx.x * NC + threadIdx.x] = s;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int stripes = min((int)blockDim.x / NC, 32);
+  const int c = threadIdx.x % NC, sidx = threadIdx.x / NC;
+  if (sidx < stripes) {
+    double acc = 0.0;
+    for (int b = sidx; b < (int)gridDim.x; b += stripes) acc += __ldcg(&part[(size_t)b * NC + c]);
+    red[sidx][c] = acc;
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < NC) {
+    double s2 = 0.0;
+    for (int w = 0; w < stripes; ++w) s2 += red[w][threadIdx.x];
+    tot[threadIdx.x] = s2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *ticket = 0u;
+    fin(tot);
+  }
+}
+
 struct StoreScalar {
   double *dst;
   __device__ void operator()(const double *t) const { *dst = t[0]; }

@@ -63,3 +63,17 @@ def test_block_padding_and_zero_columns(lib, diffusion):
         B20 = np.concatenate([B, B[:, :4]], axis=1)
         X20, its20, fl20, _ = h.pcg_block(B20, itmax=1000, tol=1e-8)
         assert np.all(fl20 == 0) and np.array_equal(its20[16:], its20[:4])
+
+
+def test_block_host_loop_matches_graph_loop(lib, diffusion):
+    """The per-iteration graph launched from a host loop (use_graph = 0, what
+    a profiler sees) gives the conditional-graph loop's results bit for bit."""
+    A, B = diffusion
+    out = []
+    for g in (1, 0):
+        with cb.Hierarchy(A, np.ones(A.shape[0]), cb.params(precision=cb.CHRONOS_FP32, ntv=1,
+                                                            use_graph=g)) as h:
+            X, its, flags, _ = h.pcg_block(B[:, :5], itmax=1000, tol=1e-8)
+            out.append((X, its, flags))
+    assert np.array_equal(out[0][1], out[1][1]) and np.all(out[1][2] == 0)
+    assert np.array_equal(out[0][0], out[1][0])
