@@ -404,8 +404,9 @@ class Hierarchy:
 
 class Batch:
     """Independent problems of uneven sizes (chronos_batch): one hierarchy per
-    problem, all solves queued together (one conditional-graph launch each,
-    own stream, largest first)."""
+    problem; by default (batch_grouped = 1) one launch sequence serves the
+    whole batch (stacked level operators, per-problem PCG_CJ scalars), else
+    one conditional-graph launch per problem on its own stream."""
 
     def __init__(self, As, prm=None):
         self._lib = load()

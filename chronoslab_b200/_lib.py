@@ -43,7 +43,7 @@ class chronos_params(C.Structure):
         ("restart", C.c_int),
         ("precision", C.c_int), ("use_graph", C.c_int), ("seed", C.c_uint64),
         ("fsai_fabs", C.c_int), ("use_bsr", C.c_int), ("exact_outer", C.c_int),
-        ("replace_ratio", C.c_double), ("spmv_format", C.c_int),
+        ("replace_ratio", C.c_double), ("spmv_format", C.c_int), ("batch_grouped", C.c_int),
     ]
 
 

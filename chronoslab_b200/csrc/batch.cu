@@ -1,22 +1,23 @@
 // Batch of independent SPD problems of uneven sizes: one hierarchy per
-// problem (each exactly what a single chronos_amg_setup builds), and a batch
-// solve that queues every problem's whole PCG_CJ -- one conditional-graph
-// launch each -- on its own stream with no host synchronisation in between,
-// largest problems first, so the small problems' short kernels overlap with
-// the large ones' on the GPU.
+// problem (each exactly what a single chronos_amg_setup builds).  The batch
+// solve either runs the grouped path of group.cu (batch_grouped = 1, the
+// default: one launch sequence for the whole batch) or queues every
+// problem's whole PCG_CJ -- one conditional-graph launch each -- on its own
+// stream with no host synchronisation in between, largest problems first.
 #include <algorithm>
 #include <cmath>
 #include <memory>
 #include <numeric>
 #include <vector>
 
-#include "hier.h"
+#include "group.h"
 
 namespace chronos {
 
 struct Batch {
   std::vector<std::unique_ptr<Hier>> h;
   std::vector<int> order;           // largest level-1 operator first
+  std::unique_ptr<GroupSolve> group;
 };
 
 }  // namespace chronos
@@ -72,6 +73,7 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
     std::stable_sort(bt->b.order.begin(), bt->b.order.end(), [&](int a, int c) {
       return bt->b.h[a]->levels[0].A.nnz > bt->b.h[c]->levels[0].A.nnz;
     });
+    if (prm->batch_grouped && group_supported(bt->b.h)) bt->b.group = group_build(bt->b.h, *prm);
     *out = bt.release();
   });
 }
@@ -82,6 +84,12 @@ int chronos_batch_solve(chronos_batch *bt, const double *const *b_h, double *con
     CHRONOS_REQUIRE(bt && b_h && x_h && iters && flags, CHRONOS_EINVAL, "null argument");
     Batch &B = bt->b;
     const int np = (int)B.h.size();
+    if (B.group) {
+      std::vector<const double *> bb(b_h, b_h + np);
+      std::vector<double *> xx(x_h, x_h + np);
+      group_solve(*B.group, bb, xx, itmax, tol, iters, flags, seconds);
+      return;
+    }
     std::vector<DBuf<double>> bd(np), xd(np);
     std::vector<char> zero(np, 0);
     for (int p = 0; p < np; ++p) {

@@ -101,6 +101,7 @@ void params_default(chronos_params *p) {
   p->exact_outer = 0;
   p->replace_ratio = 0.01;
   p->spmv_format = 0;
+  p->batch_grouped = 1;
 }
 
 void params_read(const char *fnames_path, chronos_params *p) {

@@ -111,6 +111,9 @@ typedef struct chronos_params {
                                      autotuner's choice per operator; 1 row-grouped CSR only;
                                      2 sliced ELL for every operator averaging at most 16
                                      entries per row */
+  int batch_grouped;              /* chronos_batch_*: 1 (default) one launch sequence for the
+                                     whole batch (stacked level operators, per-problem PCG
+                                     scalars); 0 one graph per problem on its own stream */
 } chronos_params;
 
 /* Reference regression-test parameters (Tests/parm_*): DOM 0.01, BAMG/NONE,
