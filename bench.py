@@ -59,6 +59,8 @@ def run_profile_solve(args):
     import chronoslab_b200 as cb
     if args.workload == "c3":
         return run_profile_block(args)
+    if args.workload == "c4":
+        return run_profile_batch(args)
     A, TV, b = build_problem(args.ne, seed=0)
     prec = cb.CHRONOS_FP32 if args.profile_solve == "fp32" else cb.CHRONOS_FP64
     # ncu cannot profile the kernel nodes of a graph holding a conditional
@@ -103,6 +105,44 @@ def run_profile_block(args):
         print(json.dumps({"profile_solve": args.profile_solve, "workload": "c3", "ne": ne,
                           "iterations": its.tolist(), "ms": sec * 1e3,
                           "levels": [h.level_info(l) for l in range(h.nlevels)]}))
+    return 0
+
+
+def c4_problems():
+    """64 problems: edge drawn uniformly in [16, 64] from the seed, even ones
+    Poisson, odd ones log-normal diffusion."""
+    import numpy as np
+    from chronoslab_b200 import problems as PB
+    rng = np.random.default_rng(0)
+    edges = rng.integers(16, 65, 64)
+    As, bs = [], []
+    for p, e in enumerate(edges):
+        if p % 2 == 0:
+            A = PB.poisson7(int(e))
+        else:
+            A, _ = PB.diffusion7(int(e), sigma=2.0, corr_len=8.0, zaniso=0.01, seed=p)
+        As.append(A)
+        bs.append(PB.uniform_rhs(A.shape[0], seed=1000 + p))
+    return As, bs
+
+
+def run_profile_batch(args):
+    """One grouped batch solve of the c4 workload bracketed by the profiler
+    range, its iterations launched from a host loop."""
+    import torch
+    import chronoslab_b200 as cb
+    As, bs = c4_problems()
+    prec = cb.CHRONOS_FP32 if args.profile_solve == "fp32" else cb.CHRONOS_FP64
+    with cb.Batch(As, cb.params(precision=prec, ntv=1, nstep=15, step_size=4,
+                                use_graph=0)) as Bt:
+        Bt.solve(bs, itmax=args.itmax, tol=args.tol)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        xs, its, fl, sec = Bt.solve(bs, itmax=args.itmax, tol=args.tol)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_solve": args.profile_solve, "workload": "c4",
+                          "iterations": [int(its.min()), int(its.max())], "ms": sec * 1e3}))
     return 0
 
 
@@ -473,16 +513,7 @@ def run_block_or_batch(args):
                                      "nnz), block of 16 RHS, SpMM V-cycles, PCG_CJ to "
                                      f"{args.tol} per column"}
     else:
-        rng = np.random.default_rng(0)
-        edges = rng.integers(16, 65, 64)
-        As, bs = [], []
-        for p, e in enumerate(edges):
-            if p % 2 == 0:
-                A = PB.poisson7(int(e))
-            else:
-                A, _ = PB.diffusion7(int(e), sigma=2.0, corr_len=8.0, zaniso=0.01, seed=p)
-            As.append(A)
-            bs.append(PB.uniform_rhs(A.shape[0], seed=1000 + p))
+        As, bs = c4_problems()
         for prec, name in ((cb.CHRONOS_FP32, "fp32"), (cb.CHRONOS_FP64, "fp64")):
             t0 = time.perf_counter()
             with cb.Batch(As, cb.params(precision=prec, ntv=1, nstep=15, step_size=4)) as Bt:

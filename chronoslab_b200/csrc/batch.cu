@@ -53,7 +53,8 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
   return batch_guard([&] {
     CHRONOS_REQUIRE(prm && n && iat_h && ja_h && val_h && out && nprob > 0, CHRONOS_EINVAL,
                     "bad argument");
-    CHRONOS_REQUIRE(prm->use_graph, CHRONOS_EINVAL, "batched solves need use_graph = 1");
+    CHRONOS_REQUIRE(prm->use_graph || prm->batch_grouped, CHRONOS_EINVAL,
+                    "per-problem batched solves need use_graph = 1");
     auto bt = std::make_unique<chronos_batch>();
     for (int p = 0; p < nprob; ++p) {
       CHRONOS_REQUIRE(n[p] > 0 && iat_h[p] && iat_h[p][0] == 0, CHRONOS_EINVAL,
@@ -74,6 +75,8 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
       return bt->b.h[a]->levels[0].A.nnz > bt->b.h[c]->levels[0].A.nnz;
     });
     if (prm->batch_grouped && group_supported(bt->b.h)) bt->b.group = group_build(bt->b.h, *prm);
+    CHRONOS_REQUIRE(bt->b.group || prm->use_graph, CHRONOS_EINVAL,
+                    "these problems need the per-problem batch path, which needs use_graph = 1");
     *out = bt.release();
   });
 }

@@ -653,7 +653,30 @@ void group_solve(GroupSolve &g, const std::vector<const double *> &b_h,
   CHRONOS_CUDA(cudaMemcpyAsync(&active, g.ctl.get(), sizeof(unsigned), cudaMemcpyDeviceToHost,
                                st));
   CHRONOS_CUDA(cudaStreamSynchronize(st));
-  if (active > 0) {
+  if (active > 0 && !g.prm.use_graph) {
+    // one iteration per graph launch from a host loop (profilers cannot see
+    // the kernel nodes of a graph holding a conditional node); same kernels
+    if (!g.exec) {
+      CHRONOS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        group_capture_iteration(g, 0, 0, tol, itmax);
+      } catch (...) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(st, &dummy);
+        throw;
+      }
+      CHRONOS_CUDA(cudaStreamEndCapture(st, &g.graph));
+      CHRONOS_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+      g.g_tol = tol;
+      g.g_itmax = itmax;
+    }
+    for (int k = 0; k < itmax && active > 0; ++k) {
+      CHRONOS_CUDA(cudaGraphLaunch(g.exec, st));
+      CHRONOS_CUDA(cudaMemcpyAsync(&active, g.ctl.get(), sizeof(unsigned),
+                                   cudaMemcpyDeviceToHost, st));
+      CHRONOS_CUDA(cudaStreamSynchronize(st));
+    }
+  } else if (active > 0) {
     if (!g.exec) {
       CHRONOS_CUDA(cudaGraphCreate(&g.graph, 0));
       cudaGraphConditionalHandle handle;

@@ -494,9 +494,9 @@ template <typename VT> inline const VT *csr_vals(const DMat &m);
 template <> inline const float *csr_vals<float>(const DMat &m) { return m.v32.get(); }
 template <> inline const double *csr_vals<double>(const DMat &m) { return m.v64.get(); }
 
-// Long-row threshold for `lanes`-lane groups: rows longer than 16 entries per
+// Long-row threshold for `lanes`-lane groups: rows longer than 32 entries per
 // lane go to whole warps.
-inline int long_row_threshold(int lanes) { return lanes >= 32 ? 0x7fffffff : 16 * lanes; }
+inline int long_row_threshold(int lanes) { return lanes >= 32 ? 0x7fffffff : 32 * lanes; }
 
 // Blocks of a grid of `cap` given to the long rows: their share of the
 // entries (at least one warp per 8 long rows' worth, at most half the grid,

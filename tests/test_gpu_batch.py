@@ -85,3 +85,15 @@ def test_batch_grouped_itmax_and_deep_mix(lib):
         for A, b, x in zip(As, bs, xs):
             assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
     assert len(depths) >= 1
+
+
+def test_batch_grouped_host_loop_matches_graph_loop(lib):
+    """use_graph = 0 launches the grouped iteration from a host loop (what a
+    profiler sees): the same results bit for bit."""
+    As, bs = make_problems(5, 5, lo=11)
+    out = []
+    for g in (1, 0):
+        with cb.Batch(As, cb.params(ntv=1, batch_grouped=1, use_graph=g)) as B:
+            out.append(B.solve(bs, itmax=1000, tol=1e-8))
+    assert np.array_equal(out[0][1], out[1][1])
+    assert all(np.array_equal(a, c) for a, c in zip(out[0][0], out[1][0]))
