@@ -630,6 +630,81 @@ static void validate_csr(const HostCSR &A) {
   }
 }
 
+// Jacobi-smoothed prolongation (prolong.m:180-196, prol_emin = SMOOTH):
+// P - omega*DA*P with DA = diag(diag(A))\A, omega = 1.9/lambda_max(DA).
+// lambda_max by Lanczos on D^{-1/2} A D^{-1/2} (the spectrum of DA; eigs'
+// tolerance 1e-3); (omega*DA)*P -- DA's entries a_ik/a_ii scaled by omega, as
+// MATLAB evaluates the expression left to right -- by the GPU SpGEMM; the
+// difference, with exact zeros dropped, on the host.
+static HostCSR smooth_prolongation(const HostCSR &A, const DMat &dA, const HostCSR &P,
+                                   cudaStream_t st) {
+  const int n = A.nrows;
+  std::vector<double> d(n, 0.0), dm(n);
+  for (int i = 0; i < n; ++i)
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+      if (A.ci[k] == i) d[i] = A.v[k];
+  for (int i = 0; i < n; ++i) {
+    CHRONOS_REQUIRE(d[i] > 0.0, CHRONOS_ENOTSPD,
+                    "prolongation smoothing: non-positive diagonal entry at row " +
+                        std::to_string(i + 1));
+    dm[i] = 1.0 / std::sqrt(d[i]);
+  }
+  DBuf<double> ddm, t1(n), t2(n);
+  ddm.upload(dm, st);
+  auto mv = [&](const double *v, double *w) {
+    device_diag_mul(n, ddm.get(), v, t1.get(), st);
+    csr_apply<double, double, double, double, MODE_PLAIN, false>(
+        st, 8, n, dA.rp, dA.ci, dA.v64, t1.get(), (const double *)nullptr, t2.get(), 1.0);
+    device_diag_mul(n, ddm.get(), t2.get(), w, st);
+  };
+  const double lam = lanczos_lmax(n, mv, 1e-3, 300, st);
+  const double omega = 1.9 / lam;
+  HostCSR W = A;
+  for (int i = 0; i < n; ++i)
+    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) W.v[k] = omega * (A.v[k] / d[i]);
+  DMat dW, dP;
+  upload_csr(W, dW, false, st);
+  upload_csr(P, dP, false, st);
+  DBuf<int> wrp, wci;
+  DBuf<double> wv;
+  int64_t nnz = 0;
+  spgemm_device(n, P.ncols, dW.rp, dW.ci, dW.v64, dP.rp, dP.ci, dP.v64, wrp, wci, wv, &nnz, st);
+  const HostCSR WP = download_csr(n, P.ncols, wrp, wci, wv, nnz, st);
+  HostCSR Ps;
+  Ps.nrows = n;
+  Ps.ncols = P.ncols;
+  Ps.rp.assign(1, 0);
+  std::vector<std::pair<int, double>> row;
+  for (int i = 0; i < n; ++i) {
+    row.clear();
+    for (int64_t k = P.rp[i]; k < P.rp[i + 1]; ++k) row.emplace_back(P.ci[k], P.v[k]);
+    std::sort(row.begin(), row.end(),
+              [](const std::pair<int, double> &a, const std::pair<int, double> &b) {
+                return a.first < b.first;
+              });
+    size_t a = 0;
+    int64_t b = WP.rp[i];
+    const int64_t be = WP.rp[i + 1];
+    while (a < row.size() || b < be) {
+      int c;
+      double v;
+      if (b >= be || (a < row.size() && row[a].first < WP.ci[b])) {
+        c = row[a].first; v = row[a].second; ++a;
+      } else if (a >= row.size() || WP.ci[b] < row[a].first) {
+        c = WP.ci[b]; v = -WP.v[b]; ++b;
+      } else {
+        c = row[a].first; v = row[a].second - WP.v[b]; ++a; ++b;
+      }
+      if (v != 0.0) {
+        Ps.ci.push_back(c);
+        Ps.v.push_back(v);
+      }
+    }
+    Ps.rp.push_back((int64_t)Ps.ci.size());
+  }
+  return Ps;
+}
+
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A0, int ntv0,
                                       const double *TV0) {
   const double t_start = now_s();
@@ -641,7 +716,8 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
   CHRONOS_REQUIRE(smeth == "AFSAI_SYM", CHRONOS_ENOTSUP, "smoother " + smeth + " is outside this path");
   CHRONOS_REQUIRE(tmeth == "NONE", CHRONOS_ENOTSUP, "test-space method " + tmeth + " is outside this path");
   CHRONOS_REQUIRE(ptype == "BAMG", CHRONOS_ENOTSUP, "prolongation " + ptype + " is outside this path");
-  CHRONOS_REQUIRE(pemin == "NONE", CHRONOS_ENOTSUP, "prolongation post-process " + pemin + " is outside this path");
+  CHRONOS_REQUIRE(pemin == "NONE" || pemin == "SMOOTH", CHRONOS_ENOTSUP,
+                  "prolongation post-process " + pemin + " is outside this path");
   CHRONOS_REQUIRE(prm.nl_agg == 0, CHRONOS_ENOTSUP, "aggressive coarsening is outside this path");
   CHRONOS_REQUIRE(prm.updateCF == 0, CHRONOS_ENOTSUP, "updateCF != 0 is outside this path");
   CHRONOS_REQUIRE(prm.filt_wgt >= 100 && prm.filt_tau <= 0, CHRONOS_ENOTSUP,
@@ -796,6 +872,7 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
                   prm.eps_prol};
     std::vector<int> c_mark;
     HostCSR Ph = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
+    if (pemin == "SMOOTH") Ph = smooth_prolongation(Al, L.A, Ph, st);
     std::vector<double> TVn((size_t)nc * ntv);
     for (int j = 0; j < ntv; ++j)
       for (int c = 0; c < nc; ++c) TVn[(size_t)j * nc + c] = TV[(size_t)j * n + clist[c]];

@@ -91,6 +91,8 @@ void convert_f64_to_f32(int64_t n, const double *src, float *dst, cudaStream_t s
 double device_dot(int n, const double *a, const double *b, double *scratch, cudaStream_t st);
 void device_axpby(int n, double a, const double *x, double b, double *y, cudaStream_t st);
 void device_scale_copy(int n, double a, const double *x, double *y, cudaStream_t st);
+// y = d .* x
+void device_diag_mul(int n, const double *d, const double *x, double *y, cudaStream_t st);
 // grad[k] = -lambda[row(k)] * u[col(k)]
 void adjoint_scatter(int n, const int *rp, const int *ci, const double *lambda, const double *u,
                      double *grad, cudaStream_t st);

@@ -582,6 +582,16 @@ void device_scale_copy(int n, double a, const double *x, double *y, cudaStream_t
   CHRONOS_CHECK_LAUNCH();
 }
 
+__global__ void k_diag_mul(int n, const double *d, const double *x, double *y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = d[i] * x[i];
+}
+
+void device_diag_mul(int n, const double *d, const double *x, double *y, cudaStream_t st) {
+  k_diag_mul<<<std::min<int64_t>(ceil_div(n, 256), 4096), 256, 0, st>>>(n, d, x, y);
+  CHRONOS_CHECK_LAUNCH();
+}
+
 // One warp per row: grad[k] = -lambda_i * u_{col(k)} over the row's entries.
 __global__ void k_adjoint_scatter(int n, const int *rp, const int *ci, const double *lam,
                                   const double *u, double *grad) {

@@ -501,6 +501,11 @@ def cpt_aspamg(param, A, TV0, rng=None, on_level=None):
         if param["prolong"]["proltype"].upper() != "BAMG":
             raise NotImplementedError("only BAMG prolongation is on this path")
         P, c_mark = ref_bamg(param["prolong"], clist.size, fcnode, S, TV)
+        emin = param["prolong"].get("prol_emin", "NONE").upper()
+        if emin == "SMOOTH":
+            P = smooth_prolongation(A, P)
+        elif emin != "NONE":
+            raise NotImplementedError("prolongation post-process " + emin)
         TV = TV[clist, :]
         Ac = galerkin(P, A)
         lev = Level(A=A, G=G, omega=omega, P=P, fcnode=fcnode,
@@ -635,6 +640,32 @@ def sqmr(Afun, rhs, tol, itmax, lprec, rprec=lambda v: v, x0=None):
         info = 1
     relres = np.linalg.norm(rhs - Afun(pnew)) / bnorm
     return pnew, info, relres, niter, resvec[:niter]
+
+
+def smooth_prolongation(A, P, tol=1e-3):
+    """prolong.m:180-196 (prol_emin = SMOOTH): DA = diag(diag(A))\\A (each row
+    divided by its diagonal entry), lambda_max = eigs(DA,1,'lm') with
+    tolerance 1e-3, omega = 1.9/lambda_max, P - omega*DA*P evaluated as
+    (omega*DA)*P; MATLAB's sparse results drop exact zeros."""
+    A = sp.csr_matrix(A)
+    d = A.diagonal()
+    DA = A.copy().astype(np.float64)
+    DA.data = DA.data / np.repeat(d, np.diff(DA.indptr))
+    n = A.shape[0]
+    v0 = np.ones(n) / np.sqrt(n)
+    try:
+        lam = spla.eigs(DA, k=1, which="LM", tol=tol, v0=v0, return_eigenvectors=False,
+                        maxiter=max(3 * n, 1000))
+    except spla.ArpackNoConvergence as e:
+        lam = e.eigenvalues
+    omega = 1.9 / float(abs(lam[0]))
+    W = DA.copy()
+    W.data = omega * W.data
+    WP = (W @ sp.csr_matrix(P)).tocsr()
+    Ps = (sp.csr_matrix(P) - WP).tocsr()
+    Ps.eliminate_zeros()
+    Ps.sort_indices()
+    return Ps
 
 
 def lmax_eigs(A, tol=1e-3, maxiter=3):

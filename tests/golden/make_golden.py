@@ -94,7 +94,19 @@ def main(ref_root):
     rhs = np.ones(A.shape[0])
     _, info, relres, niter, _ = O.sqmr(lambda v: A @ v, rhs, 1e-6, 100, Mv)
     _, it, _, flag = O.pcg_cj(Mv, lambda v: Af @ v, rhs, np.zeros_like(rhs), 1000, 1e-8)
+    # Jacobi-smoothed prolongation (prolong.m:180-196), Tests/CubeBAMG_SMOOTH.m
+    prm_s = O.default_params(8)
+    prm_s["prolong"]["prol_emin"] = "SMOOTH"
+    Hs = O.cpt_aspamg(prm_s, Af, TV0)
+    Mvs = lambda r: O.amg_vcycle(Hs, r, 0, Af)
+    _, info_s, relres_s, niter_s, _ = O.sqmr(lambda v: A @ v, rhs, 1e-6, 100, Mvs)
+    _, it_s, _, _ = O.pcg_cj(Mvs, lambda v: Af @ v, rhs, np.zeros_like(rhs), 1000, 1e-8)
     info_out = {
+        "reference_sqmr_iterations_smooth": 29,
+        "reference_sqmr_source_smooth": "Tests/CubeBAMG_SMOOTH.m:3 (tolerance max(5%, 2))",
+        "oracle_sqmr_iterations_smooth": int(niter_s),
+        "oracle_pcg_iterations_1e-8_smooth": int(it_s),
+        "levels_smooth": [int(L.A.shape[0]) for L in Hs.levels],
         "reference_sqmr_iterations": 43,
         "reference_sqmr_source": "Tests/CubeBAMG_NONE.m:3 (tolerance max(5%, 2), :34)",
         "oracle_sqmr_iterations": int(niter),

@@ -116,3 +116,21 @@ def test_diffusion_generator():
     assert np.linalg.eigvalsh(A.toarray()).min() > 0
     A2, _ = PB.diffusion7(8, seed=3)
     assert (A != A2).nnz == 0
+
+
+def test_smooth_prolongation_dense():
+    """smooth_prolongation (prolong.m:180-196) against the dense formula
+    P - 1.9/lambda_max(D^-1 A) D^-1 A P on a small Poisson problem."""
+    import scipy.sparse as sp
+    from chronoslab_b200 import problems as PB
+    A = PB.poisson7(6).tocsr()
+    n = A.shape[0]
+    P = sp.random(n, 20, density=0.1, random_state=4, format="csr")
+    Ps = O.smooth_prolongation(A, P)
+    Ad = A.toarray()
+    DA = Ad / np.diag(Ad)[:, None]
+    lam = np.max(np.abs(np.linalg.eigvals(DA)))
+    ref = P.toarray() - (1.9 / lam) * DA @ P.toarray()
+    # lambda_max is an ARPACK estimate at tolerance 1e-3
+    assert np.linalg.norm(Ps.toarray() - ref) <= 1e-4 * np.linalg.norm(ref)
+    assert not np.any(Ps.data == 0.0)
