@@ -14,6 +14,7 @@ Vectors are numpy FP64 arrays; matrices scipy.sparse CSR (0-based).
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 import scipy.sparse as sp
@@ -139,6 +140,43 @@ def afsai_cpp(M, nthread, nstep, step_size, eps):
         return None, False
     F = sp.csr_matrix((coef, ja.astype(np.int64) - 1, iat - 1), shape=(n, n))
     return F, True
+
+
+def read_matrix_bin(path):
+    """example_cpp binary CSR (Cpp_EMIN/readMat.cpp) -> scipy CSR."""
+    h = C.c_void_p()
+    check(load().chronos_read_matrix_bin(os.fsencode(path), C.byref(h)))
+    return _CsrHandle.take(h)
+
+
+def read_ext_bin(path):
+    """Chronos .Ext_bin matrix (DumpChronos.cpp) -> scipy CSR."""
+    h = C.c_void_p()
+    check(load().chronos_read_ext_bin(os.fsencode(path), C.byref(h)))
+    return _CsrHandle.take(h)
+
+
+def write_ext_bin(path, A):
+    n, iat, ja, val = _csr(A, A.shape[1])
+    check(load().chronos_write_ext_bin(os.fsencode(path), n, A.shape[1], _pi(iat), _pi(ja),
+                                       _pd(val)))
+
+
+def read_tv_ext_bin(path):
+    """Chronos .Ext_bin test space -> n x ntv array (ntv = 0 for a header-only file)."""
+    n, ntv = C.c_int(), C.c_int()
+    check(load().chronos_read_tv_ext_bin(os.fsencode(path), C.byref(n), C.byref(ntv), None))
+    TV = np.zeros(max(n.value * ntv.value, 1))
+    check(load().chronos_read_tv_ext_bin(os.fsencode(path), C.byref(n), C.byref(ntv), _pd(TV)))
+    return TV[:n.value * ntv.value].reshape(ntv.value, n.value).T.copy()
+
+
+def write_tv_ext_bin(path, TV):
+    TV = np.asarray(TV, dtype=np.float64)
+    if TV.ndim == 1:
+        TV = TV[:, None]
+    col = np.ascontiguousarray(TV.T).ravel()
+    check(load().chronos_write_tv_ext_bin(os.fsencode(path), TV.shape[0], TV.shape[1], _pd(col)))
 
 
 def fsai_pattern(A, nstep=15, step_size=1, eps=1e-3, nthread=1, fsai_fabs=0):
@@ -322,6 +360,11 @@ class Hierarchy:
         check(self._lib.chronos_hier_export(self._h, level, w, C.byref(nr), C.byref(ncl),
                                             C.byref(nnz), _pi(iat), _pi(ja), _pd(v)))
         return sp.csr_matrix((v[:nnz.value], ja[:nnz.value], iat), shape=(nr.value, ncl.value))
+
+    def dump_ext_bin(self, level, which, path):
+        """Writes operator `which` ('A', 'G', 'P') of a level in .Ext_bin."""
+        w = C.c_char(which.encode() if isinstance(which, str) else which)
+        check(self._lib.chronos_hier_dump_ext_bin(self._h, level, w, os.fsencode(path)))
 
     def setup_times(self):
         t = np.zeros(8)

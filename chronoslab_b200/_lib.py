@@ -81,6 +81,12 @@ SIGNATURES = {
     "chronos_csr_info": [_vp, _pi, _pi, _pi64],
     "chronos_csr_fetch": [_vp, _pi, _pi, _pd],
     "chronos_csr_free": [_vp],
+    "chronos_read_matrix_bin": [C.c_char_p, _pp],
+    "chronos_read_ext_bin": [C.c_char_p, _pp],
+    "chronos_write_ext_bin": [C.c_char_p, _i, _i, _pi, _pi, _pd],
+    "chronos_read_tv_ext_bin": [C.c_char_p, _pi, _pi, _pd],
+    "chronos_write_tv_ext_bin": [C.c_char_p, _i, _i, _pd],
+    "chronos_hier_dump_ext_bin": [_vp, _i, C.c_char, C.c_char_p],
     "chronos_fsai_pattern": [_i, _pi, _pi, _pd, _i, _i, _d, _i, _i, _pi, _pp],
     "chronos_coarsen": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _u64, _pi, _pi, _pp],
     "chronos_bamg": [C.POINTER(chronos_params), _i, _pi, _pi, _pi, _i, _pd, _pi, _pp],

@@ -157,6 +157,46 @@ int chronos_csr_free(chronos_csr *m) {
   return guard([&] { delete m; });
 }
 
+int chronos_read_matrix_bin(const char *path, chronos_csr **A) {
+  return guard([&] {
+    CHRONOS_REQUIRE(path && A, CHRONOS_EINVAL, "null argument");
+    *A = wrap_csr(read_matrix_bin(path));
+  });
+}
+
+int chronos_read_ext_bin(const char *path, chronos_csr **A) {
+  return guard([&] {
+    CHRONOS_REQUIRE(path && A, CHRONOS_EINVAL, "null argument");
+    *A = wrap_csr(read_ext_bin(path));
+  });
+}
+
+int chronos_write_ext_bin(const char *path, int n, int ncols, const int *iat_h, const int *ja_h,
+                          const double *val_h) {
+  return guard([&] {
+    CHRONOS_REQUIRE(path && iat_h && ja_h && val_h && n >= 0 && ncols >= 0, CHRONOS_EINVAL,
+                    "bad argument");
+    write_ext_bin(path, from_csr0(n, ncols, iat_h, ja_h, val_h));
+  });
+}
+
+int chronos_read_tv_ext_bin(const char *path, int *n, int *ntv, double *TV_h) {
+  return guard([&] {
+    CHRONOS_REQUIRE(path && n && ntv, CHRONOS_EINVAL, "null argument");
+    std::vector<double> tv;
+    read_tv_ext_bin(path, n, ntv, tv);
+    if (TV_h && !tv.empty()) std::memcpy(TV_h, tv.data(), sizeof(double) * tv.size());
+  });
+}
+
+int chronos_write_tv_ext_bin(const char *path, int n, int ntv, const double *TV_h) {
+  return guard([&] {
+    CHRONOS_REQUIRE(path && (TV_h || (size_t)n * ntv == 0) && n >= 0 && ntv >= 0,
+                    CHRONOS_EINVAL, "bad argument");
+    write_tv_ext_bin(path, n, ntv, TV_h);
+  });
+}
+
 int chronos_fsai_pattern(int n, const int *iat_h, const int *ja_h, const double *val_h, int nstep,
                          int step_size, double eps, int nthread, int fsai_fabs, int *is_posdef,
                          chronos_csr **G) {
@@ -425,6 +465,22 @@ int chronos_hier_level_info(const chronos_hier *h, int level, chronos_level_info
     info->block_rows = L.A.nb;
     info->sell_mask = (L.A.use_sell ? 1 : 0) | (L.G.use_sell ? 2 : 0) | (L.Gt.use_sell ? 4 : 0) |
                       (L.P.use_sell ? 8 : 0) | (L.Pt.use_sell ? 16 : 0);
+  });
+}
+
+int chronos_hier_dump_ext_bin(const chronos_hier *h, int level, char which, const char *path) {
+  int nr = 0, nc = 0;
+  int64_t nnz = 0;
+  int rc = chronos_hier_export(h, level, which, &nr, &nc, &nnz, nullptr, nullptr, nullptr);
+  if (rc != CHRONOS_OK) return rc;
+  return guard([&] {
+    CHRONOS_REQUIRE(path, CHRONOS_EINVAL, "null path");
+    std::vector<int> iat((size_t)nr + 1), ja(std::max<int64_t>(nnz, 1));
+    std::vector<double> v(std::max<int64_t>(nnz, 1));
+    const int rc2 = chronos_hier_export(h, level, which, &nr, &nc, &nnz, iat.data(), ja.data(),
+                                        v.data());
+    CHRONOS_REQUIRE(rc2 == CHRONOS_OK, rc2, "export failed");
+    write_ext_bin(path, from_csr0(nr, nc, iat.data(), ja.data(), v.data()));
   });
 }
 

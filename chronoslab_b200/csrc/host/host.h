@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../../../include/chronos_b200.h"
@@ -70,6 +71,14 @@ FsaiResult fsai_adaptive(const HostCSR &A, int nstep, int step_size, double eps,
 
 // Thin QR (Householder) of an n x k column-major matrix: Q overwrites X.
 void qr_orthonormalize(int n, int k, double *X);
+
+// On-disk formats of the reference (formats.cpp): example_cpp binary CSR,
+// Chronos .Ext_bin matrix and test space (column-major n x ntv in memory).
+HostCSR read_matrix_bin(const std::string &path);
+HostCSR read_ext_bin(const std::string &path);
+void write_ext_bin(const std::string &path, const HostCSR &A);
+void read_tv_ext_bin(const std::string &path, int *nrows, int *ntv, std::vector<double> &tv);
+void write_tv_ext_bin(const std::string &path, int nrows, int ntv, const double *tv_colmajor);
 
 // CSR utilities
 HostCSR csr_transpose(const HostCSR &A);

@@ -177,6 +177,24 @@ int chronos_csr_info(const chronos_csr *m, int *nrows, int *ncols, int64_t *nnz)
 int chronos_csr_fetch(const chronos_csr *m, int *iat_h, int *ja_h, double *val_h);
 int chronos_csr_free(chronos_csr *m);
 
+/* ---- on-disk formats of the reference ------------------------------------- */
+/* example_cpp binary CSR, replaces readBinaryMatrix (Cpp_EMIN/readMat.cpp:27-80):
+ * int32 rows and entries, then {int32 row, int32 column, double value} records,
+ * 1-based, grouped by row.  Returns a 0-based CSR (columns ascending). */
+int chronos_read_matrix_bin(const char *path, chronos_csr **A);
+/* Chronos .Ext_bin matrix as DumpChronos writes it (debug_stuff/dump_chronos/
+ * DumpChronos.cpp:27-36): int64 rows and entries, then {int64 row, int64 column,
+ * double value} records, 1-based.  Read returns a 0-based CSR; write takes one. */
+int chronos_read_ext_bin(const char *path, chronos_csr **A);
+int chronos_write_ext_bin(const char *path, int n, int ncols, const int *iat_h, const int *ja_h,
+                          const double *val_h);
+/* Chronos .Ext_bin test space (DumpChronos.cpp:38-45): int64 rows and columns,
+ * then the values row by row.  TV_h is n x ntv column-major; read with TV_h =
+ * NULL returns the sizes.  A file that ends after its header (the reference's
+ * dumper writes the values to the closed matrix file) reads as ntv = 0. */
+int chronos_read_tv_ext_bin(const char *path, int *n, int *ntv, double *TV_h);
+int chronos_write_tv_ext_bin(const char *path, int n, int ntv, const double *TV_h);
+
 /* Symbolic half of SYM_aFSAI_compute on the host (cpt_afsai_coef.cpp:316-543):
  * the adaptive pattern with the host FP64 values of the final local solves.
  * A: 0-based CSR, sorted rows.  G rows: strictly-lower ascending, then the
@@ -257,6 +275,9 @@ int chronos_hier_export(const chronos_hier *h, int level, char which, int *nrows
 /* Setup timings in seconds: [fsai_pattern, fsai_numeric, omega, coarsen, prolong,
  * galerkin, coarse_factor, total]. */
 int chronos_hier_setup_times(const chronos_hier *h, double *t8);
+/* Writes operator which ('A', 'G' or 'P') of a level in the .Ext_bin format
+ * (FP64 values), e.g. to feed a level to the reference's own tools. */
+int chronos_hier_dump_ext_bin(const chronos_hier *h, int level, char which, const char *path);
 
 /* Kernel timings of a built hierarchy (CUDA events on its stream, `reps`
  * launches each after one warm-up) and the algorithmic bytes each moves:

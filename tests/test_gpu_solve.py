@@ -291,3 +291,17 @@ def test_plain_stream_order_matches_pdl(lib, elast, tmp_path):
     y = np.load(out)
     assert int(y[-2]) == it and int(y[-1]) == flag == 0
     assert np.array_equal(y[:-2], x)
+
+
+def test_hierarchy_dump_ext_bin(lib, elast, tmp_path):
+    """A level operator written by the hierarchy in .Ext_bin reads back as the
+    exported operator (FP64 values)."""
+    A, TV, b = elast
+    with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32)) as h:
+        for lvl, which in ((0, "A"), (0, "P"), (1, "A")):
+            p = tmp_path / f"L{lvl}{which}.Ext_bin"
+            h.dump_ext_bin(lvl, which, str(p))
+            E = h.export(lvl, which)
+            R = cb.read_ext_bin(str(p))
+            R = R[:, :E.shape[1]] if which == "P" else R
+            assert R.shape[0] == E.shape[0] and (R != E).nnz == 0
