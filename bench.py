@@ -453,6 +453,7 @@ def run_product(args, world, rank, local):
         "vcycle_hbm_gbs": {"fp32": vgbs32, "fp64": vgbs64},
         "pcg_iteration_hbm_gbs": it_gbs,
         "setup_s": {"fp32": setup32["total"], "fp64": setup64["total"]},
+        "setup_breakdown_s": {"fp32": {k: round(v, 3) for k, v in setup32.items()}},
         "roofline": {"bound": "hbm", "kernel": "level-1 residual r = b - A x (FP32 sliced 3x3 block form)",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind,

@@ -67,8 +67,9 @@ void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st) {
   }
   // 16-bit column offsets when every row spans fewer than 65536 columns
   std::vector<int> base(std::max(h.nrows, 1), 0);
-  bool fits = h.nrows > 0;
-  for (int i = 0; i < h.nrows && fits; ++i) {
+  int fits = h.nrows > 0;
+#pragma omp parallel for schedule(static, 4096) reduction(&& : fits)
+  for (int i = 0; i < h.nrows; ++i) {
     if (h.rp[i] == h.rp[i + 1]) continue;
     int lo = h.ci[h.rp[i]], hi = lo;
     for (int64_t k = h.rp[i] + 1; k < h.rp[i + 1]; ++k) {
@@ -76,11 +77,12 @@ void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st) {
       hi = std::max(hi, h.ci[k]);
     }
     base[i] = lo;
-    fits = hi - lo <= 0xffff;
+    fits = fits && hi - lo <= 0xffff;
   }
   d.idx16 = fits;
   if (fits) {
     std::vector<uint16_t> off(std::max<int64_t>(d.nnz, 1), 0);
+#pragma omp parallel for schedule(static, 4096)
     for (int i = 0; i < h.nrows; ++i)
       for (int64_t k = h.rp[i]; k < h.rp[i + 1]; ++k) off[k] = (uint16_t)(h.ci[k] - base[i]);
     d.cbase.upload(base, st);
@@ -354,21 +356,23 @@ static std::vector<int> block_row_lengths(const HostCSR &A) {
   if (A.nrows % 3 != 0 || A.ncols % 3 != 0 || A.nrows == 0) return {};
   const int nb = A.nrows / 3;
   std::vector<int> blen(nb);
+  int ok = 1;
+#pragma omp parallel for schedule(static, 4096) reduction(&& : ok)
   for (int I = 0; I < nb; ++I) {
     const int64_t len = A.rp[3 * I + 1] - A.rp[3 * I];
-    if (len % 3 != 0) return {};
-    for (int r = 1; r < 3; ++r)
-      if (A.rp[3 * I + r + 1] - A.rp[3 * I + r] != len) return {};
+    bool good = len % 3 == 0;
+    for (int r = 1; r < 3 && good; ++r) good = A.rp[3 * I + r + 1] - A.rp[3 * I + r] == len;
     const int64_t s0 = A.rp[3 * I];
-    for (int64_t k = 0; k < len; k += 3) {
+    for (int64_t k = 0; k < len && good; k += 3) {
       const int c = A.ci[s0 + k];
-      if (c % 3 != 0) return {};
-      for (int r = 0; r < 3; ++r)
-        for (int cc = 0; cc < 3; ++cc)
-          if (A.ci[A.rp[3 * I + r] + k + cc] != c + cc) return {};
+      good = c % 3 == 0;
+      for (int r = 0; r < 3 && good; ++r)
+        for (int cc = 0; cc < 3 && good; ++cc) good = A.ci[A.rp[3 * I + r] + k + cc] == c + cc;
     }
-    blen[I] = (int)(len / 3);
+    blen[I] = good ? (int)(len / 3) : 0;
+    ok = ok && good;
   }
+  if (!ok) return {};
   return blen;
 }
 
@@ -395,6 +399,7 @@ static bool build_sell3(const HostCSR &A, const std::vector<int> &blen, int T,
   const int64_t nslots = choff[nchunk];
   sci.assign(nslots, 0);
   planes.assign((size_t)9 * nslots, 0.0);
+#pragma omp parallel for schedule(static, 4096)
   for (int I = 0; I < nb; ++I) {
     const int c = I / C, l = I % C;
     const int64_t s0 = A.rp[3 * I];

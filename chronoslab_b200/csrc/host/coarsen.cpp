@@ -13,6 +13,10 @@
 #include "host.h"
 #include "../errors.h"
 
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
 namespace chronos {
 
 // ---- MT19937 -----------------------------------------------------------------
@@ -48,32 +52,60 @@ uint32_t MT19937::next_u32() {
 }
 
 // ---- CSR transposes ---------------------------------------------------------
-HostCSR csr_transpose_map(const HostCSR &A, std::vector<int64_t> &perm) {
+// Transpose of A with rows ascending in each column.  Parallel over blocks
+// of rows: every thread counts the columns of its block, the positions are
+// laid out column by column in block order, and every thread scatters its
+// block -- the same output as the sequential pass.  perm (when given)
+// receives, for each entry of the transpose, its index in A.
+static HostCSR transpose_impl(const HostCSR &A, std::vector<int64_t> *perm) {
   HostCSR T;
   T.nrows = A.ncols;
   T.ncols = A.nrows;
   T.rp.assign((size_t)T.nrows + 1, 0);
   const int64_t nnz = A.nnz();
-  for (int64_t k = 0; k < nnz; ++k) T.rp[(size_t)A.ci[k] + 1]++;
-  for (int i = 0; i < T.nrows; ++i) T.rp[i + 1] += T.rp[i];
+  const int nc = A.ncols;
+  int nt = 1;
+#ifdef _OPENMP
+  nt = std::max(1, std::min(omp_get_max_threads(), (int)(nnz / 262144) + 1));
+#endif
+  std::vector<int> rb(nt + 1);
+  for (int t = 0; t <= nt; ++t) rb[t] = (int)((int64_t)A.nrows * t / nt);
+  std::vector<std::vector<int64_t>> pos(nt, std::vector<int64_t>(nc, 0));
+#pragma omp parallel for num_threads(nt) schedule(static, 1)
+  for (int t = 0; t < nt; ++t)
+    for (int64_t k = A.rp[rb[t]]; k < A.rp[rb[t + 1]]; ++k) pos[t][A.ci[k]]++;
+  int64_t run = 0;
+  for (int c = 0; c < nc; ++c) {
+    for (int t = 0; t < nt; ++t) {
+      const int64_t cnt = pos[t][c];
+      pos[t][c] = run;
+      run += cnt;
+    }
+    T.rp[(size_t)c + 1] = run;
+  }
   T.ci.resize(nnz);
   T.v.resize(nnz);
-  perm.resize(nnz);
-  std::vector<int64_t> pos(T.rp.begin(), T.rp.end() - 1);
-  for (int i = 0; i < A.nrows; ++i)
-    for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-      int64_t d = pos[A.ci[k]]++;
-      T.ci[d] = i;
-      T.v[d] = A.v.empty() ? 0.0 : A.v[k];
-      perm[d] = k;
-    }
+  if (perm) perm->resize(nnz);
+  const bool vals = !A.v.empty();
+#pragma omp parallel for num_threads(nt) schedule(static, 1)
+  for (int t = 0; t < nt; ++t) {
+    std::vector<int64_t> &p = pos[t];
+    for (int i = rb[t]; i < rb[t + 1]; ++i)
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
+        const int64_t d = p[A.ci[k]]++;
+        T.ci[d] = i;
+        T.v[d] = vals ? A.v[k] : 0.0;
+        if (perm) (*perm)[d] = k;
+      }
+  }
   return T;
 }
 
-HostCSR csr_transpose(const HostCSR &A) {
-  std::vector<int64_t> perm;
-  return csr_transpose_map(A, perm);
+HostCSR csr_transpose_map(const HostCSR &A, std::vector<int64_t> &perm) {
+  return transpose_impl(A, &perm);
 }
+
+HostCSR csr_transpose(const HostCSR &A) { return transpose_impl(A, nullptr); }
 
 // ---- strength of connection ------------------------------------------------
 static std::vector<double> diagonal(const HostCSR &A) {
@@ -95,15 +127,29 @@ HostCSR soc_matrix(const HostCSR &A, const char *soc_type, double tau) {
   if (t == "DOM") {
     // cpt_SoC_dom.m:26-47: s_ij = |a_ij| / sqrt(d_i d_j), strong if s_ij > tau.
     CHRONOS_REQUIRE(tau >= 0, CHRONOS_ENOTSUP, "DOM strength with tau < 0 is outside this path");
+    // rows counted, then filled, in parallel (the same entries in row order)
+    auto strong = [&](int i, int64_t k, double &s) {
+      const double a = A.v[k];
+      if (a == 0.0) return false;
+      s = std::fabs(a) / std::sqrt(d[i] * d[A.ci[k]]);
+      return s > tau;
+    };
+#pragma omp parallel for schedule(static, 4096)
     for (int i = 0; i < n; ++i) {
-      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-        double a = A.v[k];
-        if (a == 0.0) continue;
-        int j = A.ci[k];
-        double s = std::fabs(a) / std::sqrt(d[i] * d[j]);
-        if (s > tau) { S.ci.push_back(j); S.v.push_back(s); }
-      }
-      S.rp[i + 1] = (int64_t)S.ci.size();
+      int64_t c = 0;
+      double s;
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) c += strong(i, k, s) ? 1 : 0;
+      S.rp[(size_t)i + 1] = c;
+    }
+    for (int i = 0; i < n; ++i) S.rp[(size_t)i + 1] += S.rp[i];
+    S.ci.resize(S.rp[n]);
+    S.v.resize(S.rp[n]);
+#pragma omp parallel for schedule(static, 4096)
+    for (int i = 0; i < n; ++i) {
+      int64_t o = S.rp[i];
+      double s;
+      for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k)
+        if (strong(i, k, s)) { S.ci[o] = A.ci[k]; S.v[o] = s; ++o; }
     }
     return S;
   }
@@ -166,31 +212,47 @@ std::vector<int> pmis_split(const HostCSR &A, const HostCSR &S, MT19937 &rng, in
   for (int j = 0; j < n; ++j)
     if (colcnt[j] == 1) fc[j] = -2;
 
-  // S without its diagonal; its transpose gives the columns S(:,inod)
+  // S without its diagonal (rows counted, then filled, in parallel); its
+  // transpose gives the columns S(:,inod)
   HostCSR So;
   So.nrows = So.ncols = n;
   So.rp.assign((size_t)n + 1, 0);
+#pragma omp parallel for schedule(static, 4096)
   for (int i = 0; i < n; ++i) {
+    int64_t c = 0;
+    for (int64_t k = S.rp[i]; k < S.rp[i + 1]; ++k) c += (S.ci[k] != i && S.v[k] != 0.0);
+    So.rp[(size_t)i + 1] = c;
+  }
+  for (int i = 0; i < n; ++i) So.rp[(size_t)i + 1] += So.rp[i];
+  So.ci.resize(So.rp[n]);
+  So.v.assign(So.rp[n], 1.0);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < n; ++i) {
+    int64_t o = So.rp[i];
     for (int64_t k = S.rp[i]; k < S.rp[i + 1]; ++k)
-      if (S.ci[k] != i && S.v[k] != 0.0) { So.ci.push_back(S.ci[k]); So.v.push_back(1.0); }
-    So.rp[i + 1] = (int64_t)So.ci.size();
+      if (S.ci[k] != i && S.v[k] != 0.0) So.ci[o++] = S.ci[k];
   }
   HostCSR St = csr_transpose(So);                 // row j of St = column j of S
   // S_sym = |S| + |S'|: union of the patterns of row j of S and of S'
   std::vector<int64_t> sym_rp((size_t)n + 1, 0);
-  std::vector<int> sym_ci;
-  sym_ci.reserve(So.ci.size() * 2);
-  for (int j = 0; j < n; ++j) {
-    int64_t a = So.rp[j], ae = So.rp[j + 1], b = St.rp[j], be = St.rp[j + 1];
+  auto merge = [&](int j, int *out) {
+    int64_t a = So.rp[j], ae = So.rp[j + 1], b = St.rp[j], be = St.rp[j + 1], m = 0;
     while (a < ae || b < be) {
-      int ca = a < ae ? So.ci[a] : INT32_MAX, cb = b < be ? St.ci[b] : INT32_MAX;
-      int c = std::min(ca, cb);
-      sym_ci.push_back(c);
+      const int ca = a < ae ? So.ci[a] : INT32_MAX, cb = b < be ? St.ci[b] : INT32_MAX;
+      const int c = std::min(ca, cb);
+      if (out) out[m] = c;
+      ++m;
       if (ca == c) ++a;
       if (cb == c) ++b;
     }
-    sym_rp[j + 1] = (int64_t)sym_ci.size();
-  }
+    return m;
+  };
+#pragma omp parallel for schedule(static, 4096)
+  for (int j = 0; j < n; ++j) sym_rp[(size_t)j + 1] = merge(j, nullptr);
+  for (int j = 0; j < n; ++j) sym_rp[(size_t)j + 1] += sym_rp[j];
+  std::vector<int> sym_ci(sym_rp[n]);
+#pragma omp parallel for schedule(static, 4096)
+  for (int j = 0; j < n; ++j) merge(j, sym_ci.data() + sym_rp[j]);
   // nod_weight = sum(S ~= 0, 1)' + rand(nn,1)
   std::vector<double> w(n), wfree(n);
   for (int j = 0; j < n; ++j) w[j] = (double)(St.rp[j + 1] - St.rp[j]);
@@ -199,36 +261,55 @@ std::vector<int> pmis_split(const HostCSR &A, const HostCSR &S, MT19937 &rng, in
     if (fc[j] == -2) fc[j] = -1;
     wfree[j] = fc[j] == -1 ? -1.0 : w[j];
   }
-  std::vector<int> list;
-  list.reserve(n);
+  // cpt_PMIS.m's sweep makes an undecided node coarse once no undecided
+  // neighbour (in S + S') outweighs it, and then makes the nodes it strongly
+  // influences fine -- a coarse node included, which only a lighter node can
+  // do.  The outcome therefore does not depend on the order of the sweep
+  // (the weights differ: integer counts plus 53-bit random fractions), and
+  // rounds give it in parallel: every undecided node that outweighs all its
+  // undecided neighbours turns coarse (no two of them are neighbours), then
+  // the nodes they influence turn fine, until no node is undecided.
+  std::vector<int> und, next, newc;
+  und.reserve(n);
   for (int j = 0; j < n; ++j)
-    if (fc[j] == 0) list.push_back(j);
-  int64_t len = (int64_t)list.size();
-  int64_t ind = 0;
-  while (len > 0) {
-    const int inod = list[ind];
-    if (fc[inod] != 0) {
-      list[ind] = list[len - 1];
-      --len;
-    } else {
+    if (fc[j] == 0) und.push_back(j);
+  std::vector<char> pick(n, 0);
+  while (!und.empty()) {
+    const int64_t m = (int64_t)und.size();
+#pragma omp parallel for schedule(static, 1024)
+    for (int64_t q = 0; q < m; ++q) {
+      const int i = und[q];
+      const double wi = w[i];
       bool is_coarse = true;
-      const double wi = w[inod];
-      for (int64_t k = sym_rp[inod]; k < sym_rp[inod + 1]; ++k)
+      for (int64_t k = sym_rp[i]; k < sym_rp[i + 1]; ++k)
         if (wfree[sym_ci[k]] > wi) { is_coarse = false; break; }
-      if (!is_coarse) {
-        ++ind;
-      } else {
-        for (int64_t k = St.rp[inod]; k < St.rp[inod + 1]; ++k) {
-          fc[St.ci[k]] = -1;
-          wfree[St.ci[k]] = -1.0;
-        }
-        fc[inod] = 1;
-        wfree[inod] = -1.0;
-        list[ind] = list[len - 1];
-        --len;
+      pick[i] = is_coarse ? 1 : 0;
+    }
+    newc.clear();
+    for (int64_t q = 0; q < m; ++q)
+      if (pick[und[q]]) newc.push_back(und[q]);
+    CHRONOS_REQUIRE(!newc.empty(), CHRONOS_EINVAL, "PMIS made no progress (equal node weights)");
+    for (int i : newc) {
+      fc[i] = 1;
+      wfree[i] = -1.0;
+    }
+    const int64_t nn = (int64_t)newc.size();
+#pragma omp parallel for schedule(static, 256)
+    for (int64_t q = 0; q < nn; ++q) {
+      const int i = newc[q];
+      for (int64_t k = St.rp[i]; k < St.rp[i + 1]; ++k) {
+        const int j = St.ci[k];
+#pragma omp atomic write
+        fc[j] = -1;
+#pragma omp atomic write
+        wfree[j] = -1.0;
       }
     }
-    if (ind > len - 1) ind = 0;
+    next.clear();
+    for (int64_t q = 0; q < m; ++q)
+      if (fc[und[q]] == 0) next.push_back(und[q]);
+    und.swap(next);
+    for (int i : newc) pick[i] = 0;
   }
   int nc = 0, nf = 0;
   for (int j = 0; j < n; ++j) {
