@@ -276,11 +276,14 @@ def dense_chol(A):
     return L.reshape(n, n).T.copy()
 
 
-def spmv(A, x, precision=CHRONOS_FP64):
+def spmv(A, x, precision=CHRONOS_FP64, format=0, lanes=0):
+    """y = A x on the GPU through the V-cycle's apply kernels (format: 0 tuned,
+    1 row-grouped CSR, 2 sliced ELL; lanes > 0 forces the CSR lanes per row)."""
     n, ip, ix, dv = _csr(A)
     x = np.ascontiguousarray(x, np.float64)
     y = np.zeros(n, np.float64)
-    check(load().chronos_spmv(n, A.shape[1], _pi(ip), _pi(ix), _pd(dv), _pd(x), _pd(y), precision))
+    check(load().chronos_spmv(n, A.shape[1], _pi(ip), _pi(ix), _pd(dv), _pd(x), _pd(y), precision,
+                              format, lanes))
     return y
 
 

@@ -98,7 +98,7 @@ SIGNATURES = {
     "chronos_galerkin_fetch": [_vp, _pi, _pi, _pd],
     "chronos_galerkin_free": [_vp],
     "chronos_dense_chol": [_i, _pd, _pd],
-    "chronos_spmv": [_i, _i, _pi, _pi, _pd, _pd, _pd, _i],
+    "chronos_spmv": [_i, _i, _pi, _pi, _pd, _pd, _pd, _i, _i, _i],
     "chronos_amg_setup": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _i, _pd, _pp],
     "chronos_hier_free": [_vp],
     "chronos_hier_nlevels": [_vp, _pi],

@@ -392,29 +392,35 @@ int chronos_dense_chol(int n, const double *A_h, double *L_h) {
 }
 
 int chronos_spmv(int n, int ncols, const int *iat_h, const int *ja_h, const double *val_h,
-                 const double *x_h, double *y_h, int precision) {
+                 const double *x_h, double *y_h, int precision, int format, int lanes) {
   return guard([&] {
     CHRONOS_REQUIRE(x_h && y_h, CHRONOS_EINVAL, "null vector");
+    CHRONOS_REQUIRE(format >= 0 && format <= 2, CHRONOS_EINVAL, "format must be 0, 1 or 2");
+    CHRONOS_REQUIRE(lanes == 0 || lanes == 1 || lanes == 2 || lanes == 4 || lanes == 8 ||
+                        lanes == 16 || lanes == 32, CHRONOS_EINVAL,
+                    "lanes must be 0, 1, 2, 4, 8, 16 or 32");
     HostCSR A = from_csr0(n, ncols, iat_h, ja_h, val_h);
     ScopedStream s;
     DMat d;
     const bool fp32 = precision == CHRONOS_FP32;
     upload_csr(A, d, fp32, s.st);
-    autotune_lanes(d, fp32, s.st);
+    if (lanes > 0 && format != 2) set_lanes(d, lanes, s.st);
+    else autotune_lanes(d, fp32, s.st, format);
     if (fp32) {
       std::vector<float> xf(x_h, x_h + ncols), yf(n);
       DBuf<float> x, y(n);
       x.upload(xf, s.st);
-      csr_apply<float, float, float, float, MODE_PLAIN, false>(s.st, d.lanes, n, d.rp, d.ci, d.v32,
-                                                              x.get(), nullptr, y.get(), 1.0f);
+      mat_apply<float, float, float, float, MODE_PLAIN, false>(s.st, d, d.v32.get(), x.get(),
+                                                              (const float *)nullptr, y.get(),
+                                                              1.0f);
       y.download(yf.data(), n, s.st);
       CHRONOS_CUDA(cudaStreamSynchronize(s.st));
       for (int i = 0; i < n; ++i) y_h[i] = yf[i];
     } else {
       DBuf<double> x, y(n);
       x.upload(x_h, ncols, s.st);
-      csr_apply<double, double, double, double, MODE_PLAIN, false>(
-          s.st, d.lanes, n, d.rp, d.ci, d.v64, x.get(), nullptr, y.get(), 1.0);
+      mat_apply<double, double, double, double, MODE_PLAIN, false>(
+          s.st, d, d.v64.get(), x.get(), (const double *)nullptr, y.get(), 1.0);
       y.download(y_h, n, s.st);
       CHRONOS_CUDA(cudaStreamSynchronize(s.st));
     }

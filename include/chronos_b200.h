@@ -239,9 +239,13 @@ int chronos_galerkin_free(chronos_galerkin_plan *plan);
 int chronos_dense_chol(int n, const double *A_h, double *L_h);
 
 /* ---- CSR SpMV on the GPU (parity helper) ------------------------------- */
-/* y = A x, 0-based CSR, values stored in `precision` and accumulated in it. */
+/* y = A x, 0-based CSR, values stored in `precision` and accumulated in it,
+ * through the V-cycle's apply kernels.  format as chronos_params.spmv_format
+ * (0 tuned, 1 row-grouped CSR, 2 sliced ELL); lanes > 0 forces the CSR path's
+ * lanes per row (1, 2, 4, 8, 16 or 32; rows longer than 32 per lane go to
+ * whole warps). */
 int chronos_spmv(int n, int ncols, const int *iat_h, const int *ja_h, const double *val_h,
-                 const double *x_h, double *y_h, int precision);
+                 const double *x_h, double *y_h, int precision, int format, int lanes);
 
 /* ---- AMG hierarchy ------------------------------------------------------ */
 typedef struct chronos_hier chronos_hier;

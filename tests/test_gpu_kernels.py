@@ -126,3 +126,41 @@ def test_dense_chol_not_spd(lib):
     with pytest.raises(cb.ChronosError) as e:
         cb.dense_chol(A)
     assert e.value.code == -4
+
+
+def mixed_rows(n=3000, ncols=2500, seed=7):
+    """Mostly 3 entries per row, every 41st row 150-400 entries (the long-row
+    path of every group width), every 97th row empty; columns spread so
+    some rows need 32-bit columns and the rest 16-bit offsets."""
+    rng = np.random.default_rng(seed)
+    rows, cols = [], []
+    for i in range(n):
+        if i % 97 == 5:
+            continue
+        m = int(rng.integers(150, 400)) if i % 41 == 3 else 3
+        c = rng.choice(ncols, size=m, replace=False)
+        rows += [i] * m
+        cols += c.tolist()
+    vals = rng.uniform(-1, 1, len(rows))
+    A = sp.csr_matrix((vals, (rows, cols)), shape=(n, ncols))
+    A.sort_indices()
+    return A
+
+
+@pytest.mark.parametrize("ncols", [2500, 100000])          # 16-bit offsets / int32 columns
+@pytest.mark.parametrize("precision", [cb.CHRONOS_FP64, cb.CHRONOS_FP32])
+@pytest.mark.parametrize("fmt,lanes", [(1, 1), (1, 2), (1, 4), (1, 8), (1, 16), (1, 32), (2, 0),
+                                       (0, 0)])
+def test_apply_kernels_long_rows(lib, precision, fmt, lanes, ncols):
+    """Every group width of the row-grouped CSR kernel and the sliced ELL
+    kernel, with long rows (warp path), empty rows, and column spans that fit
+    16-bit offsets or need int32 columns."""
+    A = mixed_rows(ncols=ncols)
+    x = np.random.default_rng(1).uniform(-1, 1, A.shape[1])
+    y = cb.spmv(A, x, precision, format=fmt, lanes=lanes)
+    if precision == cb.CHRONOS_FP32:
+        ref = (A.astype(np.float32) @ x.astype(np.float32)).astype(np.float64)
+        assert rel(y, ref) <= 2e-6
+    else:
+        assert rel(y, A @ x) <= 1e-14
+    assert np.all(y[5::97] == 0.0)
