@@ -367,14 +367,21 @@ def run_product(args, world, rank, local):
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms32, ms64, ms32x = tt.tolist()
 
-    # end to end through the public call with host buffers
+    # end to end through the public call with host buffers: b and x0 in pinned
+    # host memory, copied to the device and the solution back inside the call
     e2e = []
-    xh = np.zeros(n)
+    bh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    xh = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    bh[:] = b
+    xh[:] = 0.0
+    h32.pcg_host(bh, xh, args.itmax, args.tol)       # untimed: the staging buffers
     barrier()
-    for _ in range(max(2, args.steps // 2)):
+    for _ in range(args.steps):
+        xh[:] = 0.0                                   # x0 = 0, set before the clock starts
         t = time.perf_counter()
-        xh, it, rv, flag, _ = h32.pcg(b, np.zeros(n), args.itmax, args.tol)
+        it, flag, _ = h32.pcg_host(bh, xh, args.itmax, args.tol)
         e2e.append((time.perf_counter() - t) * 1e3)
+        assert flag == 0, "host-buffer PCG did not converge"
     e2e_ms = sum(e2e) / len(e2e)
     if dist:
         tt = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)

@@ -400,6 +400,21 @@ class Hierarchy:
                                     C.byref(flag), C.byref(sec)))
         return x, it.value, rv[:it.value + 1], flag.value, sec.value
 
+    def pcg_host(self, b, x, itmax=1000, tol=1e-8):
+        """PCG on caller-owned host vectors, in place: b and x (x0 on entry,
+        the solution on return) are C-contiguous float64 arrays of length n,
+        passed to chronos_pcg without a copy, so pinned (page-locked) buffers
+        stay pinned for the library's host-device copies."""
+        for v in (b, x):
+            if not (isinstance(v, np.ndarray) and v.dtype == np.float64 and v.ndim == 1
+                    and v.flags.c_contiguous and v.size == self.n):
+                raise ChronosError(-1, "pcg_host: b and x must be contiguous "
+                                   "float64 arrays of length n")
+        it, flag, sec = C.c_int(), C.c_int(), C.c_double()
+        check(self._lib.chronos_pcg(self._h, _pd(b), _pd(x), itmax, tol, C.byref(it), None,
+                                    C.byref(flag), C.byref(sec)))
+        return it.value, flag.value, sec.value
+
     def pcg_dev(self, b_ptr, x_ptr, itmax=1000, tol=1e-8):
         """PCG on device FP64 vectors (raw pointers, e.g. torch tensor.data_ptr())."""
         it, flag, sec = C.c_int(), C.c_int(), C.c_double()
