@@ -224,6 +224,19 @@ def coarsen(A, prm=None, rng_skip=0):
     return fc.astype(np.int64), nc.value, _CsrHandle.take(h)
 
 
+def coarsen_device(A, prm=None, rng_skip=0):
+    """DOM strength + PMIS on the GPU: (fcnode, nc, S pattern), the same
+    splitting as coarsen()."""
+    prm = prm or params()
+    n, ip, ix, dv = _csr(A)
+    fc = np.zeros(n, np.int32)
+    nc = C.c_int()
+    h = C.c_void_p()
+    check(load().chronos_coarsen_device(C.byref(prm), n, _pi(ip), _pi(ix), _pd(dv), rng_skip,
+                                        _pi(fc), C.byref(nc), C.byref(h)))
+    return fc.astype(np.int64), nc.value, _CsrHandle.take(h)
+
+
 def bamg(S, fcnode, TV, prm=None):
     """BAMG prolongation on the host: (P, c_mark)."""
     prm = prm or params()

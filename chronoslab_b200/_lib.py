@@ -89,6 +89,8 @@ SIGNATURES = {
     "chronos_hier_dump_ext_bin": [_vp, _i, C.c_char, C.c_char_p],
     "chronos_fsai_pattern": [_i, _pi, _pi, _pd, _i, _i, _d, _i, _i, _pi, _pp],
     "chronos_coarsen": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _u64, _pi, _pi, _pp],
+    "chronos_coarsen_device": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _u64, _pi, _pi,
+                               _pp],
     "chronos_bamg": [C.POINTER(chronos_params), _i, _pi, _pi, _pi, _i, _pd, _pi, _pp],
     "chronos_fsai_compute": [_i, _i, _i, _d, _d, _i, _i, _i64, _pi64, _pi, _pd, _pi64, _pi64,
                              _pi, _pd, _pi],

@@ -23,7 +23,8 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 # The system g++ carries libgomp's link spec (a CXX from the environment may not).
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
-CU_SOURCES = ["setup_kernels.cu", "hier.cu", "block.cu", "batch.cu", "group.cu", "capi.cu"]
+CU_SOURCES = ["setup_kernels.cu", "hier.cu", "block.cu", "batch.cu", "group.cu", "capi.cu",
+              "coarsen_gpu.cu"]
 CPP_SOURCES = ["host/params.cpp", "host/coarsen.cpp", "host/bamg.cpp", "host/fsai_pattern.cpp",
                "host/formats.cpp"]
 HEADERS = ["common.cuh", "errors.h", "internal.h", "hier.h", "group.h", "spmv.cuh", "host/host.h"]

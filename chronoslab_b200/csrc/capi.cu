@@ -227,6 +227,41 @@ int chronos_coarsen(const chronos_params *prm, int n, const int *iat_h, const in
   });
 }
 
+int chronos_coarsen_device(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
+                           const double *val_h, uint64_t rng_skip, int *fcnode_h, int *nc,
+                           chronos_csr **S) {
+  return guard([&] {
+    CHRONOS_REQUIRE(prm && fcnode_h && nc && n > 0, CHRONOS_EINVAL, "bad argument");
+    std::string t(prm->SoC_type);
+    for (auto &c : t) c = (char)toupper(c);
+    CHRONOS_REQUIRE(t == "DOM", CHRONOS_ENOTSUP,
+                    "the GPU coarsening computes DOM strength only (SoC type " + t + ")");
+    HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
+    validate_csr(A);
+    MT19937 rng((uint32_t)(prm->seed ? prm->seed : 5489));
+    for (uint64_t k = 0; k < rng_skip; ++k) rng.next_res53();
+    cudaStream_t st;
+    CHRONOS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    try {
+      DMat d;
+      upload_csr(A, d, false, st);
+      HostCSR Sm;
+      std::vector<int> fc;
+      coarsen_dom_device(n, d.rp, d.ci, d.v64, prm->soc_tau, rng, Sm, fc, nc, st);
+      CHRONOS_CUDA(cudaStreamSynchronize(st));
+      std::memcpy(fcnode_h, fc.data(), sizeof(int) * n);
+      if (S) {
+        Sm.v.assign(Sm.ci.size(), 1.0);
+        *S = wrap_csr(std::move(Sm));
+      }
+    } catch (...) {
+      cudaStreamDestroy(st);
+      throw;
+    }
+    cudaStreamDestroy(st);
+  });
+}
+
 int chronos_bamg(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
                  const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
                  chronos_csr **P) {

@@ -620,7 +620,7 @@ static HostCSR download_csr(int nrows, int ncols, const DBuf<int> &rp, const DBu
   return h;
 }
 
-static void validate_csr(const HostCSR &A) {
+void validate_csr(const HostCSR &A) {
   CHRONOS_REQUIRE(A.nrows > 0 && A.ncols == A.nrows, CHRONOS_EINVAL, "matrix must be square, n > 0");
   CHRONOS_REQUIRE((int64_t)A.rp.size() == (int64_t)A.nrows + 1 && A.rp[0] == 0, CHRONOS_EINVAL,
                   "malformed CSR row pointers");
@@ -708,6 +708,16 @@ static HostCSR smooth_prolongation(const HostCSR &A, const DMat &dA, const HostC
     Ps.rp.push_back((int64_t)Ps.ci.size());
   }
   return Ps;
+}
+
+bool gpu_coarsening(const char *soc_type) {
+  static const bool on = [] {
+    const char *e = std::getenv("CHRONOS_GPU_COARSEN");
+    return !(e && e[0] == '0');
+  }();
+  std::string t(soc_type);
+  for (auto &c : t) c = (char)toupper(c);
+  return on && t == "DOM";
 }
 
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A0, int ntv0,
@@ -855,9 +865,15 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
     // ---- test space, coarsening --------------------------------------------
     t0 = now_s();
     qr_orthonormalize(n, ntv, TV.data());
-    HostCSR S = soc_matrix(Al, prm.SoC_type, prm.soc_tau);
+    HostCSR S;
     int nc = 0;
-    std::vector<int> fcn = pmis_split(Al, S, rng, &nc);
+    std::vector<int> fcn;
+    if (gpu_coarsening(prm.SoC_type)) {
+      coarsen_dom_device(n, L.A.rp, L.A.ci, L.A.v64, prm.soc_tau, rng, S, fcn, &nc, st);
+    } else {
+      S = soc_matrix(Al, prm.SoC_type, prm.soc_tau);
+      fcn = pmis_split(Al, S, rng, &nc);
+    }
     CHRONOS_REQUIRE(nc > 0 && nc < n, CHRONOS_EINVAL, "coarsening produced no usable coarse level");
     T[3] += now_s() - t0;
     // ---- BAMG prolongation -----------------------------------------------------

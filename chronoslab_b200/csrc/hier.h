@@ -12,6 +12,23 @@
 
 namespace chronos {
 
+// DOM strength of connection and PMIS C/F splitting on the GPU
+// (coarsen_gpu.cu) for the device CSR (rp, ci, v) of an n x n level:
+// fcnode numbered as the reference numbers it, nc coarse nodes, and S the
+// strength pattern (values left empty) for the host prolongation.  Draws n
+// numbers from rng, as pmis_split does; bit-identical to soc_matrix("DOM")
+// + pmis_split.
+void coarsen_dom_device(int n, const int *rp, const int *ci, const double *v, double tau,
+                        MT19937 &rng, HostCSR &S, std::vector<int> &fcnode, int *nc_out,
+                        cudaStream_t st);
+
+// Square, sorted, in-range, finite CSR, or CHRONOS_EINVAL.
+void validate_csr(const HostCSR &A);
+
+// Whether the setup coarsens on the GPU: DOM strength (the only kind the
+// GPU path computes) and CHRONOS_GPU_COARSEN not set to 0.
+bool gpu_coarsening(const char *soc_type);
+
 struct Level {
   int n = 0, nc = 0;
   bool coarsest = false;

@@ -209,6 +209,13 @@ int chronos_fsai_pattern(int n, const int *iat_h, const int *ja_h, const double 
 int chronos_coarsen(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
                     const double *val_h, uint64_t rng_skip, int *fcnode_h, int *nc,
                     chronos_csr **S);
+/* The same on the GPU for DOM strength (cpt_SoC_dom.m:26-47, cpt_PMIS.m,
+ * mark_isolated_nodes.m): identical fcnode and nc, and S with the strength
+ * pattern (values 1).  CHRONOS_ENOTSUP for another SoC type.  The hierarchy
+ * setup coarsens DOM levels this way unless CHRONOS_GPU_COARSEN=0. */
+int chronos_coarsen_device(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
+                           const double *val_h, uint64_t rng_skip, int *fcnode_h, int *nc,
+                           chronos_csr **S);
 /* cpt_ProlMEX_BAMG on the host: BAMG prolongation (n x nc) from the strength
  * pattern S, fcnode as returned by chronos_coarsen, and the test space TV
  * (n x ntv, column-major).  c_mark_h[n] (may be NULL) flags rows not
