@@ -462,6 +462,25 @@ class Hierarchy:
                                      C.byref(rel), C.byref(info)))
         return x, info.value, rel.value, it.value
 
+    def gmres(self, b, restart=50, tol=1e-6, maxit=2, x0=None, A=None):
+        """gmres_RIGHT with the V-cycle as right preconditioner; A (optional)
+        is the operator, else the level-1 operator of the hierarchy.  Returns
+        (x, flag, relres, (outer, inner), resvec)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
+        if A is not None:
+            _, ip, ix, dv = _csr(A)
+            ops = (_pi(ip), _pi(ix), _pd(dv))
+        else:
+            ops = (None, None, None)
+        io, ii, fl, nrv = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        rel = C.c_double()
+        rv = np.zeros(max(restart, 0) * max(maxit, 0) + 1)
+        check(self._lib.chronos_gmres(self._h, *ops, _pd(b), _pd(x), restart, tol, maxit,
+                                      C.byref(io), C.byref(ii), C.byref(rel), C.byref(fl),
+                                      _pd(rv), C.byref(nrv)))
+        return x, fl.value, rel.value, (io.value, ii.value), rv[:nrv.value]
+
     def adjoint_grad(self, u, g, itmax=1000, tol=1e-10):
         """dJ/dA on A's pattern for J with dJ/du = g (A SPD): returns
         (lambda, grad values in A's CSR order, iterations)."""

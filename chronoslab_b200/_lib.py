@@ -118,6 +118,7 @@ SIGNATURES = {
     "chronos_batch_info": [_vp, _i, _pi, _pi],
     "chronos_batch_free": [_vp],
     "chronos_sqmr":[_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _pi, _pd, _pi],
+    "chronos_gmres": [_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _i, _pi, _pi, _pd, _pi, _pd, _pi],
     "chronos_adjoint_grad": [_vp, _pd, _pd, _i, _d, _pd, _pd, _pi],
 }
 _RESTYPE = {"chronos_params_default": None, "chronos_version": C.c_char_p}

@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["setup_kernels.cu", "hier.cu", "block.cu", "batch.cu", "group.cu", "capi.cu",
-              "coarsen_gpu.cu"]
+              "coarsen_gpu.cu", "gmres.cu"]
 CPP_SOURCES = ["host/params.cpp", "host/coarsen.cpp", "host/bamg.cpp", "host/fsai_pattern.cpp",
                "host/formats.cpp"]
 HEADERS = ["common.cuh", "errors.h", "internal.h", "hier.h", "group.h", "spmv.cuh", "host/host.h"]

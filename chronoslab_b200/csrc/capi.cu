@@ -729,6 +729,43 @@ int chronos_sqmr(chronos_hier *hh, const int *iat_h, const int *ja_h, const doub
   });
 }
 
+int chronos_gmres(chronos_hier *hh, const int *iat_h, const int *ja_h, const double *val_h,
+                  const double *b_h, double *x_h, int restart, double tol, int maxit,
+                  int *iter_outer, int *iter_inner, double *relres, int *flag,
+                  double *resvec_h, int *nresvec) {
+  return guard([&] {
+    CHRONOS_REQUIRE(hh && b_h && x_h && iter_outer && iter_inner && relres && flag,
+                    CHRONOS_EINVAL, "null argument");
+    CHRONOS_REQUIRE(restart >= 0 && maxit >= 0, CHRONOS_EINVAL, "restart and maxit must be >= 0");
+    Hier &h = *hh->h;
+    cudaStream_t st = h.st;
+    const int n = h.levels[0].n;
+    DMat op;
+    if (iat_h) {
+      upload_csr(from_csr0(n, n, iat_h, ja_h, val_h), op, false, st);
+      autotune_lanes(op, false, st);
+    }
+    auto apply_op = [&](const double *x, double *y) {
+      if (!iat_h) { h.apply_A(x, y); return; }
+      csr_apply<double, double, double, double, MODE_PLAIN, false>(st, op.lanes, n, op.rp, op.ci,
+                                                                  op.v64, x, nullptr, y, 1.0);
+    };
+    DBuf<double> b, x;
+    b.upload(b_h, n, st);
+    x.upload(x_h, n, st);
+    GmresResult r;
+    gmres_right_device(h, apply_op, b.get(), x.get(), restart, tol, maxit, r);
+    x.download(x_h, n, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    *iter_outer = r.outer;
+    *iter_inner = r.inner;
+    *relres = r.relres;
+    *flag = r.flag;
+    if (nresvec) *nresvec = (int)r.resvec.size();
+    if (resvec_h) std::memcpy(resvec_h, r.resvec.data(), sizeof(double) * r.resvec.size());
+  });
+}
+
 int chronos_adjoint_grad(chronos_hier *hh, const double *u_h, const double *g_h, int itmax,
                          double tol, double *lambda_h, double *grad_h, int *iters) {
   return guard([&] {

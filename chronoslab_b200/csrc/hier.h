@@ -22,6 +22,21 @@ void coarsen_dom_device(int n, const int *rp, const int *ci, const double *v, do
                         MT19937 &rng, HostCSR &S, std::vector<int> &fcnode, int *nc_out,
                         cudaStream_t st);
 
+// Outcome of gmres_right_device, as gmres_RIGHT.m returns it.
+struct GmresResult {
+  int flag = 1, outer = 0, inner = 0;
+  double relres = 0.0;
+  std::vector<double> resvec;
+};
+
+struct Hier;
+// Right-preconditioned restarted GMRES (gmres.cu) on device vectors b, x (x0
+// on entry), the hierarchy's V-cycle as the preconditioner and apply_op as
+// the operator.
+void gmres_right_device(Hier &h, const std::function<void(const double *, double *)> &apply_op,
+                        const double *b, double *x, int restart, double tol, int maxit,
+                        GmresResult &res);
+
 // Square, sorted, in-range, finite CSR, or CHRONOS_EINVAL.
 void validate_csr(const HostCSR &A);
 

@@ -353,6 +353,19 @@ int chronos_batch_free(chronos_batch *b);
 int chronos_sqmr(chronos_hier *h, const int *iat_h, const int *ja_h, const double *val_h,
                  const double *b_h, double *x_h, int itmax, double tol, int *iters,
                  double *relres, int *info);
+/* gmres_RIGHT.m (LinearSolver/GMRES_CJ/gmres_RIGHT.m:7-650), as
+ * Tests/CubeBAMG_EMIN.m:30 calls it: right-preconditioned GMRES(restart) with
+ * the hierarchy's V-cycle as M, at most maxit restart cycles, operator A from
+ * (iat_h, ja_h, val_h) (0-based CSR) or, when iat_h is NULL, the hierarchy's
+ * level-1 operator.  x_h holds x0 on entry.  flag: 0 converged (explicit
+ * residual <= tol ||b||), 1 maxit cycles, 2 non-finite preconditioned vector,
+ * 3 stagnation; iter_outer / iter_inner as the reference's iter(1:2) (the
+ * total is (outer-1)*restart + inner).  resvec_h (may be NULL) receives
+ * *nresvec <= restart*maxit+1 residual norms. */
+int chronos_gmres(chronos_hier *h, const int *iat_h, const int *ja_h, const double *val_h,
+                  const double *b_h, double *x_h, int restart, double tol, int maxit,
+                  int *iter_outer, int *iter_inner, double *relres, int *flag,
+                  double *resvec_h, int *nresvec);
 
 /* ---- Adjoint ------------------------------------------------------------ */
 /* For J(u) with u = A^{-1} b and dJ/du = g: solves A lambda = g with the same

@@ -642,6 +642,200 @@ def sqmr(Afun, rhs, tol, itmax, lprec, rprec=lambda v: v, x0=None):
     return pnew, info, relres, niter, resvec[:niter]
 
 
+def _sgn(v):
+    """scalarsign: sign with sign(0) = 1."""
+    return -1.0 if v < 0 else 1.0
+
+
+def _solve_upper(R, y):
+    """Solution of R z = y for upper-triangular R (back substitution)."""
+    import scipy.linalg as sla
+    return sla.solve_triangular(np.triu(R), y, lower=False)
+
+
+def gmres_right(afun, b, restart, tol, maxit, mfun=None, x0=None):
+    """Right-preconditioned restarted GMRES with Householder Arnoldi,
+    restating gmres_RIGHT.m (LinearSolver/GMRES_CJ/gmres_RIGHT.m:7-650):
+    inner iterations test the implicit residual |w(k+1)| <= tol*||b||
+    (:398-409), confirm it with the explicit residual of x + inv(M) U y
+    (:410-485), take up to maxmsteps more steps when it is not confirmed
+    (:486-540), and restart from the iterate of minimal residual (:552-627).
+    Returns (x, flag, relres, (outer, inner), resvec)."""
+    n = b.shape[0]
+    eps = np.finfo(float).eps
+    M = mfun if mfun is not None else (lambda v: v)
+    restart = max(int(restart), 0)
+    outer, inner = max(int(maxit), 0), min(restart, n)                   # :143-157
+    n2b = np.linalg.norm(b)
+    if n2b == 0:                                                         # :160-172
+        return np.zeros(n), 0, 0.0, (0, 0), np.zeros(1)
+    x = np.zeros(n) if x0 is None else np.array(x0, dtype=float)
+    flag = 1
+    xmin = x.copy()
+    imin = jmin = 0
+    tolb = tol * n2b
+    evalxm = 0
+    stag = 0
+    moresteps = 0
+    maxmsteps = min(n // 50, 5, n - maxit)                               # :221
+    maxstagsteps = 3
+    minupdated = 0
+    r = b - afun(x)
+    normr = np.linalg.norm(r)
+    if normr <= tolb:                                                    # :226-237
+        return x, 0, normr / n2b, (0, 0), np.array([normr])
+    resvec = np.zeros(inner * outer + 1)
+    resvec[0] = normr
+    normrmin = normr
+    J = np.zeros((2, inner))
+    U = np.zeros((n, inner))
+    R = np.zeros((inner, inner))
+    w = np.zeros(inner + 1)
+    it = (0, 0)
+    outiter = initer = 0
+    normr_act = normr
+    xm = x
+
+    def expand(y, k):
+        """Product of the first k reflectors applied to y(1:k) (:412-418)."""
+        add = U[:, k - 1] * (-2.0 * y[k - 1] * U[k - 1, k - 1])
+        add[k - 1] += y[k - 1]
+        for j in range(k - 1, 0, -1):
+            add[j - 1] += y[j - 1]
+            add = add - U[:, j - 1] * (2.0 * (U[:, j - 1] @ add))
+        return add
+
+    for outiter in range(1, outer + 1):
+        u = r.copy()                                                     # :302-316
+        normr = np.linalg.norm(r)
+        beta = _sgn(r[0]) * normr
+        u[0] += beta
+        u = u / np.linalg.norm(u)
+        U[:, 0] = u
+        w[:] = 0.0
+        w[0] = -beta
+        for initer in range(1, inner + 1):
+            v = -2.0 * u[initer - 1] * u                                 # :317-331
+            v[initer - 1] += 1.0
+            for k in range(initer - 1, 0, -1):
+                v = v - U[:, k - 1] * (2.0 * (U[:, k - 1] @ v))
+            v = M(v)                                                     # :332-352
+            if not np.all(np.isfinite(v)):
+                flag = 2
+                break
+            v = afun(v)
+            for k in range(1, initer + 1):                               # :353-356
+                v = v - U[:, k - 1] * (2.0 * (U[:, k - 1] @ v))
+            if initer != n:                                              # :359-378
+                u = v.copy()
+                u[:initer] = 0.0
+                alpha = np.linalg.norm(u)
+                if alpha != 0:
+                    alpha = _sgn(v[initer]) * alpha
+                    u[initer] += alpha
+                    u = u / np.linalg.norm(u)
+                    if initer < inner:
+                        U[:, initer] = u
+                    v[initer + 1:] = 0.0
+                    v[initer] = -alpha
+            for c in range(initer - 1):                                  # :380-384
+                tmp = v[c]
+                v[c] = J[0, c] * v[c] + J[1, c] * v[c + 1]
+                v[c + 1] = -J[1, c] * tmp + J[0, c] * v[c + 1]
+            if initer != n:                                              # :387-395
+                rho = np.linalg.norm(v[initer - 1:initer + 1])
+                J[:, initer - 1] = v[initer - 1:initer + 1] / rho
+                w[initer] = -J[1, initer - 1] * w[initer - 1]
+                w[initer - 1] = J[0, initer - 1] * w[initer - 1]
+                v[initer - 1] = rho
+                v[initer] = 0.0
+            R[:, initer - 1] = v[:inner]
+            normr = abs(w[initer])                                       # :396-406
+            resvec[(outiter - 1) * inner + initer] = normr
+            normr_act = normr
+            if normr <= tolb or stag >= maxstagsteps or moresteps:       # :409
+                if evalxm == 0:                                          # :410-442
+                    ytmp = _solve_upper(R[:initer, :initer], w[:initer])
+                    add = expand(ytmp, initer)
+                    stag = stag + 1 if np.linalg.norm(add) < eps * np.linalg.norm(x) else 0
+                    add = M(add)
+                    if not np.all(np.isfinite(add)):
+                        flag = 2
+                        break
+                    xm = x + add
+                    evalxm = 1
+                else:                                                    # :443-476
+                    Rk = np.triu(R[:initer, :initer])
+                    last = w[initer - 1] / Rk[initer - 1, initer - 1]
+                    head = (-_solve_upper(Rk[:initer - 1, :initer - 1],
+                                          Rk[:initer - 1, initer - 1]) * last
+                            if initer > 1 else np.zeros(0))
+                    addvc = np.append(head, last)
+                    stag = stag + 1 if np.linalg.norm(addvc) < eps * np.linalg.norm(xm) else 0
+                    add = M(expand(addvc, initer))
+                    if not np.all(np.isfinite(add)):
+                        flag = 2
+                        break
+                    xm = xm + add
+                r = b - afun(xm)                                         # :477-484
+                if np.linalg.norm(r) <= tol * n2b:
+                    x = xm
+                    flag = 0
+                    it = (outiter, initer)
+                    break
+                normr_act = np.linalg.norm(r)
+                resvec[(outiter - 1) * inner + initer] = normr_act
+                if normr_act <= normrmin:                                # :496-508
+                    normrmin, imin, jmin, xmin, minupdated = normr_act, outiter, initer, xm, 1
+                if normr_act <= tolb:
+                    x = xm
+                    flag = 0
+                    it = (outiter, initer)
+                    break
+                if stag >= maxstagsteps and moresteps == 0:              # :515-531
+                    stag = 0
+                moresteps += 1
+                if moresteps >= maxmsteps:
+                    flag = 3
+                    it = (outiter, initer)
+                    break
+            if normr_act <= normrmin:                                    # :534-545
+                normrmin, imin, jmin, minupdated = normr_act, outiter, initer, 1
+            if stag >= maxstagsteps:
+                flag = 3
+                break
+        evalxm = 0                                                       # :552-627
+        if flag != 0:
+            idx = jmin if minupdated else initer
+            if idx > 0:
+                y = _solve_upper(R[:idx, :idx], w[:idx])
+                add = M(expand(y, idx))
+                if not np.all(np.isfinite(add)):
+                    flag = 2
+                    break
+                x = x + add
+            xmin = x
+            r = b - afun(x)
+            normr_act = np.linalg.norm(r)
+        if normr_act <= normrmin:
+            xmin, normrmin, imin, jmin = x, normr_act, outiter, initer
+        if flag == 3:
+            break
+        if normr_act <= tolb:
+            flag = 0
+            it = (outiter, initer)
+            break
+        minupdated = 0
+    relres = normr_act / n2b                                             # :637-644
+    if flag != 0:
+        x = xmin
+        it = (imin, jmin)
+    resvec = resvec[:max(outiter - 1, 0) * inner + initer + 1]           # :645-648
+    if flag == 2 and initer != 0:
+        resvec = resvec[:-1]
+    return x, flag, relres, it, resvec
+
+
 def smooth_prolongation(A, P, tol=1e-3):
     """prolong.m:180-196 (prol_emin = SMOOTH): DA = diag(diag(A))\\A (each row
     divided by its diagonal entry), lambda_max = eigs(DA,1,'lm') with

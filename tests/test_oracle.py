@@ -134,3 +134,33 @@ def test_smooth_prolongation_dense():
     # lambda_max is an ARPACK estimate at tolerance 1e-3
     assert np.linalg.norm(Ps.toarray() - ref) <= 1e-4 * np.linalg.norm(ref)
     assert not np.any(Ps.data == 0.0)
+
+
+def test_gmres_right_oracle_matches_scipy_and_edges():
+    """The gmres_RIGHT restatement: same iteration count and solution as
+    scipy's GMRES on a nonsymmetric system without preconditioner, restarts
+    that still converge, b = 0, a solved x0, and maxit exhausted (flag 1,
+    minimal-residual iterate)."""
+    import scipy.sparse.linalg as spla
+    A = O.poisson3d(8)
+    n = A.shape[0]
+    B = (A + sp.diags(np.linspace(0.0, 0.5, n - 1), 1)).tocsr()
+    b = np.random.default_rng(3).uniform(-1, 1, n)
+    x, flag, rel, it, rv = O.gmres_right(lambda v: B @ v, b, 30, 1e-8, 20)
+    count = [0]
+    xs, info = spla.gmres(B, b, rtol=1e-8, restart=30, maxiter=20,
+                          callback=lambda r: count.__setitem__(0, count[0] + 1),
+                          callback_type="pr_norm")
+    assert flag == 0 and info == 0
+    assert (it[0] - 1) * 30 + it[1] == count[0]
+    assert np.linalg.norm(x - xs) <= 1e-6 * np.linalg.norm(xs)
+    assert rel <= 1e-8 and rv.size == (it[0] - 1) * 30 + it[1] + 1
+    d = A.diagonal()
+    x, flag, rel, it, _ = O.gmres_right(lambda v: A @ v, b, 5, 1e-8, 50, mfun=lambda v: v / d)
+    assert flag == 0 and it[0] > 1 and np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
+    assert O.gmres_right(lambda v: A @ v, np.zeros(n), 5, 1e-8, 3)[1:4] == (0, 0.0, (0, 0))
+    xx = spla.spsolve(A.tocsc(), b)
+    assert O.gmres_right(lambda v: A @ v, b, 5, 1e-8, 3, x0=xx)[3] == (0, 0)
+    x, flag, rel, it, rv = O.gmres_right(lambda v: A @ v, b, 3, 1e-12, 2)
+    assert flag == 1 and rel > 1e-12 and rv.size == 2 * 3 + 1
+    assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) <= rv.min() / np.linalg.norm(b) * (1 + 1e-8)
