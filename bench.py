@@ -458,6 +458,10 @@ def run_product(args, world, rank, local):
                  "outer operator",
         "rel_err_vs_fp64_oracle": rel_err_oracle,
         "vcycle_hbm_gbs": {"fp32": vgbs32, "fp64": vgbs64},
+        "outer_spmv": {"fp32": {"ms": prof["outer_spmv_ms"],
+                                "gbs": prof["outer_spmv_bytes"] / (prof["outer_spmv_ms"] * 1e-3) / 1e9},
+                       "fp64": {"ms": prof64["outer_spmv_ms"],
+                                "gbs": prof64["outer_spmv_bytes"] / (prof64["outer_spmv_ms"] * 1e-3) / 1e9}},
         "pcg_iteration_hbm_gbs": it_gbs,
         "setup_s": {"fp32": setup32["total"], "fp64": setup64["total"]},
         "setup_breakdown_s": {"fp32": {k: round(v, 3) for k, v in setup32.items()}},
