@@ -334,6 +334,25 @@ class Hierarchy:
                                           _pd(tv), C.byref(h)))
         self._h = h
 
+    def save(self, path):
+        """Writes the hierarchy to a file that Hierarchy.load reads back
+        without the setup (chronos_hier_save)."""
+        check(self._lib.chronos_hier_save(self._h, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, path):
+        """A hierarchy rebuilt from a file written by save (chronos_hier_load)."""
+        self = cls.__new__(cls)
+        self._lib = load()
+        h = C.c_void_p()
+        check(self._lib.chronos_hier_load(os.fsencode(path), C.byref(h)))
+        self._h = h
+        info = chronos_level_info()
+        check(self._lib.chronos_hier_level_info(h, 0, C.byref(info)))
+        self.n = info.n
+        self.prm = None
+        return self
+
     def close(self):
         if getattr(self, "_h", None):
             self._lib.chronos_hier_free(self._h)

@@ -103,6 +103,8 @@ SIGNATURES = {
     "chronos_spmv": [_i, _i, _pi, _pi, _pd, _pd, _pd, _i, _i, _i],
     "chronos_amg_setup": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _i, _pd, _pp],
     "chronos_hier_free": [_vp],
+    "chronos_hier_save": [_vp, C.c_char_p],
+    "chronos_hier_load": [C.c_char_p, _pp],
     "chronos_hier_nlevels": [_vp, _pi],
     "chronos_hier_level_info": [_vp, _i, C.POINTER(chronos_level_info)],
     "chronos_hier_export": [_vp, _i, C.c_char, _pi, _pi, _pi64, _pi, _pi, _pd],

@@ -483,6 +483,27 @@ int chronos_hier_free(chronos_hier *h) {
   return guard([&] { delete h; });
 }
 
+int chronos_hier_save(const chronos_hier *h, const char *path) {
+  return guard([&] {
+    CHRONOS_REQUIRE(h && path, CHRONOS_EINVAL, "null argument");
+    save_hierarchy(*h->h, path);
+  });
+}
+
+int chronos_hier_load(const char *path, chronos_hier **out) {
+  return guard([&] {
+    CHRONOS_REQUIRE(path && out, CHRONOS_EINVAL, "null argument");
+    auto *hh = new chronos_hier();
+    try {
+      hh->h = load_hierarchy(path);
+    } catch (...) {
+      delete hh;
+      throw;
+    }
+    *out = hh;
+  });
+}
+
 int chronos_hier_nlevels(const chronos_hier *h, int *nlev) {
   return guard([&] {
     CHRONOS_REQUIRE(h && nlev, CHRONOS_EINVAL, "null argument");

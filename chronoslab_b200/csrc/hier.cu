@@ -936,6 +936,191 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
 }
 
 // ---------------------------------------------------------------------------
+// Hierarchy files: "CHRNHIER", format version, the parameter block, then per
+// level n, nc, coarsest, omega, lambda and A, followed by G and P (smoothing
+// levels) or the n x n inverse W (coarsest).  CSR as nrows, ncols, nnz, int64
+// row pointers, int32 columns, FP64 values; all little-endian, as written.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr char kHierMagic[8] = {'C', 'H', 'R', 'N', 'H', 'I', 'E', 'R'};
+constexpr uint32_t kHierVersion = 1;
+
+struct FileW {
+  FILE *f;
+  explicit FileW(const char *path) : f(std::fopen(path, "wb")) {
+    CHRONOS_REQUIRE(f, CHRONOS_EIO, std::string("cannot write ") + path);
+  }
+  ~FileW() { if (f) std::fclose(f); }
+  void put(const void *p, size_t bytes) {
+    CHRONOS_REQUIRE(bytes == 0 || std::fwrite(p, 1, bytes, f) == bytes, CHRONOS_EIO,
+                    "short write of the hierarchy file");
+  }
+  template <typename T> void val(const T &v) { put(&v, sizeof(T)); }
+  void close() {
+    CHRONOS_REQUIRE(std::fclose(f) == 0, CHRONOS_EIO, "closing the hierarchy file failed");
+    f = nullptr;
+  }
+};
+
+struct FileR {
+  FILE *f;
+  explicit FileR(const char *path) : f(std::fopen(path, "rb")) {
+    CHRONOS_REQUIRE(f, CHRONOS_EIO, std::string("cannot read ") + path);
+  }
+  ~FileR() { if (f) std::fclose(f); }
+  void get(void *p, size_t bytes) {
+    CHRONOS_REQUIRE(bytes == 0 || std::fread(p, 1, bytes, f) == bytes, CHRONOS_EIO,
+                    "truncated hierarchy file");
+  }
+  template <typename T> T val() {
+    T v;
+    get(&v, sizeof(T));
+    return v;
+  }
+};
+
+void write_csr(FileW &w, const HostCSR &m) {
+  w.val<int32_t>(m.nrows);
+  w.val<int32_t>(m.ncols);
+  w.val<int64_t>(m.nnz());
+  w.put(m.rp.data(), sizeof(int64_t) * m.rp.size());
+  w.put(m.ci.data(), sizeof(int) * (size_t)m.nnz());
+  w.put(m.v.data(), sizeof(double) * (size_t)m.nnz());
+}
+
+HostCSR read_csr(FileR &r) {
+  HostCSR m;
+  m.nrows = r.val<int32_t>();
+  m.ncols = r.val<int32_t>();
+  const int64_t nnz = r.val<int64_t>();
+  CHRONOS_REQUIRE(m.nrows >= 0 && m.ncols >= 0 && nnz >= 0 && nnz < INT32_MAX, CHRONOS_EIO,
+                  "bad matrix header in the hierarchy file");
+  m.rp.resize((size_t)m.nrows + 1);
+  m.ci.resize(nnz);
+  m.v.resize(nnz);
+  r.get(m.rp.data(), sizeof(int64_t) * m.rp.size());
+  r.get(m.ci.data(), sizeof(int) * (size_t)nnz);
+  r.get(m.v.data(), sizeof(double) * (size_t)nnz);
+  CHRONOS_REQUIRE(m.rp[0] == 0 && m.rp[m.nrows] == nnz, CHRONOS_EIO,
+                  "bad row pointers in the hierarchy file");
+  for (int i = 0; i < m.nrows; ++i)
+    CHRONOS_REQUIRE(m.rp[i + 1] >= m.rp[i], CHRONOS_EIO, "bad row pointers in the hierarchy file");
+  for (int64_t k = 0; k < nnz; ++k)
+    CHRONOS_REQUIRE(m.ci[k] >= 0 && m.ci[k] < m.ncols, CHRONOS_EIO,
+                    "column out of range in the hierarchy file");
+  return m;
+}
+
+HostCSR fetch_csr(const DMat &d, cudaStream_t st) {
+  return download_csr(d.nrows, d.ncols, d.rp, d.ci, d.v64, d.nnz, st);
+}
+
+}  // namespace
+
+void save_hierarchy(const Hier &h, const char *path) {
+  CHRONOS_REQUIRE(path, CHRONOS_EINVAL, "null path");
+  FileW w(path);
+  w.put(kHierMagic, sizeof(kHierMagic));
+  w.val<uint32_t>(kHierVersion);
+  w.val<uint32_t>((uint32_t)sizeof(chronos_params));
+  w.put(&h.prm, sizeof(chronos_params));
+  w.val<int32_t>((int32_t)h.levels.size());
+  for (const Level &L : h.levels) {
+    w.val<int32_t>(L.n);
+    w.val<int32_t>(L.nc);
+    w.val<int32_t>(L.coarsest ? 1 : 0);
+    w.val<double>(L.omega);
+    w.val<double>(L.lambda);
+    write_csr(w, fetch_csr(L.A, h.st));
+    if (L.coarsest) {
+      std::vector<double> W((size_t)L.n * L.n);
+      L.W.download(W.data(), W.size(), h.st);
+      CHRONOS_CUDA(cudaStreamSynchronize(h.st));
+      w.put(W.data(), sizeof(double) * W.size());
+    } else {
+      write_csr(w, fetch_csr(L.G, h.st));
+      write_csr(w, fetch_csr(L.P, h.st));
+    }
+  }
+  w.close();
+}
+
+std::unique_ptr<Hier> load_hierarchy(const char *path) {
+  CHRONOS_REQUIRE(path, CHRONOS_EINVAL, "null path");
+  const double t_start = now_s();
+  FileR r(path);
+  char magic[8];
+  r.get(magic, sizeof(magic));
+  CHRONOS_REQUIRE(std::memcmp(magic, kHierMagic, sizeof(magic)) == 0, CHRONOS_EIO,
+                  std::string(path) + " is not a hierarchy file");
+  CHRONOS_REQUIRE(r.val<uint32_t>() == kHierVersion, CHRONOS_EIO,
+                  "unsupported hierarchy file version");
+  CHRONOS_REQUIRE(r.val<uint32_t>() == sizeof(chronos_params), CHRONOS_EIO,
+                  "hierarchy file written with another parameter layout");
+  chronos_params prm;
+  r.get(&prm, sizeof(prm));
+  CHRONOS_REQUIRE(prm.precision == CHRONOS_FP32 || prm.precision == CHRONOS_FP64, CHRONOS_EIO,
+                  "bad precision in the hierarchy file");
+  const int nlev = r.val<int32_t>();
+  CHRONOS_REQUIRE(nlev >= 1 && nlev <= 64, CHRONOS_EIO, "bad level count in the hierarchy file");
+  auto h = std::make_unique<Hier>();
+  h->prm = prm;
+  h->precision = prm.precision;
+  const bool fp32 = prm.precision == CHRONOS_FP32;
+  CHRONOS_CUDA(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  cudaStream_t st = h->st;
+  int nprev = -1;
+  for (int l = 0; l < nlev; ++l) {
+    h->levels.emplace_back();
+    Level &L = h->levels.back();
+    L.n = r.val<int32_t>();
+    L.nc = r.val<int32_t>();
+    L.coarsest = r.val<int32_t>() != 0;
+    L.omega = r.val<double>();
+    L.lambda = r.val<double>();
+    CHRONOS_REQUIRE(L.n > 0 && (nprev < 0 || L.n == nprev) && L.coarsest == (l == nlev - 1),
+                    CHRONOS_EIO, "inconsistent levels in the hierarchy file");
+    const HostCSR A = read_csr(r);
+    CHRONOS_REQUIRE(A.nrows == L.n && A.ncols == L.n, CHRONOS_EIO,
+                    "operator size differs from its level in the hierarchy file");
+    upload_csr(A, L.A, fp32, st);
+    if (prm.use_bsr) attach_sell3(A, L.A, fp32, st);
+    if (L.coarsest) {
+      CHRONOS_REQUIRE(L.n <= 8192, CHRONOS_EIO, "coarsest level larger than 8192 rows");
+      std::vector<double> W((size_t)L.n * L.n);
+      r.get(W.data(), sizeof(double) * W.size());
+      L.W.upload(W, st);
+    } else {
+      const HostCSR G = read_csr(r), P = read_csr(r);
+      CHRONOS_REQUIRE(G.nrows == L.n && G.ncols == L.n && P.nrows == L.n && P.ncols == L.nc &&
+                          L.nc > 0 && L.nc < L.n,
+                      CHRONOS_EIO, "smoother or prolongation size differs in the hierarchy file");
+      upload_csr(G, L.G, fp32, st);
+      upload_csr(csr_transpose(G), L.Gt, fp32, st);
+      upload_csr(P, L.P, fp32, st);
+      upload_csr(csr_transpose(P), L.Pt, fp32, st);
+    }
+    alloc_vectors(L, h->precision, st);
+    nprev = L.coarsest ? -1 : L.nc;
+  }
+  for (auto &L : h->levels) {
+    const int fmt = prm.spmv_format;
+    autotune_lanes(L.A, fp32, st, fmt);
+    if (!L.coarsest) {
+      autotune_lanes(L.G, fp32, st, fmt);
+      autotune_lanes(L.Gt, fp32, st, fmt);
+      autotune_lanes(L.P, fp32, st, fmt);
+      autotune_lanes(L.Pt, fp32, st, fmt);
+    }
+  }
+  if (fp32 && prm.exact_outer) autotune_lanes(h->levels[0].A, false, st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  h->times[7] = now_s() - t_start;
+  return h;
+}
+
+// ---------------------------------------------------------------------------
 // V-cycle
 // ---------------------------------------------------------------------------
 

@@ -128,6 +128,14 @@ struct Hier {
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A,
                                       int ntv0, const double *TV0);
 
+// Serialisation of a built hierarchy (every level's operator, smoother
+// factor and prolongation in FP64, omega, lambda_max, the coarsest inverse
+// and the parameters), so a later run skips the setup: load rebuilds the
+// device layouts (FP32 copies, block form, transposes, autotuned lanes) from
+// the stored matrices and gives the same V-cycle bit for bit.
+void save_hierarchy(const Hier &h, const char *path);
+std::unique_ptr<Hier> load_hierarchy(const char *path);
+
 void params_default(chronos_params *p);
 void params_read(const char *fnames_path, chronos_params *p);
 

@@ -277,6 +277,14 @@ typedef struct chronos_level_info {
 int chronos_amg_setup(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
                       const double *val_h, int ntv0, const double *TV0_h, chronos_hier **out);
 int chronos_hier_free(chronos_hier *h);
+/* Hierarchy files (no counterpart in the reference, whose hierarchy lives in
+ * the MATLAB workspace): save writes every level's operator, smoother factor
+ * and prolongation (FP64), omega, lambda_max, the coarsest inverse and the
+ * parameters; load rebuilds a handle from such a file without the setup --
+ * same V-cycle bit for bit -- or returns CHRONOS_EIO for a file it cannot
+ * use (wrong magic, version, parameter layout, truncated or inconsistent). */
+int chronos_hier_save(const chronos_hier *h, const char *path);
+int chronos_hier_load(const char *path, chronos_hier **out);
 int chronos_hier_nlevels(const chronos_hier *h, int *nlev);
 int chronos_hier_level_info(const chronos_hier *h, int level, chronos_level_info *info);
 /* Exports level `level` (0-based) matrix `which` ('A', 'G' or 'P') as 0-based

@@ -63,3 +63,17 @@ def test_bad_csr_rejected(lib):
                                     15, 1, 1e-3, 1, 0, ctypes.byref(ok), ctypes.byref(h))
     assert code == -1 and "increasing" in _lib.last_error()
     assert cb.version().startswith("chronos_b200")
+
+
+def test_hierarchy_file_rejected_before_any_gpu_work(lib, tmp_path):
+    """chronos_hier_load checks the file's header before touching the GPU: a
+    file of another kind, a truncated one and a missing one are CHRONOS_EIO."""
+    import chronoslab_b200 as cb
+    bad = tmp_path / "not_a_hierarchy.bin"
+    bad.write_bytes(b"0123456789abcdef" * 4)
+    short = tmp_path / "truncated.bin"
+    short.write_bytes(b"CHRNHIER\x01\x00")
+    for p in (bad, short, tmp_path / "missing.bin"):
+        with pytest.raises(cb.ChronosError) as e:
+            cb.Hierarchy.load(str(p))
+        assert e.value.code == -6

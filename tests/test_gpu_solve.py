@@ -305,3 +305,34 @@ def test_hierarchy_dump_ext_bin(lib, elast, tmp_path):
             R = cb.read_ext_bin(str(p))
             R = R[:, :E.shape[1]] if which == "P" else R
             assert R.shape[0] == E.shape[0] and (R != E).nnz == 0
+
+
+@pytest.mark.parametrize("prec", [cb.CHRONOS_FP32, cb.CHRONOS_FP64])
+def test_hierarchy_save_load_round_trip(lib, elast, tmp_path, prec):
+    """A hierarchy written to a file and read back without the setup has the
+    same levels, operators and omegas, and gives the same V-cycle and PCG
+    solve bit for bit."""
+    A, TV, b = elast
+    path = str(tmp_path / "elast.chh")
+    with cb.Hierarchy(A, TV, cb.params(precision=prec)) as h:
+        h.save(path)
+        info = [h.level_info(l) for l in range(h.nlevels)]
+        z = h.vcycle(b)
+        x, it, rv, flag, _ = h.pcg(b, itmax=500, tol=1e-8)
+        ops = [(h.export(l, "A"), h.export(l, "G") if l < h.nlevels - 1 else None)
+               for l in range(h.nlevels)]
+    with cb.Hierarchy.load(path) as g:
+        assert g.nlevels == len(info) and g.n == A.shape[0]
+        for l, i in enumerate(info):
+            j = g.level_info(l)
+            assert (j["n"], j["nnz_A"], j["nnz_G"], j["nnz_P"], j["nc"]) == \
+                (i["n"], i["nnz_A"], i["nnz_G"], i["nnz_P"], i["nc"])
+            assert j["omega"] == i["omega"]
+            Al, Gl = ops[l]
+            assert (g.export(l, "A") != Al).nnz == 0
+            if Gl is not None:
+                assert (g.export(l, "G") != Gl).nnz == 0
+        assert np.array_equal(g.vcycle(b), z)
+        y, it2, rv2, flag2, _ = g.pcg(b, itmax=500, tol=1e-8)
+    assert it2 == it and flag2 == flag == 0
+    assert np.array_equal(y, x) and np.array_equal(rv2, rv)
