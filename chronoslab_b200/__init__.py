@@ -224,6 +224,13 @@ def coarsen(A, prm=None, rng_skip=0):
     return fc.astype(np.int64), nc.value, _CsrHandle.take(h)
 
 
+def device_bytes():
+    """Device memory held by the library in this process (chronos_device_bytes)."""
+    v = C.c_int64()
+    check(load().chronos_device_bytes(C.byref(v)))
+    return v.value
+
+
 def coarsen_device(A, prm=None, rng_skip=0):
     """DOM strength + PMIS on the GPU: (fcnode, nc, S pattern), the same
     splitting as coarsen()."""

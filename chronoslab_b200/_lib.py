@@ -104,6 +104,7 @@ SIGNATURES = {
     "chronos_amg_setup": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _i, _pd, _pp],
     "chronos_hier_free": [_vp],
     "chronos_hier_save": [_vp, C.c_char_p],
+    "chronos_device_bytes": [_pi64],
     "chronos_hier_load": [C.c_char_p, _pp],
     "chronos_hier_nlevels": [_vp, _pi],
     "chronos_hier_level_info": [_vp, _i, C.POINTER(chronos_level_info)],

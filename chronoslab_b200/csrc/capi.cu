@@ -483,6 +483,13 @@ int chronos_hier_free(chronos_hier *h) {
   return guard([&] { delete h; });
 }
 
+int chronos_device_bytes(int64_t *bytes) {
+  return guard([&] {
+    CHRONOS_REQUIRE(bytes, CHRONOS_EINVAL, "null argument");
+    *bytes = device_bytes_live().load();
+  });
+}
+
 int chronos_hier_save(const chronos_hier *h, const char *path) {
   return guard([&] {
     CHRONOS_REQUIRE(h && path, CHRONOS_EINVAL, "null argument");

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -26,6 +27,23 @@ namespace chronos {
 
 #define CHRONOS_CHECK_LAUNCH() CHRONOS_CUDA(cudaGetLastError())
 
+// Bytes held by live DBuf allocations of this process, and the cap that
+// CHRONOS_DEVICE_ALLOC_CAP (bytes; unset or 0: none) puts on them.  The cap
+// turns an allocation beyond it into CHRONOS_ENOMEM exactly as a failing
+// cudaMalloc would, so out-of-memory handling is testable without filling a
+// GPU.
+inline std::atomic<int64_t> &device_bytes_live() {
+  static std::atomic<int64_t> live{0};
+  return live;
+}
+inline int64_t device_alloc_cap() {
+  static const int64_t cap = [] {
+    const char *e = std::getenv("CHRONOS_DEVICE_ALLOC_CAP");
+    return e ? (int64_t)std::atoll(e) : (int64_t)0;
+  }();
+  return cap;
+}
+
 // Owning device allocation (cudaMalloc / cudaFree), movable, typed.
 template <typename T>
 class DBuf {
@@ -43,6 +61,10 @@ class DBuf {
   void alloc(size_t n) {
     release();
     if (n == 0) return;
+    const int64_t bytes = (int64_t)(n * sizeof(T)), cap = device_alloc_cap();
+    if (cap > 0 && device_bytes_live().load() + bytes > cap)
+      throw Error(CHRONOS_ENOMEM, "allocation of " + std::to_string(bytes) +
+                                      " bytes beyond CHRONOS_DEVICE_ALLOC_CAP");
     cudaError_t e = cudaMalloc(&p_, n * sizeof(T));
     if (e != cudaSuccess) {
       p_ = nullptr;
@@ -51,9 +73,13 @@ class DBuf {
                                       " bytes failed: " + cudaGetErrorString(e));
     }
     n_ = n;
+    device_bytes_live() += bytes;
   }
   void release() {
-    if (p_) cudaFree(p_);
+    if (p_) {
+      cudaFree(p_);
+      device_bytes_live() -= (int64_t)(n_ * sizeof(T));
+    }
     p_ = nullptr;
     n_ = 0;
   }

@@ -284,6 +284,11 @@ int chronos_hier_free(chronos_hier *h);
  * same V-cycle bit for bit -- or returns CHRONOS_EIO for a file it cannot
  * use (wrong magic, version, parameter layout, truncated or inconsistent). */
 int chronos_hier_save(const chronos_hier *h, const char *path);
+/* Device memory the library holds in this process (bytes; no counterpart in
+ * the reference).  The environment variable CHRONOS_DEVICE_ALLOC_CAP (bytes)
+ * caps it: an allocation beyond the cap fails with CHRONOS_ENOMEM as a failed
+ * cudaMalloc does, and the call that met it frees what it had allocated. */
+int chronos_device_bytes(int64_t *bytes);
 int chronos_hier_load(const char *path, chronos_hier **out);
 int chronos_hier_nlevels(const chronos_hier *h, int *nlev);
 int chronos_hier_level_info(const chronos_hier *h, int level, chronos_level_info *info);
