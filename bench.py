@@ -406,6 +406,7 @@ def run_product(args, world, rank, local):
     it_gbs = prof["iteration_bytes"] * it32[-1] / (ms32 * 1e-3) / 1e9
 
     levels = [h32.level_info(l) for l in range(h32.nlevels)]
+    amg = h32.amg_info()[0]
 
     cpu = None
     rel_err_oracle = None
@@ -443,6 +444,7 @@ def run_product(args, world, rank, local):
             "workload": f"Q1 elasticity {args.ne}^3 elements, {n} DOF, {A.nnz} nnz, "
                         f"BAMG + aFSAI V(1,1), PCG_CJ to {args.tol}",
             "levels": [L["n"] for L in levels],
+            "grid_complexity": amg["grid_comp"], "operator_complexity": amg["oper_comp"],
             "l2": "inputs larger than L2 (level-1 operator alone is "
                   f"{A.nnz * 12 / 1e9:.2f} GB in FP64)",
             "parallelism": f"{world} independent replica(s), one per GPU",

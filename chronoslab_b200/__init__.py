@@ -391,6 +391,25 @@ class Hierarchy:
                 "threads_per_row": info.threads_per_row, "block_rows": info.block_rows,
                 "sell_mask": info.sell_mask}
 
+    def amg_info(self):
+        """Hierarchy statistics as get_AMG_info.m:1-81 gathers them: per level
+        the rows nn, entries nt, coarse size nc and prolongation entries nt_P
+        (smoothing levels) or the dense factor's entries nt_L (coarsest), and
+        on the first level the grid and operator complexities sum(nn)/nn_1
+        and sum(nt)/nt_1."""
+        out = []
+        for l in range(self.nlevels):
+            i = self.level_info(l)
+            d = {"nn": i["n"], "nt": i["nnz_A"], "omega": i["omega"]}
+            if l < self.nlevels - 1:
+                d.update(nc=i["nc"], nt_P=i["nnz_P"], nt_G=i["nnz_G"])
+            else:
+                d.update(nt_L=i["n"] * (i["n"] + 1) // 2)
+            out.append(d)
+        out[0]["grid_comp"] = sum(d["nn"] for d in out) / out[0]["nn"]
+        out[0]["oper_comp"] = sum(d["nt"] for d in out) / out[0]["nt"]
+        return out
+
     def export(self, level, which):
         nr, ncl, nnz = C.c_int(), C.c_int(), C.c_int64()
         w = C.c_char(which.encode() if isinstance(which, str) else which)

@@ -336,3 +336,21 @@ def test_hierarchy_save_load_round_trip(lib, elast, tmp_path, prec):
         y, it2, rv2, flag2, _ = g.pcg(b, itmax=500, tol=1e-8)
     assert it2 == it and flag2 == flag == 0
     assert np.array_equal(y, x) and np.array_equal(rv2, rv)
+
+
+def test_amg_info_complexities(lib, elast):
+    """get_AMG_info's statistics from the exported level matrices: grid and
+    operator complexity, coarse sizes and prolongation entries."""
+    A, TV, b = elast
+    with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32)) as h:
+        info = h.amg_info()
+        mats = [h.export(l, "A") for l in range(h.nlevels)]
+        Ps = [h.export(l, "P") for l in range(h.nlevels - 1)]
+    assert len(info) == len(mats) >= 2
+    assert info[0]["grid_comp"] == pytest.approx(sum(M.shape[0] for M in mats) / mats[0].shape[0])
+    assert info[0]["oper_comp"] == pytest.approx(sum(M.nnz for M in mats) / mats[0].nnz)
+    for l, P in enumerate(Ps):
+        assert info[l]["nc"] == P.shape[1] == mats[l + 1].shape[0]
+        assert info[l]["nt_P"] == P.nnz
+    n_c = mats[-1].shape[0]
+    assert info[-1]["nt_L"] == n_c * (n_c + 1) // 2
