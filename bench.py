@@ -45,9 +45,10 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--itmax", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["c2", "c3", "c4"], default="c2",
-                    help="c2: elasticity (default, the headline); c3: diffusion 128^3 with a "
-                         "block of 16 right-hand sides; c4: 64 batched problems")
+    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5"], default="c2",
+                    help="c2: elasticity (default, the headline); c1: Poisson 32^3; c3: "
+                         "diffusion 128^3 with a block of 16 right-hand sides; c4: 64 batched "
+                         "problems; c5: adjoint gradient on log-normal diffusion 64^3")
     ap.add_argument("--profile-solve", choices=["fp32", "fp64"], default=None,
                     help="for ncu --profile-from-start off: build one hierarchy, warm up, "
                          "then bracket exactly one solve with the profiler range and exit")
@@ -554,6 +555,72 @@ def run_block_or_batch(args):
     return 0
 
 
+def run_c1_or_c5(args):
+    """C1 (7-point Poisson 32^3, Dirichlet eliminated, constant test vector,
+    PCG_CJ to tol from x0 = 0) or C5 (log-normal diffusion 64^3, sigma = 1:
+    gradient of J = 1/2 ||u - u*||^2 on A's pattern by a forward solve and
+    the adjoint solve on the same hierarchy); FP32 hierarchy vs FP64, solve
+    times by CUDA events inside the library, setup excluded."""
+    import numpy as np
+    import chronoslab_b200 as cb
+    from chronoslab_b200 import problems as PB
+    out = {"metric": METRIC, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32 hierarchy / f64 outer", "data": "synthetic (seeded)"}
+    res = {}
+    if args.workload == "c1":
+        A = PB.poisson7(32)
+        b = PB.uniform_rhs(A.shape[0], seed=0)
+        for prec, name in ((cb.CHRONOS_FP32, "fp32"), (cb.CHRONOS_FP64, "fp64")):
+            with cb.Hierarchy(A, np.ones((A.shape[0], 1)), cb.params(precision=prec, ntv=1)) as h:
+                for _ in range(args.warmup):
+                    h.pcg(b, itmax=args.itmax, tol=args.tol)
+                ts = []
+                for _ in range(args.steps):
+                    x, it, _, flag, sec = h.pcg(b, itmax=args.itmax, tol=args.tol)
+                    assert flag == 0
+                    ts.append(sec * 1e3)
+                res[name] = {"ms": sum(ts) / len(ts), "iters": it,
+                             "true_relres": float(np.linalg.norm(b - A @ x) / np.linalg.norm(b)),
+                             "levels": [h.level_info(l)["n"] for l in range(h.nlevels)]}
+        out["config"] = {"workload": f"7-point Poisson 32^3 ({A.shape[0]} rows, {A.nnz} nnz), "
+                                     f"DOM 0.01 + BAMG + aFSAI V(1,1), PCG_CJ to {args.tol}"}
+    else:
+        shape = (64, 64, 64)
+        logk = PB.gaussian_field(shape, 8.0, seed=5)
+        A = PB.diffusion_from_logk(logk, 0.01)
+        rng = np.random.default_rng(11)
+        b = rng.uniform(-1, 1, A.shape[0])
+        ustar = rng.uniform(-1, 1, A.shape[0]) * 0.01
+        grads = {}
+        for prec, name in ((cb.CHRONOS_FP32, "fp32"), (cb.CHRONOS_FP64, "fp64")):
+            with cb.Hierarchy(A, np.ones((A.shape[0], 1)), cb.params(precision=prec, ntv=1)) as h:
+                ts = []
+                for k in range(args.warmup + args.steps):
+                    u, it, _, flag, s1 = h.pcg(b, itmax=args.itmax, tol=1e-12)
+                    t0 = time.perf_counter()
+                    lam, g, it2 = h.adjoint_grad(u, u - ustar, itmax=args.itmax, tol=1e-12)
+                    s2 = time.perf_counter() - t0
+                    assert flag == 0
+                    if k >= args.warmup:
+                        ts.append((s1 + s2) * 1e3)
+                grads[name] = g
+                res[name] = {"ms": sum(ts) / len(ts), "iters_forward": it, "iters_adjoint": it2}
+        res["grad_rel_diff_fp32_vs_fp64"] = float(np.linalg.norm(grads["fp32"] - grads["fp64"]) /
+                                                  np.linalg.norm(grads["fp64"]))
+        out["config"] = {"workload": f"log-normal diffusion 64^3 ({A.shape[0]} rows, {A.nnz} "
+                                     "nnz), sigma 1, correlation 8 cells, z-faces x 0.01: "
+                                     "forward solve + adjoint solve + dJ/dA scatter, tol 1e-12 "
+                                     "(forward: device time; adjoint: host clock around the call)"}
+    out["value"] = res["fp32"]["ms"]
+    out["ms_per_step"] = res["fp32"]["ms"]
+    out["fp64_ms"] = res["fp64"]["ms"]
+    out["speedup_fp32_vs_fp64"] = res["fp64"]["ms"] / res["fp32"]["ms"]
+    out["detail"] = res
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     world, rank, local = dist_env()
@@ -565,6 +632,8 @@ def main():
         return run_reference(args, world, rank)
     if args.profile_solve:
         return run_profile_solve(args)
+    if args.workload in ("c1", "c5"):
+        return run_c1_or_c5(args)
     if args.workload != "c2":
         return run_block_or_batch(args)
     return run_product(args, world, rank, local)
