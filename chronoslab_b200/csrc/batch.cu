@@ -5,10 +5,16 @@
 // problem's whole PCG_CJ -- one conditional-graph launch each -- on its own
 // stream with no host synchronisation in between, largest problems first.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <exception>
 #include <memory>
+#include <mutex>
 #include <numeric>
+#include <thread>
 #include <vector>
+
+#include <omp.h>
 
 #include "group.h"
 
@@ -56,19 +62,54 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
     CHRONOS_REQUIRE(prm->use_graph || prm->batch_grouped, CHRONOS_EINVAL,
                     "per-problem batched solves need use_graph = 1");
     auto bt = std::make_unique<chronos_batch>();
-    for (int p = 0; p < nprob; ++p) {
+    for (int p = 0; p < nprob; ++p)
       CHRONOS_REQUIRE(n[p] > 0 && iat_h[p] && iat_h[p][0] == 0, CHRONOS_EINVAL,
                       "problem " + std::to_string(p) + ": 0-based CSR expected");
-      HostCSR A;
-      A.nrows = A.ncols = n[p];
-      A.rp.assign(iat_h[p], iat_h[p] + n[p] + 1);
-      A.ci.assign(ja_h[p], ja_h[p] + A.rp[n[p]]);
-      A.v.assign(val_h[p], val_h[p] + A.rp[n[p]]);
-      // scalar problems: the constant vector as TV0 (as aspAMG_main.m:92-95 for
-      // a .mat without a test space), padded with random columns if ntv > 1
-      std::vector<double> ones(n[p], 1.0);
-      bt->b.h.push_back(build_hierarchy(*prm, A, 1, ones.data()));
-    }
+    // The problems' hierarchies are independent: a few host threads build
+    // them at once (each on its own stream, with its share of the OpenMP
+    // threads), so one problem's host phases overlap another's GPU phases.
+    // Every hierarchy is what a single chronos_amg_setup builds; lane counts
+    // are tuned afterwards on a quiet GPU: the grouped solve's stacked
+    // operators, or each problem's own for the per-problem path.
+    bt->b.h.resize(nprob);
+    const int hw = std::max(1, (int)std::thread::hardware_concurrency());
+    const int nworkers = std::max(1, std::min({nprob, 8, std::max(1, hw / 2)}));
+    int dev = 0;
+    CHRONOS_CUDA(cudaGetDevice(&dev));
+    std::atomic<int> next{0};
+    std::mutex emu;
+    std::exception_ptr err;
+    auto worker = [&] {
+      const int omp_saved = omp_get_max_threads();   // the calling thread gets it back
+      try {
+        CHRONOS_CUDA(cudaSetDevice(dev));
+        omp_set_num_threads(std::max(1, hw / nworkers));
+        for (int p = next++; p < nprob; p = next++) {
+          {
+            std::lock_guard<std::mutex> lk(emu);
+            if (err) break;
+          }
+          HostCSR A;
+          A.nrows = A.ncols = n[p];
+          A.rp.assign(iat_h[p], iat_h[p] + n[p] + 1);
+          A.ci.assign(ja_h[p], ja_h[p] + A.rp[n[p]]);
+          A.v.assign(val_h[p], val_h[p] + A.rp[n[p]]);
+          // scalar problems: the constant vector as TV0 (as aspAMG_main.m:92-95
+          // for a .mat without a test space), padded with random columns if ntv > 1
+          std::vector<double> ones(n[p], 1.0);
+          bt->b.h[p] = build_hierarchy(*prm, A, 1, ones.data(), false);
+        }
+      } catch (...) {
+        std::lock_guard<std::mutex> lk(emu);
+        if (!err) err = std::current_exception();
+      }
+      omp_set_num_threads(omp_saved);
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < nworkers; ++w) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+    if (err) std::rethrow_exception(err);
     bt->b.order.resize(nprob);
     std::iota(bt->b.order.begin(), bt->b.order.end(), 0);
     std::stable_sort(bt->b.order.begin(), bt->b.order.end(), [&](int a, int c) {
@@ -77,6 +118,10 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
     if (prm->batch_grouped && group_supported(bt->b.h)) bt->b.group = group_build(bt->b.h, *prm);
     CHRONOS_REQUIRE(bt->b.group || prm->use_graph, CHRONOS_EINVAL,
                     "these problems need the per-problem batch path, which needs use_graph = 1");
+    // the grouped solve tunes its stacked operators itself; the per-problem
+    // path runs each problem's own operators
+    if (!bt->b.group)
+      for (auto &h : bt->b.h) tune_hierarchy(*h);
     *out = bt.release();
   });
 }

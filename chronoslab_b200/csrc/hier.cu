@@ -721,7 +721,7 @@ bool gpu_coarsening(const char *soc_type) {
 }
 
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A0, int ntv0,
-                                      const double *TV0) {
+                                      const double *TV0, bool tune) {
   const double t_start = now_s();
   validate_csr(A0);
   std::string smeth(prm.smoother_method), tmeth(prm.tspace_method), ptype(prm.proltype),
@@ -917,22 +917,28 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
     alloc_vectors(L, h->precision, st);
     Al = std::move(Ac);
   }
-  // SpMV lane counts
-  for (auto &L : h->levels) {
-    const int fmt = prm.spmv_format;
-    autotune_lanes(L.A, fp32, st, fmt);
-    if (!L.coarsest) {
-      autotune_lanes(L.G, fp32, st, fmt);
-      autotune_lanes(L.Gt, fp32, st, fmt);
-      autotune_lanes(L.P, fp32, st, fmt);
-      autotune_lanes(L.Pt, fp32, st, fmt);
-    }
-  }
-  // the level-1 FP64 operator of the outer PCG
-  if (fp32 && prm.exact_outer) autotune_lanes(h->levels[0].A, false, st);
+  if (tune) tune_hierarchy(*h);
   CHRONOS_CUDA(cudaStreamSynchronize(st));
   T[7] = now_s() - t_start;
   return h;
+}
+
+void tune_hierarchy(Hier &h) {
+  const bool fp32 = h.precision == CHRONOS_FP32;
+  const int fmt = h.prm.spmv_format;
+  // SpMV lane counts
+  for (auto &L : h.levels) {
+    autotune_lanes(L.A, fp32, h.st, fmt);
+    if (!L.coarsest) {
+      autotune_lanes(L.G, fp32, h.st, fmt);
+      autotune_lanes(L.Gt, fp32, h.st, fmt);
+      autotune_lanes(L.P, fp32, h.st, fmt);
+      autotune_lanes(L.Pt, fp32, h.st, fmt);
+    }
+  }
+  // the level-1 FP64 operator of the outer PCG
+  if (fp32 && h.prm.exact_outer) autotune_lanes(h.levels[0].A, false, h.st);
+  CHRONOS_CUDA(cudaStreamSynchronize(h.st));
 }
 
 // ---------------------------------------------------------------------------
@@ -1104,18 +1110,7 @@ std::unique_ptr<Hier> load_hierarchy(const char *path) {
     alloc_vectors(L, h->precision, st);
     nprev = L.coarsest ? -1 : L.nc;
   }
-  for (auto &L : h->levels) {
-    const int fmt = prm.spmv_format;
-    autotune_lanes(L.A, fp32, st, fmt);
-    if (!L.coarsest) {
-      autotune_lanes(L.G, fp32, st, fmt);
-      autotune_lanes(L.Gt, fp32, st, fmt);
-      autotune_lanes(L.P, fp32, st, fmt);
-      autotune_lanes(L.Pt, fp32, st, fmt);
-    }
-  }
-  if (fp32 && prm.exact_outer) autotune_lanes(h->levels[0].A, false, st);
-  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  tune_hierarchy(*h);
   h->times[7] = now_s() - t_start;
   return h;
 }

@@ -125,8 +125,11 @@ struct Hier {
   DBuf<double> stage_b, stage_x;    // host-buffer entry points' device staging
 };
 
+// tune = false leaves the apply kernels' lane counts and formats at their
+// defaults; tune_hierarchy then chooses them (timed on a quiet GPU).
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A,
-                                      int ntv0, const double *TV0);
+                                      int ntv0, const double *TV0, bool tune = true);
+void tune_hierarchy(Hier &h);
 
 // Serialisation of a built hierarchy (every level's operator, smoother
 // factor and prolongation in FP64, omega, lambda_max, the coarsest inverse
