@@ -620,3 +620,18 @@ def PCG_CJ(hrc, b, x0=None, itmax=15000, tol=1e-8):
 def SQMR(hrc, rhs, tol=1e-6, itmax=100, x0=None, A=None):
     """SQMR.m:1 with the V-cycle as left preconditioner: (x, info, relres, niter)."""
     return hrc.sqmr(rhs, tol, itmax, x0, A)
+
+
+def gmres_RIGHT(hrc, b, restart=None, tol=1e-6, maxit=None, x0=None, A=None):
+    """gmres_RIGHT.m:7 with the V-cycle as the right preconditioner M:
+    (x, flag, relres, iter, resvec), iter = (outer, inner).  restart None is
+    the unrestarted method (restart = n); maxit None is
+    min(ceil(n/restart), 10) cycles, or min(n, 10) iterations unrestarted, as
+    gmres_RIGHT.m:98-157 chooses."""
+    n = hrc.n
+    if restart is None or restart == n:
+        inner = min(n, 10) if maxit is None else min(int(maxit), n)
+        return hrc.gmres(b, restart=inner, tol=tol, maxit=1, x0=x0, A=A)
+    if maxit is None:
+        maxit = min(-(-n // max(int(restart), 1)), 10)
+    return hrc.gmres(b, restart=min(int(restart), n), tol=tol, maxit=int(maxit), x0=x0, A=A)

@@ -83,3 +83,18 @@ def test_edges_and_not_converged(lib):
     assert rv.size == rvo.size == 2 * 2 + 1
     assert it == ito
     assert np.linalg.norm(x - xo) <= 1e-8 * np.linalg.norm(xo)
+
+
+def test_reference_named_wrapper(lib):
+    """cb.gmres_RIGHT follows gmres_RIGHT.m's argument defaults: restarted
+    GMRES(restart) for maxit cycles, or the unrestarted method for maxit
+    iterations when restart is None."""
+    A = PB.poisson7(10)
+    n = A.shape[0]
+    b = PB.uniform_rhs(n, seed=8)
+    with cb.Hierarchy(A, np.ones((n, 1)), cb.params(precision=cb.CHRONOS_FP64)) as h:
+        r1 = cb.gmres_RIGHT(h, b, 5, 1e-8, 20)
+        r2 = h.gmres(b, restart=5, tol=1e-8, maxit=20)
+        assert r1[1] == r2[1] == 0 and r1[3] == r2[3] and np.array_equal(r1[0], r2[0])
+        x, flag, rel, it, rv = cb.gmres_RIGHT(h, b, None, 1e-8, 40)
+        assert flag == 0 and it[0] == 1 and rel <= 1e-8
