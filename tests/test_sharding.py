@@ -63,3 +63,27 @@ def test_gloo_two_ranks_partition_and_gather(tmp_path):
     parts = partition_largest_first(weights, 2)
     for i, _, rank in r0:
         assert i in parts[rank]
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    """bench.py --impl reference launched as the driver launches it for N = 2
+    (torchrun, one process per rank, rendezvous on 127.0.0.1): rank 0 alone
+    runs the reference's CPU path and prints one JSON line, rank 1 exits 0."""
+    import json
+    import subprocess
+    import sys
+    from oracle import amg_oracle as O
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+           os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2", "--ne", "8",
+           "--steps", "1", "--warmup", "3"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = lines[0]
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["steps"] == 1
+    assert d["e2e"]["value"] == d["value"] and d["cpu_baseline"]["value"] == d["value"]
