@@ -470,6 +470,7 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
     cudaEvent_t e0, e1;
     CHRONOS_CUDA(cudaEventCreate(&e0));
     CHRONOS_CUDA(cudaEventCreate(&e1));
+    DMat winner;                                    // the fastest layout, kept for d
     for (int t : {1, 2, 4}) {
       DMat probe;
       upload_sell3(A, blen, t, probe, fp32, st);
@@ -504,12 +505,30 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
       if (std::getenv("CHRONOS_TUNE_VERBOSE"))
         std::fprintf(stderr, "chronos tune: block form T=%d  %.4f ms per residual pair + outer\n",
                      t, tmin / 4);
-      if (tmin < best) { best = tmin; T = t; }
+      if (tmin < best) {
+        best = tmin;
+        T = t;
+        winner = std::move(probe);
+      }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    tune_store_locked(key, T);
+    {
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      tune_store_locked(key, T);
+    }
+    // the timed layout becomes d's block form (no second build and upload)
+    d.nb = winner.nb;
+    d.sell_T = winner.sell_T;
+    d.nchunk = winner.nchunk;
+    d.nnzb = winner.nnzb;
+    d.nslots = winner.nslots;
+    d.choff = std::move(winner.choff);
+    d.chw = std::move(winner.chw);
+    d.sci = std::move(winner.sci);
+    d.bv64 = std::move(winner.bv64);
+    d.bv32 = std::move(winner.bv32);
+    return;
   }
   upload_sell3(A, blen, T, d, fp32, st);
 }
