@@ -77,3 +77,48 @@ def test_hierarchy_file_rejected_before_any_gpu_work(lib, tmp_path):
         with pytest.raises(cb.ChronosError) as e:
             cb.Hierarchy.load(str(p))
         assert e.value.code == -6
+
+
+C_CALLER = r"""
+#include "chronos_b200.h"
+#include <stdio.h>
+#include <string.h>
+
+int main(int argc, char **argv) {
+  chronos_params p;
+  chronos_params_default(&p);
+  if (p.nLevMax <= 0 || strcmp(p.smoother_method, "AFSAI_SYM") != 0) return 2;
+  /* a status, not an exception, for a bad argument; the message is kept */
+  if (chronos_amg_setup(&p, 0, 0, 0, 0, 0, 0, 0) != CHRONOS_EINVAL) return 3;
+  char msg[256];
+  chronos_last_error(msg, (int)sizeof msg);
+  if (strlen(msg) == 0) return 4;
+  chronos_hier *h = 0;
+  if (chronos_hier_load(argv[argc - 1], &h) != CHRONOS_EIO || h) return 5;
+  printf("ok %d %s\n", p.nLevMax, p.smoother_method);
+  return 0;
+}
+"""
+
+
+def test_header_is_c_and_library_links_from_c(lib, tmp_path):
+    """include/chronos_b200.h compiles as C99 (-pedantic, warnings as
+    errors) and a C caller links against the library and gets statuses and
+    messages back without a GPU."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if not gcc:
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    libdir = os.path.join(root, "chronoslab_b200")
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror",
+                    "-I", os.path.join(root, "include"), str(src), "-L", libdir,
+                    "-lchronos_b200", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe), str(tmp_path / "missing.chh")], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.startswith("ok ")
