@@ -7,6 +7,17 @@
 
 #include "hier.h"
 #include "spmv.cuh"
+#include <nvtx3/nvToolsExt.h>
+
+namespace {
+// NVTX range over one C ABI call (shown by nsys and usable with ncu --nvtx).
+struct CallRange {
+  explicit CallRange(const char *name) { nvtxRangePushA(name); }
+  ~CallRange() { nvtxRangePop(); }
+  CallRange(const CallRange &) = delete;
+  CallRange &operator=(const CallRange &) = delete;
+};
+}  // namespace
 
 namespace chronos {
 
@@ -231,6 +242,7 @@ int chronos_coarsen_device(const chronos_params *prm, int n, const int *iat_h, c
                            const double *val_h, uint64_t rng_skip, int *fcnode_h, int *nc,
                            chronos_csr **S) {
   return guard([&] {
+    CallRange range_("chronos_coarsen_device");
     CHRONOS_REQUIRE(prm && fcnode_h && nc && n > 0, CHRONOS_EINVAL, "bad argument");
     std::string t(prm->SoC_type);
     for (auto &c : t) c = (char)toupper(c);
@@ -317,6 +329,7 @@ int chronos_fsai_compute(int nthread, int n_step, int step_size, double tau, dou
                          const int *ja_M_h, const double *coef_M_h, int64_t *nterm_G,
                          int64_t *iat_G_h, int *ja_G_h, double *coef_G_h, int *is_posdef) {
   return guard([&] {
+    CallRange range_("chronos_fsai_compute");
     CHRONOS_REQUIRE(nterm_G && iat_G_h && ja_G_h && coef_G_h && is_posdef, CHRONOS_EINVAL,
                     "null output");
     CHRONOS_REQUIRE(nrows == nrows_M, CHRONOS_ENOTSUP,
@@ -344,6 +357,7 @@ int chronos_fsai_numeric(int n, const int64_t *iat_A_h, const int *ja_A_h, const
                          const int64_t *iat_G_h, const int *ja_G_h, double *val_G_h,
                          int *is_posdef) {
   return guard([&] {
+    CallRange range_("chronos_fsai_numeric");
     CHRONOS_REQUIRE(val_G_h && is_posdef && iat_G_h && ja_G_h, CHRONOS_EINVAL, "null argument");
     HostCSR A = from_mex_csr(n, n, iat_A_h, ja_A_h, val_A_h);
     HostCSR G;
@@ -465,6 +479,7 @@ int chronos_spmv(int n, int ncols, const int *iat_h, const int *ja_h, const doub
 int chronos_amg_setup(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
                       const double *val_h, int ntv0, const double *TV0_h, chronos_hier **out) {
   return guard([&] {
+    CallRange range_("chronos_amg_setup");
     CHRONOS_REQUIRE(prm && out, CHRONOS_EINVAL, "null argument");
     CHRONOS_REQUIRE(ntv0 == 0 || TV0_h, CHRONOS_EINVAL, "TV0 missing");
     HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
@@ -499,6 +514,7 @@ int chronos_hier_save(const chronos_hier *h, const char *path) {
 
 int chronos_hier_load(const char *path, chronos_hier **out) {
   return guard([&] {
+    CallRange range_("chronos_hier_load");
     CHRONOS_REQUIRE(path && out, CHRONOS_EINVAL, "null argument");
     auto *hh = new chronos_hier();
     try {
@@ -609,6 +625,7 @@ int chronos_diag_fix(int n, const int *iat_h, const int *ja_h, double *val_h) {
 
 int chronos_vcycle(chronos_hier *hh, const double *b_h, double *x_h, int nrhs) {
   return guard([&] {
+    CallRange range_("chronos_vcycle");
     CHRONOS_REQUIRE(hh && b_h && x_h && nrhs >= 1, CHRONOS_EINVAL, "bad argument");
     Hier &h = *hh->h;
     const int n = h.levels[0].n;
@@ -625,6 +642,7 @@ int chronos_vcycle(chronos_hier *hh, const double *b_h, double *x_h, int nrhs) {
 int chronos_pcg_dev(chronos_hier *hh, const double *b_d, double *x_d, int itmax, double tol,
                     int *iters, double *resvec_h, int *flag, double *seconds) {
   return guard([&] {
+    CallRange range_("chronos_pcg_dev");
     CHRONOS_REQUIRE(hh && b_d && x_d && iters && flag, CHRONOS_EINVAL, "null argument");
     std::vector<double> rv;
     int it = 0, fl = 0;
@@ -644,6 +662,7 @@ int chronos_pcg_dev(chronos_hier *hh, const double *b_d, double *x_d, int itmax,
 int chronos_pcg(chronos_hier *hh, const double *b_h, double *x_h, int itmax, double tol,
                 int *iters, double *resvec_h, int *flag, double *seconds) {
   return guard([&] {
+    CallRange range_("chronos_pcg");
     CHRONOS_REQUIRE(hh && b_h && x_h && iters && flag, CHRONOS_EINVAL, "null argument");
     Hier &h = *hh->h;
     const int n = h.levels[0].n;
@@ -666,6 +685,7 @@ int chronos_pcg(chronos_hier *hh, const double *b_h, double *x_h, int itmax, dou
 int chronos_pcg_block(chronos_hier *hh, int nrhs, const double *B_h, double *X_h, int itmax,
                       double tol, int *iters_h, int *flags_h, double *seconds) {
   return guard([&] {
+    CallRange range_("chronos_pcg_block");
     CHRONOS_REQUIRE(hh && B_h && X_h && iters_h && flags_h && nrhs >= 1, CHRONOS_EINVAL,
                     "bad argument");
     Hier &h = *hh->h;
@@ -687,6 +707,7 @@ int chronos_sqmr(chronos_hier *hh, const int *iat_h, const int *ja_h, const doub
                  const double *b_h, double *x_h, int itmax, double tol, int *iters,
                  double *relres, int *info) {
   return guard([&] {
+    CallRange range_("chronos_sqmr");
     CHRONOS_REQUIRE(hh && b_h && x_h && iters && relres && info, CHRONOS_EINVAL, "null argument");
     Hier &h = *hh->h;
     cudaStream_t st = h.st;
@@ -762,6 +783,7 @@ int chronos_gmres(chronos_hier *hh, const int *iat_h, const int *ja_h, const dou
                   int *iter_outer, int *iter_inner, double *relres, int *flag,
                   double *resvec_h, int *nresvec) {
   return guard([&] {
+    CallRange range_("chronos_gmres");
     CHRONOS_REQUIRE(hh && b_h && x_h && iter_outer && iter_inner && relres && flag,
                     CHRONOS_EINVAL, "null argument");
     CHRONOS_REQUIRE(restart >= 0 && maxit >= 0, CHRONOS_EINVAL, "restart and maxit must be >= 0");
@@ -797,6 +819,7 @@ int chronos_gmres(chronos_hier *hh, const int *iat_h, const int *ja_h, const dou
 int chronos_adjoint_grad(chronos_hier *hh, const double *u_h, const double *g_h, int itmax,
                          double tol, double *lambda_h, double *grad_h, int *iters) {
   return guard([&] {
+    CallRange range_("chronos_adjoint_grad");
     CHRONOS_REQUIRE(hh && u_h && g_h && lambda_h && grad_h && iters, CHRONOS_EINVAL, "null argument");
     Hier &h = *hh->h;
     const int n = h.levels[0].n;

@@ -25,6 +25,8 @@
 #include <omp.h>
 #endif
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "hier.h"
 #include "spmv.cuh"
 
@@ -33,6 +35,26 @@ namespace chronos {
 static double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
+
+// One phase of the setup: adds its wall time to *acc and marks an NVTX range
+// of the same name, so timeline tools (nsys, ncu --nvtx) show the phases.
+class SetupPhase {
+ public:
+  SetupPhase(const char *name, double *acc) : t0_(now_s()), acc_(acc) { nvtxRangePushA(name); }
+  SetupPhase(const SetupPhase &) = delete;
+  SetupPhase &operator=(const SetupPhase &) = delete;
+  ~SetupPhase() { end(); }
+  void end() {
+    if (!acc_) return;
+    *acc_ += now_s() - t0_;
+    acc_ = nullptr;
+    nvtxRangePop();
+  }
+
+ private:
+  double t0_;
+  double *acc_;
+};
 
 PcgState::~PcgState() {
   if (exec) cudaGraphExecDestroy(exec);
@@ -799,7 +821,7 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
     upload_csr(Al, L.A, fp32, st);
     if (prm.use_bsr) attach_sell3(Al, L.A, fp32, st);
     if (n <= prm.maxCoarseSZ || level >= prm.nLevMax) {
-      const double t0 = now_s();
+      SetupPhase ph6("chronos setup: coarse factor", &T[6]);
       CHRONOS_REQUIRE(n <= 8192, CHRONOS_ENOTSUP, "coarsest level larger than 8192 rows");
       std::vector<double> dense((size_t)n * n, 0.0);
       for (int i = 0; i < n; ++i)
@@ -813,17 +835,17 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
       dense_inverse_from_chol(n, Ld.get(), L.W.get(), st);
       L.coarsest = true;
       alloc_vectors(L, h->precision, st);
-      T[6] += now_s() - t0;
+      ph6.end();
       break;
     }
     // ---- smoother: adaptive FSAI (host pattern, GPU values) ----------------
-    double t0 = now_s();
+    SetupPhase ph0("chronos setup: fsai pattern", &T[0]);
     FsaiResult fr = fsai_adaptive(Al, prm.nstep, prm.step_size, prm.epsilon, nth,
                                    prm.fsai_fabs == 0);
     CHRONOS_REQUIRE(fr.posdef, CHRONOS_ENOTSPD,
                     "matrix deemed indefinite during FSAI (the nonsymmetric fallback is outside this path)");
-    T[0] += now_s() - t0;
-    t0 = now_s();
+    ph0.end();
+    SetupPhase ph1("chronos setup: fsai numeric", &T[1]);
     {
       HostCSR &Gh = fr.G;
       std::vector<int> rowlen(n);
@@ -863,9 +885,9 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
       }
       CHRONOS_CUDA(cudaStreamSynchronize(st));
     }
-    T[1] += now_s() - t0;
+    ph1.end();
     // ---- omega = min(1, 1.9 / lambda_max(G A G')) ----------------------------
-    t0 = now_s();
+    SetupPhase ph2("chronos setup: omega", &T[2]);
     {
       DBuf<double> t1(n), t2(n);
       Level *Lp = &L;
@@ -880,9 +902,9 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
       L.lambda = lanczos_lmax(n, mv, 5e-4, 200, st);
       L.omega = std::min(1.0, 1.9 / L.lambda);
     }
-    T[2] += now_s() - t0;
+    ph2.end();
     // ---- test space, coarsening --------------------------------------------
-    t0 = now_s();
+    SetupPhase ph3("chronos setup: coarsening", &T[3]);
     qr_orthonormalize(n, ntv, TV.data());
     HostCSR S;
     int nc = 0;
@@ -894,9 +916,9 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
       fcn = pmis_split(Al, S, rng, &nc);
     }
     CHRONOS_REQUIRE(nc > 0 && nc < n, CHRONOS_EINVAL, "coarsening produced no usable coarse level");
-    T[3] += now_s() - t0;
+    ph3.end();
     // ---- BAMG prolongation -----------------------------------------------------
-    t0 = now_s();
+    SetupPhase ph4("chronos setup: prolongation", &T[4]);
     std::vector<int> fc0(n);
     std::vector<int> clist;
     clist.reserve(nc);
@@ -917,9 +939,9 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
     for (int j = 0; j < ntv; ++j)
       for (int c = 0; c < nc; ++c) TVn[(size_t)j * nc + c] = TV[(size_t)j * n + clist[c]];
     TV.swap(TVn);
-    T[4] += now_s() - t0;
+    ph4.end();
     // ---- Galerkin on the GPU ---------------------------------------------------
-    t0 = now_s();
+    SetupPhase ph5("chronos setup: galerkin", &T[5]);
     L.nc = nc;
     upload_csr(Ph, L.P, fp32, st);
     HostCSR Pt = csr_transpose(Ph);
@@ -932,7 +954,7 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
     spgemm_device(nc, nc, L.Pt.rp, L.Pt.ci, L.Pt.v64, aprp, apci, apv, acrp, acci, acv, &nnz_ac,
                   st);
     HostCSR Ac = download_csr(nc, nc, acrp, acci, acv, nnz_ac, st);
-    T[5] += now_s() - t0;
+    ph5.end();
     alloc_vectors(L, h->precision, st);
     Al = std::move(Ac);
   }
