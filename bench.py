@@ -431,6 +431,14 @@ def run_product(args, world, rank, local):
                "sample": f"one full FP64 PCG_CJ solve to {args.tol} of the same system "
                          f"({ito} iterations) with the oracle's C/OpenMP V-cycle on the "
                          f"GPU hierarchy's FP64 level matrices"}
+        # one host thread: a bounded sample of k iterations, scaled to the full count
+        k1 = min(8, max(ito, 1))
+        CH1 = CO.CHierarchy(O.hierarchy_from_parts(parts), threads=1)
+        t = time.perf_counter()
+        CH1.pcg(b, itmax=k1, tol=0.0)
+        one_ms = (time.perf_counter() - t) * 1e3 * ito / k1
+        cpu["one_core"] = {"value": one_ms, "unit": "ms", "cores": 1,
+                           "sample": f"{k1} PCG_CJ iterations on one thread, scaled to {ito}"}
 
     launches = (prof["kernels_per_iteration"] * it32[-1] + prof["kernels_per_solve"]) * args.steps \
         + (prof64["kernels_per_iteration"] * it64[-1] + prof64["kernels_per_solve"]) * args.steps \
