@@ -354,3 +354,27 @@ def test_amg_info_complexities(lib, elast):
         assert info[l]["nt_P"] == P.nnz
     n_c = mats[-1].shape[0]
     assert info[-1]["nt_L"] == n_c * (n_c + 1) // 2
+
+
+def test_c1_poisson32_against_the_reference_hierarchy(lib):
+    """The C1 configuration at full size (7-point Poisson 32^3, RHS U[-1,1],
+    x0 = 0, PCG_CJ to 1e-8): the GPU solve (FP64 and FP32 hierarchies) takes
+    the iteration count of the CPU path built with the reference's own FSAI
+    and BAMG C++ (oracle/_ref) within one, and agrees with its solution."""
+    from oracle import c_oracle as CO
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    A = PB.poisson7(32)
+    n = A.shape[0]
+    b = PB.uniform_rhs(n, seed=0)
+    prm = O.default_params()
+    prm["tspace"]["ntv"] = 1
+    CH = CO.CHierarchy(CO.reference_hierarchy(A, np.ones((n, 1)), prm))
+    xo, ito, _, flo = CH.pcg(b, itmax=500, tol=1e-8)
+    assert flo == 0
+    for prec in (cb.CHRONOS_FP64, cb.CHRONOS_FP32):
+        with cb.Hierarchy(A, np.ones((n, 1)), cb.params(precision=prec, ntv=1)) as h:
+            x, it, _, flag, _ = h.pcg(b, itmax=500, tol=1e-8)
+        assert flag == 0 and abs(it - ito) <= 1
+        assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
+        assert rel(x, xo) <= 1e-6
