@@ -378,3 +378,28 @@ def test_c1_poisson32_against_the_reference_hierarchy(lib):
         assert flag == 0 and abs(it - ito) <= 1
         assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
         assert rel(x, xo) <= 1e-6
+
+
+def test_elasticity_against_the_reference_hierarchy(lib):
+    """Q1 elasticity 20^3 (the C2 family at a size the CPU path builds in
+    seconds; six rigid-body modes, BAMG, aFSAI): the GPU hierarchy has the
+    level sizes of the CPU path built with the reference's own FSAI and BAMG
+    C++, and its PCG_CJ (FP64 and FP32) takes the same iteration count within
+    one and agrees with that path's solution."""
+    from oracle import c_oracle as CO
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    A, X = PB.elasticity_q1(20, return_coords=True)
+    TV = PB.rbm_test_space(X)
+    b = PB.elasticity_rhs(A, X, seed=0)
+    H = CO.reference_hierarchy(A, TV, O.default_params())
+    xo, ito, _, flo = CO.CHierarchy(H).pcg(b, itmax=500, tol=1e-8)
+    assert flo == 0
+    for prec in (cb.CHRONOS_FP64, cb.CHRONOS_FP32):
+        with cb.Hierarchy(A, TV, cb.params(precision=prec)) as h:
+            assert [h.level_info(l)["n"] for l in range(h.nlevels)] == \
+                [lv.A.shape[0] for lv in H.levels]
+            x, it, _, flag, _ = h.pcg(b, itmax=500, tol=1e-8)
+        assert flag == 0 and abs(it - ito) <= 1
+        assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
+        assert rel(x, xo) <= 1e-6
