@@ -341,6 +341,61 @@ class Hierarchy:
                                           _pd(tv), C.byref(h)))
         self._h = h
 
+    @classmethod
+    def with_prolongation(cls, A, prolong, prm=None):
+        """cpt_aspAMG with every level's P from the caller (chronos_amg_setup_prolong):
+        `prolong` is a callable (level, A_level) -> P (scipy CSR, n x nc), called
+        for each level that is not the coarsest with the 1-based level number and
+        the level's operator, or a list of P matrices taken in order.  The
+        library computes FSAI, omega, the Galerkin products and the coarse
+        factor; coarsening and the prolongation stay with the caller, as
+        cpt_aspAMG.m:224-225 calls prolong(...) on the host."""
+        from ._lib import PROLONG_FN
+        self = cls.__new__(cls)
+        self._lib = load()
+        self.prm = prm or params()
+        n, ip, ix, dv = _csr(A)
+        self.n = n
+        if not callable(prolong):
+            plist = list(prolong)
+            prolong = lambda level, Al: plist[level - 1]   # noqa: E731
+        keep = []          # the arrays of the latest P stay alive until the next call
+        errors = []
+
+        def cb(ctx, level, nl, iat, ja, val, out):
+            try:
+                nnz = iat[nl]
+                rp = np.ctypeslib.as_array(iat, shape=(nl + 1,)).copy()
+                Al = sp.csr_matrix((np.ctypeslib.as_array(val, shape=(max(nnz, 1),))[:nnz].copy(),
+                                    np.ctypeslib.as_array(ja, shape=(max(nnz, 1),))[:nnz].copy(),
+                                    rp), shape=(nl, nl))
+                P = sp.csr_matrix(prolong(level, Al))
+                P.sort_indices()
+                pp = np.ascontiguousarray(P.indptr, dtype=np.int32)
+                pi = np.ascontiguousarray(P.indices, dtype=np.int32)
+                pv = np.ascontiguousarray(P.data, dtype=np.float64)
+                if pi.size == 0:
+                    pi, pv = np.zeros(1, np.int32), np.zeros(1)
+                keep[:] = [pp, pi, pv]
+                out[0].nc = int(P.shape[1])
+                out[0].iat_P_h = _pi(pp)
+                out[0].ja_P_h = _pi(pi)
+                out[0].val_P_h = _pd(pv)
+                return 0
+            except Exception as e:       # noqa: BLE001 -- reported after the call
+                errors.append(e)
+                return -1
+
+        fn = PROLONG_FN(cb)
+        h = C.c_void_p()
+        code = self._lib.chronos_amg_setup_prolong(C.byref(self.prm), n, _pi(ip), _pi(ix), _pd(dv),
+                                                   fn, None, C.byref(h))
+        if errors:
+            raise errors[0]
+        check(code)
+        self._h = h
+        return self
+
     def save(self, path):
         """Writes the hierarchy to a file that Hierarchy.load reads back
         without the setup (chronos_hier_save)."""

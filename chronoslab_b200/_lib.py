@@ -62,6 +62,17 @@ class chronos_profile(C.Structure):
                 ("kernels_per_solve", C.c_int)]
 
 
+class chronos_prolongation(C.Structure):
+    _fields_ = [("nc", C.c_int), ("iat_P_h", C.POINTER(C.c_int)),
+                ("ja_P_h", C.POINTER(C.c_int)), ("val_P_h", C.POINTER(C.c_double))]
+
+
+# int (*)(void *ctx, int level, int n, const int *iat, const int *ja, const double *val,
+#         chronos_prolongation *P)
+PROLONG_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                         C.POINTER(C.c_int), C.POINTER(C.c_double),
+                         C.POINTER(chronos_prolongation))
+
 _i = C.c_int
 _i64 = C.c_int64
 _u64 = C.c_uint64
@@ -102,6 +113,8 @@ SIGNATURES = {
     "chronos_dense_chol": [_i, _pd, _pd],
     "chronos_spmv": [_i, _i, _pi, _pi, _pd, _pd, _pd, _i, _i, _i],
     "chronos_amg_setup": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _i, _pd, _pp],
+    "chronos_amg_setup_prolong": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, PROLONG_FN, _vp,
+                                  _pp],
     "chronos_hier_free": [_vp],
     "chronos_hier_save": [_vp, C.c_char_p],
     "chronos_device_bytes": [_pi64],

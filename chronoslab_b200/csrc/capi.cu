@@ -494,6 +494,39 @@ int chronos_amg_setup(const chronos_params *prm, int n, const int *iat_h, const 
   });
 }
 
+int chronos_amg_setup_prolong(const chronos_params *prm, int n, const int *iat_h,
+                              const int *ja_h, const double *val_h, chronos_prolong_fn prolong,
+                              void *ctx, chronos_hier **out) {
+  return guard([&] {
+    CallRange range_("chronos_amg_setup_prolong");
+    CHRONOS_REQUIRE(prm && out && prolong, CHRONOS_EINVAL, "null argument");
+    HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
+    const ProlongFn fn = [&](int level, const HostCSR &Al) {
+      const int nl = Al.nrows;
+      std::vector<int> rp(Al.rp.begin(), Al.rp.end());
+      chronos_prolongation P{};
+      const int rc = prolong(ctx, level, nl, rp.data(), Al.ci.data(), Al.v.data(), &P);
+      CHRONOS_REQUIRE(rc == 0, CHRONOS_EINVAL,
+                      "prolongation callback failed at level " + std::to_string(level) +
+                          " (returned " + std::to_string(rc) + ")");
+      CHRONOS_REQUIRE(P.iat_P_h && P.nc > 0 && P.nc < nl && P.iat_P_h[0] == 0 &&
+                          P.iat_P_h[nl] >= 0 && (P.iat_P_h[nl] == 0 || (P.ja_P_h && P.val_P_h)),
+                      CHRONOS_EINVAL,
+                      "prolongation callback returned no usable P at level " +
+                          std::to_string(level) + " (0 < nc < n, 0-based row pointers)");
+      return from_csr0(nl, P.nc, P.iat_P_h, P.ja_P_h, P.val_P_h);
+    };
+    auto *hh = new chronos_hier();
+    try {
+      hh->h = build_hierarchy(*prm, A, 0, nullptr, true, &fn);
+    } catch (...) {
+      delete hh;
+      throw;
+    }
+    *out = hh;
+  });
+}
+
 int chronos_hier_free(chronos_hier *h) {
   return guard([&] { delete h; });
 }

@@ -604,11 +604,59 @@ static double tridiag_lmax(const std::vector<double> &a, const std::vector<doubl
   return hi;
 }
 
+// |last component| of the unit eigenvector of the symmetric tridiagonal (a, b)
+// for its largest eigenvalue theta: inverse iteration with the shift
+// theta + delta, which leaves T - shift negative definite, so the LDL'
+// recurrence of each solve needs no pivoting.
+static double tridiag_last_component(const std::vector<double> &a, const std::vector<double> &b,
+                                     double theta) {
+  const int m = (int)a.size();
+  if (m == 1) return 1.0;
+  double scale = 0.0;
+  for (int i = 0; i < m; ++i) scale = std::max(scale, std::fabs(a[i]));
+  const double shift = theta + 1e-10 * std::max(scale, std::fabs(theta)) + 1e-300;
+  std::vector<double> y(m, 1.0 / std::sqrt((double)m)), d(m), l(m);
+  for (int i = 0; i < m; ++i) {           // LDL' of T - shift
+    d[i] = a[i] - shift - (i > 0 ? l[i - 1] * l[i - 1] * d[i - 1] : 0.0);
+    if (d[i] == 0.0) d[i] = -1e-300;
+    if (i + 1 < m) l[i] = b[i] / d[i];
+  }
+  for (int it = 0; it < 3; ++it) {
+    for (int i = 1; i < m; ++i) y[i] -= l[i - 1] * y[i - 1];
+    for (int i = 0; i < m; ++i) y[i] /= d[i];
+    for (int i = m - 2; i >= 0; --i) y[i] -= l[i] * y[i + 1];
+    double nrm = 0.0;
+    for (int i = 0; i < m; ++i) nrm += y[i] * y[i];
+    nrm = std::sqrt(nrm);
+    if (!(nrm > 0.0) || !std::isfinite(nrm)) return 1.0;
+    for (int i = 0; i < m; ++i) y[i] /= nrm;
+  }
+  return std::fabs(y[m - 1]);
+}
+
+// Largest eigenvalue of the operator mv by Lanczos.  The start vector is
+// random, as eigs' default is (here uniform in [-1/2, 1/2) from MT19937
+// seeded 5489, normalised, so the value is reproducible): a structured start
+// such as the ones vector can be nearly orthogonal to the top eigenvector --
+// on Cubo_4820's operator it first converges to an eigenvalue 15 % below the
+// largest.  Stops as ARPACK's dsaupd does for eigs(...,opts.tol): once the
+// Ritz pair's residual norm beta_j |s_j| (s the unit eigenvector of the
+// tridiagonal for theta) is at most tol |theta|.
 double lanczos_lmax(int n, const std::function<void(const double *, double *)> &mv, double tol,
                     int maxit, cudaStream_t st) {
   DBuf<double> v(n), vp(n), w(n), scratch(256);
-  std::vector<double> ones(n, 1.0 / std::sqrt((double)n));
-  v.upload(ones, st);
+  std::vector<double> v0(n);
+  {
+    MT19937 r(5489u);
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) {
+      v0[i] = r.next_res53() - 0.5;
+      nrm += v0[i] * v0[i];
+    }
+    nrm = std::sqrt(nrm);
+    for (int i = 0; i < n; ++i) v0[i] /= nrm;
+  }
+  v.upload(v0, st);
   vp.zero(st);
   std::vector<double> a, b;
   double theta = 0.0, beta = 0.0;
@@ -620,7 +668,7 @@ double lanczos_lmax(int n, const std::function<void(const double *, double *)> &
     a.push_back(alpha);
     beta = std::sqrt(std::max(device_dot(n, w.get(), w.get(), scratch.get(), st), 0.0));
     const double th = tridiag_lmax(a, b);
-    const bool conv = j > 0 && std::fabs(th - theta) <= tol * std::fabs(th);
+    const bool conv = beta * tridiag_last_component(a, b, th) <= tol * std::fabs(th);
     theta = th;
     if (conv || beta <= 1e-300 * std::fabs(theta)) break;
     b.push_back(beta);
@@ -762,7 +810,7 @@ bool gpu_coarsening(const char *soc_type) {
 }
 
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A0, int ntv0,
-                                      const double *TV0, bool tune) {
+                                      const double *TV0, bool tune, const ProlongFn *prolong) {
   const double t_start = now_s();
   validate_csr(A0);
   std::string smeth(prm.smoother_method), tmeth(prm.tspace_method), ptype(prm.proltype),
@@ -770,12 +818,14 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
   for (auto *s : {&smeth, &tmeth, &ptype, &pemin})
     for (auto &c : *s) c = (char)toupper(c);
   CHRONOS_REQUIRE(smeth == "AFSAI_SYM", CHRONOS_ENOTSUP, "smoother " + smeth + " is outside this path");
-  CHRONOS_REQUIRE(tmeth == "NONE", CHRONOS_ENOTSUP, "test-space method " + tmeth + " is outside this path");
-  CHRONOS_REQUIRE(ptype == "BAMG", CHRONOS_ENOTSUP, "prolongation " + ptype + " is outside this path");
-  CHRONOS_REQUIRE(pemin == "NONE" || pemin == "SMOOTH", CHRONOS_ENOTSUP,
-                  "prolongation post-process " + pemin + " is outside this path");
-  CHRONOS_REQUIRE(prm.nl_agg == 0, CHRONOS_ENOTSUP, "aggressive coarsening is outside this path");
-  CHRONOS_REQUIRE(prm.updateCF == 0, CHRONOS_ENOTSUP, "updateCF != 0 is outside this path");
+  if (!prolong) {   // with a caller-supplied P these choices are the caller's
+    CHRONOS_REQUIRE(tmeth == "NONE", CHRONOS_ENOTSUP, "test-space method " + tmeth + " is outside this path");
+    CHRONOS_REQUIRE(ptype == "BAMG", CHRONOS_ENOTSUP, "prolongation " + ptype + " is outside this path");
+    CHRONOS_REQUIRE(pemin == "NONE" || pemin == "SMOOTH", CHRONOS_ENOTSUP,
+                    "prolongation post-process " + pemin + " is outside this path");
+    CHRONOS_REQUIRE(prm.nl_agg == 0, CHRONOS_ENOTSUP, "aggressive coarsening is outside this path");
+    CHRONOS_REQUIRE(prm.updateCF == 0, CHRONOS_ENOTSUP, "updateCF != 0 is outside this path");
+  }
   CHRONOS_REQUIRE(prm.filt_wgt >= 100 && prm.filt_tau <= 0, CHRONOS_ENOTSUP,
                   "prolongation / coarse-operator filtering is outside this path");
   CHRONOS_REQUIRE(prm.ntv >= 1 && prm.nstep >= 0 && prm.step_size >= 1 &&
@@ -803,13 +853,16 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
   MT19937 rng((uint32_t)(prm.seed ? prm.seed : 5489));
   int n = A0.nrows;
   const int ntv = prm.ntv;
-  std::vector<double> TV((size_t)n * ntv, 0.0);          // column-major
-  const int ncopy = std::min(std::max(ntv0, 0), ntv);
-  for (int j = 0; j < ncopy; ++j)
-    std::copy(TV0 + (size_t)j * n, TV0 + (size_t)(j + 1) * n, TV.begin() + (size_t)j * n);
-  for (int j = std::max(ntv0, 0); j < ntv; ++j)           // rand(n, ntv-ntv0), column-major
-    for (int i = 0; i < n; ++i) TV[(size_t)j * n + i] = rng.next_res53();
-  qr_orthonormalize(n, ntv, TV.data());
+  std::vector<double> TV;                                  // column-major n x ntv
+  if (!prolong) {
+    TV.assign((size_t)n * ntv, 0.0);
+    const int ncopy = std::min(std::max(ntv0, 0), ntv);
+    for (int j = 0; j < ncopy; ++j)
+      std::copy(TV0 + (size_t)j * n, TV0 + (size_t)(j + 1) * n, TV.begin() + (size_t)j * n);
+    for (int j = std::max(ntv0, 0); j < ntv; ++j)         // rand(n, ntv-ntv0), column-major
+      for (int i = 0; i < n; ++i) TV[(size_t)j * n + i] = rng.next_res53();
+    qr_orthonormalize(n, ntv, TV.data());
+  }
 
   HostCSR Al = A0;
   std::array<double, 8> &T = h->times;
@@ -903,11 +956,35 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
       L.omega = std::min(1.0, 1.9 / L.lambda);
     }
     ph2.end();
+    HostCSR Ph;
+    int nc = 0;
+    if (prolong) {
+      // ---- prolongation from the caller (coarsening, C/F split, P pattern and
+      // values are the caller's host code, as cpt_aspAMG.m:224-225 calls prolong)
+      SetupPhase ph4("chronos setup: prolongation (caller)", &T[4]);
+      Ph = (*prolong)(level, Al);
+      nc = Ph.ncols;
+      CHRONOS_REQUIRE(Ph.nrows == n && nc > 0 && nc < n &&
+                          (int64_t)Ph.rp.size() == (int64_t)n + 1 && Ph.rp[0] == 0 &&
+                          (int64_t)Ph.ci.size() == Ph.rp[n] && Ph.v.size() == Ph.ci.size(),
+                      CHRONOS_EINVAL,
+                      "caller's prolongation of level " + std::to_string(level) +
+                          " must be n x nc CSR with 0 < nc < n");
+      for (int i = 0; i < n; ++i) {
+        CHRONOS_REQUIRE(Ph.rp[i + 1] >= Ph.rp[i], CHRONOS_EINVAL,
+                        "caller's prolongation: decreasing row pointers");
+        for (int64_t k = Ph.rp[i]; k < Ph.rp[i + 1]; ++k)
+          CHRONOS_REQUIRE(Ph.ci[k] >= 0 && Ph.ci[k] < nc && (k == Ph.rp[i] || Ph.ci[k] > Ph.ci[k - 1]) &&
+                              std::isfinite(Ph.v[k]),
+                          CHRONOS_EINVAL,
+                          "caller's prolongation: columns must be ascending in [0, nc), values finite");
+      }
+      ph4.end();
+    } else {
     // ---- test space, coarsening --------------------------------------------
     SetupPhase ph3("chronos setup: coarsening", &T[3]);
     qr_orthonormalize(n, ntv, TV.data());
     HostCSR S;
-    int nc = 0;
     std::vector<int> fcn;
     if (gpu_coarsening(prm.SoC_type)) {
       coarsen_dom_device(n, L.A.rp, L.A.ci, L.A.v64, prm.soc_tau, rng, S, fcn, &nc, st);
@@ -933,13 +1010,14 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
                   prm.prol_np > 0 ? prm.prol_np : nth, prm.maxcond, prm.maxrownrm, prm.tol_vol,
                   prm.eps_prol};
     std::vector<int> c_mark;
-    HostCSR Ph = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
+    Ph = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
     if (pemin == "SMOOTH") Ph = smooth_prolongation(Al, L.A, Ph, st);
     std::vector<double> TVn((size_t)nc * ntv);
     for (int j = 0; j < ntv; ++j)
       for (int c = 0; c < nc; ++c) TVn[(size_t)j * nc + c] = TV[(size_t)j * n + clist[c]];
     TV.swap(TVn);
     ph4.end();
+    }
     // ---- Galerkin on the GPU ---------------------------------------------------
     SetupPhase ph5("chronos setup: galerkin", &T[5]);
     L.nc = nc;
@@ -1025,6 +1103,16 @@ struct FileR {
     get(&v, sizeof(T));
     return v;
   }
+  // bytes between the read position and the end of the file
+  int64_t remaining() {
+    const long pos = std::ftell(f);
+    CHRONOS_REQUIRE(pos >= 0 && std::fseek(f, 0, SEEK_END) == 0, CHRONOS_EIO,
+                    "cannot seek in the hierarchy file");
+    const long end = std::ftell(f);
+    CHRONOS_REQUIRE(end >= pos && std::fseek(f, pos, SEEK_SET) == 0, CHRONOS_EIO,
+                    "cannot seek in the hierarchy file");
+    return (int64_t)(end - pos);
+  }
 };
 
 void write_csr(FileW &w, const HostCSR &m) {
@@ -1043,6 +1131,10 @@ HostCSR read_csr(FileR &r) {
   const int64_t nnz = r.val<int64_t>();
   CHRONOS_REQUIRE(m.nrows >= 0 && m.ncols >= 0 && nnz >= 0 && nnz < INT32_MAX, CHRONOS_EIO,
                   "bad matrix header in the hierarchy file");
+  // a corrupt header must not size host buffers beyond what the file holds
+  const int64_t need = 8 * ((int64_t)m.nrows + 1) + 12 * nnz;
+  CHRONOS_REQUIRE(need <= r.remaining(), CHRONOS_EIO,
+                  "truncated hierarchy file (matrix header larger than the file)");
   m.rp.resize((size_t)m.nrows + 1);
   m.ci.resize(nnz);
   m.v.resize(nnz);

@@ -125,10 +125,19 @@ struct Hier {
   DBuf<double> stage_b, stage_x;    // host-buffer entry points' device staging
 };
 
+// Source of a level's prolongation outside the library: given the 1-based
+// level number and the level's operator (FP64, from the GPU Galerkin product
+// on levels > 1), returns P (n x nc, 0-based CSR, sorted rows).
+using ProlongFn = std::function<HostCSR(int level, const HostCSR &A)>;
+
 // tune = false leaves the apply kernels' lane counts and formats at their
 // defaults; tune_hierarchy then chooses them (timed on a quiet GPU).
+// prolong != nullptr takes every level's P from it (coarsening, C/F splitting
+// and the prolongation stay with the caller; TV0 is unused); otherwise the
+// library's own coarsening and BAMG build P from the test space.
 std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A,
-                                      int ntv0, const double *TV0, bool tune = true);
+                                      int ntv0, const double *TV0, bool tune = true,
+                                      const ProlongFn *prolong = nullptr);
 void tune_hierarchy(Hier &h);
 
 // Serialisation of a built hierarchy (every level's operator, smoother

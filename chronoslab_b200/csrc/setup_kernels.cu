@@ -643,12 +643,38 @@ static int *noalloc_scratch_address() {
   return g_noalloc_addr[dev];
 }
 
-// Sorts rows into the 16 / 32 / 64 buckets of fsai_numeric_device; a row
-// longer than 64 strictly-lower entries sets flag bit 1.
-__global__ void k_fsai_bucket_rows(int n, const int *__restrict__ grp, int *scratch) {
+// Checks row i of both patterns and sorts it into the 16 / 32 / 64 buckets of
+// fsai_numeric_device.  The numeric kernel indexes A's rows by G's columns and
+// writes G's row at gval[grp[i] .. grp[i+1]-1] with the diagonal last, so a
+// malformed row sets flag bit 2 (and is not bucketed): a G row without
+// entries, a last column other than i, strictly-lower columns not ascending
+// or outside [0, i); an A row whose pointers decrease or whose columns are not
+// ascending inside [0, n); row pointers of either that do not start at 0.
+// A row longer than 64 strictly-lower entries sets flag bit 1.
+__global__ void k_fsai_bucket_rows(int n, const int *__restrict__ arp, const int *__restrict__ aci,
+                                   const int *__restrict__ grp, const int *__restrict__ gci,
+                                   int *scratch) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int m = grp[i + 1] - grp[i] - 1;
+  const int gs = grp[i], ge = grp[i + 1];
+  bool bad = ge <= gs || (i == 0 && (gs != 0 || arp[0] != 0));
+  if (!bad) {
+    bad = gci[ge - 1] != i;
+    for (int k = gs, prev = -1; !bad && k < ge - 1; ++k) {
+      const int c = gci[k];
+      bad = c <= prev || c >= i;
+      prev = c;
+    }
+  }
+  const int as = arp[i], ae = arp[i + 1];
+  bad = bad || ae < as;
+  for (int k = as, prev = -1; !bad && k < ae; ++k) {
+    const int c = aci[k];
+    bad = c <= prev || c >= n;
+    prev = c;
+  }
+  if (bad) { atomicOr(scratch + 3, 4); return; }
+  const int m = ge - gs - 1;
   int b;
   if (m <= 16) b = 0;
   else if (m <= 32) b = 1;
@@ -666,11 +692,17 @@ int fsai_numeric_noalloc(int n, const int *arp, const int *aci, const double *av
   int *scr = noalloc_scratch_address();
   // the previous call's contents remain: clear the counts and the flag word
   CHRONOS_CUDA(cudaMemsetAsync(scr, 0, kNoAllocHeader * sizeof(int), st));
-  k_fsai_bucket_rows<<<ceil_div(n, 256), 256, 0, st>>>(n, grp, scr);
+  k_fsai_bucket_rows<<<ceil_div(n, 256), 256, 0, st>>>(n, arp, aci, grp, gci, scr);
   CHRONOS_CHECK_LAUNCH();
   int hdr[4] = {0, 0, 0, 0};
   CHRONOS_CUDA(cudaMemcpyAsync(hdr, scr, sizeof(hdr), cudaMemcpyDeviceToHost, st));
   CHRONOS_CUDA(cudaStreamSynchronize(st));
+  // no numeric kernel runs on a malformed pattern: it would read A and write
+  // G's values outside the rows the caller's buffers hold
+  CHRONOS_REQUIRE(!(hdr[3] & 4), CHRONOS_EINVAL,
+                  "malformed CSR: a G row is empty, does not end with its diagonal or has "
+                  "strictly-lower columns not ascending in [0, i); or A's row pointers / "
+                  "columns are not a sorted 0-based CSR");
   CHRONOS_REQUIRE(!(hdr[3] & 2), CHRONOS_ENOTSUP,
                   "FSAI local system larger than 64 (nstep*step_size)");
   auto run = [&](auto kern, int cnt, int bucket, int mmax, int warps) {

@@ -165,7 +165,11 @@ int chronos_fsai_numeric(int n, const int64_t *iat_A_h, const int *ja_A_h, const
  * process exits; n is limited to 1048576 rows (larger n returns
  * CHRONOS_EINVAL).  The first call on a device looks up the array's device
  * address for that device.  All calls share the array: calls that overlap on
- * the GPU race on it and must be serialised by the caller. */
+ * the GPU race on it and must be serialised by the caller.
+ * Both patterns are checked on the device before any value is computed: an
+ * empty G row, a G row not ending with its diagonal or with strictly-lower
+ * columns not ascending in [0, i), or A row pointers / columns that are not a
+ * sorted 0-based CSR return CHRONOS_EINVAL with val_G_d untouched. */
 int chronos_fsai_numeric_noalloc(int n, const int *iat_A_d, const int *ja_A_d,
                                  const double *val_A_d, const int *iat_G_d, const int *ja_G_d,
                                  double *val_G_d, int *is_posdef, void *stream);
@@ -276,6 +280,37 @@ typedef struct chronos_level_info {
  * computeAMG.m:5-10 Dirichlet fix is the caller's, see chronos_diag_fix). */
 int chronos_amg_setup(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
                       const double *val_h, int ntv0, const double *TV0_h, chronos_hier **out);
+
+/* A level's prolongation as the caller's host code computed it: P is n x nc,
+ * 0-based CSR, columns ascending in each row.  The arrays belong to the
+ * caller and must stay valid until the callback is called again or the
+ * setup returns; the library copies them. */
+typedef struct chronos_prolongation {
+  int nc;                   /* coarse size, 0 < nc < n */
+  const int *iat_P_h;       /* n + 1 row pointers, iat_P_h[0] = 0 */
+  const int *ja_P_h;        /* iat_P_h[n] coarse columns */
+  const double *val_P_h;    /* iat_P_h[n] values */
+} chronos_prolongation;
+/* Called once per level that is not the coarsest, with the 1-based level
+ * number and that level's operator (host FP64 0-based CSR, sorted rows; the
+ * GPU Galerkin product from level 2 on).  Returns 0 after filling *P, or a
+ * nonzero value to abort the setup (chronos_amg_setup_prolong then returns
+ * CHRONOS_EINVAL). */
+typedef int (*chronos_prolong_fn)(void *ctx, int level, int n, const int *iat_A_h,
+                                  const int *ja_A_h, const double *val_A_h,
+                                  chronos_prolongation *P);
+/* cpt_aspAMG with the prolongation from the caller (aspAMG/cpt_aspAMG.m:224-225
+ * calls prolong(...), and :277 forms Anext = Pf'*(A*Pf)): coarsening, C/F
+ * splitting, the test space and the prolongation -- P's pattern and values,
+ * any post-process included -- stay on the caller's host code, level by level,
+ * while the library computes everything else as chronos_amg_setup does: FSAI
+ * pattern and values, lambda_max and omega, the Galerkin product on the GPU
+ * (pattern and values reproducible bit for bit), the coarse factor.  The
+ * stopping rule is the reference's (n <= maxCoarseSZ or nLevMax levels); the
+ * test-space, prolongation and coarsening fields of prm are not used. */
+int chronos_amg_setup_prolong(const chronos_params *prm, int n, const int *iat_h,
+                              const int *ja_h, const double *val_h, chronos_prolong_fn prolong,
+                              void *ctx, chronos_hier **out);
 int chronos_hier_free(chronos_hier *h);
 /* Hierarchy files (no counterpart in the reference, whose hierarchy lives in
  * the MATLAB workspace): save writes every level's operator, smoother factor
