@@ -189,23 +189,35 @@ def fsai_pattern(A, nstep=15, step_size=1, eps=1e-3, nthread=1, fsai_fabs=0):
     return _CsrHandle.take(h), bool(ok.value)
 
 
-def fsai_numeric(A, G):
+def fsai_numeric(A, G, base=1, precision=CHRONOS_FP64, stream=None):
     """GPU numeric phase on the pattern of G (rows: strictly-lower ascending,
-    diagonal last).  Returns (values in G's order, is_posdef)."""
+    diagonal last), passed to chronos_fsai_numeric as 1-based (the MEX
+    layout, base=1) or 0-based (base=0) CSR.  Returns (values in G's order
+    as float64, or float32 for precision=CHRONOS_FP32; is_posdef).  stream:
+    a cudaStream_t handle as an int (e.g. torch's stream.cuda_stream) or None."""
     A = sp.csr_matrix(A)
     A.sort_indices()
     G = sp.csr_matrix(G)
     n = A.shape[0]
-    out = np.zeros(G.nnz, np.float64)
+    out = np.zeros(G.nnz, np.float64 if precision == CHRONOS_FP64 else np.float32)
     ok = C.c_int()
-    iatA = A.indptr.astype(np.int64) + 1
-    jaA = A.indices.astype(np.int32) + 1
-    iatG = G.indptr.astype(np.int64) + 1
-    jaG = G.indices.astype(np.int32) + 1
+    iatA = A.indptr.astype(np.int64) + base
+    jaA = A.indices.astype(np.int32) + base
+    iatG = G.indptr.astype(np.int64) + base
+    jaG = G.indices.astype(np.int32) + base
     dA = np.ascontiguousarray(A.data, np.float64)
-    check(load().chronos_fsai_numeric(n, _pi64(iatA), _pi(jaA), _pd(dA), _pi64(iatG), _pi(jaG),
-                                      _pd(out), C.byref(ok)))
+    check(load().chronos_fsai_numeric(n, base, _pi64(iatA), _pi(jaA), _pd(dA), _pi64(iatG),
+                                      _pi(jaG), precision, out.ctypes.data_as(C.c_void_p),
+                                      C.byref(ok), _stream(stream)))
     return out, bool(ok.value)
+
+
+def _stream(s):
+    """cudaStream_t argument from None (the legacy default stream), an int
+    handle or an object with a cuda_stream attribute (torch.cuda.Stream)."""
+    if s is None:
+        return None
+    return C.c_void_p(int(getattr(s, "cuda_stream", s)))
 
 
 # ---------------------------------------------------------------------------
@@ -496,21 +508,28 @@ class Hierarchy:
         check(self._lib.chronos_hier_profile(self._h, reps, C.byref(p)))
         return {k: getattr(p, k) for k, _ in chronos_profile._fields_}
 
-    def vcycle(self, b):
+    def vcycle(self, b, stream=None):
         b = np.asarray(b, dtype=np.float64)
         nrhs = 1 if b.ndim == 1 else b.shape[1]
         bc = np.ascontiguousarray(b.T if b.ndim == 2 else b).ravel()
         x = np.zeros_like(bc)
-        check(self._lib.chronos_vcycle(self._h, _pd(bc), _pd(x), nrhs))
+        check(self._lib.chronos_vcycle(self._h, _pd(bc), _pd(x), nrhs, _stream(stream)))
         return x if b.ndim == 1 else x.reshape(nrhs, self.n).T
 
-    def pcg(self, b, x0=None, itmax=1000, tol=1e-8):
+    def pcg(self, b, x0=None, itmax=1000, tol=1e-8, A=None, stream=None):
+        """PCG_CJ; A (optional) is the operator prodA (0-based CSR of the
+        level-1 size), else the hierarchy's level-1 operator."""
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
         it, flag, sec = C.c_int(), C.c_int(), C.c_double()
         rv = np.zeros(max(itmax, 0) + 1)
-        check(self._lib.chronos_pcg(self._h, _pd(b), _pd(x), itmax, tol, C.byref(it), _pd(rv),
-                                    C.byref(flag), C.byref(sec)))
+        if A is not None:
+            _, ip, ix, dv = _csr(A)
+            ops = (_pi(ip), _pi(ix), _pd(dv))
+        else:
+            ops = (None, None, None)
+        check(self._lib.chronos_pcg(self._h, *ops, _pd(b), _pd(x), itmax, tol, C.byref(it),
+                                    _pd(rv), C.byref(flag), C.byref(sec), _stream(stream)))
         return x, it.value, rv[:it.value + 1], flag.value, sec.value
 
     def pcg_host(self, b, x, itmax=1000, tol=1e-8):
@@ -524,18 +543,20 @@ class Hierarchy:
                 raise ChronosError(-1, "pcg_host: b and x must be contiguous "
                                    "float64 arrays of length n")
         it, flag, sec = C.c_int(), C.c_int(), C.c_double()
-        check(self._lib.chronos_pcg(self._h, _pd(b), _pd(x), itmax, tol, C.byref(it), None,
-                                    C.byref(flag), C.byref(sec)))
+        check(self._lib.chronos_pcg(self._h, None, None, None, _pd(b), _pd(x), itmax, tol,
+                                    C.byref(it), None, C.byref(flag), C.byref(sec), None))
         return it.value, flag.value, sec.value
 
-    def pcg_dev(self, b_ptr, x_ptr, itmax=1000, tol=1e-8):
-        """PCG on device FP64 vectors (raw pointers, e.g. torch tensor.data_ptr())."""
+    def pcg_dev(self, b_ptr, x_ptr, itmax=1000, tol=1e-8, stream=None):
+        """PCG on device FP64 vectors (raw pointers, e.g. torch tensor.data_ptr()),
+        ordered on `stream` (torch.cuda.Stream, an int handle, or None)."""
         it, flag, sec = C.c_int(), C.c_int(), C.c_double()
         check(self._lib.chronos_pcg_dev(self._h, C.c_void_p(b_ptr), C.c_void_p(x_ptr), itmax, tol,
-                                        C.byref(it), None, C.byref(flag), C.byref(sec)))
+                                        C.byref(it), None, C.byref(flag), C.byref(sec),
+                                        _stream(stream)))
         return it.value, flag.value, sec.value
 
-    def pcg_block(self, B, X0=None, itmax=1000, tol=1e-8):
+    def pcg_block(self, B, X0=None, itmax=1000, tol=1e-8, stream=None):
         B = np.asarray(B, dtype=np.float64)
         nrhs = B.shape[1]
         bc = np.ascontiguousarray(B.T).ravel()
@@ -544,7 +565,7 @@ class Hierarchy:
         fl = np.zeros(nrhs, np.int32)
         sec = C.c_double()
         check(self._lib.chronos_pcg_block(self._h, nrhs, _pd(bc), _pd(xc), itmax, tol, _pi(its),
-                                          _pi(fl), C.byref(sec)))
+                                          _pi(fl), C.byref(sec), _stream(stream)))
         return xc.reshape(nrhs, self.n).T, its, fl, sec.value
 
     def sqmr(self, b, tol=1e-6, itmax=100, x0=None, A=None):

@@ -105,7 +105,7 @@ SIGNATURES = {
     "chronos_bamg": [C.POINTER(chronos_params), _i, _pi, _pi, _pi, _i, _pd, _pi, _pp],
     "chronos_fsai_compute": [_i, _i, _i, _d, _d, _i, _i, _i64, _pi64, _pi, _pd, _pi64, _pi64,
                              _pi, _pd, _pi],
-    "chronos_fsai_numeric": [_i, _pi64, _pi, _pd, _pi64, _pi, _pd, _pi],
+    "chronos_fsai_numeric": [_i, _i, _pi64, _pi, _pd, _pi64, _pi, _i, _vp, _pi, _vp],
     "chronos_fsai_numeric_noalloc": [_i, _vp, _vp, _vp, _vp, _vp, _vp, _pi, _vp],
     "chronos_galerkin_compute": [_i, _i, _pi, _pi, _pd, _pi, _pi, _pd, _pi64, _pp],
     "chronos_galerkin_fetch": [_vp, _pi, _pi, _pd],
@@ -125,10 +125,10 @@ SIGNATURES = {
     "chronos_hier_setup_times": [_vp, _pd],
     "chronos_hier_profile": [_vp, _i, C.POINTER(chronos_profile)],
     "chronos_diag_fix": [_i, _pi, _pi, _pd],
-    "chronos_vcycle": [_vp, _pd, _pd, _i],
-    "chronos_pcg": [_vp, _pd, _pd, _i, _d, _pi, _pd, _pi, _pd],
-    "chronos_pcg_dev": [_vp, _vp, _vp, _i, _d, _pi, _pd, _pi, _pd],
-    "chronos_pcg_block": [_vp, _i, _pd, _pd, _i, _d, _pi, _pi, _pd],
+    "chronos_vcycle": [_vp, _pd, _pd, _i, _vp],
+    "chronos_pcg": [_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _pi, _pd, _pi, _pd, _vp],
+    "chronos_pcg_dev": [_vp, _vp, _vp, _i, _d, _pi, _pd, _pi, _pd, _vp],
+    "chronos_pcg_block": [_vp, _i, _pd, _pd, _i, _d, _pi, _pi, _pd, _vp],
     "chronos_batch_setup": [C.POINTER(chronos_params), _i, _pi, _pp, _pp, _pp, _pp],
     "chronos_batch_solve": [_vp, _pp, _pp, _i, _d, _pi, _pi, _pd],
     "chronos_batch_info": [_vp, _i, _pi, _pi],

@@ -90,15 +90,59 @@ static HostCSR from_csr0(int n, int ncols, const int *iat, const int *ja, const 
   return h;
 }
 
+// True for memory the device owns (cudaMalloc'd or managed); host memory,
+// registered or not, and any pointer when no GPU is present are host memory.
+static bool is_device_pointer(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice;
+}
+
+// from_csr0 for arrays in host or device memory (chronos_amg_setup takes A
+// from either, as a MEX caller may hold it on the host or in a gpuArray).
+static HostCSR from_csr0_any(int n, int ncols, const int *iat, const int *ja, const double *v) {
+  if (!is_device_pointer(iat)) return from_csr0(n, ncols, iat, ja, v);
+  CHRONOS_REQUIRE(n > 0, CHRONOS_EINVAL, "n must be positive");
+  std::vector<int> rp((size_t)n + 1);
+  CHRONOS_CUDA(cudaMemcpy(rp.data(), iat, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost));
+  CHRONOS_REQUIRE(rp[0] == 0 && rp[n] >= 0, CHRONOS_EINVAL, "0-based CSR expected (iat[0] == 0)");
+  std::vector<int> ci(std::max(rp[n], 1));
+  std::vector<double> vv(std::max(rp[n], 1));
+  if (rp[n] > 0) {
+    CHRONOS_REQUIRE(ja && v, CHRONOS_EINVAL, "null CSR input");
+    CHRONOS_CUDA(cudaMemcpy(ci.data(), ja, sizeof(int) * (size_t)rp[n], cudaMemcpyDeviceToHost));
+    CHRONOS_CUDA(cudaMemcpy(vv.data(), v, sizeof(double) * (size_t)rp[n], cudaMemcpyDeviceToHost));
+  }
+  return from_csr0(n, ncols, rp.data(), ci.data(), vv.data());
+}
+
 struct ScopedStream {
   cudaStream_t st = nullptr;
   ScopedStream() { CHRONOS_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking)); }
   ~ScopedStream() { if (st) { cudaStreamSynchronize(st); cudaStreamDestroy(st); } }
 };
 
+// Records an event on `from` and makes `to` wait for it.
+static void stream_wait(cudaStream_t to, cudaStream_t from) {
+  cudaEvent_t e;
+  CHRONOS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaError_t r = cudaEventRecord(e, from);
+  if (r == cudaSuccess) r = cudaStreamWaitEvent(to, e, 0);
+  cudaEventDestroy(e);
+  CHRONOS_CUDA(r);
+}
+
 // Device-side FSAI numeric phase on a host pattern; vals out in G's order.
-static int fsai_values(const HostCSR &A, const HostCSR &G, std::vector<double> &gval) {
+// join: the work starts after what the caller's stream (null: the legacy
+// default stream) has queued, and that stream waits for the work.
+static int fsai_values(const HostCSR &A, const HostCSR &G, std::vector<double> &gval,
+                       cudaStream_t caller = nullptr, bool join = false) {
   ScopedStream s;
+  if (join) stream_wait(s.st, caller);
   DMat dA, dG;
   upload_csr(A, dA, false, s.st);
   upload_csr(G, dG, false, s.st);
@@ -116,6 +160,7 @@ static int fsai_values(const HostCSR &A, const HostCSR &G, std::vector<double> &
   gval.resize(G.nnz());
   dG.v64.download(gval.data(), G.nnz(), s.st);
   CHRONOS_CUDA(cudaStreamSynchronize(s.st));
+  if (join) stream_wait(caller, s.st);
   return fl;
 }
 
@@ -353,27 +398,55 @@ int chronos_fsai_compute(int nthread, int n_step, int step_size, double tau, dou
   });
 }
 
-int chronos_fsai_numeric(int n, const int64_t *iat_A_h, const int *ja_A_h, const double *val_A_h,
-                         const int64_t *iat_G_h, const int *ja_G_h, double *val_G_h,
-                         int *is_posdef) {
+int chronos_fsai_numeric(int n, int base, const int64_t *iat_A_h, const int *ja_A_h,
+                         const double *val_A_h, const int64_t *iat_G_h, const int *ja_G_h,
+                         int out_precision, void *val_G_h, int *is_posdef, void *stream) {
   return guard([&] {
     CallRange range_("chronos_fsai_numeric");
-    CHRONOS_REQUIRE(val_G_h && is_posdef && iat_G_h && ja_G_h, CHRONOS_EINVAL, "null argument");
-    HostCSR A = from_mex_csr(n, n, iat_A_h, ja_A_h, val_A_h);
+    CHRONOS_REQUIRE(val_G_h && is_posdef && iat_G_h && ja_G_h && iat_A_h, CHRONOS_EINVAL,
+                    "null argument");
+    CHRONOS_REQUIRE(base == 0 || base == 1, CHRONOS_EINVAL, "base must be 0 or 1");
+    CHRONOS_REQUIRE(out_precision == CHRONOS_FP64 || out_precision == CHRONOS_FP32,
+                    CHRONOS_EINVAL, "out_precision must be CHRONOS_FP64 or CHRONOS_FP32");
+    CHRONOS_REQUIRE(n > 0 && iat_A_h[0] == base && iat_G_h[0] == base, CHRONOS_EINVAL,
+                    "row pointers must start at the given base");
+    // the MEX layout shifted to 1-based when the caller's arrays are 0-based
+    std::vector<int64_t> ia;
+    std::vector<int> ja;
+    const int64_t *iat = iat_A_h;
+    const int *jat = ja_A_h;
+    if (base == 0) {
+      ia.assign(iat_A_h, iat_A_h + n + 1);
+      for (auto &v : ia) v += 1;
+      CHRONOS_REQUIRE(ia[n] >= 1, CHRONOS_EINVAL, "decreasing row pointers");
+      ja.assign(ja_A_h, ja_A_h + (ia[n] - 1));
+      for (auto &v : ja) v += 1;
+      iat = ia.data();
+      jat = ja.data();
+    }
+    HostCSR A = from_mex_csr(n, n, iat, jat, val_A_h);
     HostCSR G;
     G.nrows = G.ncols = n;
     G.rp.resize((size_t)n + 1);
-    for (int i = 0; i <= n; ++i) G.rp[i] = iat_G_h[i] - 1;
-    CHRONOS_REQUIRE(G.rp[0] == 0, CHRONOS_EINVAL, "1-based G pattern expected");
+    for (int i = 0; i <= n; ++i) {
+      G.rp[i] = iat_G_h[i] - base;
+      CHRONOS_REQUIRE(i == 0 || G.rp[i] >= G.rp[i - 1], CHRONOS_EINVAL,
+                      "decreasing G row pointers");
+    }
     G.ci.resize(G.rp[n]);
     for (int64_t k = 0; k < G.rp[n]; ++k) {
-      G.ci[k] = ja_G_h[k] - 1;
+      G.ci[k] = ja_G_h[k] - base;
       CHRONOS_REQUIRE(G.ci[k] >= 0 && G.ci[k] < n, CHRONOS_EINVAL, "G column out of range");
     }
     G.v.assign(G.rp[n], 0.0);
     std::vector<double> gval;
-    const int fl = fsai_values(A, G, gval);
-    std::memcpy(val_G_h, gval.data(), sizeof(double) * gval.size());
+    const int fl = fsai_values(A, G, gval, static_cast<cudaStream_t>(stream), true);
+    if (out_precision == CHRONOS_FP64) {
+      std::memcpy(val_G_h, gval.data(), sizeof(double) * gval.size());
+    } else {
+      float *o = static_cast<float *>(val_G_h);
+      for (size_t k = 0; k < gval.size(); ++k) o[k] = (float)gval[k];
+    }
     *is_posdef = fl == 0 ? 1 : 0;
   });
 }
@@ -482,7 +555,13 @@ int chronos_amg_setup(const chronos_params *prm, int n, const int *iat_h, const 
     CallRange range_("chronos_amg_setup");
     CHRONOS_REQUIRE(prm && out, CHRONOS_EINVAL, "null argument");
     CHRONOS_REQUIRE(ntv0 == 0 || TV0_h, CHRONOS_EINVAL, "TV0 missing");
-    HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
+    HostCSR A = from_csr0_any(n, n, iat_h, ja_h, val_h);
+    std::vector<double> tv;
+    if (ntv0 > 0 && is_device_pointer(TV0_h)) {
+      tv.resize((size_t)n * ntv0);
+      CHRONOS_CUDA(cudaMemcpy(tv.data(), TV0_h, sizeof(double) * tv.size(), cudaMemcpyDeviceToHost));
+      TV0_h = tv.data();
+    }
     auto *hh = new chronos_hier();
     try {
       hh->h = build_hierarchy(*prm, A, ntv0, TV0_h);
@@ -500,7 +579,7 @@ int chronos_amg_setup_prolong(const chronos_params *prm, int n, const int *iat_h
   return guard([&] {
     CallRange range_("chronos_amg_setup_prolong");
     CHRONOS_REQUIRE(prm && out && prolong, CHRONOS_EINVAL, "null argument");
-    HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
+    HostCSR A = from_csr0_any(n, n, iat_h, ja_h, val_h);
     const ProlongFn fn = [&](int level, const HostCSR &Al) {
       const int nl = Al.nrows;
       std::vector<int> rp(Al.rp.begin(), Al.rp.end());
@@ -656,29 +735,31 @@ int chronos_diag_fix(int n, const int *iat_h, const int *ja_h, double *val_h) {
   });
 }
 
-int chronos_vcycle(chronos_hier *hh, const double *b_h, double *x_h, int nrhs) {
+int chronos_vcycle(chronos_hier *hh, const double *b_h, double *x_h, int nrhs, void *stream) {
   return guard([&] {
     CallRange range_("chronos_vcycle");
     CHRONOS_REQUIRE(hh && b_h && x_h && nrhs >= 1, CHRONOS_EINVAL, "bad argument");
     Hier &h = *hh->h;
     const int n = h.levels[0].n;
-    DBuf<double> b(n), x(n);
+    if (h.stage_b.size() < (size_t)n) { h.stage_b.alloc(n); h.stage_x.alloc(n); }
+    CallerStream order(h, stream);
     for (int c = 0; c < nrhs; ++c) {
-      b.upload(b_h + (size_t)c * n, n, h.st);
-      h.vcycle(b.get(), x.get(), nullptr, nullptr);
-      x.download(x_h + (size_t)c * n, n, h.st);
+      h.stage_b.upload(b_h + (size_t)c * n, n, h.st);
+      h.vcycle(h.stage_b.get(), h.stage_x.get(), nullptr, nullptr);
+      h.stage_x.download(x_h + (size_t)c * n, n, h.st);
     }
     CHRONOS_CUDA(cudaStreamSynchronize(h.st));
   });
 }
 
 int chronos_pcg_dev(chronos_hier *hh, const double *b_d, double *x_d, int itmax, double tol,
-                    int *iters, double *resvec_h, int *flag, double *seconds) {
+                    int *iters, double *resvec_h, int *flag, double *seconds, void *stream) {
   return guard([&] {
     CallRange range_("chronos_pcg_dev");
     CHRONOS_REQUIRE(hh && b_d && x_d && iters && flag, CHRONOS_EINVAL, "null argument");
     std::vector<double> rv;
     int it = 0, fl = 0;
+    CallerStream order(*hh->h, stream);
     try {
       hh->h->pcg_solve(b_d, x_d, itmax, tol, &it, &fl, resvec_h ? &rv : nullptr, seconds);
     } catch (const Error &e) {
@@ -692,15 +773,29 @@ int chronos_pcg_dev(chronos_hier *hh, const double *b_d, double *x_d, int itmax,
   });
 }
 
-int chronos_pcg(chronos_hier *hh, const double *b_h, double *x_h, int itmax, double tol,
-                int *iters, double *resvec_h, int *flag, double *seconds) {
+int chronos_pcg(chronos_hier *hh, const int *iat_h, const int *ja_h, const double *val_h,
+                const double *b_h, double *x_h, int itmax, double tol, int *iters,
+                double *resvec_h, int *flag, double *seconds, void *stream) {
   return guard([&] {
     CallRange range_("chronos_pcg");
     CHRONOS_REQUIRE(hh && b_h && x_h && iters && flag, CHRONOS_EINVAL, "null argument");
     Hier &h = *hh->h;
     const int n = h.levels[0].n;
+    // the caller's operator serves this call only: later calls (and the
+    // other entry points) apply the hierarchy's level-1 operator again
+    struct OperatorScope {
+      Hier &h;
+      ~OperatorScope() {
+        try { h.set_outer_operator(nullptr); } catch (...) {}
+      }
+    } op_scope{h};
+    if (iat_h) {
+      const HostCSR op = from_csr0(n, n, iat_h, ja_h, val_h);
+      h.set_outer_operator(&op);
+    }
     // staging buffers live with the handle: no allocation per call
     if (h.stage_b.size() < (size_t)n) { h.stage_b.alloc(n); h.stage_x.alloc(n); }
+    CallerStream order(h, stream);
     DBuf<double> &b = h.stage_b, &x = h.stage_x;
     b.upload(b_h, n, h.st);
     x.upload(x_h, n, h.st);
@@ -716,13 +811,14 @@ int chronos_pcg(chronos_hier *hh, const double *b_h, double *x_h, int itmax, dou
 }
 
 int chronos_pcg_block(chronos_hier *hh, int nrhs, const double *B_h, double *X_h, int itmax,
-                      double tol, int *iters_h, int *flags_h, double *seconds) {
+                      double tol, int *iters_h, int *flags_h, double *seconds, void *stream) {
   return guard([&] {
     CallRange range_("chronos_pcg_block");
     CHRONOS_REQUIRE(hh && B_h && X_h && iters_h && flags_h && nrhs >= 1, CHRONOS_EINVAL,
                     "bad argument");
     Hier &h = *hh->h;
     const int n = h.levels[0].n;
+    CallerStream order(h, stream);
     double total = 0.0;
     // chunks of at most 16 columns, each one SpMM block solve
     for (int c0 = 0; c0 < nrhs; c0 += 16) {

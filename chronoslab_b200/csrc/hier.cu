@@ -67,7 +67,24 @@ Hier::~Hier() {
   levels.clear();
   if (pcg.exec) { cudaGraphExecDestroy(pcg.exec); pcg.exec = nullptr; }
   if (pcg.graph) { cudaGraphDestroy(pcg.graph); pcg.graph = nullptr; }
+  if (ev_in) cudaEventDestroy(ev_in);
+  if (ev_out) cudaEventDestroy(ev_out);
   if (st) cudaStreamDestroy(st);
+}
+
+CallerStream::CallerStream(Hier &h, void *stream)
+    : h_(h), caller_(static_cast<cudaStream_t>(stream)) {
+  if (!h_.ev_in) CHRONOS_CUDA(cudaEventCreateWithFlags(&h_.ev_in, cudaEventDisableTiming));
+  if (!h_.ev_out) CHRONOS_CUDA(cudaEventCreateWithFlags(&h_.ev_out, cudaEventDisableTiming));
+  CHRONOS_CUDA(cudaEventRecord(h_.ev_in, caller_));
+  CHRONOS_CUDA(cudaStreamWaitEvent(h_.st, h_.ev_in, 0));
+}
+
+CallerStream::~CallerStream() {
+  // runs on normal return and on error: the caller's stream never overtakes
+  // work the handle queued
+  if (cudaEventRecord(h_.ev_out, h_.st) == cudaSuccess)
+    cudaStreamWaitEvent(caller_, h_.ev_out, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -1776,7 +1793,30 @@ static int reduce_blocks(int n) {
 // True when the outer PCG applies the stored FP32 values with true-residual
 // replacement (FP32 hierarchy, exact_outer = 0).
 static bool mixed_outer(const Hier &h) {
-  return h.precision == CHRONOS_FP32 && !h.prm.exact_outer;
+  return h.precision == CHRONOS_FP32 && !h.prm.exact_outer && !h.use_user_op;
+}
+
+static void drop_pcg_graph(PcgState &s) {
+  if (s.exec) { cudaGraphExecDestroy(s.exec); s.exec = nullptr; }
+  if (s.graph) { cudaGraphDestroy(s.graph); s.graph = nullptr; }
+}
+
+void Hier::set_outer_operator(const HostCSR *A) {
+  if (A) {
+    CHRONOS_REQUIRE(A->nrows == levels[0].n && A->ncols == levels[0].n, CHRONOS_EINVAL,
+                    "the operator must have the hierarchy's level-1 size");
+    CHRONOS_CUDA(cudaStreamSynchronize(st));   // the previous operator may still be in use
+    user_op = DMat();
+    upload_csr(*A, user_op, false, st);
+    autotune_lanes(user_op, false, st);
+    drop_pcg_graph(pcg);                       // the graph holds the operator's pointers
+    use_user_op = true;
+  } else if (use_user_op) {
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    drop_pcg_graph(pcg);
+    use_user_op = false;
+    user_op = DMat();
+  }
 }
 
 // Captures one PCG_CJ iteration (PCG_CJ.m:36-64) into the current stream capture.
@@ -1793,7 +1833,7 @@ static void capture_iteration(Hier &h, cudaGraphConditionalHandle handle, int us
              (const double *)sc);
   CHRONOS_CHECK_LAUNCH();
   unsigned *tk = s.tickets.get();
-  launch_pcg_spmv(st, h.levels[0].A, mixed, s.p.get(), s.res.get(), s.axp.get(),
+  launch_pcg_spmv(st, h.outer_A(), mixed, s.p.get(), s.res.get(), s.axp.get(),
                   s.part.get() + 4 * 3 * 2048, tk + 1, sc);
   launch_pdl(k_pcg_xr_update, nb, 256, st, n, s.x.get(), s.res.get(), (const double *)s.p.get(),
              (const double *)s.axp.get(), s.part.get() + 8 * 3 * 2048, tk + 2, sc,
@@ -1822,8 +1862,7 @@ static void ensure_pcg_state(Hier &h, int itmax) {
     // resvec is baked into the graph: rebuild it when the buffer moves
     s.resvec.alloc((size_t)itmax + 1);
     s.resvec_cap = itmax + 1;
-    if (s.exec) { cudaGraphExecDestroy(s.exec); s.exec = nullptr; }
-    if (s.graph) { cudaGraphDestroy(s.graph); s.graph = nullptr; }
+    drop_pcg_graph(s);
   }
 }
 
@@ -1903,7 +1942,7 @@ void Hier::pcg_solve(const double *b, double *x, int itmax, double tol, int *ite
   CHRONOS_CUDA(cudaMemcpyAsync(s.x.get(), x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   if (mixed_outer(*this))
     CHRONOS_CUDA(cudaMemcpyAsync(s.b.get(), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  op_apply<double, double, double, double, MODE_RESID, false>(st, levels[0].A, s.x.get(), b,
+  op_apply<double, double, double, double, MODE_RESID, false>(st, outer_A(), s.x.get(), b,
                                                               s.res.get(), 1.0);
   const int nb = reduce_blocks(n);
   double *part = s.part.get();
@@ -1988,7 +2027,7 @@ void Hier::pcg_enqueue(const double *b, double *x, int itmax, double tol) {
   CHRONOS_CUDA(cudaMemcpyAsync(s.x.get(), x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
   if (mixed_outer(*this))
     CHRONOS_CUDA(cudaMemcpyAsync(s.b.get(), b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
-  op_apply<double, double, double, double, MODE_RESID, false>(st, levels[0].A, s.x.get(), b,
+  op_apply<double, double, double, double, MODE_RESID, false>(st, outer_A(), s.x.get(), b,
                                                               s.res.get(), 1.0);
   const int nb = reduce_blocks(n);
   k_dot_store<<<nb, 256, 0, st>>>(n, b, b, s.part.get(), s.tickets.get() + 3,

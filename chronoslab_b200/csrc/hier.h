@@ -102,7 +102,18 @@ struct Hier {
   cudaStream_t st = nullptr;
   std::array<double, 8> times{};   // setup timings
   PcgState pcg;
+  // Operator of the outer PCG when the caller passes one (PCG_CJ's prodA,
+  // PCG_CJ.m:1): FP64 CSR of the level-1 size; otherwise levels[0].A.
+  DMat user_op;
+  bool use_user_op = false;
+  // events that order st after a caller's stream and the caller's stream after st
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   ~Hier();
+
+  const DMat &outer_A() const { return use_user_op ? user_op : levels[0].A; }
+  // Sets (A != nullptr) or clears the outer operator; the PCG graph is
+  // rebuilt when the operator in use changes.
+  void set_outer_operator(const HostCSR *A);
 
   // one V-cycle: out = M^{-1} b on device FP64 vectors of length n0;
   // when dw != nullptr also *dot_out = out . dw (deterministic).
@@ -129,6 +140,23 @@ struct Hier {
 // level number and the level's operator (FP64, from the GPU Galerkin product
 // on levels > 1), returns P (n x nc, 0-based CSR, sorted rows).
 using ProlongFn = std::function<HostCSR(int level, const HostCSR &A)>;
+
+// Orders a handle's work on a caller's CUDA stream: on construction the
+// handle's stream waits for what the caller's stream has queued so far; on
+// destruction the caller's stream waits for what the handle queued.  Event
+// joins only: no device-wide synchronisation.  A null caller stream means
+// the legacy default stream.
+class CallerStream {
+ public:
+  CallerStream(Hier &h, void *stream);
+  ~CallerStream();
+  CallerStream(const CallerStream &) = delete;
+  CallerStream &operator=(const CallerStream &) = delete;
+
+ private:
+  Hier &h_;
+  cudaStream_t caller_;
+};
 
 // tune = false leaves the apply kernels' lane counts and formats at their
 // defaults; tune_hierarchy then chooses them (timed on a quiet GPU).

@@ -9,8 +9,9 @@
  * Ownership: input pointers are borrowed and never freed by the library; the
  * library owns everything a handle (chronos_hier, chronos_galerkin_plan) holds
  * until the matching *_free call.  One handle is used by one host thread at a
- * time and on one CUDA stream.  Pointers named *_h are host memory; *_d are
- * device memory of the current device.
+ * time; the solve calls order their device work on the caller's stream
+ * argument (see "Streams of the solve entry points").  Pointers named *_h are
+ * host memory; *_d are device memory of the current device.
  *
  * Reference interfaces replaced (paths inside the ChronosLab project):
  *   chronos_fsai_compute   <- SYM_aFSAI_compute MEX
@@ -141,12 +142,17 @@ int chronos_fsai_compute(int nthread, int n_step, int step_size, double tau, dou
                          const int64_t *iat_M_h, const int *ja_M_h, const double *coef_M_h,
                          int64_t *nterm_G, int64_t *iat_G_h, int *ja_G_h, double *coef_G_h,
                          int *is_posdef);
-/* Numeric phase only: G values on a given pattern (1-based CSR of G, each row
- * strictly-lower ascending then the diagonal).  A is 1-based CSR (int64 iat,
- * int32 ja).  One dense SPD solve per row on the GPU, FP64. */
-int chronos_fsai_numeric(int n, const int64_t *iat_A_h, const int *ja_A_h, const double *val_A_h,
-                         const int64_t *iat_G_h, const int *ja_G_h, double *val_G_h,
-                         int *is_posdef);
+/* Numeric phase only: G values on a given pattern (CSR of G, each row
+ * strictly-lower ascending then the diagonal).  A and G are CSR with int64
+ * row pointers and int32 columns, 0-based (base = 0) or 1-based as the MEX
+ * passes them (base = 1).  One dense SPD solve per row on the GPU in FP64;
+ * val_G_h receives double values (out_precision = CHRONOS_FP64) or float
+ * values rounded from them (CHRONOS_FP32).  The work is ordered on `stream`
+ * (a cudaStream_t; NULL: the legacy default stream) and the call returns
+ * after it completes. */
+int chronos_fsai_numeric(int n, int base, const int64_t *iat_A_h, const int *ja_A_h,
+                         const double *val_A_h, const int64_t *iat_G_h, const int *ja_G_h,
+                         int out_precision, void *val_G_h, int *is_posdef, void *stream);
 
 /* FSAI numeric phase that allocates nothing.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot let a library
@@ -271,8 +277,9 @@ typedef struct chronos_level_info {
   int sell_mask;        /* bits 0-4: A, G, G', P, P' applied in sliced ELL form */
 } chronos_level_info;
 
-/* Builds the hierarchy of A (0-based CSR, FP64, host memory) with the test
- * space TV0 (n x ntv0, column-major; may be NULL with ntv0 = 0).  Coarsening
+/* Builds the hierarchy of A (0-based CSR, FP64, in host or device memory)
+ * with the test space TV0 (n x ntv0, column-major, host or device; may be NULL
+ * with ntv0 = 0).  Coarsening
  * (SoC + PMIS), C/F splitting and the BAMG prolongation run on the host as in
  * the reference; FSAI values, lambda_max, the Galerkin products and the
  * coarse Cholesky run on the GPU.  prm->precision selects the stored
@@ -356,24 +363,39 @@ int chronos_hier_profile(chronos_hier *h, int reps, chronos_profile *out);
  * (lambda_max by a GPU Lanczos run).  Updates val_h in place. */
 int chronos_diag_fix(int n, const int *iat_h, const int *ja_h, double *val_h);
 
+/* Streams of the solve entry points: `stream` is a cudaStream_t (NULL: the
+ * legacy default stream).  The call's device work starts after the work the
+ * stream has queued before the call, and work queued on the stream after the
+ * call starts after the call's device work; the ordering uses events, with no
+ * device-wide synchronisation.  Calls that return host results (iterations,
+ * flags, host vectors) wait for their own work before returning.  Handles are
+ * independent: two handles used from two host threads on two streams run
+ * concurrently. */
+
 /* One V(nupre,nupost) cycle x = M^{-1} b (x0 absent), host vectors, FP64 in/out.
  * nrhs columns, column-major (leading dimension n). */
-int chronos_vcycle(chronos_hier *h, const double *b_h, double *x_h, int nrhs);
+int chronos_vcycle(chronos_hier *h, const double *b_h, double *x_h, int nrhs, void *stream);
 
-/* PCG_CJ on the level-1 operator with the V-cycle preconditioner, x0 = x_h on
- * input.  resvec_h (itmax+1 entries, may be NULL) receives ||r_k||/||b||.
- * flag = 1 when not converged (PCG_CJ.m:69-71).  seconds (may be NULL)
- * receives the device time of the solve (CUDA events, copies excluded). */
-int chronos_pcg(chronos_hier *h, const double *b_h, double *x_h, int itmax, double tol,
-                int *iters, double *resvec_h, int *flag, double *seconds);
-/* Same on device vectors (b_d, x_d: n FP64), the hot path without copies. */
+/* PCG_CJ with the V-cycle preconditioner, x0 = x_h on input.  The operator is
+ * PCG_CJ's prodA (PCG_CJ.m:1; aspAMG_main.m:199-202 passes @(x)A*x): the
+ * 0-based FP64 CSR (iat_h, ja_h, val_h) of the hierarchy's level-1 size,
+ * copied to the device on every call that passes it, or the hierarchy's
+ * level-1 operator when iat_h is NULL.  resvec_h (itmax+1 entries, may be NULL)
+ * receives ||r_k||/||b||.  flag = 1 when not converged (PCG_CJ.m:69-71).
+ * seconds (may be NULL) receives the device time of the solve (CUDA events,
+ * copies excluded). */
+int chronos_pcg(chronos_hier *h, const int *iat_h, const int *ja_h, const double *val_h,
+                const double *b_h, double *x_h, int itmax, double tol, int *iters,
+                double *resvec_h, int *flag, double *seconds, void *stream);
+/* Same on device vectors (b_d, x_d: n FP64) with the hierarchy's level-1
+ * operator, the hot path without copies. */
 int chronos_pcg_dev(chronos_hier *h, const double *b_d, double *x_d, int itmax, double tol,
-                    int *iters, double *resvec_h, int *flag, double *seconds);
+                    int *iters, double *resvec_h, int *flag, double *seconds, void *stream);
 /* Block of nrhs independent right-hand sides (column-major n x nrhs) solved
  * together: one SpMM V-cycle per iteration, per-column PCG_CJ recurrences and
  * stopping tests.  iters_h[nrhs], flags_h[nrhs]. */
 int chronos_pcg_block(chronos_hier *h, int nrhs, const double *B_h, double *X_h, int itmax,
-                      double tol, int *iters_h, int *flags_h, double *seconds);
+                      double tol, int *iters_h, int *flags_h, double *seconds, void *stream);
 
 /* ---- Batch of independent problems of uneven sizes ---------------------- */
 /* One hierarchy per problem (each what chronos_amg_setup builds for it with

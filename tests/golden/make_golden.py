@@ -123,4 +123,8 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    from oracle.refdir import reference_dir
+    ref = sys.argv[1] if len(sys.argv) > 1 else reference_dir()
+    if not ref:
+        sys.exit("reference tree not found: pass its path or set CHRONOS_REFERENCE_DIR")
+    main(ref)

@@ -13,7 +13,10 @@ import chronoslab_b200 as cb
 from chronoslab_b200._lib import ChronosError
 from oracle import amg_oracle as O
 
-REF_BIN = ("/root/reference/sources/Preconditioner/AMG/prolong/EMIN/example_cpp/matrix.bin")
+from oracle.refdir import reference_file
+
+REF_BIN = reference_file("sources", "Preconditioner", "AMG", "prolong", "EMIN", "example_cpp",
+                         "matrix.bin")
 
 
 def random_matrix(n, seed, density=0.05):
@@ -94,7 +97,7 @@ def test_format_errors(lib, tmp_path):
         cb.read_ext_bin(str(bad))
 
 
-@pytest.mark.skipif(not os.path.exists(REF_BIN), reason="reference example file not mounted")
+@pytest.mark.skipif(REF_BIN is None, reason="reference example file not present")
 def test_reads_reference_example_matrix(lib):
     """The reference's own example_cpp/matrix.bin (Cubo level 1) read through
     the C ABI equals the oracle's restatement of readBinaryMatrix."""

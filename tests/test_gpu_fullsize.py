@@ -1,0 +1,122 @@
+"""Parity at the full sizes of the block, batch and adjoint configurations.
+
+* Log-normal anisotropic diffusion 128^3 (2,097,152 rows) with a block of 16
+  seeded right-hand sides, solved together by SpMM V-cycles: every column's
+  iteration count within one of the oracle's PCG_CJ (C/OpenMP, FP64) on the
+  GPU hierarchy's own level matrices, and every true relative residual at
+  most 1e-8.
+* The 64 problems of the batch configuration (Poisson and log-normal
+  diffusion, grid edge drawn uniformly in [16, 64], FSAI 15 steps of 4): every
+  problem's batch iteration count within one of its own single solve and of
+  the oracle's PCG_CJ on that solve's levels.
+* Adjoint on log-normal diffusion 64^3 (sigma = 1): dJ/dlog k from the GPU
+  adjoint against central differences, h = 1e-6 along 32 seeded directions.
+"""
+import numpy as np
+import pytest
+import torch
+
+import chronoslab_b200 as cb
+from chronoslab_b200 import problems as PB
+from chronoslab_b200.autodiff import DiffusionPattern, diffusion_values, solve
+from oracle import amg_oracle as O
+from oracle import c_oracle as CO
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_pcg_on_levels(h):
+    """The oracle's C PCG_CJ on the hierarchy's exported FP64 level matrices."""
+    parts = []
+    for l in range(h.nlevels):
+        p = {"A": h.export(l, "A")}
+        if l < h.nlevels - 1:
+            p.update(G=h.export(l, "G"), P=h.export(l, "P"), omega=h.level_info(l)["omega"])
+        parts.append(p)
+    return CO.CHierarchy(O.hierarchy_from_parts(parts))
+
+
+def test_block16_diffusion128(lib):
+    A, _ = PB.diffusion7(128, sigma=2.0, corr_len=8.0, zaniso=0.01, seed=0)
+    n = A.shape[0]
+    assert n == 2097152
+    B = PB.uniform_rhs(n, seed=1, ncols=16)
+    for prec, tol_it in ((cb.CHRONOS_FP64, 1), (cb.CHRONOS_FP32, 2)):
+        with cb.Hierarchy(A, np.ones(n), cb.params(precision=prec, ntv=1)) as h:
+            X, its, flags, _ = h.pcg_block(B, itmax=1000, tol=1e-8)
+            CH = oracle_pcg_on_levels(h)
+        assert np.all(flags == 0)
+        for j in range(16):
+            assert np.linalg.norm(B[:, j] - A @ X[:, j]) <= 1e-8 * np.linalg.norm(B[:, j]), j
+        for j in range(16):
+            xo, ito, _, flo = CH.pcg(B[:, j], itmax=1000, tol=1e-8)
+            assert flo == 0 and abs(int(its[j]) - ito) <= tol_it, (prec, j, int(its[j]), ito)
+            assert np.linalg.norm(X[:, j] - xo) <= 1e-6 * np.linalg.norm(xo)
+
+
+def _c4_problems():
+    rng = np.random.default_rng(0)
+    edges = rng.integers(16, 65, 64)
+    As, bs = [], []
+    for p, e in enumerate(edges):
+        if p % 2 == 0:
+            A = PB.poisson7(int(e))
+        else:
+            A, _ = PB.diffusion7(int(e), sigma=2.0, corr_len=8.0, zaniso=0.01, seed=p)
+        As.append(A)
+        bs.append(PB.uniform_rhs(A.shape[0], seed=1000 + p))
+    return As, bs
+
+
+def test_batch64_problems(lib):
+    As, bs = _c4_problems()
+    sizes = [A.shape[0] for A in As]
+    assert min(sizes) >= 16 ** 3 and max(sizes) <= 64 ** 3
+    prm = dict(ntv=1, nstep=15, step_size=4)
+    with cb.Batch(As, cb.params(precision=cb.CHRONOS_FP32, **prm)) as Bt:
+        xs, its, fl, _ = Bt.solve(bs, itmax=1000, tol=1e-8)
+    assert np.all(fl == 0)
+    for p, (A, b) in enumerate(zip(As, bs)):
+        assert np.linalg.norm(b - A @ xs[p]) <= 1e-8 * np.linalg.norm(b), p
+        with cb.Hierarchy(A, np.ones(A.shape[0]), cb.params(precision=cb.CHRONOS_FP32, **prm)) as h:
+            x, it, _, flag, _ = h.pcg(b, itmax=1000, tol=1e-8)
+            CH = oracle_pcg_on_levels(h)
+        _, ito, _, flo = CH.pcg(b, itmax=1000, tol=1e-8)
+        assert flag == 0 and flo == 0
+        assert abs(int(its[p]) - it) <= 1, (p, int(its[p]), it)
+        assert abs(int(its[p]) - ito) <= 2 and abs(it - ito) <= 2, (p, int(its[p]), it, ito)
+
+
+def test_adjoint_fd_diffusion64(lib):
+    """C5 at full size: the FP64-hierarchy adjoint gradient against central
+    finite differences of the GPU forward solves (h = 1e-6, 32 seeded
+    directions, solves to 1e-14), relative error at most 1e-6."""
+    rng = np.random.default_rng(7)
+    shape = (64, 64, 64)
+    logk = PB.gaussian_field(shape, 8.0, seed=5)                 # sigma = 1
+    pat = DiffusionPattern(shape, 0.01)
+    b = rng.uniform(-1, 1, pat.n)
+    logk_star = logk + 0.1 * PB.gaussian_field(shape, 8.0, seed=6)
+    vstar = diffusion_values(torch.from_numpy(logk_star), pat)
+    prm = cb.params(precision=cb.CHRONOS_FP64, ntv=1)
+    ustar = solve(vstar, torch.from_numpy(b), pat.indptr, pat.indices, prm=prm, tol=1e-14,
+                  itmax=4000).numpy()
+
+    def J_and_grad(lk, need_grad):
+        t = torch.from_numpy(lk).requires_grad_(need_grad)
+        u = solve(diffusion_values(t, pat), torch.from_numpy(b), pat.indptr, pat.indices,
+                  prm=prm, tol=1e-14, itmax=4000)
+        J = 0.5 * torch.sum((u - torch.from_numpy(ustar)) ** 2)
+        if need_grad:
+            J.backward()
+            return J.item(), t.grad.numpy()
+        return J.item(), None
+
+    _, g = J_and_grad(logk, True)
+    h = 1e-6
+    errs = []
+    for _ in range(32):
+        d = rng.standard_normal(shape)
+        fd = (J_and_grad(logk + h * d, False)[0] - J_and_grad(logk - h * d, False)[0]) / (2 * h)
+        errs.append(abs(fd - np.sum(g * d)) / max(abs(fd), 1e-300))
+    assert max(errs) <= 1e-6, (max(errs), np.median(errs))

@@ -143,8 +143,9 @@ def test_params_files(lib, tmp_path):
 
 
 def test_reference_parameter_files_if_present(lib):
-    fn = "/root/reference/Tests/aspAMG.fnames"
-    if not os.path.exists(fn):
+    from oracle.refdir import reference_file
+    fn = reference_file("Tests", "aspAMG.fnames")
+    if fn is None:
         pytest.skip("reference tree not mounted")
     p = cb.readDefaultParams(fn)
     assert p.SoC_type == b"DOM" and p.soc_tau == 0.01 and p.nupre == 1 and p.ntv == 6
