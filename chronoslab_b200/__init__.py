@@ -382,6 +382,10 @@ class Hierarchy:
                                     np.ctypeslib.as_array(ja, shape=(max(nnz, 1),))[:nnz].copy(),
                                     rp), shape=(nl, nl))
                 P = sp.csr_matrix(prolong(level, Al))
+                if P.shape[0] != nl:
+                    # the library reads n + 1 row pointers from the returned array
+                    raise ChronosError(-1, f"prolongation of level {level} has {P.shape[0]} "
+                                           f"rows, the level has {nl}")
                 P.sort_indices()
                 pp = np.ascontiguousarray(P.indptr, dtype=np.int32)
                 pi = np.ascontiguousarray(P.indices, dtype=np.int32)
@@ -508,6 +512,16 @@ class Hierarchy:
         check(self._lib.chronos_hier_profile(self._h, reps, C.byref(p)))
         return {k: getattr(p, k) for k, _ in chronos_profile._fields_}
 
+    def _operator(self, A):
+        """0-based CSR pointers of an operator of the hierarchy's level-1 size.
+        The C ABI reads n + 1 row pointers from the caller's array, so the
+        size is checked here, before the call."""
+        if A.shape != (self.n, self.n):
+            raise ChronosError(-1, f"operator of shape {A.shape}, the hierarchy has n = {self.n}")
+        _, ip, ix, dv = _csr(A)
+        self._op_keep = (ip, ix, dv)
+        return (_pi(ip), _pi(ix), _pd(dv))
+
     def vcycle(self, b, stream=None):
         b = np.asarray(b, dtype=np.float64)
         nrhs = 1 if b.ndim == 1 else b.shape[1]
@@ -524,8 +538,7 @@ class Hierarchy:
         it, flag, sec = C.c_int(), C.c_int(), C.c_double()
         rv = np.zeros(max(itmax, 0) + 1)
         if A is not None:
-            _, ip, ix, dv = _csr(A)
-            ops = (_pi(ip), _pi(ix), _pd(dv))
+            ops = self._operator(A)
         else:
             ops = (None, None, None)
         check(self._lib.chronos_pcg(self._h, *ops, _pd(b), _pd(x), itmax, tol, C.byref(it),
@@ -575,8 +588,7 @@ class Hierarchy:
         x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
         it, info, rel = C.c_int(), C.c_int(), C.c_double()
         if A is not None:
-            _, ip, ix, dv = _csr(A)
-            ops = (_pi(ip), _pi(ix), _pd(dv))
+            ops = self._operator(A)
         else:
             ops = (None, None, None)
         check(self._lib.chronos_sqmr(self._h, *ops, _pd(b), _pd(x), itmax, tol, C.byref(it),
@@ -590,8 +602,7 @@ class Hierarchy:
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros(self.n) if x0 is None else np.array(x0, dtype=np.float64)
         if A is not None:
-            _, ip, ix, dv = _csr(A)
-            ops = (_pi(ip), _pi(ix), _pd(dv))
+            ops = self._operator(A)
         else:
             ops = (None, None, None)
         io, ii, fl, nrv = C.c_int(), C.c_int(), C.c_int(), C.c_int()

@@ -88,35 +88,47 @@ def test_batch64_problems(lib):
 
 
 def test_adjoint_fd_diffusion64(lib):
-    """C5 at full size: the FP64-hierarchy adjoint gradient against central
-    finite differences of the GPU forward solves (h = 1e-6, 32 seeded
-    directions, solves to 1e-14), relative error at most 1e-6."""
+    """C5 at full size: the FP64-hierarchy adjoint gradient (through the
+    torch.autograd binding) against central finite differences, h = 1e-6
+    along 32 seeded directions, relative error at most 1e-6.  The finite
+    differences evaluate J(log k +- h d) by GPU PCG solves to 1e-14 of the
+    perturbed operators, all preconditioned by the hierarchy of log k (the
+    operator argument of chronos_pcg): a hierarchy rebuilt for each
+    perturbation can coarsen differently, and the two solves' 1e-14-level
+    errors would then no longer cancel in the difference."""
+    import scipy.sparse as sp
     rng = np.random.default_rng(7)
     shape = (64, 64, 64)
     logk = PB.gaussian_field(shape, 8.0, seed=5)                 # sigma = 1
     pat = DiffusionPattern(shape, 0.01)
     b = rng.uniform(-1, 1, pat.n)
     logk_star = logk + 0.1 * PB.gaussian_field(shape, 8.0, seed=6)
-    vstar = diffusion_values(torch.from_numpy(logk_star), pat)
     prm = cb.params(precision=cb.CHRONOS_FP64, ntv=1)
-    ustar = solve(vstar, torch.from_numpy(b), pat.indptr, pat.indices, prm=prm, tol=1e-14,
-                  itmax=4000).numpy()
 
-    def J_and_grad(lk, need_grad):
-        t = torch.from_numpy(lk).requires_grad_(need_grad)
+    def assemble(lk):
+        v = diffusion_values(torch.from_numpy(lk), pat).numpy()
+        return sp.csr_matrix((v, pat.indices, pat.indptr), shape=(pat.n, pat.n))
+
+    with cb.Hierarchy(assemble(logk), np.ones(pat.n), prm) as h0:
+        def forward(lk):
+            u, it, _, flag, _ = h0.pcg(b, itmax=4000, tol=1e-14, A=assemble(lk))
+            assert flag == 0
+            return u
+
+        ustar = forward(logk_star)
+
+        def J(lk):
+            return 0.5 * float(np.sum((forward(lk) - ustar) ** 2))
+
+        t = torch.from_numpy(logk).requires_grad_(True)
         u = solve(diffusion_values(t, pat), torch.from_numpy(b), pat.indptr, pat.indices,
                   prm=prm, tol=1e-14, itmax=4000)
-        J = 0.5 * torch.sum((u - torch.from_numpy(ustar)) ** 2)
-        if need_grad:
-            J.backward()
-            return J.item(), t.grad.numpy()
-        return J.item(), None
-
-    _, g = J_and_grad(logk, True)
-    h = 1e-6
-    errs = []
-    for _ in range(32):
-        d = rng.standard_normal(shape)
-        fd = (J_and_grad(logk + h * d, False)[0] - J_and_grad(logk - h * d, False)[0]) / (2 * h)
-        errs.append(abs(fd - np.sum(g * d)) / max(abs(fd), 1e-300))
+        (0.5 * torch.sum((u - torch.from_numpy(ustar)) ** 2)).backward()
+        g = t.grad.numpy()
+        hstep = 1e-6
+        errs = []
+        for _ in range(32):
+            d = rng.standard_normal(shape)
+            fd = (J(logk + hstep * d) - J(logk - hstep * d)) / (2 * hstep)
+            errs.append(abs(fd - np.sum(g * d)) / max(abs(fd), 1e-300))
     assert max(errs) <= 1e-6, (max(errs), np.median(errs))
