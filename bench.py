@@ -498,68 +498,121 @@ def run_product(args, world, rank, local):
     return 0
 
 
-def run_block_or_batch(args):
+def run_block_or_batch(args, world=1, rank=0):
     """C3 (block of 16 right-hand sides, SpMM V-cycles) or C4 (64 independent
-    problems of uneven sizes, queued together); FP32 hierarchy vs FP64."""
+    problems of uneven sizes, queued together); FP32 hierarchy vs FP64.  With
+    N ranks (one per GPU) the units are split with no collective on the data
+    path: C4's problems largest-first by stored entries, C3's columns in
+    contiguous ranges (every rank holds the operator's hierarchy); each step
+    is timed on the device by every rank for its share, and the step's time
+    is the slowest rank's (NCCL max), the total work staying 64 problems /
+    16 columns (strong scaling).  The per-unit iterations and flags are
+    gathered once at the end."""
     import numpy as np
+    import torch
     import chronoslab_b200 as cb
     from chronoslab_b200 import problems as PB
-    out = {"metric": METRIC, "unit": "ms", "n_gpus": 1, "steps": args.steps,
-           "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+    from chronoslab_b200.sharding import ShardedBatch, ShardedBlock
+    dist = None
+    if world > 1:
+        import torch.distributed as tdist
+        from datetime import timedelta
+        torch.cuda.set_device(0)
+        tdist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                 device_id=torch.device("cuda", 0))
+        dist = tdist
+    out = {"metric": METRIC, "unit": "ms", "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "higher_is_better": False,
+           "scaling": "strong" if world > 1 else "weak",
            "vs_baseline": None, "dtype": "f32 hierarchy / f64 outer",
            "data": "synthetic (seeded)"}
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def slowest(ms):
+        if not dist:
+            return ms
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return t.item()
+
     res = {}
     if args.workload == "c3":
         ne = 128 if args.ne == 80 else args.ne
         A, _ = PB.diffusion7(ne, sigma=2.0, corr_len=8.0, zaniso=0.01, seed=0)
         B = PB.uniform_rhs(A.shape[0], seed=1, ncols=16)
-        ones = np.ones(A.shape[0])
         for prec, name in ((cb.CHRONOS_FP32, "fp32"), (cb.CHRONOS_FP64, "fp64")):
-            with cb.Hierarchy(A, ones, cb.params(precision=prec, ntv=1)) as h:
-                for _ in range(args.warmup):
-                    h.pcg_block(B, itmax=args.itmax, tol=args.tol)
-                ts = []
-                for _ in range(args.steps):
-                    X, its, fl, sec = h.pcg_block(B, itmax=args.itmax, tol=args.tol)
-                    assert np.all(fl == 0)
-                    ts.append(sec * 1e3)
-                one = []
+            sh = ShardedBlock(A, 16, world, rank, dist, prm=cb.params(precision=prec, ntv=1))
+            for _ in range(args.warmup):
+                sh.solve_local(B, itmax=args.itmax, tol=args.tol)
+            barrier()
+            ts = []
+            for _ in range(args.steps):
+                X, its, fl, sec = sh.solve_local(B, itmax=args.itmax, tol=args.tol)
+                assert np.all(np.asarray(fl) == 0)
+                ts.append(sec * 1e3)
+            barrier()
+            relres = max((np.linalg.norm(B[:, j] - A @ X[:, k]) / np.linalg.norm(B[:, j])
+                          for k, j in enumerate(range(sh.lo, sh.hi))), default=0.0)
+            one = []
+            if sh.local is not None:
                 for _ in range(2):
-                    x, it, _, f, sec1 = h.pcg(B[:, 0], itmax=args.itmax, tol=args.tol)
+                    _, _, _, _, sec1 = sh.local.pcg(B[:, sh.lo], itmax=args.itmax, tol=args.tol)
                     one.append(sec1 * 1e3)
-                relres = max(np.linalg.norm(B[:, j] - A @ X[:, j]) / np.linalg.norm(B[:, j])
-                             for j in range(16))
-                res[name] = {"ms": sum(ts) / len(ts), "iters": its.tolist(),
-                             "single_rhs_ms": min(one), "true_relres_max": relres,
-                             "levels": [h.level_info(l)["n"] for l in range(h.nlevels)]}
+            units, _ = sh.solve(B, itmax=args.itmax, tol=args.tol, gather_x=False)
+            res[name] = {"ms": slowest(sum(ts) / len(ts)),
+                         "iters": [units[j]["iters"] for j in range(16)],
+                         "single_rhs_ms": min(one) if one else None,
+                         "true_relres_max": float(slowest(relres)),
+                         "levels": ([sh.local.level_info(l)["n"] for l in range(sh.local.nlevels)]
+                                    if sh.local is not None else None)}
+            sh.close()
         out["config"] = {"workload": f"log-normal diffusion {ne}^3 ({A.shape[0]} rows, {A.nnz} "
                                      "nnz), block of 16 RHS, SpMM V-cycles, PCG_CJ to "
-                                     f"{args.tol} per column"}
+                                     f"{args.tol} per column",
+                         "parallelism": f"columns split over {world} rank(s)" if world > 1
+                         else "one GPU"}
     else:
         As, bs = c4_problems()
         for prec, name in ((cb.CHRONOS_FP32, "fp32"), (cb.CHRONOS_FP64, "fp64")):
             t0 = time.perf_counter()
-            with cb.Batch(As, cb.params(precision=prec, ntv=1, nstep=15, step_size=4)) as Bt:
-                setup = time.perf_counter() - t0
-                for _ in range(args.warmup):
-                    Bt.solve(bs, itmax=args.itmax, tol=args.tol)
-                ts = []
-                for _ in range(args.steps):
-                    xs, its, fl, sec = Bt.solve(bs, itmax=args.itmax, tol=args.tol)
-                    assert np.all(fl == 0)
-                    ts.append(sec * 1e3)
-                res[name] = {"ms": sum(ts) / len(ts), "setup_s": setup,
-                             "iters_min_max": [int(its.min()), int(its.max())]}
+            sh = ShardedBatch(As, world, rank, dist,
+                              prm=cb.params(precision=prec, ntv=1, nstep=15, step_size=4))
+            setup = time.perf_counter() - t0
+            for _ in range(args.warmup):
+                sh.solve_local(bs, itmax=args.itmax, tol=args.tol)
+            barrier()
+            ts = []
+            for _ in range(args.steps):
+                xs, its, fl, sec = sh.solve_local(bs, itmax=args.itmax, tol=args.tol)
+                assert np.all(np.asarray(fl) == 0)
+                ts.append(sec * 1e3)
+            barrier()
+            units, _ = sh.solve(bs, itmax=args.itmax, tol=args.tol, gather_x=False)
+            its_all = [units[p]["iters"] for p in range(len(As))]
+            res[name] = {"ms": slowest(sum(ts) / len(ts)), "setup_s": slowest(setup),
+                         "iters_min_max": [int(min(its_all)), int(max(its_all))],
+                         "problems_per_rank": [len(p) for p in sh.parts]}
+            sh.close()
         out["config"] = {"workload": "64 independent problems (Poisson / log-normal diffusion, "
                                      f"edge U[16,64]: {min(A.shape[0] for A in As)} to "
                                      f"{max(A.shape[0] for A in As)} rows), FSAI 15 steps x 4, "
-                                     "batch solve, PCG_CJ to 1e-8 each"}
+                                     "batch solve, PCG_CJ to 1e-8 each",
+                         "parallelism": f"problems split largest-first over {world} rank(s)"
+                         if world > 1 else "one GPU"}
     out["value"] = res["fp32"]["ms"]
     out["ms_per_step"] = res["fp32"]["ms"]
     out["fp64_ms"] = res["fp64"]["ms"]
     out["speedup_fp32_vs_fp64"] = res["fp64"]["ms"] / res["fp32"]["ms"]
     out["detail"] = res
-    print(json.dumps(out))
+    if rank == 0:
+        print(json.dumps(out))
+    if dist:
+        dist.destroy_process_group()
     return 0
 
 
@@ -643,7 +696,7 @@ def main():
     if args.workload in ("c1", "c5"):
         return run_c1_or_c5(args)
     if args.workload != "c2":
-        return run_block_or_batch(args)
+        return run_block_or_batch(args, world, rank)
     return run_product(args, world, rank, local)
 
 

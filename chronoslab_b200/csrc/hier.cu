@@ -303,8 +303,7 @@ void tune_store_locked(const TuneKey &k, int L) {
 void autotune_lanes(DMat &m, bool fp32, cudaStream_t st, int format) {
   if (m.nrows <= 0) return;
   // 'H': the hybrid CSR kernel (k_csrh_apply); the index width is part of the
-  // shape.  A cached value >= 100 means the sliced ELL form with lanes - 100
-  // for the CSR paths.
+  // shape.  A cached value is lanes + 100 * form (decoded at the end).
   const TuneKey key(m.idx16 ? 'h' : 'H', m.nrows, m.nnz, m.ncols, fp32);
   int L = -1;
   {
@@ -376,14 +375,17 @@ void autotune_lanes(DMat &m, bool fp32, cudaStream_t st, int format) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     tune_store_locked(key, L);
   }
-  if (format == 1 && L >= 100) L -= 100;
-  if (format == 2 && L < 100 && (double)m.nnz <= 16.0 * m.nrows) L += 100;
-  if (L >= 100 && build_sell(m, fp32, st)) {
+  // L = lanes + 100 * form: 0 row-grouped CSR, 1 sliced ELL
+  int form = L / 100;
+  const int lanes = L % 100;
+  if (format == 1) form = 0;
+  if (format == 2 && form == 0 && (double)m.nnz <= 16.0 * m.nrows) form = 1;
+  if (form == 1 && build_sell(m, fp32, st)) {
     m.use_sell = true;
-    m.lanes = L - 100;
+    m.lanes = lanes;
     set_long_rows(m, kSellLongRow, st);
   } else {
-    set_lanes(m, L >= 100 ? L - 100 : L, st);
+    set_lanes(m, lanes, st);
   }
 }
 

@@ -91,11 +91,14 @@ def test_adjoint_fd_diffusion64(lib):
     """C5 at full size: the FP64-hierarchy adjoint gradient (through the
     torch.autograd binding) against central finite differences, h = 1e-6
     along 32 seeded directions, relative error at most 1e-6.  The finite
-    differences evaluate J(log k +- h d) by GPU PCG solves to 1e-14 of the
-    perturbed operators, all preconditioned by the hierarchy of log k (the
-    operator argument of chronos_pcg): a hierarchy rebuilt for each
-    perturbation can coarsen differently, and the two solves' 1e-14-level
-    errors would then no longer cancel in the difference."""
+    differences need a forward map that is smooth at the 1e-14 level: J(log k
+    +- h d) comes from GPU PCG solves of the perturbed operators, all
+    preconditioned by the hierarchy of log k (the operator argument of
+    chronos_pcg) and all running exactly the iteration count that the solve
+    at log k needs for 1e-14 (each checked to reach it).  A hierarchy rebuilt
+    per perturbation, or a solve that stops one iteration earlier than its
+    partner, leaves 1e-14-level solve errors that no longer cancel in the
+    difference.  J(+) - J(-) is formed as 1/2 sum (u+ - u-)(u+ + u- - 2 u*)."""
     import scipy.sparse as sp
     rng = np.random.default_rng(7)
     shape = (64, 64, 64)
@@ -110,15 +113,17 @@ def test_adjoint_fd_diffusion64(lib):
         return sp.csr_matrix((v, pat.indices, pat.indptr), shape=(pat.n, pat.n))
 
     with cb.Hierarchy(assemble(logk), np.ones(pat.n), prm) as h0:
+        _, it0, _, flag0, _ = h0.pcg(b, itmax=4000, tol=1e-14)
+        assert flag0 == 0
+
         def forward(lk):
-            u, it, _, flag, _ = h0.pcg(b, itmax=4000, tol=1e-14, A=assemble(lk))
-            assert flag == 0
+            A = assemble(lk)
+            u, it, rv, _, _ = h0.pcg(b, itmax=it0, tol=0.0, A=A)
+            assert it == it0 and rv[-1] <= 2e-14
             return u
 
-        ustar = forward(logk_star)
-
-        def J(lk):
-            return 0.5 * float(np.sum((forward(lk) - ustar) ** 2))
+        ustar, _, _, fl, _ = h0.pcg(b, itmax=4000, tol=1e-14, A=assemble(logk_star))
+        assert fl == 0
 
         t = torch.from_numpy(logk).requires_grad_(True)
         u = solve(diffusion_values(t, pat), torch.from_numpy(b), pat.indptr, pat.indices,
@@ -129,6 +134,7 @@ def test_adjoint_fd_diffusion64(lib):
         errs = []
         for _ in range(32):
             d = rng.standard_normal(shape)
-            fd = (J(logk + hstep * d) - J(logk - hstep * d)) / (2 * hstep)
+            up, um = forward(logk + hstep * d), forward(logk - hstep * d)
+            fd = 0.5 * float(np.sum((up - um) * (up + um - 2.0 * ustar))) / (2 * hstep)
             errs.append(abs(fd - np.sum(g * d)) / max(abs(fd), 1e-300))
     assert max(errs) <= 1e-6, (max(errs), np.median(errs))

@@ -1,5 +1,7 @@
-"""Multi-rank plumbing of batched problems, on the CPU with gloo (world size 2):
-largest-first partition, no collective on the data path, a final gather."""
+"""Multi-rank plumbing of batched problems and blocks of right-hand sides, on
+the CPU with gloo (world size 2): largest-first partition of problems,
+contiguous split of columns, no collective on the data path, a final gather;
+the ranks run real AMG-PCG solves (the oracle's, on the CPU)."""
 import os
 import socket
 
@@ -9,7 +11,7 @@ import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from chronoslab_b200.sharding import gather_results, partition_largest_first
+from chronoslab_b200.sharding import partition_largest_first, split_columns
 
 
 def test_partition_balances_and_covers():
@@ -27,6 +29,12 @@ def test_partition_balances_and_covers():
             assert [w[i] for i in p] == sorted((w[i] for i in p), reverse=True)
 
 
+def test_split_columns():
+    assert split_columns(16, 1) == [(0, 16)]
+    assert split_columns(16, 3) == [(0, 6), (6, 11), (11, 16)]
+    assert split_columns(2, 4) == [(0, 1), (1, 2), (2, 2), (2, 2)]
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
@@ -35,34 +43,107 @@ def _free_port():
     return port
 
 
-def _worker(rank, world, port, weights, out_dir):
+class _CpuBatch:
+    """CPU stand-in for the GPU Batch in multi-rank tests: each problem solved
+    by the oracle's PCG_CJ (C, one thread) on the hierarchy built with the
+    reference's FSAI/BAMG C++."""
+
+    def __init__(self, As):
+        from oracle import amg_oracle as O
+        from oracle import c_oracle as CO
+        prm = O.default_params()
+        prm["tspace"]["ntv"] = 1
+        self.H = [CO.CHierarchy(CO.reference_hierarchy(A, None, prm), threads=1) for A in As]
+
+    def solve(self, bs, itmax=1000, tol=1e-8):
+        xs, its, fls = [], [], []
+        for H, b in zip(self.H, bs):
+            x, it, _, flag = H.pcg(b, itmax=itmax, tol=tol)
+            xs.append(x)
+            its.append(it)
+            fls.append(flag)
+        return xs, its, fls, 0.0
+
+
+def _problems():
+    from chronoslab_b200 import problems as PB
+    rng = np.random.default_rng(3)
+    As, bs = [], []
+    for p, e in enumerate(rng.integers(6, 13, 7)):
+        A = PB.poisson7(int(e)) if p % 2 == 0 else PB.diffusion7(int(e), seed=p)[0]
+        As.append(A)
+        bs.append(PB.uniform_rhs(A.shape[0], seed=50 + p))
+    return As, bs
+
+
+def _run_sharded(world, rank, dist):
+    from chronoslab_b200 import problems as PB
+    from chronoslab_b200.sharding import ShardedBatch, ShardedBlock
+    As, bs = _problems()
+    sb = ShardedBatch(As, world, rank, dist, make_batch=_CpuBatch)
+    res, times = sb.solve(bs)
+    A = PB.diffusion7(10, seed=9)[0]
+    B = PB.uniform_rhs(A.shape[0], seed=10, ncols=5)
+    blk = ShardedBlock(A, B.shape[1], world, rank, dist, make_block=_CpuBlockOf)
+    cres, ctimes = blk.solve(B)
+    return sb.parts, res, times, blk.ranges, cres
+
+
+class _CpuBlockOf(_CpuBatch):
+    """CPU stand-in for a Hierarchy's pcg_block: the columns one by one."""
+
+    def __init__(self, A):
+        super().__init__([A])
+
+    def pcg_block(self, B, itmax=1000, tol=1e-8):
+        H = self.H[0]
+        xs, its, fls = [], [], []
+        for j in range(B.shape[1]):
+            x, it, _, flag = H.pcg(B[:, j], itmax=itmax, tol=tol)
+            xs.append(x)
+            its.append(it)
+            fls.append(flag)
+        return np.stack(xs, axis=1), its, fls, 0.0
+
+
+def _worker(rank, world, port, out_dir):
+    import pickle
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
-        parts = partition_largest_first(weights, world)
-        # stand-in for each rank's batch solve: per-problem results
-        local = {i: {"iters": 3 * i + 1, "rank": rank} for i in parts[rank]}
-        merged = gather_results(local, world, dist)
-        np.save(os.path.join(out_dir, f"rank{rank}.npy"),
-                np.array([[i, merged[i]["iters"], merged[i]["rank"]] for i in sorted(merged)]))
+        out = _run_sharded(world, rank, dist)
+        with open(os.path.join(out_dir, f"rank{rank}.pkl"), "wb") as f:
+            pickle.dump(out, f)
     finally:
         dist.destroy_process_group()
 
 
-def test_gloo_two_ranks_partition_and_gather(tmp_path):
-    weights = [5, 100, 30, 30, 7, 64, 1, 12]
+def test_gloo_two_ranks_sharded_solves_match_one_rank(tmp_path):
+    """A batch of 7 independent problems and a block of 5 right-hand sides,
+    each solved for real (the oracle's AMG-PCG on the CPU), split over two
+    gloo ranks: every rank ends with every unit's result, each rank solved
+    only its share, and the merged results equal one rank's solving all."""
+    import pickle
+    from oracle import amg_oracle as O
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
     port = _free_port()
-    mp.start_processes(_worker, args=(2, port, weights, str(tmp_path)), nprocs=2,
-                       start_method="spawn", join=True)
-    r0 = np.load(tmp_path / "rank0.npy")
-    r1 = np.load(tmp_path / "rank1.npy")
-    assert np.array_equal(r0, r1)
-    assert list(r0[:, 0]) == list(range(len(weights)))
-    assert list(r0[:, 1]) == [3 * i + 1 for i in range(len(weights))]
-    parts = partition_largest_first(weights, 2)
-    for i, _, rank in r0:
-        assert i in parts[rank]
+    mp.start_processes(_worker, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn",
+                       join=True)
+    outs = [pickle.load(open(tmp_path / f"rank{r}.pkl", "rb")) for r in range(2)]
+    one = _run_sharded(1, 0, None)
+    parts, res1, _, ranges, cres1 = one
+    assert len(parts) == 1 and len(ranges) == 1
+    for r, (parts2, res2, times2, ranges2, cres2) in enumerate(outs):
+        assert sorted(times2) == [0, 1]
+        assert sorted(i for p in parts2 for i in p) == list(range(len(res1)))
+        assert ranges2 == [(0, 3), (3, 5)]
+        for units1, units2 in ((res1, res2), (cres1, cres2)):
+            assert sorted(units2) == sorted(units1)
+            for i in units1:
+                assert units2[i]["iters"] == units1[i]["iters"] and units2[i]["flag"] == 0
+                assert np.array_equal(units2[i]["x"], units1[i]["x"])
 
 
 def test_reference_arm_under_torchrun_two_ranks():
