@@ -212,6 +212,28 @@ def fsai_numeric(A, G, base=1, precision=CHRONOS_FP64, stream=None):
     return out, bool(ok.value)
 
 
+def fsai_numeric_batch(As, Gs, tile_set=-1):
+    """GPU FSAI numeric phase of several problems in one batched launch per
+    tile size (chronos_fsai_numeric_batch).  Returns (list of value arrays in
+    each G's order, list of is_posdef, the tile set run)."""
+    mats = [_csr(A) for A in As]
+    Gs = [sp.csr_matrix(G) for G in Gs]
+    npb = len(mats)
+    P = C.c_void_p * npb
+    gp = [np.ascontiguousarray(G.indptr, dtype=np.int32) for G in Gs]
+    gi = [np.ascontiguousarray(G.indices, dtype=np.int32) for G in Gs]
+    outs = [np.zeros(max(G.nnz, 1)) for G in Gs]
+    ok = np.zeros(npb, np.int32)
+    used = C.c_int(-1)
+    n = np.array([m[0] for m in mats], dtype=np.int32)
+    check(load().chronos_fsai_numeric_batch(
+        npb, _pi(n), P(*[m[1].ctypes.data for m in mats]), P(*[m[2].ctypes.data for m in mats]),
+        P(*[m[3].ctypes.data for m in mats]), P(*[a.ctypes.data for a in gp]),
+        P(*[a.ctypes.data for a in gi]), P(*[o.ctypes.data for o in outs]), _pi(ok), tile_set,
+        C.byref(used)))
+    return [o[:G.nnz] for o, G in zip(outs, Gs)], [bool(v) for v in ok], used.value
+
+
 def _stream(s):
     """cudaStream_t argument from None (the legacy default stream), an int
     handle or an object with a cuda_stream attribute (torch.cuda.Stream)."""
@@ -499,10 +521,11 @@ class Hierarchy:
         check(self._lib.chronos_hier_dump_ext_bin(self._h, level, w, os.fsencode(path)))
 
     def setup_times(self):
-        t = np.zeros(8)
-        check(self._lib.chronos_hier_setup_times(self._h, _pd(t)))
+        """Setup phases in seconds; the phases other than "total" sum to it."""
         keys = ["fsai_pattern", "fsai_numeric", "omega", "coarsen", "prolong", "galerkin",
-                "coarse_factor", "total"]
+                "coarse_factor", "total", "uploads", "layouts", "autotune", "other"]
+        t = np.zeros(len(keys))
+        check(self._lib.chronos_hier_setup_phases(self._h, _pd(t), len(keys)))
         return dict(zip(keys, t.tolist()))
 
     def profile(self, reps=20):
@@ -672,6 +695,14 @@ class Batch:
         nl, n0 = C.c_int(), C.c_int()
         check(self._lib.chronos_batch_info(self._h, p, C.byref(nl), C.byref(n0)))
         return nl.value
+
+    def setup_times(self):
+        """Hierarchy.setup_times' phases summed over the problems (thread time)."""
+        keys = ["fsai_pattern", "fsai_numeric", "omega", "coarsen", "prolong", "galerkin",
+                "coarse_factor", "total", "uploads", "layouts", "autotune", "other"]
+        t = np.zeros(len(keys))
+        check(self._lib.chronos_batch_setup_phases(self._h, _pd(t), len(keys)))
+        return dict(zip(keys, t.tolist()))
 
     def solve(self, bs, itmax=1000, tol=1e-8):
         """Returns (xs, iters, flags, seconds)."""

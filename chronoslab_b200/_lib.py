@@ -107,6 +107,7 @@ SIGNATURES = {
                              _pi, _pd, _pi],
     "chronos_fsai_numeric": [_i, _i, _pi64, _pi, _pd, _pi64, _pi, _i, _vp, _pi, _vp],
     "chronos_fsai_numeric_noalloc": [_i, _vp, _vp, _vp, _vp, _vp, _vp, _pi, _vp],
+    "chronos_fsai_numeric_batch": [_i, _pi, _pp, _pp, _pp, _pp, _pp, _pp, _pi, _i, _pi],
     "chronos_galerkin_compute": [_i, _i, _pi, _pi, _pd, _pi, _pi, _pd, _pi64, _pp],
     "chronos_galerkin_fetch": [_vp, _pi, _pi, _pd],
     "chronos_galerkin_free": [_vp],
@@ -123,6 +124,7 @@ SIGNATURES = {
     "chronos_hier_level_info": [_vp, _i, C.POINTER(chronos_level_info)],
     "chronos_hier_export": [_vp, _i, C.c_char, _pi, _pi, _pi64, _pi, _pi, _pd],
     "chronos_hier_setup_times": [_vp, _pd],
+    "chronos_hier_setup_phases": [_vp, _pd, _i],
     "chronos_hier_profile": [_vp, _i, C.POINTER(chronos_profile)],
     "chronos_diag_fix": [_i, _pi, _pi, _pd],
     "chronos_vcycle": [_vp, _pd, _pd, _i, _vp],
@@ -132,6 +134,7 @@ SIGNATURES = {
     "chronos_batch_setup": [C.POINTER(chronos_params), _i, _pi, _pp, _pp, _pp, _pp],
     "chronos_batch_solve": [_vp, _pp, _pp, _i, _d, _pi, _pi, _pd],
     "chronos_batch_info": [_vp, _i, _pi, _pi],
+    "chronos_batch_setup_phases": [_vp, _pd, _i],
     "chronos_batch_free": [_vp],
     "chronos_sqmr":[_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _pi, _pd, _pi],
     "chronos_gmres": [_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _i, _pi, _pi, _pd, _pi, _pd, _pi],

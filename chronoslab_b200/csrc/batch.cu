@@ -6,6 +6,7 @@
 // stream with no host synchronisation in between, largest problems first.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <exception>
 #include <memory>
@@ -19,6 +20,10 @@
 #include "group.h"
 
 namespace chronos {
+
+static double now_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 
 struct Batch {
   std::vector<std::unique_ptr<Hier>> h;
@@ -65,51 +70,99 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
     for (int p = 0; p < nprob; ++p)
       CHRONOS_REQUIRE(n[p] > 0 && iat_h[p] && iat_h[p][0] == 0, CHRONOS_EINVAL,
                       "problem " + std::to_string(p) + ": 0-based CSR expected");
-    // The problems' hierarchies are independent: a few host threads build
-    // them at once (each on its own stream, with its share of the OpenMP
-    // threads), so one problem's host phases overlap another's GPU phases.
-    // Every hierarchy is what a single chronos_amg_setup builds; lane counts
-    // are tuned afterwards on a quiet GPU: the grouped solve's stacked
-    // operators, or each problem's own for the per-problem path.
+    // The problems' hierarchies are built level-synchronously: every round
+    // begins the next level of each unfinished problem (operator upload, FSAI
+    // pattern on the host) on a few host threads at once, each problem on its
+    // own stream with its share of the OpenMP threads; then the FSAI numeric
+    // phase of all those levels runs as one batched launch per tile size
+    // (fsai_numeric_batched, bucket edges tuned per batch shape); then the
+    // levels are ended (omega, coarsening, prolongation, Galerkin) on the
+    // host threads again.  Every hierarchy is what a single
+    // chronos_amg_setup builds; lane counts are tuned afterwards on a quiet
+    // GPU: the grouped solve's stacked operators, or each problem's own for
+    // the per-problem path.
     bt->b.h.resize(nprob);
     const int hw = std::max(1, (int)std::thread::hardware_concurrency());
     const int nworkers = std::max(1, std::min({nprob, 8, std::max(1, hw / 2)}));
     int dev = 0;
     CHRONOS_CUDA(cudaGetDevice(&dev));
-    std::atomic<int> next{0};
-    std::mutex emu;
-    std::exception_ptr err;
-    auto worker = [&] {
-      const int omp_saved = omp_get_max_threads();   // the calling thread gets it back
-      try {
-        CHRONOS_CUDA(cudaSetDevice(dev));
-        omp_set_num_threads(std::max(1, hw / nworkers));
-        for (int p = next++; p < nprob; p = next++) {
-          {
-            std::lock_guard<std::mutex> lk(emu);
-            if (err) break;
+    // runs f(p) for every p of `items` on the worker threads; the first error is rethrown
+    auto parallel = [&](const std::vector<int> &items, const auto &f) {
+      std::atomic<size_t> next{0};
+      std::mutex emu;
+      std::exception_ptr err;
+      auto worker = [&] {
+        const int omp_saved = omp_get_max_threads();   // the calling thread gets it back
+        try {
+          CHRONOS_CUDA(cudaSetDevice(dev));
+          omp_set_num_threads(std::max(1, hw / nworkers));
+          for (size_t k = next++; k < items.size(); k = next++) {
+            {
+              std::lock_guard<std::mutex> lk(emu);
+              if (err) break;
+            }
+            f(items[k]);
           }
-          HostCSR A;
-          A.nrows = A.ncols = n[p];
-          A.rp.assign(iat_h[p], iat_h[p] + n[p] + 1);
-          A.ci.assign(ja_h[p], ja_h[p] + A.rp[n[p]]);
-          A.v.assign(val_h[p], val_h[p] + A.rp[n[p]]);
-          // scalar problems: the constant vector as TV0 (as aspAMG_main.m:92-95
-          // for a .mat without a test space), padded with random columns if ntv > 1
-          std::vector<double> ones(n[p], 1.0);
-          bt->b.h[p] = build_hierarchy(*prm, A, 1, ones.data(), false);
+        } catch (...) {
+          std::lock_guard<std::mutex> lk(emu);
+          if (!err) err = std::current_exception();
         }
-      } catch (...) {
-        std::lock_guard<std::mutex> lk(emu);
-        if (!err) err = std::current_exception();
-      }
-      omp_set_num_threads(omp_saved);
+        omp_set_num_threads(omp_saved);
+      };
+      std::vector<std::thread> pool;
+      const int nw = std::min<int>(nworkers, (int)items.size());
+      for (int w = 1; w < nw; ++w) pool.emplace_back(worker);
+      worker();
+      for (auto &t : pool) t.join();
+      if (err) std::rethrow_exception(err);
     };
-    std::vector<std::thread> pool;
-    for (int w = 1; w < nworkers; ++w) pool.emplace_back(worker);
-    worker();
-    for (auto &t : pool) t.join();
-    if (err) std::rethrow_exception(err);
+    std::vector<std::unique_ptr<HierBuilder>> builders(nprob);
+    std::vector<int> active(nprob);
+    std::iota(active.begin(), active.end(), 0);
+    parallel(active, [&](int p) {
+      HostCSR A;
+      A.nrows = A.ncols = n[p];
+      A.rp.assign(iat_h[p], iat_h[p] + n[p] + 1);
+      A.ci.assign(ja_h[p], ja_h[p] + A.rp[n[p]]);
+      A.v.assign(val_h[p], val_h[p] + A.rp[n[p]]);
+      // scalar problems: the constant vector as TV0 (as aspAMG_main.m:92-95
+      // for a .mat without a test space), padded with random columns if ntv > 1
+      std::vector<double> ones(n[p], 1.0);
+      builders[p] = std::make_unique<HierBuilder>(*prm, A, 1, ones.data());
+    });
+    cudaStream_t bst;
+    CHRONOS_CUDA(cudaStreamCreateWithFlags(&bst, cudaStreamNonBlocking));
+    try {
+      std::vector<char> more(nprob, 0);
+      while (!active.empty()) {
+        parallel(active, [&](int p) {
+          more[p] = builders[p]->begin_level() ? 1 : 0;
+          if (!more[p]) bt->b.h[p] = builders[p]->finish(false);
+        });
+        std::vector<int> next_active;
+        std::vector<FsaiJob> jobs;
+        for (int p : active)
+          if (more[p]) {
+            next_active.push_back(p);
+            jobs.push_back(builders[p]->fsai_job());
+          }
+        if (next_active.empty()) break;
+        const double t0 = now_seconds();
+        const std::vector<int> fl = fsai_numeric_batched(jobs, bst);
+        const double share = (now_seconds() - t0) / (double)jobs.size();
+        std::vector<int> flag_of(nprob, 0);
+        for (size_t k = 0; k < next_active.size(); ++k) {
+          flag_of[next_active[k]] = fl[k];
+          builders[next_active[k]]->add_numeric_time(share);
+        }
+        parallel(next_active, [&](int p) { builders[p]->end_level(flag_of[p]); });
+        active.swap(next_active);
+      }
+    } catch (...) {
+      cudaStreamDestroy(bst);
+      throw;
+    }
+    cudaStreamDestroy(bst);
     bt->b.order.resize(nprob);
     std::iota(bt->b.order.begin(), bt->b.order.end(), 0);
     std::stable_sort(bt->b.order.begin(), bt->b.order.end(), [&](int a, int c) {
@@ -187,6 +240,15 @@ int chronos_batch_solve(chronos_batch *bt, const double *const *b_h, double *con
     for (auto &e : done) cudaEventDestroy(e);
     cudaStreamDestroy(fork);
     if (seconds) *seconds = ms * 1e-3;
+  });
+}
+
+int chronos_batch_setup_phases(const chronos_batch *bt, double *t, int n) {
+  return batch_guard([&] {
+    CHRONOS_REQUIRE(bt && t && n >= 0, CHRONOS_EINVAL, "bad argument");
+    for (int i = 0; i < n; ++i) t[i] = 0.0;
+    for (const auto &h : bt->b.h)
+      for (int i = 0; i < n && i < (int)h->times.size(); ++i) t[i] += h->times[i];
   });
 }
 

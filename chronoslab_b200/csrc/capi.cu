@@ -289,10 +289,6 @@ int chronos_coarsen_device(const chronos_params *prm, int n, const int *iat_h, c
   return guard([&] {
     CallRange range_("chronos_coarsen_device");
     CHRONOS_REQUIRE(prm && fcnode_h && nc && n > 0, CHRONOS_EINVAL, "bad argument");
-    std::string t(prm->SoC_type);
-    for (auto &c : t) c = (char)toupper(c);
-    CHRONOS_REQUIRE(t == "DOM", CHRONOS_ENOTSUP,
-                    "the GPU coarsening computes DOM strength only (SoC type " + t + ")");
     HostCSR A = from_csr0(n, n, iat_h, ja_h, val_h);
     validate_csr(A);
     MT19937 rng((uint32_t)(prm->seed ? prm->seed : 5489));
@@ -304,7 +300,7 @@ int chronos_coarsen_device(const chronos_params *prm, int n, const int *iat_h, c
       upload_csr(A, d, false, st);
       HostCSR Sm;
       std::vector<int> fc;
-      coarsen_dom_device(n, d.rp, d.ci, d.v64, prm->soc_tau, rng, Sm, fc, nc, st);
+      coarsen_device(n, d.rp, d.ci, d.v64, prm->SoC_type, prm->soc_tau, rng, Sm, fc, nc, st);
       CHRONOS_CUDA(cudaStreamSynchronize(st));
       std::memcpy(fcnode_h, fc.data(), sizeof(int) * n);
       if (S) {
@@ -448,6 +444,58 @@ int chronos_fsai_numeric(int n, int base, const int64_t *iat_A_h, const int *ja_
       for (size_t k = 0; k < gval.size(); ++k) o[k] = (float)gval[k];
     }
     *is_posdef = fl == 0 ? 1 : 0;
+  });
+}
+
+int chronos_fsai_numeric_batch(int nprob, const int *n, const int *const *iat_A_h,
+                               const int *const *ja_A_h, const double *const *val_A_h,
+                               const int *const *iat_G_h, const int *const *ja_G_h,
+                               double *const *val_G_h, int *is_posdef, int tile_set,
+                               int *tile_set_used) {
+  return guard([&] {
+    CallRange range_("chronos_fsai_numeric_batch");
+    CHRONOS_REQUIRE(nprob > 0 && n && iat_A_h && ja_A_h && val_A_h && iat_G_h && ja_G_h &&
+                        val_G_h && is_posdef, CHRONOS_EINVAL, "null argument");
+    CHRONOS_REQUIRE(tile_set >= -1 && tile_set < fsai_bucket_set_count(), CHRONOS_EINVAL,
+                    "tile_set must be -1 (tuned) or a candidate index");
+    ScopedStream s;
+    std::vector<DMat> dA(nprob), dG(nprob);
+    std::vector<std::vector<int>> rowlen(nprob);
+    std::vector<FsaiJob> jobs(nprob);
+    for (int p = 0; p < nprob; ++p) {
+      const HostCSR A = from_csr0(n[p], n[p], iat_A_h[p], ja_A_h[p], val_A_h[p]);
+      HostCSR G;
+      G.nrows = G.ncols = n[p];
+      G.rp.assign(iat_G_h[p], iat_G_h[p] + n[p] + 1);
+      CHRONOS_REQUIRE(G.rp[0] == 0, CHRONOS_EINVAL, "0-based G pattern expected");
+      rowlen[p].resize(n[p]);
+      for (int i = 0; i < n[p]; ++i) {
+        CHRONOS_REQUIRE(G.rp[i + 1] > G.rp[i], CHRONOS_EINVAL, "a G row without entries");
+        rowlen[p][i] = (int)(G.rp[i + 1] - G.rp[i]);
+      }
+      G.ci.assign(ja_G_h[p], ja_G_h[p] + G.rp[n[p]]);
+      G.v.assign(G.ci.size(), 0.0);
+      for (int i = 0; i < n[p]; ++i) {
+        CHRONOS_REQUIRE(G.ci[G.rp[i + 1] - 1] == i, CHRONOS_EINVAL,
+                        "FSAI pattern rows must end with their diagonal");
+        for (int64_t k = G.rp[i]; k + 1 < G.rp[i + 1]; ++k)
+          CHRONOS_REQUIRE(G.ci[k] >= 0 && G.ci[k] < i && (k == G.rp[i] || G.ci[k] > G.ci[k - 1]),
+                          CHRONOS_EINVAL,
+                          "FSAI pattern rows must list strictly-lower columns ascending");
+      }
+      upload_csr(A, dA[p], false, s.st);
+      upload_csr(G, dG[p], false, s.st);
+      jobs[p] = FsaiJob{n[p], dA[p].rp.get(), dA[p].ci.get(), dA[p].v64.get(), dG[p].rp.get(),
+                        dG[p].ci.get(), dG[p].v64.get(), &rowlen[p]};
+    }
+    int used = -1;
+    const std::vector<int> fl = fsai_numeric_batched(jobs, s.st, &used, tile_set);
+    for (int p = 0; p < nprob; ++p) {
+      dG[p].v64.download(val_G_h[p], dG[p].nnz, s.st);
+      is_posdef[p] = fl[p] == 0 ? 1 : 0;
+    }
+    CHRONOS_CUDA(cudaStreamSynchronize(s.st));
+    if (tile_set_used) *tile_set_used = used;
   });
 }
 
@@ -700,6 +748,13 @@ int chronos_hier_export(const chronos_hier *h, int level, char which, int *nrows
     m->ci.download(ja_h, m->nnz, h->h->st);
     m->v64.download(val_h, m->nnz, h->h->st);
     CHRONOS_CUDA(cudaStreamSynchronize(h->h->st));
+  });
+}
+
+int chronos_hier_setup_phases(const chronos_hier *h, double *t, int n) {
+  return guard([&] {
+    CHRONOS_REQUIRE(h && t && n >= 0, CHRONOS_EINVAL, "bad argument");
+    for (int i = 0; i < n && i < (int)h->h->times.size(); ++i) t[i] = h->h->times[i];
   });
 }
 

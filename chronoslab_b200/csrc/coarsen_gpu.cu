@@ -1,11 +1,19 @@
-// Strength of connection (DOM) and the PMIS C/F splitting on the GPU.
+// Strength of connection (DOM or CLA) and the PMIS C/F splitting on the GPU.
 //
-// The same outputs as soc_matrix("DOM") and pmis_split on the host
+// The same outputs as soc_matrix and pmis_split on the host
 // (host/coarsen.cpp), bit for bit:
 //  * cpt_SoC_dom.m:26-47 — s_ij = |a_ij| / sqrt(a_ii a_jj), entry (i, j) of S
 //    when a_ij != 0 and s_ij > tau.  A warp per row compacts the strong
 //    entries with ballots, so S keeps A's column order within each row;
 //    the quotient and square root are IEEE-rounded as on the host.
+//  * cpt_SoC_cla.m:109-159 — column statistics of the off-diagonal nonzeros
+//    (the most negative value, counting the column's implicit zeros, and the
+//    largest magnitude; a zero statistic reads as 1), then s_ij =
+//    |a_ij| / max(maxabs_i, maxabs_j) when no off-diagonal entry is
+//    negative, else a_ij / max(min_i, min_j); off-diagonal (i, j) is strong
+//    when s_ij > tau, and every diagonal entry is in S (S + speye).  The
+//    column statistics are exact: atomic max / min on integer keys that order
+//    as the doubles do.
 //  * mark_isolated_nodes.m — columns of A with a single nonzero are
 //    Dirichlet nodes (fine from the start).
 //  * cpt_PMIS.m — node weight = strong connections in the node's column of S
@@ -25,6 +33,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <string>
 #include <vector>
 
 #include "host/host.h"
@@ -64,22 +73,93 @@ __device__ __forceinline__ bool dom_strong(double a, double di, double dj, doubl
   return s > tau;
 }
 
+// Entry (i, j, a) of S, cpt_SoC_dom.m.
+struct DomStrength {
+  const double *d;
+  double tau;
+  __device__ bool operator()(int i, int j, double a) const { return dom_strong(a, d[i], d[j], tau); }
+};
+
+// Entry (i, j, a) of S + speye, cpt_SoC_cla.m (column statistics finished).
+struct ClaStrength {
+  const double *maxabs, *minc;
+  const int *any_negative;
+  double tau;
+  __device__ bool operator()(int i, int j, double a) const {
+    if (i == j) return true;
+    if (a == 0.0) return false;
+    const double s = *any_negative ? a / fmax(minc[i], minc[j])
+                                   : fabs(a) / fmax(maxabs[i], maxabs[j]);
+    return s > tau;
+  }
+};
+
+// Integer keys that order as the doubles they encode (no NaN): the bits of
+// a non-negative double, the complement of a negative one's, top bit set for
+// the non-negative half.
+__device__ __forceinline__ unsigned long long order_key(double x) {
+  const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double order_value(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+
+// cpt_SoC_cla.m's column statistics over the off-diagonal nonzeros of A:
+// kmin[j] = key of min(0, smallest a_ij) (the column's implicit zeros make 0
+// a candidate), kmax[j] = bits of the largest |a_ij|; any_negative set when
+// some off-diagonal entry is negative.
+__global__ void k_cla_colstats(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                               const double *__restrict__ v, unsigned long long *__restrict__ kmin,
+                               unsigned long long *__restrict__ kmax, int *__restrict__ any_negative) {
+  const int lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw)
+    for (int k = rp[i] + lane; k < rp[i + 1]; k += 32) {
+      const int j = ci[k];
+      const double a = v[k];
+      if (j == i || a == 0.0) continue;
+      if (a < 0.0) {
+        atomicMin(kmin + j, order_key(a));
+        atomicExch(any_negative, 1);
+      }
+      atomicMax(kmax + j, (unsigned long long)__double_as_longlong(fabs(a)));
+    }
+}
+
+// Statistics to values; a zero one reads as 1 (cpt_SoC_cla.m).
+__global__ void k_cla_finish(int n, const unsigned long long *__restrict__ kmin,
+                             const unsigned long long *__restrict__ kmax, double *__restrict__ minc,
+                             double *__restrict__ maxabs) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const double mn = order_value(kmin[j]);
+    const double mx = __longlong_as_double((long long)kmax[j]);
+    minc[j] = mn == 0.0 ? 1.0 : mn;
+    maxabs[j] = mx == 0.0 ? 1.0 : mx;
+  }
+}
+
+__global__ void k_fill_u64(int n, unsigned long long *p, unsigned long long val) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) p[j] = val;
+}
+
 // Per row: strong entries (S), strong off-diagonal entries (S without its
 // diagonal), and the nonzeros of each column of A.
-__global__ void k_dom_count(int n, const int *__restrict__ rp, const int *__restrict__ ci,
-                            const double *__restrict__ v, const double *__restrict__ d, double tau,
-                            int *__restrict__ cnt_s, int *__restrict__ cnt_o,
-                            int *__restrict__ colcnt) {
+template <typename Strong>
+__global__ void k_strength_count(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                 const double *__restrict__ v, Strong strong,
+                                 int *__restrict__ cnt_s, int *__restrict__ cnt_o,
+                                 int *__restrict__ colcnt) {
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
     int cs = 0, co = 0;
-    const double di = d[i];
     for (int k = rp[i] + lane; k < rp[i + 1]; k += 32) {
       const int j = ci[k];
       const double a = v[k];
       if (a != 0.0) atomicAdd(colcnt + j, 1);
-      if (dom_strong(a, di, d[j], tau)) {
+      if (strong(i, j, a)) {
         ++cs;
         co += (j != i);
       }
@@ -97,16 +177,16 @@ __global__ void k_dom_count(int n, const int *__restrict__ rp, const int *__rest
 
 // Ordered compaction of the strong entries of each row into S and of the
 // strong off-diagonal ones into So.
-__global__ void k_dom_fill(int n, const int *__restrict__ rp, const int *__restrict__ ci,
-                           const double *__restrict__ v, const double *__restrict__ d, double tau,
-                           const int *__restrict__ srp, int *__restrict__ sci,
-                           const int *__restrict__ orp, int *__restrict__ oci) {
+template <typename Strong>
+__global__ void k_strength_fill(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                const double *__restrict__ v, Strong pred,
+                                const int *__restrict__ srp, int *__restrict__ sci,
+                                const int *__restrict__ orp, int *__restrict__ oci) {
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
   const int nw = (gridDim.x * blockDim.x) >> 5;
   for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nw) {
     int ps = srp[i], po = orp[i];
-    const double di = d[i];
     const int e = rp[i + 1];
     for (int k0 = rp[i]; k0 < e; k0 += 32) {
       const int k = k0 + lane;
@@ -114,7 +194,7 @@ __global__ void k_dom_fill(int n, const int *__restrict__ rp, const int *__restr
       int j = 0;
       if (k < e) {
         j = ci[k];
-        strong = dom_strong(v[k], di, d[j], tau);
+        strong = pred(i, j, v[k]);
       }
       const bool off = strong && j != i;
       const unsigned bs = __ballot_sync(0xffffffffu, strong);
@@ -223,10 +303,15 @@ void exclusive_scan(const int *in, int *out, int n, cudaStream_t st) {
 
 }  // namespace
 
-void coarsen_dom_device(int n, const int *rp, const int *ci, const double *v, double tau,
-                        MT19937 &rng, HostCSR &S, std::vector<int> &fcnode, int *nc_out,
-                        cudaStream_t st) {
-  CHRONOS_REQUIRE(tau >= 0, CHRONOS_ENOTSUP, "DOM strength with tau < 0 is outside this path");
+void coarsen_device(int n, const int *rp, const int *ci, const double *v, const char *soc_type,
+                    double tau, MT19937 &rng, HostCSR &S, std::vector<int> &fcnode, int *nc_out,
+                    cudaStream_t st) {
+  std::string t(soc_type);
+  for (auto &c : t) c = (char)toupper(c);
+  CHRONOS_REQUIRE(t == "DOM" || t == "CLA", CHRONOS_ENOTSUP,
+                  "the GPU coarsening computes DOM or CLA strength (SoC type " + t + ")");
+  CHRONOS_REQUIRE(tau >= 0, CHRONOS_ENOTSUP, t + " strength with tau < 0 is outside this path");
+  const bool cla = t == "CLA";
   const int g = warp_grid(n);
   const int ge = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, kCoarsenThreads),
                                                              (int64_t)num_sms() * 16));
@@ -236,10 +321,43 @@ void coarsen_dom_device(int n, const int *rp, const int *ci, const double *v, do
   colcnt.zero(st);
   k_row_diag<<<g, kCoarsenThreads, 0, st>>>(n, rp, ci, v, d.get());
   CHRONOS_CHECK_LAUNCH();
+  DBuf<double> minc, maxabs;
+  DBuf<int> anyneg;
+  if (cla) {
+    // S + speye keeps every diagonal entry: rows must store a nonzero one
+    // (an SPD operator always does; the host inserts a missing one)
+    std::vector<double> dh(n);
+    d.download(dh.data(), n, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i)
+      CHRONOS_REQUIRE(dh[i] != 0.0, CHRONOS_ENOTSUP,
+                      "CLA strength on the GPU needs a stored nonzero diagonal in every row");
+    DBuf<unsigned long long> kmin(n), kmax(n);
+    minc.alloc(n);
+    maxabs.alloc(n);
+    anyneg.alloc(1);
+    anyneg.zero(st);
+    kmax.zero(st);                                   // +0.0
+    k_fill_u64<<<ge, kCoarsenThreads, 0, st>>>(n, kmin.get(), 0x8000000000000000ull);   // key(+0.0)
+    CHRONOS_CHECK_LAUNCH();
+    k_cla_colstats<<<g, kCoarsenThreads, 0, st>>>(n, rp, ci, v, kmin.get(), kmax.get(),
+                                                  anyneg.get());
+    CHRONOS_CHECK_LAUNCH();
+    k_cla_finish<<<ge, kCoarsenThreads, 0, st>>>(n, kmin.get(), kmax.get(), minc.get(),
+                                                 maxabs.get());
+    CHRONOS_CHECK_LAUNCH();
+    CHRONOS_CUDA(cudaStreamSynchronize(st));         // kmin, kmax released here
+  }
+  const DomStrength dom{d.get(), tau};
+  const ClaStrength clas{maxabs.get(), minc.get(), anyneg.get(), tau};
   CHRONOS_CUDA(cudaMemsetAsync(cnt_s.get() + n, 0, sizeof(int), st));
   CHRONOS_CUDA(cudaMemsetAsync(cnt_o.get() + n, 0, sizeof(int), st));
-  k_dom_count<<<g, kCoarsenThreads, 0, st>>>(n, rp, ci, v, d.get(), tau, cnt_s.get(), cnt_o.get(),
-                                             colcnt.get());
+  if (cla)
+    k_strength_count<<<g, kCoarsenThreads, 0, st>>>(n, rp, ci, v, clas, cnt_s.get(), cnt_o.get(),
+                                                    colcnt.get());
+  else
+    k_strength_count<<<g, kCoarsenThreads, 0, st>>>(n, rp, ci, v, dom, cnt_s.get(), cnt_o.get(),
+                                                    colcnt.get());
   CHRONOS_CHECK_LAUNCH();
   exclusive_scan(cnt_s.get(), srp.get(), n + 1, st);
   exclusive_scan(cnt_o.get(), orp.get(), n + 1, st);
@@ -248,8 +366,12 @@ void coarsen_dom_device(int n, const int *rp, const int *ci, const double *v, do
   CHRONOS_CUDA(cudaMemcpyAsync(&nnz_o, orp.get() + n, sizeof(int), cudaMemcpyDeviceToHost, st));
   CHRONOS_CUDA(cudaStreamSynchronize(st));
   DBuf<int> sci(std::max(nnz_s, 1)), oci(std::max(nnz_o, 1)), tci(std::max(nnz_o, 1));
-  k_dom_fill<<<g, kCoarsenThreads, 0, st>>>(n, rp, ci, v, d.get(), tau, srp.get(), sci.get(),
-                                            orp.get(), oci.get());
+  if (cla)
+    k_strength_fill<<<g, kCoarsenThreads, 0, st>>>(n, rp, ci, v, clas, srp.get(), sci.get(),
+                                                   orp.get(), oci.get());
+  else
+    k_strength_fill<<<g, kCoarsenThreads, 0, st>>>(n, rp, ci, v, dom, srp.get(), sci.get(),
+                                                   orp.get(), oci.get());
   CHRONOS_CHECK_LAUNCH();
   // S' of the off-diagonal part: column counts, row pointers, unordered fill
   DBuf<int> tcnt((size_t)n + 1), trp((size_t)n + 1), cursor(n);

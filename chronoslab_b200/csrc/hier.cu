@@ -825,17 +825,20 @@ bool gpu_coarsening(const char *soc_type) {
   }();
   std::string t(soc_type);
   for (auto &c : t) c = (char)toupper(c);
-  return on && t == "DOM";
+  return on && (t == "DOM" || t == "CLA");
 }
 
-std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A0, int ntv0,
-                                      const double *TV0, bool tune, const ProlongFn *prolong) {
-  const double t_start = now_s();
+HierBuilder::HierBuilder(const chronos_params &prm_in, const HostCSR &A0, int ntv0,
+                         const double *TV0, const ProlongFn *prolong)
+    : prm_(prm_in), prolong_(prolong), t_start_(now_s()),
+      rng_((uint32_t)(prm_in.seed ? prm_in.seed : 5489)) {
+  const chronos_params &prm = prm_;
   validate_csr(A0);
   std::string smeth(prm.smoother_method), tmeth(prm.tspace_method), ptype(prm.proltype),
       pemin(prm.prol_emin);
   for (auto *s : {&smeth, &tmeth, &ptype, &pemin})
     for (auto &c : *s) c = (char)toupper(c);
+  pemin_ = pemin;
   CHRONOS_REQUIRE(smeth == "AFSAI_SYM", CHRONOS_ENOTSUP, "smoother " + smeth + " is outside this path");
   if (!prolong) {   // with a caller-supplied P these choices are the caller's
     CHRONOS_REQUIRE(tmeth == "NONE", CHRONOS_ENOTSUP, "test-space method " + tmeth + " is outside this path");
@@ -853,212 +856,282 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
   CHRONOS_REQUIRE(prm.precision == CHRONOS_FP32 || prm.precision == CHRONOS_FP64, CHRONOS_EINVAL,
                   "precision must be CHRONOS_FP32 or CHRONOS_FP64");
 
-  auto h = std::make_unique<Hier>();
-  h->prm = prm;
-  h->precision = prm.precision;
-  const bool fp32 = prm.precision == CHRONOS_FP32;
-  CHRONOS_CUDA(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
-  cudaStream_t st = h->st;
-  const int nthreads = prm.nthread > 0 ? prm.nthread : 0;
-  int nth = nthreads;
-  if (nth <= 0) {
+  h_ = std::make_unique<Hier>();
+  h_->prm = prm;
+  h_->precision = prm.precision;
+  fp32_ = prm.precision == CHRONOS_FP32;
+  CHRONOS_CUDA(cudaStreamCreateWithFlags(&h_->st, cudaStreamNonBlocking));
+  nth_ = prm.nthread > 0 ? prm.nthread : 0;
+  if (nth_ <= 0) {
 #ifdef _OPENMP
-    nth = omp_get_max_threads();
+    nth_ = omp_get_max_threads();
 #else
-    nth = 1;
+    nth_ = 1;
 #endif
   }
-
-  MT19937 rng((uint32_t)(prm.seed ? prm.seed : 5489));
-  int n = A0.nrows;
-  const int ntv = prm.ntv;
-  std::vector<double> TV;                                  // column-major n x ntv
+  const int n = A0.nrows;
+  ntv_ = prm.ntv;
   if (!prolong) {
-    TV.assign((size_t)n * ntv, 0.0);
-    const int ncopy = std::min(std::max(ntv0, 0), ntv);
+    TV_.assign((size_t)n * ntv_, 0.0);                    // column-major n x ntv
+    const int ncopy = std::min(std::max(ntv0, 0), ntv_);
     for (int j = 0; j < ncopy; ++j)
-      std::copy(TV0 + (size_t)j * n, TV0 + (size_t)(j + 1) * n, TV.begin() + (size_t)j * n);
-    for (int j = std::max(ntv0, 0); j < ntv; ++j)         // rand(n, ntv-ntv0), column-major
-      for (int i = 0; i < n; ++i) TV[(size_t)j * n + i] = rng.next_res53();
-    qr_orthonormalize(n, ntv, TV.data());
+      std::copy(TV0 + (size_t)j * n, TV0 + (size_t)(j + 1) * n, TV_.begin() + (size_t)j * n);
+    for (int j = std::max(ntv0, 0); j < ntv_; ++j)        // rand(n, ntv-ntv0), column-major
+      for (int i = 0; i < n; ++i) TV_[(size_t)j * n + i] = rng_.next_res53();
+    SetupPhase ph3("chronos setup: coarsening", &h_->times[3]);
+    qr_orthonormalize(n, ntv_, TV_.data());
   }
+  Al_ = A0;
+}
 
-  HostCSR Al = A0;
-  std::array<double, 8> &T = h->times;
-  for (int level = 1;; ++level) {
-    h->levels.emplace_back();
-    Level &L = h->levels.back();
-    n = Al.nrows;
-    L.n = n;
-    upload_csr(Al, L.A, fp32, st);
-    if (prm.use_bsr) attach_sell3(Al, L.A, fp32, st);
-    if (n <= prm.maxCoarseSZ || level >= prm.nLevMax) {
-      SetupPhase ph6("chronos setup: coarse factor", &T[6]);
-      CHRONOS_REQUIRE(n <= 8192, CHRONOS_ENOTSUP, "coarsest level larger than 8192 rows");
-      std::vector<double> dense((size_t)n * n, 0.0);
-      for (int i = 0; i < n; ++i)
-        for (int64_t k = Al.rp[i]; k < Al.rp[i + 1]; ++k) dense[(size_t)Al.ci[k] * n + i] = Al.v[k];
-      DBuf<double> Ld;
-      Ld.upload(dense, st);
-      const int info = dense_cholesky_device(n, Ld.get(), st);
-      CHRONOS_REQUIRE(info == 0, CHRONOS_ENOTSPD,
-                      "coarsest-level Cholesky failed at pivot " + std::to_string(info));
-      L.W.alloc((size_t)n * n);
-      dense_inverse_from_chol(n, Ld.get(), L.W.get(), st);
-      L.coarsest = true;
-      alloc_vectors(L, h->precision, st);
-      ph6.end();
-      break;
-    }
-    // ---- smoother: adaptive FSAI (host pattern, GPU values) ----------------
-    SetupPhase ph0("chronos setup: fsai pattern", &T[0]);
-    FsaiResult fr = fsai_adaptive(Al, prm.nstep, prm.step_size, prm.epsilon, nth,
-                                   prm.fsai_fabs == 0);
-    CHRONOS_REQUIRE(fr.posdef, CHRONOS_ENOTSPD,
-                    "matrix deemed indefinite during FSAI (the nonsymmetric fallback is outside this path)");
-    ph0.end();
-    SetupPhase ph1("chronos setup: fsai numeric", &T[1]);
-    {
-      HostCSR &Gh = fr.G;
-      std::vector<int> rowlen(n);
-      for (int i = 0; i < n; ++i) rowlen[i] = (int)(Gh.rp[i + 1] - Gh.rp[i]);
-      upload_csr(Gh, L.G, false, st);       // pattern (+ host values, overwritten)
-      const int fl = fsai_numeric_device(n, L.A.rp, L.A.ci, L.A.v64, L.G.rp, L.G.ci, L.G.v64,
-                                         rowlen, st);
-      CHRONOS_REQUIRE(fl == 0, CHRONOS_ENOTSPD, "FSAI numeric phase met a non-SPD local system");
-      // NaN-diagonal repair (smoother.m:61-71): row -> 1/sqrt(a_ii) e_i
-      std::vector<double> gv(L.G.nnz);
-      L.G.v64.download(gv.data(), L.G.nnz, st);
-      CHRONOS_CUDA(cudaStreamSynchronize(st));
-      bool fixed = false;
-      for (int i = 0; i < n; ++i) {
-        const int64_t dpos = Gh.rp[i + 1] - 1;
-        if (std::isnan(gv[dpos])) {
-          double aii = 0;
-          for (int64_t k = Al.rp[i]; k < Al.rp[i + 1]; ++k) if (Al.ci[k] == i) aii = Al.v[k];
-          for (int64_t k = Gh.rp[i]; k < dpos; ++k) gv[k] = 0.0;
-          gv[dpos] = 1.0 / std::sqrt(aii);
-          fixed = true;
-        }
-      }
-      if (fixed) L.G.v64.upload(gv, st);
-      std::vector<int64_t> perm;
-      HostCSR Gt = csr_transpose_map(Gh, perm);
-      Gt.v.assign(Gt.ci.size(), 0.0);
-      upload_csr(Gt, L.Gt, false, st);
-      DBuf<int64_t> dperm;
-      dperm.upload(perm, st);
-      gather_values(L.G.nnz, L.G.v64.get(), dperm.get(), L.Gt.v64.get(), st);
-      if (fp32) {
-        L.G.v32.alloc(std::max<int64_t>(L.G.nnz, 1));
-        L.Gt.v32.alloc(std::max<int64_t>(L.Gt.nnz, 1));
-        convert_f64_to_f32(L.G.nnz, L.G.v64.get(), L.G.v32.get(), st);
-        convert_f64_to_f32(L.Gt.nnz, L.Gt.v64.get(), L.Gt.v32.get(), st);
-      }
-      CHRONOS_CUDA(cudaStreamSynchronize(st));
-    }
-    ph1.end();
-    // ---- omega = min(1, 1.9 / lambda_max(G A G')) ----------------------------
-    SetupPhase ph2("chronos setup: omega", &T[2]);
-    {
-      DBuf<double> t1(n), t2(n);
-      Level *Lp = &L;
-      auto mv = [&](const double *v, double *w) {
-        csr_apply<double, double, double, double, MODE_PLAIN, false>(
-            st, 8, n, Lp->Gt.rp, Lp->Gt.ci, Lp->Gt.v64, v, nullptr, t1.get(), 1.0);
-        csr_apply<double, double, double, double, MODE_PLAIN, false>(
-            st, 8, n, Lp->A.rp, Lp->A.ci, Lp->A.v64, t1.get(), nullptr, t2.get(), 1.0);
-        csr_apply<double, double, double, double, MODE_PLAIN, false>(
-            st, 8, n, Lp->G.rp, Lp->G.ci, Lp->G.v64, t2.get(), nullptr, w, 1.0);
-      };
-      L.lambda = lanczos_lmax(n, mv, 5e-4, 200, st);
-      L.omega = std::min(1.0, 1.9 / L.lambda);
-    }
-    ph2.end();
-    HostCSR Ph;
-    int nc = 0;
-    if (prolong) {
-      // ---- prolongation from the caller (coarsening, C/F split, P pattern and
-      // values are the caller's host code, as cpt_aspAMG.m:224-225 calls prolong)
-      SetupPhase ph4("chronos setup: prolongation (caller)", &T[4]);
-      Ph = (*prolong)(level, Al);
-      nc = Ph.ncols;
-      CHRONOS_REQUIRE(Ph.nrows == n && nc > 0 && nc < n &&
-                          (int64_t)Ph.rp.size() == (int64_t)n + 1 && Ph.rp[0] == 0 &&
-                          (int64_t)Ph.ci.size() == Ph.rp[n] && Ph.v.size() == Ph.ci.size(),
-                      CHRONOS_EINVAL,
-                      "caller's prolongation of level " + std::to_string(level) +
-                          " must be n x nc CSR with 0 < nc < n");
-      for (int i = 0; i < n; ++i) {
-        CHRONOS_REQUIRE(Ph.rp[i + 1] >= Ph.rp[i], CHRONOS_EINVAL,
-                        "caller's prolongation: decreasing row pointers");
-        for (int64_t k = Ph.rp[i]; k < Ph.rp[i + 1]; ++k)
-          CHRONOS_REQUIRE(Ph.ci[k] >= 0 && Ph.ci[k] < nc && (k == Ph.rp[i] || Ph.ci[k] > Ph.ci[k - 1]) &&
-                              std::isfinite(Ph.v[k]),
-                          CHRONOS_EINVAL,
-                          "caller's prolongation: columns must be ascending in [0, nc), values finite");
-      }
-      ph4.end();
-    } else {
-    // ---- test space, coarsening --------------------------------------------
-    SetupPhase ph3("chronos setup: coarsening", &T[3]);
-    qr_orthonormalize(n, ntv, TV.data());
-    HostCSR S;
-    std::vector<int> fcn;
-    if (gpu_coarsening(prm.SoC_type)) {
-      coarsen_dom_device(n, L.A.rp, L.A.ci, L.A.v64, prm.soc_tau, rng, S, fcn, &nc, st);
-    } else {
-      S = soc_matrix(Al, prm.SoC_type, prm.soc_tau);
-      fcn = pmis_split(Al, S, rng, &nc);
-    }
-    CHRONOS_REQUIRE(nc > 0 && nc < n, CHRONOS_EINVAL, "coarsening produced no usable coarse level");
-    ph3.end();
-    // ---- BAMG prolongation -----------------------------------------------------
-    SetupPhase ph4("chronos setup: prolongation", &T[4]);
-    std::vector<int> fc0(n);
-    std::vector<int> clist;
-    clist.reserve(nc);
-    for (int i = 0; i < n; ++i) {
-      fc0[i] = fcn[i] > 0 ? fcn[i] - 1 : -1;
-      if (fcn[i] > 0) clist.push_back(i);
-    }
-    std::vector<double> TVr((size_t)n * ntv);
-    for (int i = 0; i < n; ++i)
-      for (int j = 0; j < ntv; ++j) TVr[(size_t)i * ntv + j] = TV[(size_t)j * n + i];
-    BamgParams bp{prm.itmax_vol, prm.dist_min, prm.dist_max, ntv,
-                  prm.prol_np > 0 ? prm.prol_np : nth, prm.maxcond, prm.maxrownrm, prm.tol_vol,
-                  prm.eps_prol};
-    std::vector<int> c_mark;
-    Ph = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
-    if (pemin == "SMOOTH") Ph = smooth_prolongation(Al, L.A, Ph, st);
-    std::vector<double> TVn((size_t)nc * ntv);
-    for (int j = 0; j < ntv; ++j)
-      for (int c = 0; c < nc; ++c) TVn[(size_t)j * nc + c] = TV[(size_t)j * n + clist[c]];
-    TV.swap(TVn);
-    ph4.end();
-    }
-    // ---- Galerkin on the GPU ---------------------------------------------------
-    SetupPhase ph5("chronos setup: galerkin", &T[5]);
-    L.nc = nc;
-    upload_csr(Ph, L.P, fp32, st);
-    HostCSR Pt = csr_transpose(Ph);
-    upload_csr(Pt, L.Pt, fp32, st);
-    DBuf<int> aprp, apci, acrp, acci;
-    DBuf<double> apv, acv;
-    int64_t nnz_ap = 0, nnz_ac = 0;
-    spgemm_device(n, nc, L.A.rp, L.A.ci, L.A.v64, L.P.rp, L.P.ci, L.P.v64, aprp, apci, apv,
-                  &nnz_ap, st);
-    spgemm_device(nc, nc, L.Pt.rp, L.Pt.ci, L.Pt.v64, aprp, apci, apv, acrp, acci, acv, &nnz_ac,
-                  st);
-    HostCSR Ac = download_csr(nc, nc, acrp, acci, acv, nnz_ac, st);
-    ph5.end();
-    alloc_vectors(L, h->precision, st);
-    Al = std::move(Ac);
+HierBuilder::~HierBuilder() = default;
+
+bool HierBuilder::begin_level() {
+  const chronos_params &prm = prm_;
+  ++level_;
+  Hier &H = *h_;
+  cudaStream_t st = H.st;
+  std::array<double, 12> &T = H.times;
+  H.levels.emplace_back();
+  Level &L = H.levels.back();
+  const int n = Al_.nrows;
+  L.n = n;
+  {
+    SetupPhase ph8("chronos setup: uploads", &T[8]);
+    upload_csr(Al_, L.A, fp32_, st);
+    if (prm.use_bsr) attach_sell3(Al_, L.A, fp32_, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
   }
-  if (tune) tune_hierarchy(*h);
+  if (n <= prm.maxCoarseSZ || level_ >= prm.nLevMax) {
+    SetupPhase ph6("chronos setup: coarse factor", &T[6]);
+    CHRONOS_REQUIRE(n <= 8192, CHRONOS_ENOTSUP, "coarsest level larger than 8192 rows");
+    std::vector<double> dense((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+      for (int64_t k = Al_.rp[i]; k < Al_.rp[i + 1]; ++k) dense[(size_t)Al_.ci[k] * n + i] = Al_.v[k];
+    DBuf<double> Ld;
+    Ld.upload(dense, st);
+    const int info = dense_cholesky_device(n, Ld.get(), st);
+    CHRONOS_REQUIRE(info == 0, CHRONOS_ENOTSPD,
+                    "coarsest-level Cholesky failed at pivot " + std::to_string(info));
+    L.W.alloc((size_t)n * n);
+    dense_inverse_from_chol(n, Ld.get(), L.W.get(), st);
+    L.coarsest = true;
+    alloc_vectors(L, H.precision, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    return false;
+  }
+  // ---- smoother: adaptive FSAI (host pattern, GPU values) ----------------
+  SetupPhase ph0("chronos setup: fsai pattern", &T[0]);
+  FsaiResult fr = fsai_adaptive(Al_, prm.nstep, prm.step_size, prm.epsilon, nth_,
+                                prm.fsai_fabs == 0);
+  CHRONOS_REQUIRE(fr.posdef, CHRONOS_ENOTSPD,
+                  "matrix deemed indefinite during FSAI (the nonsymmetric fallback is outside this path)");
+  Gh_ = std::move(fr.G);
+  rowlen_.resize(n);
+  for (int i = 0; i < n; ++i) rowlen_[i] = (int)(Gh_.rp[i + 1] - Gh_.rp[i]);
+  upload_csr(Gh_, L.G, false, st);       // pattern (+ host values, overwritten)
   CHRONOS_CUDA(cudaStreamSynchronize(st));
-  T[7] = now_s() - t_start;
-  return h;
+  return true;
+}
+
+FsaiJob HierBuilder::fsai_job() const {
+  const Level &L = h_->levels.back();
+  FsaiJob j;
+  j.n = L.n;
+  j.arp = L.A.rp.get();
+  j.aci = L.A.ci.get();
+  j.av = L.A.v64.get();
+  j.grp = L.G.rp.get();
+  j.gci = L.G.ci.get();
+  j.gval = L.G.v64.get();
+  j.rowlen = &rowlen_;
+  return j;
+}
+
+int HierBuilder::fsai_numeric_single() {
+  Level &L = h_->levels.back();
+  SetupPhase ph1("chronos setup: fsai numeric", &h_->times[1]);
+  return fsai_numeric_device(L.n, L.A.rp, L.A.ci, L.A.v64, L.G.rp, L.G.ci, L.G.v64, rowlen_,
+                             h_->st);
+}
+
+void HierBuilder::add_numeric_time(double seconds) { h_->times[1] += seconds; }
+
+void HierBuilder::end_level(int fl) {
+  const chronos_params &prm = prm_;
+  Hier &H = *h_;
+  cudaStream_t st = H.st;
+  std::array<double, 12> &T = H.times;
+  Level &L = H.levels.back();
+  const int n = L.n;
+  const int level = level_;
+  const ProlongFn *prolong = prolong_;
+  const int ntv = ntv_;
+  const int nth = nth_;
+  const bool fp32 = fp32_;
+  HostCSR &Al = Al_;
+  std::vector<double> &TV = TV_;
+  MT19937 &rng = rng_;
+  const std::string &pemin = pemin_;
+  CHRONOS_REQUIRE(fl == 0, CHRONOS_ENOTSPD, "FSAI numeric phase met a non-SPD local system");
+  SetupPhase ph1("chronos setup: fsai numeric", &T[1]);
+  {
+    HostCSR &Gh = Gh_;
+    // NaN-diagonal repair (smoother.m:61-71): row -> 1/sqrt(a_ii) e_i
+    std::vector<double> gv(L.G.nnz);
+    L.G.v64.download(gv.data(), L.G.nnz, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    bool fixed = false;
+    for (int i = 0; i < n; ++i) {
+      const int64_t dpos = Gh.rp[i + 1] - 1;
+      if (std::isnan(gv[dpos])) {
+        double aii = 0;
+        for (int64_t k = Al.rp[i]; k < Al.rp[i + 1]; ++k) if (Al.ci[k] == i) aii = Al.v[k];
+        for (int64_t k = Gh.rp[i]; k < dpos; ++k) gv[k] = 0.0;
+        gv[dpos] = 1.0 / std::sqrt(aii);
+        fixed = true;
+      }
+    }
+    if (fixed) L.G.v64.upload(gv, st);
+    ph1.end();
+    SetupPhase ph9("chronos setup: layouts", &T[9]);
+    std::vector<int64_t> perm;
+    HostCSR Gt = csr_transpose_map(Gh, perm);
+    Gt.v.assign(Gt.ci.size(), 0.0);
+    upload_csr(Gt, L.Gt, false, st);
+    DBuf<int64_t> dperm;
+    dperm.upload(perm, st);
+    gather_values(L.G.nnz, L.G.v64.get(), dperm.get(), L.Gt.v64.get(), st);
+    if (fp32) {
+      L.G.v32.alloc(std::max<int64_t>(L.G.nnz, 1));
+      L.Gt.v32.alloc(std::max<int64_t>(L.Gt.nnz, 1));
+      convert_f64_to_f32(L.G.nnz, L.G.v64.get(), L.G.v32.get(), st);
+      convert_f64_to_f32(L.Gt.nnz, L.Gt.v64.get(), L.Gt.v32.get(), st);
+    }
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+  }
+  ph1.end();
+  // ---- omega = min(1, 1.9 / lambda_max(G A G')) ----------------------------
+  SetupPhase ph2("chronos setup: omega", &T[2]);
+  {
+    DBuf<double> t1(n), t2(n);
+    Level *Lp = &L;
+    auto mv = [&](const double *v, double *w) {
+      csr_apply<double, double, double, double, MODE_PLAIN, false>(
+          st, 8, n, Lp->Gt.rp, Lp->Gt.ci, Lp->Gt.v64, v, nullptr, t1.get(), 1.0);
+      csr_apply<double, double, double, double, MODE_PLAIN, false>(
+          st, 8, n, Lp->A.rp, Lp->A.ci, Lp->A.v64, t1.get(), nullptr, t2.get(), 1.0);
+      csr_apply<double, double, double, double, MODE_PLAIN, false>(
+          st, 8, n, Lp->G.rp, Lp->G.ci, Lp->G.v64, t2.get(), nullptr, w, 1.0);
+    };
+    L.lambda = lanczos_lmax(n, mv, 5e-4, 200, st);
+    L.omega = std::min(1.0, 1.9 / L.lambda);
+  }
+  ph2.end();
+  HostCSR Ph;
+  int nc = 0;
+  if (prolong) {
+    // ---- prolongation from the caller (coarsening, C/F split, P pattern and
+    // values are the caller's host code, as cpt_aspAMG.m:224-225 calls prolong)
+    SetupPhase ph4("chronos setup: prolongation (caller)", &T[4]);
+    Ph = (*prolong)(level, Al);
+    nc = Ph.ncols;
+    CHRONOS_REQUIRE(Ph.nrows == n && nc > 0 && nc < n &&
+                        (int64_t)Ph.rp.size() == (int64_t)n + 1 && Ph.rp[0] == 0 &&
+                        (int64_t)Ph.ci.size() == Ph.rp[n] && Ph.v.size() == Ph.ci.size(),
+                    CHRONOS_EINVAL,
+                    "caller's prolongation of level " + std::to_string(level) +
+                        " must be n x nc CSR with 0 < nc < n");
+    for (int i = 0; i < n; ++i) {
+      CHRONOS_REQUIRE(Ph.rp[i + 1] >= Ph.rp[i], CHRONOS_EINVAL,
+                      "caller's prolongation: decreasing row pointers");
+      for (int64_t k = Ph.rp[i]; k < Ph.rp[i + 1]; ++k)
+        CHRONOS_REQUIRE(Ph.ci[k] >= 0 && Ph.ci[k] < nc && (k == Ph.rp[i] || Ph.ci[k] > Ph.ci[k - 1]) &&
+                            std::isfinite(Ph.v[k]),
+                        CHRONOS_EINVAL,
+                        "caller's prolongation: columns must be ascending in [0, nc), values finite");
+    }
+    ph4.end();
+  } else {
+  // ---- test space, coarsening --------------------------------------------
+  SetupPhase ph3("chronos setup: coarsening", &T[3]);
+  qr_orthonormalize(n, ntv, TV.data());
+  HostCSR S;
+  std::vector<int> fcn;
+  if (gpu_coarsening(prm.SoC_type)) {
+    coarsen_device(n, L.A.rp, L.A.ci, L.A.v64, prm.SoC_type, prm.soc_tau, rng, S, fcn, &nc,
+                   st);
+  } else {
+    S = soc_matrix(Al, prm.SoC_type, prm.soc_tau);
+    fcn = pmis_split(Al, S, rng, &nc);
+  }
+  CHRONOS_REQUIRE(nc > 0 && nc < n, CHRONOS_EINVAL, "coarsening produced no usable coarse level");
+  ph3.end();
+  // ---- BAMG prolongation -----------------------------------------------------
+  SetupPhase ph4("chronos setup: prolongation", &T[4]);
+  std::vector<int> fc0(n);
+  std::vector<int> clist;
+  clist.reserve(nc);
+  for (int i = 0; i < n; ++i) {
+    fc0[i] = fcn[i] > 0 ? fcn[i] - 1 : -1;
+    if (fcn[i] > 0) clist.push_back(i);
+  }
+  std::vector<double> TVr((size_t)n * ntv);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < ntv; ++j) TVr[(size_t)i * ntv + j] = TV[(size_t)j * n + i];
+  BamgParams bp{prm.itmax_vol, prm.dist_min, prm.dist_max, ntv,
+                prm.prol_np > 0 ? prm.prol_np : nth, prm.maxcond, prm.maxrownrm, prm.tol_vol,
+                prm.eps_prol};
+  std::vector<int> c_mark;
+  Ph = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
+  if (pemin == "SMOOTH") Ph = smooth_prolongation(Al, L.A, Ph, st);
+  std::vector<double> TVn((size_t)nc * ntv);
+  for (int j = 0; j < ntv; ++j)
+    for (int c = 0; c < nc; ++c) TVn[(size_t)j * nc + c] = TV[(size_t)j * n + clist[c]];
+  TV.swap(TVn);
+  ph4.end();
+  }
+  // ---- Galerkin on the GPU ---------------------------------------------------
+  SetupPhase ph9("chronos setup: layouts", &T[9]);
+  L.nc = nc;
+  upload_csr(Ph, L.P, fp32, st);
+  HostCSR Pt = csr_transpose(Ph);
+  upload_csr(Pt, L.Pt, fp32, st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  ph9.end();
+  SetupPhase ph5("chronos setup: galerkin", &T[5]);
+  DBuf<int> aprp, apci, acrp, acci;
+  DBuf<double> apv, acv;
+  int64_t nnz_ap = 0, nnz_ac = 0;
+  spgemm_device(n, nc, L.A.rp, L.A.ci, L.A.v64, L.P.rp, L.P.ci, L.P.v64, aprp, apci, apv,
+                &nnz_ap, st);
+  spgemm_device(nc, nc, L.Pt.rp, L.Pt.ci, L.Pt.v64, aprp, apci, apv, acrp, acci, acv, &nnz_ac,
+                st);
+  HostCSR Ac = download_csr(nc, nc, acrp, acci, acv, nnz_ac, st);
+  ph5.end();
+  alloc_vectors(L, H.precision, st);
+  Al = std::move(Ac);
+}
+
+std::unique_ptr<Hier> HierBuilder::finish(bool tune) {
+  std::array<double, 12> &T = h_->times;
+  if (tune) {
+    SetupPhase ph10("chronos setup: autotune", &T[10]);
+    tune_hierarchy(*h_);
+  }
+  CHRONOS_CUDA(cudaStreamSynchronize(h_->st));
+  T[7] = now_s() - t_start_;
+  double named = 0.0;
+  for (int k : {0, 1, 2, 3, 4, 5, 6, 8, 9, 10}) named += T[k];
+  T[11] = std::max(0.0, T[7] - named);
+  return std::move(h_);
+}
+
+std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A0, int ntv0,
+                                      const double *TV0, bool tune, const ProlongFn *prolong) {
+  HierBuilder b(prm, A0, ntv0, TV0, prolong);
+  while (b.begin_level()) b.end_level(b.fsai_numeric_single());
+  return b.finish(tune);
 }
 
 void tune_hierarchy(Hier &h) {

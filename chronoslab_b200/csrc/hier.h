@@ -5,6 +5,7 @@
 #include <array>
 #include <functional>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "host/host.h"
@@ -12,15 +13,15 @@
 
 namespace chronos {
 
-// DOM strength of connection and PMIS C/F splitting on the GPU
+// DOM or CLA strength of connection and PMIS C/F splitting on the GPU
 // (coarsen_gpu.cu) for the device CSR (rp, ci, v) of an n x n level:
 // fcnode numbered as the reference numbers it, nc coarse nodes, and S the
 // strength pattern (values left empty) for the host prolongation.  Draws n
-// numbers from rng, as pmis_split does; bit-identical to soc_matrix("DOM")
+// numbers from rng, as pmis_split does; bit-identical to soc_matrix(soc_type)
 // + pmis_split.
-void coarsen_dom_device(int n, const int *rp, const int *ci, const double *v, double tau,
-                        MT19937 &rng, HostCSR &S, std::vector<int> &fcnode, int *nc_out,
-                        cudaStream_t st);
+void coarsen_device(int n, const int *rp, const int *ci, const double *v, const char *soc_type,
+                    double tau, MT19937 &rng, HostCSR &S, std::vector<int> &fcnode, int *nc_out,
+                    cudaStream_t st);
 
 // Outcome of gmres_right_device, as gmres_RIGHT.m returns it.
 struct GmresResult {
@@ -40,8 +41,8 @@ void gmres_right_device(Hier &h, const std::function<void(const double *, double
 // Square, sorted, in-range, finite CSR, or CHRONOS_EINVAL.
 void validate_csr(const HostCSR &A);
 
-// Whether the setup coarsens on the GPU: DOM strength (the only kind the
-// GPU path computes) and CHRONOS_GPU_COARSEN not set to 0.
+// Whether the setup coarsens on the GPU: DOM or CLA strength and
+// CHRONOS_GPU_COARSEN not set to 0.
 bool gpu_coarsening(const char *soc_type);
 
 struct Level {
@@ -100,7 +101,11 @@ struct Hier {
   int precision = CHRONOS_FP32;
   std::vector<Level> levels;
   cudaStream_t st = nullptr;
-  std::array<double, 8> times{};   // setup timings
+  // setup timings (s): fsai_pattern, fsai_numeric, omega, coarsen (with the
+  // test space), prolong, galerkin, coarse_factor, total, uploads (operators
+  // and their block form), layouts (transposes and FP32 copies of G and P),
+  // autotune, other (the rest of total)
+  std::array<double, 12> times{};
   PcgState pcg;
   // Operator of the outer PCG when the caller passes one (PCG_CJ's prodA,
   // PCG_CJ.m:1): FP64 CSR of the level-1 size; otherwise levels[0].A.
@@ -167,6 +172,38 @@ std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &
                                       int ntv0, const double *TV0, bool tune = true,
                                       const ProlongFn *prolong = nullptr);
 void tune_hierarchy(Hier &h);
+
+// One hierarchy built level by level (what build_hierarchy runs): a level is
+// begun (its operator uploaded; the coarsest factored, begin_level then
+// returning false; otherwise its FSAI pattern computed on the host and
+// uploaded), its FSAI numeric phase run -- alone (fsai_numeric_single) or,
+// by a batch setup, together with other builders' (fsai_job) -- and ended
+// (omega, coarsening, prolongation, Galerkin product of the next level).
+class HierBuilder {
+ public:
+  HierBuilder(const chronos_params &prm, const HostCSR &A0, int ntv0, const double *TV0,
+              const ProlongFn *prolong = nullptr);
+  ~HierBuilder();
+  bool begin_level();
+  FsaiJob fsai_job() const;
+  int fsai_numeric_single();             // returns the flags word
+  void add_numeric_time(double seconds); // a batched numeric phase's share
+  void end_level(int fsai_flags);
+  std::unique_ptr<Hier> finish(bool tune);
+
+ private:
+  chronos_params prm_;
+  const ProlongFn *prolong_;
+  double t_start_;
+  MT19937 rng_;
+  std::unique_ptr<Hier> h_;
+  bool fp32_ = false;
+  int nth_ = 1, ntv_ = 1, level_ = 0;
+  std::string pemin_;
+  std::vector<double> TV_;
+  HostCSR Al_, Gh_;
+  std::vector<int> rowlen_;
+};
 
 // Serialisation of a built hierarchy (every level's operator, smoother
 // factor and prolongation in FP64, omega, lambda_max, the coarsest inverse

@@ -66,6 +66,26 @@ int fsai_numeric_device(int n, const int *arp, const int *aci, const double *av,
                         const int *gci, double *gval, const std::vector<int> &rowlen_h,
                         cudaStream_t st);
 
+// One problem of fsai_numeric_batched: device CSR of A, G's pattern and the
+// buffer of G's values; rowlen: the host row lengths of G.
+struct FsaiJob {
+  int n = 0;
+  const int *arp = nullptr, *aci = nullptr;
+  const double *av = nullptr;
+  const int *grp = nullptr, *gci = nullptr;
+  double *gval = nullptr;
+  const std::vector<int> *rowlen = nullptr;
+};
+// The FSAI numeric phase of all jobs at once: one launch per tile size over
+// every job's rows, the tile sizes (bucket edges) chosen by timing candidate
+// sets on the batch (cached per batch shape).  Returns each job's flags word
+// (bit 0: non-SPD local block); chosen_set (may be null) receives the index of
+// the set used.  Values are those of fsai_numeric_device, bit for bit.
+// force_set >= 0 uses that candidate set instead of the tuned one.
+std::vector<int> fsai_numeric_batched(const std::vector<FsaiJob> &jobs, cudaStream_t st,
+                                      int *chosen_set = nullptr, int force_set = -1);
+int fsai_bucket_set_count();
+
 // ---- Galerkin (setup_kernels.cu) ---------------------------------------------
 // C = X * Y (X: m x k, Y: k x ncols), Gustavson accumulation order, exact
 // zeros dropped, columns sorted.  Output arrays allocated here.

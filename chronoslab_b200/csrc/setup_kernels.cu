@@ -14,8 +14,12 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
 #include <mutex>
 #include <numeric>
+#include <string>
 
 #include "internal.h"
 
@@ -37,20 +41,18 @@ __device__ __forceinline__ int find_col(const int *aci, int k, int ke, int c) {
   return -1;
 }
 
+// Row i of G by one warp (cpt_afsai_coef.cpp:440-541): gathers A[P,P] and
+// -A[P,i] into the warp's shared-memory tile M (MMAX x MMAX, row-major lower,
+// then rhs and y), factors and solves, and writes the scaled row.  Sets bit 0
+// of *flags for a non-SPD local block or a non-positive Schur complement.
 template <int MMAX>
-__global__ void k_fsai_numeric(int nb, const int *__restrict__ rows, const int *__restrict__ arp,
-                               const int *__restrict__ aci, const double *__restrict__ av,
-                               const int *__restrict__ grp, const int *__restrict__ gci,
-                               double *__restrict__ gval, int *flags) {
-  extern __shared__ double smem[];
-  constexpr int STRIDE = MMAX * MMAX + 3 * MMAX;
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int wglob = blockIdx.x * (blockDim.x >> 5) + wib;
-  if (wglob >= nb) return;                      // warp-uniform exit
-  double *M = smem + (size_t)wib * STRIDE;      // row-major lower: M[j*MMAX + l], l <= j
+__device__ __forceinline__ void fsai_row(int i, const int *__restrict__ arp,
+                                         const int *__restrict__ aci, const double *__restrict__ av,
+                                         const int *__restrict__ grp, const int *__restrict__ gci,
+                                         double *__restrict__ gval, int *flags, double *M,
+                                         int lane) {
   double *rhs = M + MMAX * MMAX;                // -A[i,P] (kept for the Schur term)
   double *y = rhs + MMAX;                       // solution
-  const int i = rows[wglob];
   const int gs = grp[i], ge = grp[i + 1];
   const int m = ge - gs - 1;                    // strictly-lower entries
   const int *P = gci + gs;
@@ -131,6 +133,44 @@ __global__ void k_fsai_numeric(int nb, const int *__restrict__ rows, const int *
   if (lane == 0) gval[gs + m] = s;
 }
 
+template <int MMAX>
+__global__ void k_fsai_numeric(int nb, const int *__restrict__ rows, const int *__restrict__ arp,
+                               const int *__restrict__ aci, const double *__restrict__ av,
+                               const int *__restrict__ grp, const int *__restrict__ gci,
+                               double *__restrict__ gval, int *flags) {
+  extern __shared__ double smem[];
+  constexpr int STRIDE = MMAX * MMAX + 3 * MMAX;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int wglob = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (wglob >= nb) return;                      // warp-uniform exit
+  fsai_row<MMAX>(rows[wglob], arp, aci, av, grp, gci, gval, flags, smem + (size_t)wib * STRIDE,
+                 lane);
+}
+
+// One problem of a batched FSAI numeric launch (device pointers).
+struct FsaiProblemDev {
+  const int *arp, *aci;
+  const double *av;
+  const int *grp, *gci;
+  double *gval;
+};
+
+// The rows of many problems in one launch: item k = (problem, row); flags
+// per problem.
+template <int MMAX>
+__global__ void k_fsai_numeric_batched(int nb, const int2 *__restrict__ items,
+                                       const FsaiProblemDev *__restrict__ tab, int *flags) {
+  extern __shared__ double smem[];
+  constexpr int STRIDE = MMAX * MMAX + 3 * MMAX;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int wglob = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (wglob >= nb) return;                      // warp-uniform exit
+  const int2 it = items[wglob];
+  const FsaiProblemDev pr = tab[it.x];
+  fsai_row<MMAX>(it.y, pr.arp, pr.aci, pr.av, pr.grp, pr.gci, pr.gval, flags + it.x,
+                 smem + (size_t)wib * STRIDE, lane);
+}
+
 int fsai_numeric_device(int n, const int *arp, const int *aci, const double *av, const int *grp,
                         const int *gci, double *gval, const std::vector<int> &rowlen_h,
                         cudaStream_t st) {
@@ -163,6 +203,159 @@ int fsai_numeric_device(int n, const int *arp, const int *aci, const double *av,
   CHRONOS_CUDA(cudaMemcpyAsync(&fl, flags.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
   CHRONOS_CUDA(cudaStreamSynchronize(st));
   return fl;
+}
+
+// -----------------------------------------------------------------------------
+// FSAI numeric phase of many problems at once (a batch's level): every row of
+// every problem goes to the smallest shared-memory tile (MMAX) that holds its
+// local system, and each tile size is one launch over all problems' rows.
+// Which tile sizes exist -- the bucket edges -- is chosen per batch shape by
+// timing the candidate sets below on the batch's own rows (CUDA events); a
+// row's arithmetic does not depend on its tile, so every set gives the same
+// values bit for bit and the timed runs may overwrite one another.
+// -----------------------------------------------------------------------------
+
+namespace {
+
+const std::vector<std::vector<int>> &fsai_bucket_sets() {
+  static const std::vector<std::vector<int>> sets = {
+      {16, 32, 64}, {8, 16, 32, 64}, {16, 24, 32, 48, 64}, {8, 16, 24, 32, 48, 64}};
+  return sets;
+}
+
+// warps per block of a tile size (shared memory: warps * (MMAX^2 + 3 MMAX) doubles)
+int fsai_tile_warps(int mmax) { return mmax <= 24 ? 8 : mmax <= 32 ? 4 : 2; }
+
+template <int MMAX>
+void launch_fsai_batched(int cnt, const int2 *items, const FsaiProblemDev *tab, int *flags,
+                         cudaStream_t st) {
+  if (cnt == 0) return;
+  const int warps = fsai_tile_warps(MMAX);
+  const size_t sm = (size_t)warps * (MMAX * MMAX + 3 * MMAX) * sizeof(double);
+  CHRONOS_CUDA(cudaFuncSetAttribute(k_fsai_numeric_batched<MMAX>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_fsai_numeric_batched<MMAX><<<ceil_div(cnt, warps), warps * 32, sm, st>>>(cnt, items, tab,
+                                                                            flags);
+  CHRONOS_CHECK_LAUNCH();
+}
+
+void launch_fsai_tile(int mmax, int cnt, const int2 *items, const FsaiProblemDev *tab, int *flags,
+                      cudaStream_t st) {
+  switch (mmax) {
+    case 8: launch_fsai_batched<8>(cnt, items, tab, flags, st); break;
+    case 16: launch_fsai_batched<16>(cnt, items, tab, flags, st); break;
+    case 24: launch_fsai_batched<24>(cnt, items, tab, flags, st); break;
+    case 32: launch_fsai_batched<32>(cnt, items, tab, flags, st); break;
+    case 48: launch_fsai_batched<48>(cnt, items, tab, flags, st); break;
+    case 64: launch_fsai_batched<64>(cnt, items, tab, flags, st); break;
+    default: throw Error(CHRONOS_EINVAL, "no FSAI tile of this size");
+  }
+}
+
+std::mutex g_fsai_tune_mu;
+std::map<std::string, int> g_fsai_tune;       // batch shape -> index of the chosen set
+
+}  // namespace
+
+int fsai_bucket_set_count() { return (int)fsai_bucket_sets().size(); }
+
+std::vector<int> fsai_numeric_batched(const std::vector<FsaiJob> &jobs, cudaStream_t st,
+                                      int *chosen_set, int force_set) {
+  CHRONOS_REQUIRE(force_set < (int)fsai_bucket_sets().size(), CHRONOS_EINVAL,
+                  "no such FSAI tile set");
+  const int nj = (int)jobs.size();
+  std::vector<int> out(nj, 0);
+  if (nj == 0) return out;
+  // local sizes: histogram (the batch's shape) and the largest
+  std::vector<int64_t> hist(65, 0);
+  for (const auto &j : jobs)
+    for (int i = 0; i < j.n; ++i) {
+      const int m = (*j.rowlen)[i] - 1;
+      CHRONOS_REQUIRE(m >= 0 && m <= 64, m > 64 ? CHRONOS_ENOTSUP : CHRONOS_EINVAL,
+                      "FSAI local system larger than 64 (nstep*step_size) or an empty row");
+      hist[m]++;
+    }
+  std::vector<FsaiProblemDev> tab_h(nj);
+  for (int p = 0; p < nj; ++p)
+    tab_h[p] = {jobs[p].arp, jobs[p].aci, jobs[p].av, jobs[p].grp, jobs[p].gci, jobs[p].gval};
+  DBuf<FsaiProblemDev> tab;
+  tab.upload(tab_h, st);
+  DBuf<int> flags(nj);
+  // items of one bucket set, bucket by bucket: (problem, row)
+  const auto &sets = fsai_bucket_sets();
+  auto build_items = [&](const std::vector<int> &set, std::vector<int2> &items,
+                         std::vector<int> &start) {
+    const int nb = (int)set.size();
+    std::vector<int> bucket_of(65);
+    for (int m = 0; m <= 64; ++m) {
+      int b = 0;
+      while (set[b] < m) ++b;
+      bucket_of[m] = b;
+    }
+    start.assign(nb + 1, 0);
+    for (int m = 0; m <= 64; ++m) start[bucket_of[m] + 1] += (int)hist[m];
+    for (int b = 0; b < nb; ++b) start[b + 1] += start[b];
+    items.resize(start[nb]);
+    std::vector<int> cur(start.begin(), start.end() - 1);
+    for (int p = 0; p < nj; ++p)
+      for (int i = 0; i < jobs[p].n; ++i) items[cur[bucket_of[(*jobs[p].rowlen)[i] - 1]]++] = {p, i};
+  };
+  auto run = [&](const std::vector<int> &set, const DBuf<int2> &items, const std::vector<int> &start) {
+    flags.zero(st);
+    for (size_t b = 0; b < set.size(); ++b)
+      launch_fsai_tile(set[b], start[b + 1] - start[b], items.get() + start[b], tab.get(),
+                       flags.get(), st);
+  };
+  std::string key;
+  for (int m = 0; m <= 64; ++m)
+    if (hist[m]) key += std::to_string(m) + ":" + std::to_string(hist[m]) + ",";
+  int choice = force_set >= 0 ? force_set : -1;
+  if (choice < 0) {
+    std::lock_guard<std::mutex> lk(g_fsai_tune_mu);
+    auto it = g_fsai_tune.find(key);
+    if (it != g_fsai_tune.end()) choice = it->second;
+  }
+  const int64_t rows = std::accumulate(hist.begin(), hist.end(), (int64_t)0);
+  if (choice < 0 && rows < 20000) choice = 0;            // small batch: launch-bound either way
+  std::vector<int2> items_h;
+  std::vector<int> start;
+  DBuf<int2> items;
+  if (choice < 0) {
+    const bool verbose = std::getenv("CHRONOS_TUNE_VERBOSE") != nullptr;
+    cudaEvent_t e0, e1;
+    CHRONOS_CUDA(cudaEventCreate(&e0));
+    CHRONOS_CUDA(cudaEventCreate(&e1));
+    float best = 1e30f;
+    for (int s = 0; s < (int)sets.size(); ++s) {
+      build_items(sets[s], items_h, start);
+      items.upload(items_h, st);
+      run(sets[s], items, start);                         // warm-up (the attributes, caches)
+      CHRONOS_CUDA(cudaEventRecord(e0, st));
+      run(sets[s], items, start);
+      CHRONOS_CUDA(cudaEventRecord(e1, st));
+      CHRONOS_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (verbose) {
+        std::string edges;
+        for (int m : sets[s]) edges += std::to_string(m) + " ";
+        std::fprintf(stderr, "chronos tune: fsai batch %lld rows, tiles %s %.4f ms\n",
+                     (long long)rows, edges.c_str(), ms);
+      }
+      if (ms < best) { best = ms; choice = s; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::lock_guard<std::mutex> lk(g_fsai_tune_mu);
+    g_fsai_tune[key] = choice;
+  }
+  build_items(sets[choice], items_h, start);
+  items.upload(items_h, st);
+  run(sets[choice], items, start);
+  flags.download(out.data(), nj, st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  if (chosen_set) *chosen_set = choice;
+  return out;
 }
 
 // =============================================================================

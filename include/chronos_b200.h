@@ -154,6 +154,24 @@ int chronos_fsai_numeric(int n, int base, const int64_t *iat_A_h, const int *ja_
                          const double *val_A_h, const int64_t *iat_G_h, const int *ja_G_h,
                          int out_precision, void *val_G_h, int *is_posdef, void *stream);
 
+/* The FSAI numeric phase of many problems at once (no counterpart call in the
+ * reference, which runs the MEX once per matrix): one launch per
+ * shared-memory tile size over every problem's rows, each row in the
+ * smallest tile that holds its local system.  The tile sizes -- the bucket
+ * edges -- are candidate sets {16,32,64}, {8,16,32,64}, {16,24,32,48,64},
+ * {8,16,24,32,48,64} (tile_set 0..3); tile_set = -1 picks the fastest by
+ * timing them on these rows (remembered per shape of the batch, in-process).
+ * The values do not depend on the set: per problem they are those of
+ * chronos_fsai_numeric bit for bit.  0-based CSR (int32) per problem; rows of
+ * G strictly-lower ascending, then the diagonal; is_posdef[p] as the MEX's
+ * flag; tile_set_used (may be NULL) receives the set run.  The batch setup
+ * (chronos_batch_setup) runs each level's FSAI this way. */
+int chronos_fsai_numeric_batch(int nprob, const int *n, const int *const *iat_A_h,
+                               const int *const *ja_A_h, const double *const *val_A_h,
+                               const int *const *iat_G_h, const int *const *ja_G_h,
+                               double *const *val_G_h, int *is_posdef, int tile_set,
+                               int *tile_set_used);
+
 /* FSAI numeric phase that allocates nothing.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot let a library
  * call cudaMalloc or cudaFree: hosts that own all device memory through their
@@ -219,10 +237,11 @@ int chronos_fsai_pattern(int n, const int *iat_h, const int *ja_h, const double 
 int chronos_coarsen(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
                     const double *val_h, uint64_t rng_skip, int *fcnode_h, int *nc,
                     chronos_csr **S);
-/* The same on the GPU for DOM strength (cpt_SoC_dom.m:26-47, cpt_PMIS.m,
- * mark_isolated_nodes.m): identical fcnode and nc, and S with the strength
- * pattern (values 1).  CHRONOS_ENOTSUP for another SoC type.  The hierarchy
- * setup coarsens DOM levels this way unless CHRONOS_GPU_COARSEN=0. */
+/* The same on the GPU for DOM strength (cpt_SoC_dom.m:26-47) or CLA strength
+ * (cpt_SoC_cla.m:109-159; every row must store a nonzero diagonal), with
+ * cpt_PMIS.m and mark_isolated_nodes.m: identical fcnode and nc, and S with
+ * the strength pattern (values 1).  CHRONOS_ENOTSUP for another SoC type.
+ * The hierarchy setup coarsens this way unless CHRONOS_GPU_COARSEN=0. */
 int chronos_coarsen_device(const chronos_params *prm, int n, const int *iat_h, const int *ja_h,
                            const double *val_h, uint64_t rng_skip, int *fcnode_h, int *nc,
                            chronos_csr **S);
@@ -341,6 +360,11 @@ int chronos_hier_export(const chronos_hier *h, int level, char which, int *nrows
 /* Setup timings in seconds: [fsai_pattern, fsai_numeric, omega, coarsen, prolong,
  * galerkin, coarse_factor, total]. */
 int chronos_hier_setup_times(const chronos_hier *h, double *t8);
+/* All setup phases (no counterpart in the reference): the first n of [the
+ * eight above, uploads (operators and their 3x3 block form), layouts
+ * (transposes and FP32 copies of G and P), autotune, other (total minus the
+ * named phases)], n <= 12. */
+int chronos_hier_setup_phases(const chronos_hier *h, double *t, int n);
 /* Writes operator which ('A', 'G' or 'P') of a level in the .Ext_bin format
  * (FP64 values), e.g. to feed a level to the reference's own tools. */
 int chronos_hier_dump_ext_bin(const chronos_hier *h, int level, char which, const char *path);
@@ -413,6 +437,9 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
 int chronos_batch_solve(chronos_batch *b, const double *const *b_h, double *const *x_h,
                         int itmax, double tol, int *iters, int *flags, double *seconds);
 int chronos_batch_info(const chronos_batch *b, int p, int *nlevels, int *n0);
+/* The setup phases of chronos_hier_setup_phases summed over the batch's
+ * problems (thread time: problems are built several at once). */
+int chronos_batch_setup_phases(const chronos_batch *b, double *t, int n);
 int chronos_batch_free(chronos_batch *b);
 
 /* SQMR (SQMR.m) with the V-cycle as left preconditioner and identity right.

@@ -97,3 +97,40 @@ def test_batch_grouped_host_loop_matches_graph_loop(lib):
             out.append(B.solve(bs, itmax=1000, tol=1e-8))
     assert np.array_equal(out[0][1], out[1][1])
     assert all(np.array_equal(a, c) for a, c in zip(out[0][0], out[1][0]))
+
+
+def test_fsai_numeric_batch_bit_identical_for_every_tile_set(lib):
+    """One batched FSAI numeric phase over several problems (local systems up
+    to 60: FSAI 15 steps of 4) gives, for every candidate set of tile sizes
+    and for the tuned one, each problem's values of chronos_fsai_numeric bit
+    for bit; a batch of more than 20,000 rows is tuned."""
+    As = [PB.poisson7(32), PB.diffusion7(14, sigma=2.0, corr_len=4.0, seed=3)[0],
+          PB.elasticity_q1(6), PB.poisson7(9)]
+    Gs = []
+    for A in As:
+        G, ok = cb.fsai_pattern(A, nstep=15, step_size=4, eps=1e-3, nthread=8)
+        assert ok
+        Gs.append(G)
+    assert max(np.diff(G.indptr).max() for G in Gs) - 1 > 32
+    want = [cb.fsai_numeric(A, G, base=0)[0] for A, G in zip(As, Gs)]
+    for ts in (0, 1, 2, 3, -1):
+        vals, oks, used = cb.fsai_numeric_batch(As, Gs, tile_set=ts)
+        assert all(oks) and (used == ts if ts >= 0 else 0 <= used <= 3)
+        for v, w in zip(vals, want):
+            assert np.array_equal(v, w), ts
+
+
+def test_batch_hierarchies_equal_single_builds(lib):
+    """The level-synchronous batch setup (FSAI numeric batched across the
+    problems) builds every problem's hierarchy as a single setup does: the
+    same levels (the batched values themselves are checked bit for bit above,
+    the solves against single ones in test_batch_matches_single_solves), and
+    the batched numeric phase's time is attributed to the problems."""
+    As, _ = make_problems(5, 6, lo=10)
+    prm = cb.params(precision=cb.CHRONOS_FP64, ntv=1, nstep=15, step_size=4, batch_grouped=0)
+    with cb.Batch(As, prm) as B:
+        for p, A in enumerate(As):
+            with cb.Hierarchy(A, np.ones(A.shape[0]), prm) as h:
+                assert h.nlevels == B.nlevels(p)
+        t = B.setup_times()
+        assert t["fsai_numeric"] > 0.0

@@ -1,5 +1,5 @@
-"""GPU strength of connection (DOM) and PMIS C/F splitting against the host
-splitting and the reference's golden one, bit for bit, through the C ABI."""
+"""GPU strength of connection (DOM and CLA) and PMIS C/F splitting against the
+host splitting and the reference's golden one, bit for bit, through the C ABI."""
 import numpy as np
 import pytest
 import scipy.sparse as sp
@@ -42,19 +42,27 @@ def with_dirichlet(A, rows):
     return A
 
 
-@pytest.mark.parametrize("case", ["elasticity", "poisson", "diffusion", "dirichlet"])
-@pytest.mark.parametrize("tau", [0.01, 0.25])
-def test_matches_host(lib, case, tau):
+def _case(case):
     if case == "elasticity":
-        A = PB.elasticity_q1(7)
-    elif case == "poisson":
-        A = PB.poisson7(14)
-    elif case == "diffusion":
-        A = PB.diffusion7(12, sigma=1.0, corr_len=3.0, seed=4)[0]
-    else:
-        A = with_dirichlet(PB.poisson7(9), [0, 5, 17, 300, 728])
+        return PB.elasticity_q1(7)
+    if case == "poisson":
+        return PB.poisson7(14)
+    if case == "diffusion":
+        return PB.diffusion7(12, sigma=1.0, corr_len=3.0, seed=4)[0]
+    if case == "nonneg":                 # every off-diagonal entry >= 0: CLA's |a| branch
+        A = abs(PB.poisson7(10)).tocsr()
+        A.sort_indices()
+        return A
+    return with_dirichlet(PB.poisson7(9), [0, 5, 17, 300, 728])
+
+
+@pytest.mark.parametrize("soc", ["DOM", "CLA"])
+@pytest.mark.parametrize("case", ["elasticity", "poisson", "diffusion", "dirichlet", "nonneg"])
+@pytest.mark.parametrize("tau", [0.01, 0.25])
+def test_matches_host(lib, case, tau, soc):
+    A = _case(case)
     for skip in (0, 37):
-        same_split(A, cb.params(SoC_type="DOM", soc_tau=tau), skip)
+        same_split(A, cb.params(SoC_type=soc, soc_tau=tau), skip)
 
 
 def test_empty_strength(lib):
@@ -65,10 +73,30 @@ def test_empty_strength(lib):
     assert nc == A.shape[0]
 
 
-def test_cla_is_not_on_the_gpu(lib):
-    A = PB.poisson7(6)
-    with pytest.raises(cb.ChronosError):
-        cb.coarsen_device(A, cb.params(SoC_type="CLA", soc_tau=0.25))
+def test_cla_setup_on_the_gpu_matches_host_coarsening(lib):
+    """A hierarchy with CLA strength (tau 0.25, as FlowCLAS_0.m) coarsens on the
+    GPU by default and on the host with CHRONOS_GPU_COARSEN=0 in a child
+    process: the same level sizes and the same PCG_CJ iterations."""
+    import json
+    import os
+    import subprocess
+    import sys
+    code = ("import json, numpy as np, chronoslab_b200 as cb;"
+            "from chronoslab_b200 import problems as PB;"
+            "A = PB.diffusion7(20, sigma=1.0, corr_len=4.0, seed=2)[0];"
+            "b = PB.uniform_rhs(A.shape[0], seed=3);"
+            "h = cb.Hierarchy(A, np.ones(A.shape[0]), cb.params(SoC_type='CLA', soc_tau=0.25, ntv=1));"
+            "x, it, _, fl, _ = h.pcg(b);"
+            "print(json.dumps([[h.level_info(l)['n'] for l in range(h.nlevels)], it, fl]))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = []
+    for flag in ("1", "0"):
+        env = dict(os.environ, CHRONOS_GPU_COARSEN=flag)
+        r = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs.append(json.loads(r.stdout.strip().splitlines()[-1]))
+    assert outs[0] == outs[1] and outs[0][2] == 0
 
 
 def test_hierarchy_levels_match_host_split(lib):

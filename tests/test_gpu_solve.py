@@ -443,3 +443,15 @@ def test_diag_fix_against_eigs(lib, cubo):
     assert np.array_equal(dg[keep], d[keep])
     off = (Ag - sp.diags(dg)) - (A - sp.diags(d))
     assert abs(off).max() == 0.0
+
+
+def test_setup_phases_sum_to_total(lib, elast):
+    """Every second of the setup falls in a named phase: the twelve entries
+    minus the total sum to the total, and the named ones are not negative."""
+    A, TV, b = elast
+    with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP32)) as h:
+        t = h.setup_times()
+    assert len(t) == 12 and all(v >= 0.0 for v in t.values())
+    parts = sum(v for k, v in t.items() if k != "total")
+    assert abs(parts - t["total"]) <= 1e-6 * max(t["total"], 1.0) + 1e-9
+    assert t["uploads"] > 0.0 and t["layouts"] > 0.0
