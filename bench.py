@@ -595,7 +595,9 @@ def run_block_or_batch(args, world=1, rank=0):
             units, _ = sh.solve(bs, itmax=args.itmax, tol=args.tol, gather_x=False)
             its_all = [units[p]["iters"] for p in range(len(As))]
             phases = (sh.local.setup_times() if sh.local is not None else {})
+            walls = (sh.local.setup_wall() if sh.local is not None else {})
             res[name] = {"ms": slowest(sum(ts) / len(ts)), "setup_s": slowest(setup),
+                         "setup_wall_s": {k: round(v, 3) for k, v in walls.items()},
                          "setup_thread_s": {k: round(v, 3) for k, v in phases.items()},
                          "iters_min_max": [int(min(its_all)), int(max(its_all))],
                          "problems_per_rank": [len(p) for p in sh.parts]}

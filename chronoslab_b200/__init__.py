@@ -704,6 +704,13 @@ class Batch:
         check(self._lib.chronos_batch_setup_phases(self._h, _pd(t), len(keys)))
         return dict(zip(keys, t.tolist()))
 
+    def setup_wall(self):
+        """The batch setup's wall clock (s) by stage."""
+        keys = ["first_levels", "fsai_numeric_batched", "rest", "tune_group", "total"]
+        t = np.zeros(len(keys))
+        check(self._lib.chronos_batch_setup_wall(self._h, _pd(t)))
+        return dict(zip(keys, t.tolist()))
+
     def solve(self, bs, itmax=1000, tol=1e-8):
         """Returns (xs, iters, flags, seconds)."""
         npb = len(self.ns)

@@ -135,6 +135,7 @@ SIGNATURES = {
     "chronos_batch_solve": [_vp, _pp, _pp, _i, _d, _pi, _pi, _pd],
     "chronos_batch_info": [_vp, _i, _pi, _pi],
     "chronos_batch_setup_phases": [_vp, _pd, _i],
+    "chronos_batch_setup_wall": [_vp, _pd],
     "chronos_batch_free": [_vp],
     "chronos_sqmr":[_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _pi, _pd, _pi],
     "chronos_gmres": [_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _i, _pi, _pi, _pd, _pi, _pd, _pi],

@@ -27,6 +27,9 @@ static double now_seconds() {
 
 struct Batch {
   std::vector<std::unique_ptr<Hier>> h;
+  // setup wall clock (s): first levels begun, batched FSAI numeric phase of
+  // the first levels, the rest of the hierarchies, tuning / grouping, total
+  double wall[5] = {0, 0, 0, 0, 0};
   std::vector<int> order;           // largest level-1 operator first
   std::unique_ptr<GroupSolve> group;
 };
@@ -70,23 +73,26 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
     for (int p = 0; p < nprob; ++p)
       CHRONOS_REQUIRE(n[p] > 0 && iat_h[p] && iat_h[p][0] == 0, CHRONOS_EINVAL,
                       "problem " + std::to_string(p) + ": 0-based CSR expected");
-    // The problems' hierarchies are built level-synchronously: every round
-    // begins the next level of each unfinished problem (operator upload, FSAI
-    // pattern on the host) on a few host threads at once, each problem on its
-    // own stream with its share of the OpenMP threads; then the FSAI numeric
-    // phase of all those levels runs as one batched launch per tile size
-    // (fsai_numeric_batched, bucket edges tuned per batch shape); then the
-    // levels are ended (omega, coarsening, prolongation, Galerkin) on the
-    // host threads again.  Every hierarchy is what a single
+    // The problems' first levels are begun together (operator upload, FSAI
+    // pattern on the host) on a few host threads at once, largest problems
+    // first, each on its own stream with its share of the OpenMP threads;
+    // the FSAI numeric phase of all first levels -- most of the batch's rows --
+    // then runs as one batched launch per tile size (fsai_numeric_batched,
+    // tile sizes tuned per batch shape); then every problem goes on alone on
+    // the host threads, largest first: its first level ended (omega,
+    // coarsening, prolongation, Galerkin) and its deeper levels built as a
+    // single setup builds them.  Every hierarchy is what a single
     // chronos_amg_setup builds; lane counts are tuned afterwards on a quiet
     // GPU: the grouped solve's stacked operators, or each problem's own for
     // the per-problem path.
+    DeferFrees defer_frees;          // no thread's free waits on the others' queued work
     bt->b.h.resize(nprob);
     const int hw = std::max(1, (int)std::thread::hardware_concurrency());
     const int nworkers = std::max(1, std::min({nprob, 8, std::max(1, hw / 2)}));
     int dev = 0;
     CHRONOS_CUDA(cudaGetDevice(&dev));
-    // runs f(p) for every p of `items` on the worker threads; the first error is rethrown
+    // runs f(p) for every p of `items`, in that order, on the worker threads;
+    // the first error is rethrown
     auto parallel = [&](const std::vector<int> &items, const auto &f) {
       std::atomic<size_t> next{0};
       std::mutex emu;
@@ -116,10 +122,16 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
       for (auto &t : pool) t.join();
       if (err) std::rethrow_exception(err);
     };
+    std::vector<int> largest(nprob);
+    std::iota(largest.begin(), largest.end(), 0);
+    std::stable_sort(largest.begin(), largest.end(), [&](int a, int c) {
+      return iat_h[a][n[a]] > iat_h[c][n[c]];
+    });
     std::vector<std::unique_ptr<HierBuilder>> builders(nprob);
-    std::vector<int> active(nprob);
-    std::iota(active.begin(), active.end(), 0);
-    parallel(active, [&](int p) {
+    std::vector<char> more(nprob, 0);
+    double *wall = bt->b.wall;
+    const double t0 = now_seconds();
+    parallel(largest, [&](int p) {
       HostCSR A;
       A.nrows = A.ncols = n[p];
       A.rp.assign(iat_h[p], iat_h[p] + n[p] + 1);
@@ -129,40 +141,48 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
       // for a .mat without a test space), padded with random columns if ntv > 1
       std::vector<double> ones(n[p], 1.0);
       builders[p] = std::make_unique<HierBuilder>(*prm, A, 1, ones.data());
+      more[p] = builders[p]->begin_level() ? 1 : 0;
     });
-    cudaStream_t bst;
-    CHRONOS_CUDA(cudaStreamCreateWithFlags(&bst, cudaStreamNonBlocking));
-    try {
-      std::vector<char> more(nprob, 0);
-      while (!active.empty()) {
-        parallel(active, [&](int p) {
-          more[p] = builders[p]->begin_level() ? 1 : 0;
-          if (!more[p]) bt->b.h[p] = builders[p]->finish(false);
-        });
-        std::vector<int> next_active;
-        std::vector<FsaiJob> jobs;
-        for (int p : active)
-          if (more[p]) {
-            next_active.push_back(p);
-            jobs.push_back(builders[p]->fsai_job());
-          }
-        if (next_active.empty()) break;
-        const double t0 = now_seconds();
-        const std::vector<int> fl = fsai_numeric_batched(jobs, bst);
-        const double share = (now_seconds() - t0) / (double)jobs.size();
-        std::vector<int> flag_of(nprob, 0);
-        for (size_t k = 0; k < next_active.size(); ++k) {
-          flag_of[next_active[k]] = fl[k];
-          builders[next_active[k]]->add_numeric_time(share);
-        }
-        parallel(next_active, [&](int p) { builders[p]->end_level(flag_of[p]); });
-        active.swap(next_active);
+    const double t1 = now_seconds();
+    std::vector<int> batched;
+    std::vector<FsaiJob> jobs;
+    for (int p : largest)
+      if (more[p]) {
+        batched.push_back(p);
+        jobs.push_back(builders[p]->fsai_job());
       }
-    } catch (...) {
+    std::vector<int> flag_of(nprob, 0);
+    if (!jobs.empty()) {
+      cudaStream_t bst;
+      CHRONOS_CUDA(cudaStreamCreateWithFlags(&bst, cudaStreamNonBlocking));
+      std::vector<int> fl;
+      try {
+        fl = fsai_numeric_batched(jobs, bst);
+      } catch (...) {
+        cudaStreamDestroy(bst);
+        throw;
+      }
       cudaStreamDestroy(bst);
-      throw;
+      const double share = (now_seconds() - t1) / (double)jobs.size();
+      for (size_t k = 0; k < batched.size(); ++k) {
+        flag_of[batched[k]] = fl[k];
+        builders[batched[k]]->add_numeric_time(share);
+      }
     }
-    cudaStreamDestroy(bst);
+    const double t2 = now_seconds();
+    parallel(largest, [&](int p) {
+      HierBuilder &b = *builders[p];
+      if (more[p]) {
+        b.end_level(flag_of[p]);
+        while (b.begin_level()) b.end_level(b.fsai_numeric_single());
+      }
+      bt->b.h[p] = b.finish(false);
+      builders[p].reset();
+    });
+    const double t3 = now_seconds();
+    wall[0] = t1 - t0;
+    wall[1] = t2 - t1;
+    wall[2] = t3 - t2;
     bt->b.order.resize(nprob);
     std::iota(bt->b.order.begin(), bt->b.order.end(), 0);
     std::stable_sort(bt->b.order.begin(), bt->b.order.end(), [&](int a, int c) {
@@ -175,6 +195,8 @@ int chronos_batch_setup(const chronos_params *prm, int nprob, const int *n,
     // path runs each problem's own operators
     if (!bt->b.group)
       for (auto &h : bt->b.h) tune_hierarchy(*h);
+    bt->b.wall[3] = now_seconds() - t3;
+    bt->b.wall[4] = now_seconds() - t0;
     *out = bt.release();
   });
 }
@@ -240,6 +262,13 @@ int chronos_batch_solve(chronos_batch *bt, const double *const *b_h, double *con
     for (auto &e : done) cudaEventDestroy(e);
     cudaStreamDestroy(fork);
     if (seconds) *seconds = ms * 1e-3;
+  });
+}
+
+int chronos_batch_setup_wall(const chronos_batch *bt, double *t5) {
+  return batch_guard([&] {
+    CHRONOS_REQUIRE(bt && t5, CHRONOS_EINVAL, "bad argument");
+    for (int i = 0; i < 5; ++i) t5[i] = bt->b.wall[i];
   });
 }
 

@@ -7,8 +7,10 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "errors.h"
@@ -44,6 +46,46 @@ inline int64_t device_alloc_cap() {
   return cap;
 }
 
+// Deferred frees.  cudaFree waits for all work queued on the device, so
+// while a batch setup builds hierarchies on several host threads, one
+// thread's free of a setup temporary would wait for every other thread's
+// queued kernels.  Inside a DeferFrees scope (any thread) the buffers a DBuf
+// lets go of are kept -- never reused -- and freed when the outermost scope
+// ends, after one device synchronisation.  They stay counted in
+// device_bytes_live() until then.
+struct DeferredFrees {
+  std::mutex mu;
+  std::vector<std::pair<void *, int64_t>> list;
+  std::atomic<int> depth{0};
+};
+inline DeferredFrees &deferred_frees() {
+  static DeferredFrees d;
+  return d;
+}
+inline void flush_deferred_frees() {
+  DeferredFrees &d = deferred_frees();
+  std::vector<std::pair<void *, int64_t>> list;
+  {
+    std::lock_guard<std::mutex> lk(d.mu);
+    list.swap(d.list);
+  }
+  if (list.empty()) return;
+  cudaDeviceSynchronize();
+  for (auto &e : list) {
+    cudaFree(e.first);
+    device_bytes_live() -= e.second;
+  }
+}
+class DeferFrees {
+ public:
+  DeferFrees() { deferred_frees().depth++; }
+  ~DeferFrees() {
+    if (--deferred_frees().depth == 0) flush_deferred_frees();
+  }
+  DeferFrees(const DeferFrees &) = delete;
+  DeferFrees &operator=(const DeferFrees &) = delete;
+};
+
 // Owning device allocation (cudaMalloc / cudaFree), movable, typed.
 template <typename T>
 class DBuf {
@@ -77,8 +119,14 @@ class DBuf {
   }
   void release() {
     if (p_) {
-      cudaFree(p_);
-      device_bytes_live() -= (int64_t)(n_ * sizeof(T));
+      DeferredFrees &d = deferred_frees();
+      if (d.depth.load() > 0) {
+        std::lock_guard<std::mutex> lk(d.mu);
+        d.list.emplace_back(p_, (int64_t)(n_ * sizeof(T)));
+      } else {
+        cudaFree(p_);
+        device_bytes_live() -= (int64_t)(n_ * sizeof(T));
+      }
     }
     p_ = nullptr;
     n_ = 0;

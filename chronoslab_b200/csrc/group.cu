@@ -16,6 +16,9 @@
 //    and the loop -- one conditional CUDA graph -- ends when no problem is
 //    active.  The outer product uses the FP64 operator.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <numeric>
 #include <vector>
@@ -321,32 +324,46 @@ k_group_dense(int nrows, const int *__restrict__ row_prob, const int *__restrict
 // host: stacking and the solve
 // ---------------------------------------------------------------------------
 
-static HostCSR fetch_csr(const DMat &m, cudaStream_t st) {
-  HostCSR h;
-  h.nrows = m.nrows;
-  h.ncols = m.ncols;
-  h.rp.assign(m.rp_h.begin(), m.rp_h.end());
-  h.ci.resize(m.nnz);
-  h.v.resize(m.nnz);
-  if (m.nnz) {
-    m.ci.download(h.ci.data(), m.nnz, st);
-    m.v64.download(h.v.data(), m.nnz, st);
-  }
-  CHRONOS_CUDA(cudaStreamSynchronize(st));
-  return h;
-}
+// One block of a block-diagonal stack: a device matrix, the column offset
+// of its block, and a scale applied to its values.
+struct StackPart {
+  const DMat *m;
+  int coff;
+  double scale;
+};
 
-// Appends B below the rows of S, its columns shifted by coff, values scaled.
-static void append_block(HostCSR &S, const HostCSR &B, int coff, double scale) {
-  if (S.rp.empty()) S.rp.push_back(0);
-  for (int i = 0; i < B.nrows; ++i) {
-    for (int64_t k = B.rp[i]; k < B.rp[i + 1]; ++k) {
-      S.ci.push_back(B.ci[k] + coff);
-      S.v.push_back(B.v[k] * scale);
-    }
-    S.rp.push_back((int64_t)S.ci.size());
+// The blocks stacked row-wise into one host CSR of ncols columns: sizes
+// summed first, every block downloaded straight into its slice, then the
+// column shifts, scales and row pointers applied in one parallel pass.
+static HostCSR stack_blocks(const std::vector<StackPart> &parts, int ncols, cudaStream_t st) {
+  HostCSR S;
+  S.ncols = ncols;
+  S.nrows = 0;
+  std::vector<int64_t> roff(parts.size() + 1, 0), koff(parts.size() + 1, 0);
+  for (size_t b = 0; b < parts.size(); ++b) {
+    roff[b + 1] = roff[b] + parts[b].m->nrows;
+    koff[b + 1] = koff[b] + parts[b].m->nnz;
   }
-  S.nrows += B.nrows;
+  S.nrows = (int)roff.back();
+  S.rp.assign((size_t)S.nrows + 1, 0);
+  S.ci.resize(koff.back());
+  S.v.resize(koff.back());
+  for (size_t b = 0; b < parts.size(); ++b)
+    if (parts[b].m->nnz) {
+      parts[b].m->ci.download(S.ci.data() + koff[b], parts[b].m->nnz, st);
+      parts[b].m->v64.download(S.v.data() + koff[b], parts[b].m->nnz, st);
+    }
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int b = 0; b < (int)parts.size(); ++b) {
+    const StackPart &q = parts[b];
+    for (int64_t k = koff[b]; k < koff[b + 1]; ++k) {
+      S.ci[k] += q.coff;
+      if (q.scale != 1.0) S.v[k] *= q.scale;
+    }
+    for (int i = 0; i < q.m->nrows; ++i) S.rp[roff[b] + i + 1] = koff[b] + q.m->rp_h[i + 1];
+  }
+  return S;
 }
 
 bool group_supported(const std::vector<std::unique_ptr<Hier>> &h) {
@@ -396,7 +413,9 @@ std::unique_ptr<GroupSolve> group_build(const std::vector<std::unique_ptr<Hier>>
     }
     L0.nS = L0.nV = o;
   }
+  const bool verbose = std::getenv("CHRONOS_TUNE_VERBOSE") != nullptr;
   for (int l = 0; l < lmax; ++l) {
+    const auto tl0 = std::chrono::steady_clock::now();
     GroupLevel &L = g.lev[l], &N = g.lev[l + 1];
     N.off.assign(np, -1);
     int o = 0;
@@ -406,25 +425,29 @@ std::unique_ptr<GroupSolve> group_build(const std::vector<std::unique_ptr<Hier>>
     for (int p : L.S)
       if (depth[p] == l + 1) { N.C.push_back(p); N.off[p] = o; o += hs[p]->levels[l + 1].n; }
     N.nV = o;
-    HostCSR A, Gm, Gt, P, Pt;
-    A.ncols = Gm.ncols = Gt.ncols = L.nS;
-    P.ncols = N.nV;
-    Pt.ncols = L.nS;
+    std::vector<StackPart> pa, pg, pgt, pp, ppt;
     for (int p : L.S) {
       const Level &lv = hs[p]->levels[l];
-      append_block(A, fetch_csr(lv.A, st), L.off[p], 1.0);
-      append_block(Gm, fetch_csr(lv.G, st), L.off[p], 1.0);
-      append_block(Gt, fetch_csr(lv.Gt, st), L.off[p], lv.omega);
-      append_block(P, fetch_csr(lv.P, st), N.off[p], 1.0);
+      pa.push_back({&lv.A, L.off[p], 1.0});
+      pg.push_back({&lv.G, L.off[p], 1.0});
+      pgt.push_back({&lv.Gt, L.off[p], lv.omega});
+      pp.push_back({&lv.P, N.off[p], 1.0});
     }
     for (const auto *grp : {&N.S, &N.C})
-      for (int p : *grp) append_block(Pt, fetch_csr(hs[p]->levels[l].Pt, st), L.off[p], 1.0);
-    upload_csr(A, L.A, fp32, st);
-    upload_csr(Gm, L.G, fp32, st);
-    upload_csr(Gt, L.Gt, fp32, st);
-    upload_csr(P, L.P, fp32, st);
-    upload_csr(Pt, L.Pt, fp32, st);
+      for (int p : *grp) ppt.push_back({&hs[p]->levels[l].Pt, L.off[p], 1.0});
+    upload_csr(stack_blocks(pa, L.nS, st), L.A, fp32, st);
+    upload_csr(stack_blocks(pg, L.nS, st), L.G, fp32, st);
+    upload_csr(stack_blocks(pgt, L.nS, st), L.Gt, fp32, st);
+    upload_csr(stack_blocks(pp, N.nV, st), L.P, fp32, st);
+    upload_csr(stack_blocks(ppt, L.nS, st), L.Pt, fp32, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    const auto tl1 = std::chrono::steady_clock::now();
     for (DMat *m : {&L.A, &L.G, &L.Gt, &L.P, &L.Pt}) autotune_lanes(*m, fp32, st, prm.spmv_format);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    if (verbose)
+      std::fprintf(stderr, "chronos group: level %d stacked in %.3f s, tuned in %.3f s\n", l,
+                   std::chrono::duration<double>(tl1 - tl0).count(),
+                   std::chrono::duration<double>(std::chrono::steady_clock::now() - tl1).count());
   }
   for (auto &L : g.lev) {
     const size_t m = (size_t)std::max(L.nV, 1);
@@ -462,11 +485,9 @@ std::unique_ptr<GroupSolve> group_build(const std::vector<std::unique_ptr<Hier>>
   }
   // finest operators of all problems for the outer product (FP64)
   {
-    HostCSR A;
-    A.ncols = g.lev[0].nV;
-    for (int p = 0; p < np; ++p)
-      append_block(A, fetch_csr(hs[p]->levels[0].A, st), g.lev[0].off[p], 1.0);
-    upload_csr(A, g.A0, false, st);
+    std::vector<StackPart> pa;
+    for (int p = 0; p < np; ++p) pa.push_back({&hs[p]->levels[0].A, g.lev[0].off[p], 1.0});
+    upload_csr(stack_blocks(pa, g.lev[0].nV, st), g.A0, false, st);
     autotune_lanes(g.A0, false, st, 1);
   }
   // per-problem rows and blocks of the vector kernels

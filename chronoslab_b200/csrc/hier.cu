@@ -828,10 +828,19 @@ bool gpu_coarsening(const char *soc_type) {
   return on && (t == "DOM" || t == "CLA");
 }
 
+// Adds the duration of a builder call to its active time.
+struct HierBuilder::Active {
+  double &acc;
+  double t0;
+  explicit Active(double &a) : acc(a), t0(now_s()) {}
+  ~Active() { acc += now_s() - t0; }
+};
+
 HierBuilder::HierBuilder(const chronos_params &prm_in, const HostCSR &A0, int ntv0,
                          const double *TV0, const ProlongFn *prolong)
-    : prm_(prm_in), prolong_(prolong), t_start_(now_s()),
+    : prm_(prm_in), prolong_(prolong),
       rng_((uint32_t)(prm_in.seed ? prm_in.seed : 5489)) {
+  Active act(active_);
   const chronos_params &prm = prm_;
   validate_csr(A0);
   std::string smeth(prm.smoother_method), tmeth(prm.tspace_method), ptype(prm.proltype),
@@ -887,6 +896,7 @@ HierBuilder::HierBuilder(const chronos_params &prm_in, const HostCSR &A0, int nt
 HierBuilder::~HierBuilder() = default;
 
 bool HierBuilder::begin_level() {
+  Active act(active_);
   const chronos_params &prm = prm_;
   ++level_;
   Hier &H = *h_;
@@ -949,15 +959,20 @@ FsaiJob HierBuilder::fsai_job() const {
 }
 
 int HierBuilder::fsai_numeric_single() {
+  Active act(active_);
   Level &L = h_->levels.back();
   SetupPhase ph1("chronos setup: fsai numeric", &h_->times[1]);
   return fsai_numeric_device(L.n, L.A.rp, L.A.ci, L.A.v64, L.G.rp, L.G.ci, L.G.v64, rowlen_,
                              h_->st);
 }
 
-void HierBuilder::add_numeric_time(double seconds) { h_->times[1] += seconds; }
+void HierBuilder::add_numeric_time(double seconds) {
+  h_->times[1] += seconds;
+  active_ += seconds;
+}
 
 void HierBuilder::end_level(int fl) {
+  Active act(active_);
   const chronos_params &prm = prm_;
   Hier &H = *h_;
   cudaStream_t st = H.st;
@@ -1115,12 +1130,15 @@ void HierBuilder::end_level(int fl) {
 
 std::unique_ptr<Hier> HierBuilder::finish(bool tune) {
   std::array<double, 12> &T = h_->times;
-  if (tune) {
-    SetupPhase ph10("chronos setup: autotune", &T[10]);
-    tune_hierarchy(*h_);
+  {
+    Active act(active_);
+    if (tune) {
+      SetupPhase ph10("chronos setup: autotune", &T[10]);
+      tune_hierarchy(*h_);
+    }
+    CHRONOS_CUDA(cudaStreamSynchronize(h_->st));
   }
-  CHRONOS_CUDA(cudaStreamSynchronize(h_->st));
-  T[7] = now_s() - t_start_;
+  T[7] = active_;
   double named = 0.0;
   for (int k : {0, 1, 2, 3, 4, 5, 6, 8, 9, 10}) named += T[k];
   T[11] = std::max(0.0, T[7] - named);

@@ -192,9 +192,12 @@ class HierBuilder {
   std::unique_ptr<Hier> finish(bool tune);
 
  private:
+  // time spent inside this builder's calls (its total; waits between calls
+  // of a batch setup are not part of it)
+  double active_ = 0.0;
+  struct Active;
   chronos_params prm_;
   const ProlongFn *prolong_;
-  double t_start_;
   MT19937 rng_;
   std::unique_ptr<Hier> h_;
   bool fp32_ = false;

@@ -440,6 +440,10 @@ int chronos_batch_info(const chronos_batch *b, int p, int *nlevels, int *n0);
 /* The setup phases of chronos_hier_setup_phases summed over the batch's
  * problems (thread time: problems are built several at once). */
 int chronos_batch_setup_phases(const chronos_batch *b, double *t, int n);
+/* The batch setup's wall clock in seconds: [first levels begun (operators,
+ * FSAI patterns), batched FSAI numeric phase of the first levels, the rest of
+ * the hierarchies, tuning and grouping, total]. */
+int chronos_batch_setup_wall(const chronos_batch *b, double *t5);
 int chronos_batch_free(chronos_batch *b);
 
 /* SQMR (SQMR.m) with the V-cycle as left preconditioner and identity right.
