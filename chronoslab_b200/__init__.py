@@ -278,8 +278,11 @@ def coarsen_device(A, prm=None, rng_skip=0):
     return fc.astype(np.int64), nc.value, _CsrHandle.take(h)
 
 
-def bamg(S, fcnode, TV, prm=None):
-    """BAMG prolongation on the host: (P, c_mark)."""
+def bamg(S, fcnode, TV, prm=None, device=False, max_neigh=0):
+    """BAMG prolongation: (P, c_mark) from the host restatement, or with
+    device=True from the GPU (chronos_bamg_device; the same bits; max_neigh
+    caps a GPU thread's neighbourhood, 0 automatic), then (P, c_mark, rows
+    computed on the host)."""
     prm = prm or params()
     S = sp.csr_matrix(S)
     S.sort_indices()
@@ -292,6 +295,11 @@ def bamg(S, fcnode, TV, prm=None):
     tvc = np.ascontiguousarray(TV.T).ravel()      # column-major
     cm = np.zeros(n, np.int32)
     h = C.c_void_p()
+    if device:
+        hr = C.c_int(-1)
+        check(load().chronos_bamg_device(C.byref(prm), n, _pi(ip), _pi(ix), _pi(fc), ntv, _pd(tvc),
+                                         _pi(cm), max_neigh, C.byref(h), C.byref(hr)))
+        return _CsrHandle.take(h), cm, hr.value
     check(load().chronos_bamg(C.byref(prm), n, _pi(ip), _pi(ix), _pi(fc), ntv, _pd(tvc), _pi(cm),
                               C.byref(h)))
     return _CsrHandle.take(h), cm

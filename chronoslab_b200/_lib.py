@@ -103,6 +103,8 @@ SIGNATURES = {
     "chronos_coarsen_device": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _u64, _pi, _pi,
                                _pp],
     "chronos_bamg": [C.POINTER(chronos_params), _i, _pi, _pi, _pi, _i, _pd, _pi, _pp],
+    "chronos_bamg_device": [C.POINTER(chronos_params), _i, _pi, _pi, _pi, _i, _pd, _pi, _i, _pp,
+                            _pi],
     "chronos_fsai_compute": [_i, _i, _i, _d, _d, _i, _i, _i64, _pi64, _pi, _pd, _pi64, _pi64,
                              _pi, _pd, _pi],
     "chronos_fsai_numeric": [_i, _i, _pi64, _pi, _pd, _pi64, _pi, _i, _vp, _pi, _vp],

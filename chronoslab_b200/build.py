@@ -24,7 +24,10 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["setup_kernels.cu", "hier.cu", "block.cu", "batch.cu", "group.cu", "capi.cu",
-              "coarsen_gpu.cu", "gmres.cu"]
+              "coarsen_gpu.cu", "gmres.cu", "bamg_gpu.cu"]
+# per-file flags: the GPU BAMG reproduces the host restatement (built with
+# -ffp-contract=off) bit for bit, so its products and sums are not fused
+CU_EXTRA = {"bamg_gpu.cu": ["-fmad=false"]}
 CPP_SOURCES = ["host/params.cpp", "host/coarsen.cpp", "host/bamg.cpp", "host/fsai_pattern.cpp",
                "host/formats.cpp"]
 HEADERS = ["common.cuh", "errors.h", "internal.h", "hier.h", "group.h", "spmv.cuh", "host/host.h"]
@@ -61,7 +64,7 @@ def build(verbose=False, jobs=None):
         o = os.path.join(BUILD, src.replace("/", "_") + ".o")
         objs.append(o)
         if _newer(o, [s] + hdrs):
-            tasks.append([NVCC] + NVCC_FLAGS + ["-c", s, "-o", o])
+            tasks.append([NVCC] + NVCC_FLAGS + CU_EXTRA.get(src, []) + ["-c", s, "-o", o])
     for src in CPP_SOURCES:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src.replace("/", "_") + ".o")

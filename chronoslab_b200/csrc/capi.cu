@@ -315,9 +315,9 @@ int chronos_coarsen_device(const chronos_params *prm, int n, const int *iat_h, c
   });
 }
 
-int chronos_bamg(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
-                 const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
-                 chronos_csr **P) {
+static int bamg_entry(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
+                      const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
+                      chronos_csr **P, bool device, int *host_rows, int max_neigh) {
   return guard([&] {
     CHRONOS_REQUIRE(prm && iat_S_h && ja_S_h && fcnode_h && TV_h && P && ntv >= 1 && n > 0,
                     CHRONOS_EINVAL, "bad argument");
@@ -340,10 +340,30 @@ int chronos_bamg(const chronos_params *prm, int n, const int *iat_S_h, const int
     BamgParams bp{prm->itmax_vol, prm->dist_min, prm->dist_max, ntv, nth, prm->maxcond,
                   prm->maxrownrm, prm->tol_vol, prm->eps_prol};
     std::vector<int> cm;
-    HostCSR Pm = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, cm);
+    HostCSR Pm;
+    if (device) {
+      ScopedStream ss;
+      Pm = bamg_prolongation_device(bp, S, fc0, nc, TVr.data(), ntv, cm, ss.st, host_rows,
+                                    max_neigh);
+    } else {
+      Pm = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, cm);
+    }
     if (c_mark_h) std::memcpy(c_mark_h, cm.data(), sizeof(int) * n);
     *P = wrap_csr(std::move(Pm));
   });
+}
+
+int chronos_bamg(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
+                 const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
+                 chronos_csr **P) {
+  return bamg_entry(prm, n, iat_S_h, ja_S_h, fcnode_h, ntv, TV_h, c_mark_h, P, false, nullptr, 0);
+}
+
+int chronos_bamg_device(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
+                        const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
+                        int max_neigh, chronos_csr **P, int *host_rows) {
+  return bamg_entry(prm, n, iat_S_h, ja_S_h, fcnode_h, ntv, TV_h, c_mark_h, P, true, host_rows,
+                    max_neigh);
 }
 
 void chronos_params_default(chronos_params *p) {

@@ -818,6 +818,18 @@ static HostCSR smooth_prolongation(const HostCSR &A, const DMat &dA, const HostC
   return Ps;
 }
 
+// Off by default: on C2 (elasticity 80^3) the host restatement on the box's
+// host threads builds the three prolongations in 0.56 s, the GPU in 0.70 s
+// (kernels 0.21, 0.17 and 0.07 s; coarse levels have few rows and large
+// neighbourhoods).
+bool gpu_bamg() {
+  static const bool on = [] {
+    const char *e = std::getenv("CHRONOS_GPU_BAMG");
+    return e && e[0] == '1';
+  }();
+  return on;
+}
+
 bool gpu_coarsening(const char *soc_type) {
   static const bool on = [] {
     const char *e = std::getenv("CHRONOS_GPU_COARSEN");
@@ -1098,7 +1110,9 @@ void HierBuilder::end_level(int fl) {
                 prm.prol_np > 0 ? prm.prol_np : nth, prm.maxcond, prm.maxrownrm, prm.tol_vol,
                 prm.eps_prol};
   std::vector<int> c_mark;
-  Ph = bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
+  Ph = gpu_bamg() && ntv <= 16
+           ? bamg_prolongation_device(bp, S, fc0, nc, TVr.data(), ntv, c_mark, st)
+                  : bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
   if (pemin == "SMOOTH") Ph = smooth_prolongation(Al, L.A, Ph, st);
   std::vector<double> TVn((size_t)nc * ntv);
   for (int j = 0; j < ntv; ++j)

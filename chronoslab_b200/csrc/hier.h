@@ -141,6 +141,17 @@ struct Hier {
   DBuf<double> stage_b, stage_x;    // host-buffer entry points' device staging
 };
 
+// BAMG prolongation with the GPU doing the per-row work (bamg_gpu.cu): the
+// result of bamg_prolongation bit for bit; rows whose neighbourhood outgrows
+// the GPU's per-thread scratch (max_neigh nodes, 0: chosen by the level's
+// size) are computed on the host (their count in *host_rows, may be null).
+HostCSR bamg_prolongation_device(const BamgParams &prm, const HostCSR &S,
+                                 const std::vector<int> &fc, int nc, const double *TV, int ntv,
+                                 std::vector<int> &c_mark, cudaStream_t st,
+                                 int *host_rows = nullptr, int max_neigh = 0);
+// Whether the setup runs BAMG on the GPU: when CHRONOS_GPU_BAMG=1.
+bool gpu_bamg();
+
 // Source of a level's prolongation outside the library: given the 1-based
 // level number and the level's operator (FP64, from the GPU Galerkin product
 // on levels > 1), returns P (n x nc, 0-based CSR, sorted rows).

@@ -233,78 +233,104 @@ int reduce_set(double limit, const BamgParams &p, int inod, int rank, const std:
 
 }  // namespace
 
+namespace {
+
+// One fine row (BAMG.cpp:119-225): neighbourhood rings, fit, set reduction.
+// Appends the row's columns and values; returns its c_mark.
+int bamg_row(const BamgParams &p, const HostCSR &S, const std::vector<int> &fc, const double *TV,
+             int ntv, int inod, RowWork &wk, std::vector<int> &cols, std::vector<double> &vals) {
+  const int mmax = p.mmax;
+  int cmark = 0;
+  wk.neigh.assign(1, inod);
+  wk.mark[inod] = 1;
+  int b = 0, e = 1, distance = 0;
+  while (distance < p.dist_min) {
+    ++distance;
+    add_ring(S, b, e, wk.neigh, wk.mark);
+    if ((int)wk.neigh.size() == e) break;
+    b = e;
+    e = (int)wk.neigh.size();
+  }
+  const double bnorm = dnrm2(ntv, TV + (size_t)inod * ntv);
+  const double res_ass = p.eps * bnorm;
+  double res_row = 0.0, row_nrm = 0.0;
+  int rank = 0;
+  bool more = true;
+  while (more) {
+    bool has_cand;
+    rank = fit_row(mmax, p, inod, fc, TV, ntv, wk, &res_row, &row_nrm, &has_cand);
+    if (row_nrm < p.maxrownrm && (res_row < res_ass || rank == ntv)) {
+      more = false;
+    } else if (distance < p.dist_max) {
+      ++distance;
+      const int before = (int)wk.neigh.size();
+      add_ring(S, b, e, wk.neigh, wk.mark);
+      if ((int)wk.neigh.size() == before) {
+        more = false;
+        if (!has_cand) {
+          cmark = 1;
+        } else {
+          if (row_nrm > kRelaxFac * p.maxrownrm)
+            rank = reduce_set(kRelaxFac * p.maxrownrm, p, inod, rank, fc, TV, ntv, wk, &row_nrm);
+          res_row = rank == 0 ? bnorm : dnrm2(ntv - rank, wk.coef.data() + rank);
+          if (!(res_row < res_ass)) cmark = 1;
+        }
+      }
+      b = e;
+      e = (int)wk.neigh.size();
+    } else {
+      more = false;
+      if (row_nrm > kRelaxFac * p.maxrownrm)
+        rank = reduce_set(kRelaxFac * p.maxrownrm, p, inod, rank, fc, TV, ntv, wk, &row_nrm);
+      res_row = rank == 0 ? bnorm : dnrm2(ntv - rank, wk.coef.data() + rank);
+      if (res_row > res_ass) cmark = 1;
+    }
+  }
+  for (int k = 0; k < rank; ++k) {
+    if (wk.coef[k] == 0.0) continue;              // explicit zeros are dropped
+    cols.push_back(fc[wk.int_list[k]]);
+    vals.push_back(wk.coef[k]);
+  }
+  for (int v : wk.neigh) wk.mark[v] = 0;
+  return cmark;
+}
+
+}  // namespace
+
+void bamg_rows_host(const BamgParams &p, const HostCSR &S, const std::vector<int> &fc,
+                    const double *TV, int ntv, const std::vector<int> &rows,
+                    std::vector<std::vector<int>> &rcols, std::vector<std::vector<double>> &rvals,
+                    std::vector<int> &c_mark) {
+  const int n = S.nrows;
+#pragma omp parallel num_threads(p.nthreads)
+  {
+    RowWork wk;
+    wk.mark.assign(n, 0);
+#pragma omp for schedule(dynamic, 32)
+    for (int r = 0; r < (int)rows.size(); ++r) {
+      const int inod = rows[r];
+      rcols[inod].clear();
+      rvals[inod].clear();
+      if (fc[inod] >= 0) {
+        rcols[inod].assign(1, fc[inod]);
+        rvals[inod].assign(1, 1.0);
+        c_mark[inod] = 0;
+        continue;
+      }
+      c_mark[inod] = bamg_row(p, S, fc, TV, ntv, inod, wk, rcols[inod], rvals[inod]);
+    }
+  }
+}
+
 HostCSR bamg_prolongation(const BamgParams &p, const HostCSR &S, const std::vector<int> &fc,
                           int nc, const double *TV, int ntv, std::vector<int> &c_mark) {
   const int n = S.nrows;
   c_mark.assign(n, 0);
   std::vector<std::vector<int>> rcols(n);
   std::vector<std::vector<double>> rvals(n);
-  const int mmax = p.mmax;
-
-#pragma omp parallel num_threads(p.nthreads)
-  {
-    RowWork wk;
-    wk.mark.assign(n, 0);
-#pragma omp for schedule(dynamic, 32)
-    for (int inod = 0; inod < n; ++inod) {
-      if (fc[inod] >= 0) {
-        rcols[inod].assign(1, fc[inod]);
-        rvals[inod].assign(1, 1.0);
-        continue;
-      }
-      wk.neigh.assign(1, inod);
-      wk.mark[inod] = 1;
-      int b = 0, e = 1, distance = 0;
-      while (distance < p.dist_min) {
-        ++distance;
-        add_ring(S, b, e, wk.neigh, wk.mark);
-        if ((int)wk.neigh.size() == e) break;
-        b = e;
-        e = (int)wk.neigh.size();
-      }
-      const double bnorm = dnrm2(ntv, TV + (size_t)inod * ntv);
-      const double res_ass = p.eps * bnorm;
-      double res_row = 0.0, row_nrm = 0.0;
-      int rank = 0;
-      bool more = true;
-      while (more) {
-        bool has_cand;
-        rank = fit_row(mmax, p, inod, fc, TV, ntv, wk, &res_row, &row_nrm, &has_cand);
-        if (row_nrm < p.maxrownrm && (res_row < res_ass || rank == ntv)) {
-          more = false;
-        } else if (distance < p.dist_max) {
-          ++distance;
-          const int before = (int)wk.neigh.size();
-          add_ring(S, b, e, wk.neigh, wk.mark);
-          if ((int)wk.neigh.size() == before) {
-            more = false;
-            if (!has_cand) {
-              c_mark[inod] = 1;
-            } else {
-              if (row_nrm > kRelaxFac * p.maxrownrm)
-                rank = reduce_set(kRelaxFac * p.maxrownrm, p, inod, rank, fc, TV, ntv, wk, &row_nrm);
-              res_row = rank == 0 ? bnorm : dnrm2(ntv - rank, wk.coef.data() + rank);
-              if (!(res_row < res_ass)) c_mark[inod] = 1;
-            }
-          }
-          b = e;
-          e = (int)wk.neigh.size();
-        } else {
-          more = false;
-          if (row_nrm > kRelaxFac * p.maxrownrm)
-            rank = reduce_set(kRelaxFac * p.maxrownrm, p, inod, rank, fc, TV, ntv, wk, &row_nrm);
-          res_row = rank == 0 ? bnorm : dnrm2(ntv - rank, wk.coef.data() + rank);
-          if (res_row > res_ass) c_mark[inod] = 1;
-        }
-      }
-      for (int k = 0; k < rank; ++k) {
-        if (wk.coef[k] == 0.0) continue;              // explicit zeros are dropped
-        rcols[inod].push_back(fc[wk.int_list[k]]);
-        rvals[inod].push_back(wk.coef[k]);
-      }
-      for (int v : wk.neigh) wk.mark[v] = 0;
-    }
-  }
+  std::vector<int> rows(n);
+  for (int i = 0; i < n; ++i) rows[i] = i;
+  bamg_rows_host(p, S, fc, TV, ntv, rows, rcols, rvals, c_mark);
   HostCSR P;
   P.nrows = n;
   P.ncols = nc;

@@ -56,6 +56,12 @@ struct BamgParams {
 // to the requested accuracy.
 HostCSR bamg_prolongation(const BamgParams &prm, const HostCSR &S, const std::vector<int> &fc,
                           int nc, const double *TV, int ntv, std::vector<int> &c_mark);
+// The rows `rows` of the same prolongation: rcols[i], rvals[i] and c_mark[i]
+// (sized n by the caller) for each listed row i.
+void bamg_rows_host(const BamgParams &prm, const HostCSR &S, const std::vector<int> &fc,
+                    const double *TV, int ntv, const std::vector<int> &rows,
+                    std::vector<std::vector<int>> &rcols, std::vector<std::vector<double>> &rvals,
+                    std::vector<int> &c_mark);
 
 // ---- adaptive FSAI pattern search (cpt_afsai_coef.cpp) ----------------------
 // Rows of G hold their strictly-lower columns ascending, then the diagonal.

@@ -252,6 +252,18 @@ int chronos_coarsen_device(const chronos_params *prm, int n, const int *iat_h, c
 int chronos_bamg(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
                  const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
                  chronos_csr **P);
+/* The same prolongation with the per-row work on the GPU (one thread per fine
+ * row: neighbourhood rings, maximum-volume selection, least-squares fit, set
+ * reduction; MEX_BAMG_Prol/BAMG.cpp:119-225): P and c_mark equal chronos_bamg's
+ * bit for bit (at most 16 test vectors).  Each thread's scratch holds up to
+ * max_neigh neighbourhood nodes (a power of two in [16, 8192]; 0: 512 to 8192,
+ * from a 2 GiB budget and the number of rows); a row whose neighbourhood
+ * outgrows it is computed on the host, their count going to host_rows (may
+ * be NULL).  The hierarchy setup builds BAMG prolongations this way when
+ * CHRONOS_GPU_BAMG=1. */
+int chronos_bamg_device(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
+                        const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
+                        int max_neigh, chronos_csr **P, int *host_rows);
 
 /* ---- Galerkin product P'*(A*P) on the GPU (0-based CSR, FP64) --------- */
 typedef struct chronos_galerkin_plan chronos_galerkin_plan;
