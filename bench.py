@@ -439,6 +439,25 @@ def run_product(args, world, rank, local):
         one_ms = (time.perf_counter() - t) * 1e3 * ito / k1
         cpu["one_core"] = {"value": one_ms, "unit": "ms", "cores": 1,
                            "sample": f"{k1} PCG_CJ iterations on one thread, scaled to {ito}"}
+        # Iteration parity on the reference's own prolongation (a check, not
+        # timed): the CPU path built with the reference's FSAI/BAMG C++, and
+        # the GPU hierarchy built on that path's P level by level, beside the
+        # GPU hierarchy on this library's own coarsening and BAMG.
+        if O.ref_available():
+            H = CO.reference_hierarchy(A, TV, O.default_params())
+            _, itr, _, flr = CO.CHierarchy(H, threads=threads).pcg(b, itmax=args.itmax,
+                                                                   tol=args.tol)
+            Ps = [lv.P for lv in H.levels[:-1]]
+            on_ref = {}
+            for prec, name in ((cb.CHRONOS_FP64, "fp64"), (cb.CHRONOS_FP32, "fp32")):
+                with cb.Hierarchy.with_prolongation(A, Ps, cb.params(precision=prec)) as hp:
+                    _, itp, _, flp, _ = hp.pcg(b, itmax=args.itmax, tol=args.tol)
+                on_ref[name] = itp if flp == 0 else None
+            cpu["iteration_parity"] = {
+                "reference_path": itr if flr == 0 else None,
+                "gpu_on_reference_prolongation": on_ref,
+                "gpu_own_coarsening_and_bamg": {"fp32": it32[-1], "fp64": it64[-1]},
+                "levels_reference_path": [lv.A.shape[0] for lv in H.levels]}
 
     launches = (prof["kernels_per_iteration"] * it32[-1] + prof["kernels_per_solve"]) * args.steps \
         + (prof64["kernels_per_iteration"] * it64[-1] + prof64["kernels_per_solve"]) * args.steps \
