@@ -18,12 +18,18 @@ run here: no MATLAB/Octave), following the reference files line by line:
   cpt_SoC_dom/cla   sources/Preconditioner/AMG/coarsen/cpt_SoC_{dom,cla}.m
   cpt_PMIS          sources/Preconditioner/AMG/coarsen/cpt_PMIS.m:1-102
   cpt_ProlMEX_BAMG  sources/Preconditioner/AMG/prolong/cpt_ProlMEX_BAMG.m:1-72
+  EMIN              sources/Preconditioner/AMG/prolong/prolong.m:207-235 with
+                    EMIN/MEX_EMIN/MEX_cptProlPatt.cpp (pattern) and
+                    EMIN/Cpp_EMIN/EMIN_matfree.cpp, DEFL_PCG_matfree.cpp,
+                    gather_B_QR.cpp, KP_spmat.cpp, Orth_Q.cpp (energy minimisation)
   computeAMG        sources/utils/computeAMG.m:1-51
   mk_rbm_3d         sources/utils/mk_rbm_3d.m:1-27
 
 The reference's own C++ kernels are used through oracle/_ref (built by
 oracle/Makefile from the unmodified reference sources): compute_local_fsai
-(FSAI) and BAMG (prolongation).  MATLAB built-ins are replaced by their
+(FSAI), BAMG (prolongation), and the EMIN pattern and energy minimisation;
+the EMIN restatement here (emin_pattern, emin_enhance) is checked against
+the latter.  MATLAB built-ins are replaced by their
 published counterparts: sparse products by scipy (Gustavson, exact zeros
 dropped as MATLAB does), chol by numpy's LAPACK Cholesky, eigs by ARPACK
 (scipy.sparse.linalg.eigsh), rand after rng(0) by MT19937 seeded 5489 with
@@ -90,7 +96,11 @@ def read_params(fnames_path):
                     "itmax_Vol": int(float(pro[3])), "tol_Vol": float(pro[4]),
                     "dist_min": int(float(pro[5])), "dist_max": int(float(pro[6])),
                     "maxcond": float(pro[7]), "maxrownrm": float(pro[8]),
-                    "eps_prol": float(pro[9]), "updateCF": int(float(pro[10]))},
+                    "eps_prol": float(pro[9]), "updateCF": int(float(pro[10])),
+                    "patt_pow": int(float(pro[11])), "patt_tau": float(pro[12]),
+                    "nnzr_max": int(float(pro[13])), "itmax_emin": int(float(pro[14])),
+                    "energ_tol": float(pro[15]), "condmax_emin": float(pro[16]),
+                    "prec_emin": int(float(pro[17])), "solv_emin": int(float(pro[18]))},
         "filter": {"np": int(float(fil[0])), "filt_wgt": float(fil[1]),
                    "filt_tol": float(fil[2]), "filt_tau": float(fil[3]),
                    "min_patt": int(float(fil[4]))},
@@ -112,7 +122,9 @@ def default_params(nthread=None):
         "coarsen": {"SoC_type": "DOM", "tau": 0.01, "nl_agg": 0},
         "prolong": {"proltype": "BAMG", "prol_emin": "NONE", "np": nthread,
                     "itmax_Vol": 100, "tol_Vol": 0.01, "dist_min": 1, "dist_max": 10,
-                    "maxcond": 1e13, "maxrownrm": 5.0, "eps_prol": 1e-10, "updateCF": 0},
+                    "maxcond": 1e13, "maxrownrm": 5.0, "eps_prol": 1e-10, "updateCF": 0,
+                    "patt_pow": 2, "patt_tau": 0.01, "nnzr_max": 30, "itmax_emin": 10,
+                    "energ_tol": 1e-3, "condmax_emin": 1e10, "prec_emin": 1, "solv_emin": 4},
         "filter": {"np": nthread, "filt_wgt": 170.0, "filt_tol": 0.1, "filt_tau": 0.0,
                    "min_patt": 0},
         "general": {"ascii_input": False, "rhs_build": "unit_rhs", "symmetric": True,
@@ -183,7 +195,8 @@ def _ref_lib(name):
 
 
 def ref_available():
-    return all(os.path.exists(os.path.join(REF_DIR, f"libref_{n}.so")) for n in ("fsai", "bamg"))
+    return all(os.path.exists(os.path.join(REF_DIR, f"libref_{n}.so"))
+               for n in ("fsai", "bamg", "emin"))
 
 
 def _ptr(a, ctype):
@@ -260,6 +273,87 @@ def ref_bamg(prm, nc, fcnode, S, TV):
     P.eliminate_zeros()      # the MEX gateway skips explicit zeros (gateway :131-137)
     P.sort_indices()
     return P, c_mark
+
+
+class _RefCsr(ctypes.Structure):
+    _fields_ = [("nrows", ctypes.c_int), ("ncols", ctypes.c_int), ("nnz", ctypes.c_int),
+                ("rp", ctypes.POINTER(ctypes.c_int)), ("ci", ctypes.POINTER(ctypes.c_int)),
+                ("v", ctypes.POINTER(ctypes.c_double))]
+
+
+def _csr32(M):
+    M = sp.csr_matrix(M)
+    M.sort_indices()
+    return (M, M.indptr.astype(np.int32), M.indices.astype(np.int32),
+            np.ascontiguousarray(M.data, dtype=np.float64))
+
+
+def _take_ref_csr(lib, res):
+    m, nnz = res.nrows, res.nnz
+    rp = np.ctypeslib.as_array(res.rp, shape=(m + 1,)).astype(np.int64).copy()
+    ci = np.ctypeslib.as_array(res.ci, shape=(max(nnz, 1),))[:nnz].astype(np.int64).copy()
+    v = np.ctypeslib.as_array(res.v, shape=(max(nnz, 1),))[:nnz].copy()
+    shape = (m, res.ncols)
+    lib.ref_csr_free(ctypes.byref(res))
+    return sp.csr_matrix((v, ci, rp), shape=shape)
+
+
+def _fc_c(fcnode):
+    """MATLAB fcnode (coarse index + 1 > 0, fine < 0) -> the C++ convention of
+    MEX_EMIN_enhance_prol.m:73 (coarse index >= 0, fine < 0)."""
+    return np.where(np.asarray(fcnode) > 0, np.asarray(fcnode) - 1, -1).astype(np.int32)
+
+
+def ref_emin_pattern(kpow, S, P, fcnode, nnzr, nnzr_min, np_threads=1):
+    """MEX_cptProlPatt (the reference's C++, oracle/_ref) as prolong.m:222 calls
+    it; fcnode in MATLAB's convention.  Returns the n x nc pattern (CSR with the
+    values the MEX returns: 1 on P's own entries, S*P's on the added ones)."""
+    S, sr, sc, sv = _csr32(S)
+    P, pr_, pc, pv = _csr32(P)
+    n, nc = P.shape
+    fc = _fc_c(fcnode)
+    res = _RefCsr()
+    lib = _ref_lib("emin")
+    rc = lib.ref_emin_pattern(ctypes.c_int(kpow), ctypes.c_int(n), ctypes.c_int(nc),
+                              _ptr(sr, ctypes.c_int), _ptr(sc, ctypes.c_int),
+                              _ptr(sv, ctypes.c_double), _ptr(pr_, ctypes.c_int),
+                              _ptr(pc, ctypes.c_int), _ptr(pv, ctypes.c_double),
+                              _ptr(fc, ctypes.c_int), ctypes.c_int(nnzr), ctypes.c_int(nnzr_min),
+                              ctypes.c_int(np_threads), ctypes.byref(res))
+    if rc != 0:
+        raise RuntimeError("reference MEX_cptProlPatt raised an error")
+    return _take_ref_csr(lib, res)
+
+
+def ref_emin(prm, A, Ppatt, P, TV, fcnode, spd=True):
+    """EMIN_ImpProl (the reference's C++, oracle/_ref) with the arguments of
+    MEX_EMIN_enhance_prol.m:29-98; fcnode in MATLAB's convention.  Returns
+    (P, info) with P's exact zeros dropped as sparse() does there (:102)."""
+    A, ar, ac, av = _csr32(A)
+    P, pr_, pc, pv = _csr32(P)
+    Pp, tr, tc, _ = _csr32(Ppatt)
+    n, nc = P.shape
+    TVr = np.ascontiguousarray(TV, dtype=np.float64)
+    fc = _fc_c(fcnode)
+    res = _RefCsr()
+    info = np.zeros(12)
+    lib = _ref_lib("emin")
+    ierr = lib.ref_emin(ctypes.c_int(prm["np"]), ctypes.c_int(prm["itmax_emin"]),
+                        ctypes.c_double(prm["energ_tol"]), ctypes.c_double(prm["condmax_emin"]),
+                        ctypes.c_int(prm["prec_emin"]), ctypes.c_int(prm["solv_emin"]),
+                        ctypes.c_int(n), ctypes.c_int(nc), ctypes.c_int(TVr.shape[1]),
+                        _ptr(fc, ctypes.c_int), ctypes.c_int(1 if spd else 0),
+                        _ptr(ar, ctypes.c_int), _ptr(ac, ctypes.c_int), _ptr(av, ctypes.c_double),
+                        _ptr(pr_, ctypes.c_int), _ptr(pc, ctypes.c_int), _ptr(pv, ctypes.c_double),
+                        _ptr(tr, ctypes.c_int), _ptr(tc, ctypes.c_int),
+                        _ptr(TVr, ctypes.c_double), ctypes.byref(res),
+                        _ptr(info, ctypes.c_double))
+    if ierr != 0:
+        raise RuntimeError(f"reference EMIN failed with code {ierr}")
+    Pout = _take_ref_csr(lib, res)
+    Pout.eliminate_zeros()
+    Pout.sort_indices()
+    return Pout, info
 
 
 # ----------------------------------------------------------------------------
@@ -504,6 +598,8 @@ def cpt_aspamg(param, A, TV0, rng=None, on_level=None):
         emin = param["prolong"].get("prol_emin", "NONE").upper()
         if emin == "SMOOTH":
             P = smooth_prolongation(A, P)
+        elif emin == "EMIN":
+            P = emin_reference(param, A, S, P, TV, fcnode)
         elif emin != "NONE":
             raise NotImplementedError("prolongation post-process " + emin)
         TV = TV[clist, :]
@@ -515,6 +611,23 @@ def cpt_aspamg(param, A, TV0, rng=None, on_level=None):
             on_level(level, lev)
         A = Ac
     return hier
+
+
+def emin_reference(param, A, S, P, TV, fcnode):
+    """prolong.m:207-235 with the reference's own C++ (oracle/_ref): S_emin is
+    the coarsening's S when it is DOM with tau = patt_tau, else
+    cpt_SoC_dom(patt_tau, A); Ppatt = MEX_cptProlPatt(patt_pow, S_emin, P,
+    fcnode, nnzr_max, ntv, np); P = MEX_EMIN_enhance_prol(...)."""
+    pro, coa = param["prolong"], param["coarsen"]
+    if coa["SoC_type"].upper() == "DOM" and coa["tau"] == pro["patt_tau"]:
+        S_emin = S
+    else:
+        S_emin = soc_dom(pro["patt_tau"], A)
+    ntv = np.asarray(TV).shape[1]
+    Ppatt = ref_emin_pattern(pro["patt_pow"], S_emin, P, fcnode, pro["nnzr_max"], ntv,
+                             pro["np"])
+    Pe, _ = ref_emin(pro, A, Ppatt, P, TV, fcnode)
+    return Pe
 
 
 def hierarchy_from_parts(parts, nupre=1, nupost=1):
@@ -860,6 +973,216 @@ def smooth_prolongation(A, P, tol=1e-3):
     Ps.eliminate_zeros()
     Ps.sort_indices()
     return Ps
+
+
+def emin_pattern(kpow, S, P, fcnode, nnzr_max, nnzr_min):
+    """MEX_cptProlPatt.cpp:234-490 restated (prolong.m:222 passes kpow =
+    patt_pow, nnzr_min = ntv).  fcnode in MATLAB's convention.  Each power
+    step lists, per row i, the columns of (S * P_cur)(i, :) outside P's own
+    row in first-seen order (S's row order, then P_cur's), with values summed
+    in that order; keeps the nonzero ones; when there are more than the budget
+    nnzr - |P(i,:)|, keeps the budget's worth of largest |value| (ties: lower
+    column first); adds P's own columns with value 1; sorts by column.  Coarse
+    rows are empty after the last step.  kpow <= 1 keeps P's fine rows."""
+    P0 = sp.csr_matrix(P)
+    P0.sort_indices()
+    S = sp.csr_matrix(S)
+    S.sort_indices()
+    n, nc = P0.shape
+    fcnode = np.asarray(fcnode)
+    nnzr = max(nnzr_max, nnzr_min)
+    if kpow <= 1:
+        keep = np.repeat(fcnode <= 0, np.diff(P0.indptr))
+        rows = np.repeat(np.arange(n), np.diff(P0.indptr))[keep]
+        return sp.csr_matrix((P0.data[keep], (rows, P0.indices[keep])), shape=(n, nc))
+    Pc = P0
+    for ipow in range(2, kpow + 1):
+        last = ipow == kpow
+        indptr, cols, vals = [0], [], []
+        for i in range(n):
+            if last and fcnode[i] > 0:
+                indptr.append(len(cols))
+                continue
+            own = P0.indices[P0.indptr[i]:P0.indptr[i + 1]]
+            budget = max(0, nnzr - own.size)
+            if budget == 0:
+                cols.extend(own.tolist())
+                vals.extend([1.0] * own.size)
+                indptr.append(len(cols))
+                continue
+            own_set = set(own.tolist())
+            acc = {}
+            for ks in range(S.indptr[i], S.indptr[i + 1]):
+                j, sij = S.indices[ks], S.data[ks]
+                for kp in range(Pc.indptr[j], Pc.indptr[j + 1]):
+                    c = int(Pc.indices[kp])
+                    if c in own_set:
+                        continue
+                    if c in acc:
+                        acc[c] = acc[c] + sij * Pc.data[kp]
+                    else:
+                        acc[c] = sij * Pc.data[kp]
+            cand = [(c, v) for c, v in acc.items() if v != 0.0]
+            if len(cand) > budget:
+                cand = sorted(cand, key=lambda cv: (-abs(cv[1]), cv[0]))[:budget]
+            cand += [(int(c), 1.0) for c in own]
+            cand.sort(key=lambda cv: cv[0])
+            cols.extend(c for c, _ in cand)
+            vals.extend(v for _, v in cand)
+            indptr.append(len(cols))
+        Pc = sp.csr_matrix((np.array(vals, dtype=np.float64), np.array(cols, dtype=np.int64),
+                            np.array(indptr, dtype=np.int64)), shape=(n, nc))
+    return Pc
+
+
+def _orth_q(Q, nr, x):
+    """Orth_Q.cpp:6-74 for one row block: x - Q (Q' x)."""
+    return x - Q @ (Q.T @ x)
+
+
+def emin_enhance(prm, A, Ppatt, P, TV, fcnode):
+    """EMIN_matfree.cpp:69-308 with solv_emin = 4 (SPMAT), prec_emin = 1
+    (Jacobi) and an SPD A, restated.  fcnode in MATLAB's convention; Ppatt's
+    coarse rows are empty (MEX_cptProlPatt).  Unknowns are P's fine-row
+    entries on the pattern, row-major.  Steps:
+
+      copy_Prol.cpp:7-53       P0 = P on the pattern (zero where P has none)
+      gather_B_QR.cpp:33-587   per fine row i with pattern columns c_1..c_m,
+                               B = TV(coarse nodes c_k, :) (m x ntv);
+                               g = TV(i,:)' - B' p0; m > ntv and
+                               max|R_kk|/min|R_kk| <= condmax: Householder QR,
+                               p0 += Q R^-T g, keep Q; otherwise thin SVD,
+                               rank = 1 + #{k >= 1: s_0 < condmax |s_k|}
+                               (0 if s_0 <= 1e-15), p0 += U_r S_r^-1 V_r' g,
+                               keep [U_r, 0]
+      gather_f.cpp:1-50        f(i,c) = -A(c, i) on the pattern
+      cpt_Trace_Acc.cpp:4-18   Tr_A = sum of A's diagonal over coarse nodes
+      load_Jacobi.cpp:4-21     D(i,c) = 1/A(i,i) (1 when |A(i,i)| <= 1e-15)
+      KP_spmat.cpp:11-73       K x = (A X)|pattern, X = x on the fine rows
+      DEFL_PCG_matfree.cpp     projected PCG on K d = K p0 - f, projector
+                               I - Q Q' per row, Jacobi preconditioner, at
+                               most itmax_emin steps, stop when the step's
+                               energy decrease falls below energ_tol times
+                               the first step's; P = P0 - d
+      Prol_add_Cnodes.cpp      coarse rows: identity entries
+
+    Returns (P n x nc with exact zeros dropped, iterations)."""
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    Pp = sp.csr_matrix(Ppatt)
+    Pp.sort_indices()
+    Pin = sp.csr_matrix(P)
+    Pin.sort_indices()
+    n, nc = Pin.shape
+    TV = np.asarray(TV, dtype=np.float64)
+    ntv = TV.shape[1]
+    fcnode = np.asarray(fcnode)
+    coarse = fcnode > 0
+    c2glo = np.flatnonzero(coarse)[np.argsort(fcnode[coarse])]
+    rp, ci = Pp.indptr, Pp.indices
+    nt = int(rp[n])
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    # copy_Prol
+    p0 = np.zeros(nt)
+    for i in np.flatnonzero(~coarse):
+        pos = {int(c): k for k, c in enumerate(ci[rp[i]:rp[i + 1]], start=rp[i])}
+        for k in range(Pin.indptr[i], Pin.indptr[i + 1]):
+            kk = pos.get(int(Pin.indices[k]))
+            if kk is not None:
+                p0[kk] = Pin.data[k]
+    # gather_B_QR
+    condmax = prm["condmax_emin"]
+    Qs = {}
+    for i in np.flatnonzero(~coarse):
+        a, b = rp[i], rp[i + 1]
+        m = b - a
+        if m == 0:
+            continue
+        B = TV[c2glo[ci[a:b]], :]
+        g = TV[i, :] - B.T @ p0[a:b]
+        done = False
+        if m > ntv:
+            Q, R = np.linalg.qr(B, mode="reduced")
+            d = np.abs(np.diag(R))
+            if not d.max() / d.min() > condmax:
+                y = scipy.linalg.solve_triangular(R, g, trans="T", lower=False)
+                p0[a:b] += Q @ y
+                Qs[i] = Q
+                done = True
+        if not done:
+            U, sv, Vt = np.linalg.svd(B, full_matrices=False)
+            r = 0
+            if sv[0] > 1e-15:
+                r = 1
+                if m > 1:
+                    while sv[0] < condmax * abs(sv[r]):
+                        r += 1
+                        if r == min(ntv, m):
+                            break
+            if r > 0:
+                w = (Vt[:r, :] @ g) / sv[:r]
+                p0[a:b] += U[:, :r] @ w
+            Q = np.zeros((m, ntv))
+            Q[:, :r] = U[:, :r]
+            Qs[i] = Q
+
+    def orth(x):
+        y = x.copy()
+        for i, Q in Qs.items():
+            a, b = rp[i], rp[i + 1]
+            y[a:b] = _orth_q(Q, b - a, x[a:b])
+        return y
+
+    # gather_f (A symmetric: A(c, i) = A(i, c))
+    Ad = A.toarray() if n <= 20000 else None
+    if Ad is not None:
+        f = -Ad[c2glo[ci], rows] if nt else np.zeros(0)
+    else:
+        f = -np.asarray(A[c2glo[ci], rows]).ravel()
+    dA = A.diagonal()
+    tr_a = float(dA[coarse].sum())
+    dinv = np.where(np.abs(dA) > 1e-15, 1.0 / np.where(dA == 0, 1.0, dA), 1.0)[rows]
+
+    def kp(x):
+        X = sp.csr_matrix((x, ci, rp), shape=(n, nc))
+        C = (A @ X).tocsr()
+        return np.asarray(C[rows, ci]).ravel() if nt else np.zeros(0)
+
+    v = kp(p0)
+    init_energy = tr_a + p0 @ v - 2.0 * (p0 @ f)
+    res = orth(v - f)
+    dp = np.zeros(nt)
+    it = 0
+    itmax, en_tol = prm["itmax_emin"], prm["energ_tol"]
+    exit_test = itmax <= 0 or np.linalg.norm(res) < 1e-15
+    gamma_old, pvec, de0 = 0.0, None, 1.0
+    while not exit_test:
+        it += 1
+        z = orth(dinv * res)
+        gamma = res @ z
+        pvec = z.copy() if it == 1 else z + (gamma / gamma_old) * pvec
+        gamma_old = gamma
+        qkp = orth(kp(pvec))
+        denom = qkp @ pvec
+        if abs(denom) < 1e-18:
+            break
+        dek = gamma * gamma / denom
+        alpha = gamma / denom
+        dp += alpha * pvec
+        res -= alpha * qkp
+        if it == 1:
+            de0 = dek
+        exit_test = it == itmax or dek / de0 < en_tol
+    del init_energy
+    pf = p0 - dp
+    # Prol_add_Cnodes + sparse(): coarse rows -> identity, exact zeros dropped
+    r_out = np.concatenate([rows, c2glo])
+    c_out = np.concatenate([ci, np.arange(nc)])
+    v_out = np.concatenate([pf, np.ones(nc)])
+    Pout = sp.csr_matrix((v_out, (r_out, c_out)), shape=(n, nc))
+    Pout.eliminate_zeros()
+    Pout.sort_indices()
+    return Pout, it
 
 
 def lmax_eigs(A, tol=1e-3, maxiter=3):

@@ -19,7 +19,10 @@ Writes, next to this script:
                      TV = qr(TV0) and Tests/parm_PROLONG settings.
   small_ref.npz      the reference FSAI on small Poisson (8^3) and Q1
                      elasticity (4^3 elements) matrices.
-  cubo_ref.json      reference-pinned and oracle iteration counts.
+  cubo_ref.json      reference-pinned and oracle iteration counts (also with
+                     the Jacobi-smoothed and the energy-minimised
+                     prolongations; the EMIN keys come from emin_counts,
+                     which can be rerun alone: make_golden.py --emin).
 """
 from __future__ import annotations
 
@@ -101,7 +104,8 @@ def main(ref_root):
     Mvs = lambda r: O.amg_vcycle(Hs, r, 0, Af)
     _, info_s, relres_s, niter_s, _ = O.sqmr(lambda v: A @ v, rhs, 1e-6, 100, Mvs)
     _, it_s, _, _ = O.pcg_cj(Mvs, lambda v: Af @ v, rhs, np.zeros_like(rhs), 1000, 1e-8)
-    info_out = {
+    info_out = emin_counts(A, Af, TV0)
+    info_out.update({
         "reference_sqmr_iterations_smooth": 29,
         "reference_sqmr_source_smooth": "Tests/CubeBAMG_SMOOTH.m:3 (tolerance max(5%, 2))",
         "oracle_sqmr_iterations_smooth": int(niter_s),
@@ -116,13 +120,57 @@ def main(ref_root):
         "nnz_G_level1": int(G.nnz),
         "nc_level1": int(clist.size),
         "diag_fix": float(fixval),
-    }
+    })
     with open(os.path.join(HERE, "cubo_ref.json"), "w") as f:
         json.dump(info_out, f, indent=1)
     print(json.dumps(info_out, indent=1))
 
 
+def emin_counts(A, Af, TV0):
+    """Energy-minimised prolongation (prolong.m:207-235, the reference's EMIN
+    C++ from oracle/_ref) on Cubo_4820, as Tests/CubeBAMG_EMIN.m runs it."""
+    prm = O.default_params(8)
+    prm["prolong"]["prol_emin"] = "EMIN"
+    H = O.cpt_aspamg(prm, Af, TV0)
+    Mv = lambda r: O.amg_vcycle(H, r, 0, Af)
+    rhs = np.ones(A.shape[0])
+    _, info, relres, niter, _ = O.sqmr(lambda v: A @ v, rhs, 1e-6, 100, Mv)
+    _, it, _, _ = O.pcg_cj(Mv, lambda v: Af @ v, rhs, np.zeros_like(rhs), 1000, 1e-8)
+    return {
+        "reference_sqmr_iterations_emin": 20,
+        "reference_sqmr_source_emin": "Tests/CubeBAMG_EMIN.m:3 (tolerance max(5%, 2), :34)",
+        "oracle_sqmr_iterations_emin": int(niter),
+        "oracle_pcg_iterations_1e-8_emin": int(it),
+        "levels_emin": [int(L.A.shape[0]) for L in H.levels],
+    }
+
+
+def update_emin_counts():
+    """Adds the EMIN keys to an existing cubo_ref.json (the other fixtures
+    are left as they are)."""
+    z = np.load(os.path.join(HERE, "cubo_A_upper.npz"))
+    n = int(z["n"])
+    U = sp.csr_matrix((z["data"], z["indices"], z["indptr"]), shape=(n, n))
+    A = (U + sp.triu(U, 1).T).tocsr()
+    A.sort_indices()
+    Af = A.copy()
+    d = Af.diagonal()
+    d[d == 1.0] = float(z["diag_fix"])
+    Af.setdiag(d)
+    Af.sort_indices()
+    path = os.path.join(HERE, "cubo_ref.json")
+    with open(path) as f:
+        info = json.load(f)
+    info.update(emin_counts(A, Af, z["TV0"]))
+    with open(path, "w") as f:
+        json.dump(info, f, indent=1)
+    print(json.dumps(info, indent=1))
+
+
 if __name__ == "__main__":
+    if sys.argv[1:] == ["--emin"]:
+        update_emin_counts()
+        sys.exit(0)
     from oracle.refdir import reference_dir
     ref = sys.argv[1] if len(sys.argv) > 1 else reference_dir()
     if not ref:
