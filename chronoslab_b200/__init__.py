@@ -26,7 +26,8 @@ __all__ = [
     "CHRONOS_FP32", "CHRONOS_FP64", "ChronosError", "Hierarchy", "Batch", "params",
     "readDefaultParams",
     "cpt_aspAMG", "AMG_Vcycle", "PCG_CJ", "SQMR", "SYM_aFSAI_compute", "afsai_cpp",
-    "fsai_numeric", "fsai_pattern", "coarsen", "bamg", "galerkin", "dense_chol", "spmv",
+    "fsai_numeric", "fsai_pattern", "coarsen", "bamg", "emin_pattern", "emin", "galerkin",
+    "dense_chol", "spmv",
     "diag_fix", "version",
 ]
 
@@ -303,6 +304,63 @@ def bamg(S, fcnode, TV, prm=None, device=False, max_neigh=0):
     check(load().chronos_bamg(C.byref(prm), n, _pi(ip), _pi(ix), _pi(fc), ntv, _pd(tvc), _pi(cm),
                               C.byref(h)))
     return _CsrHandle.take(h), cm
+
+
+def emin_pattern(S, P, fcnode, kpow=2, nnzr_max=30, nnzr_min=None):
+    """EMIN prolongation pattern on the GPU (chronos_emin_pattern; replaces
+    MEX_cptProlPatt as prolong.m:222 calls it).  S: strength matrix with
+    values, P: n x nc prolongation, fcnode as coarsen returns it; nnzr_min
+    defaults to ntv as prolong.m passes it (give it explicitly).  Returns
+    (pattern n x nc with the MEX's values, rows computed on the host)."""
+    S = sp.csr_matrix(S)
+    S.sort_indices()
+    P = sp.csr_matrix(P)
+    P.sort_indices()
+    n, nc = P.shape
+    if S.shape != (n, n) or np.size(fcnode) != n:
+        raise ValueError("S must be n x n and fcnode of length n")
+    if nnzr_min is None:
+        raise ValueError("nnzr_min (the number of test vectors) is required")
+    fc = np.ascontiguousarray(fcnode, dtype=np.int32)
+    si, sx, sv = (S.indptr.astype(np.int32), S.indices.astype(np.int32),
+                  np.ascontiguousarray(S.data, np.float64))
+    pi, px, pv = (P.indptr.astype(np.int32), P.indices.astype(np.int32),
+                  np.ascontiguousarray(P.data, np.float64))
+    h = C.c_void_p()
+    hr = C.c_int(0)
+    check(load().chronos_emin_pattern(kpow, n, nc, _pi(si), _pi(sx), _pd(sv), _pi(pi), _pi(px),
+                                      _pd(pv), _pi(fc), nnzr_max, nnzr_min, C.byref(h),
+                                      C.byref(hr)))
+    return _CsrHandle.take(h), hr.value
+
+
+def emin(A, P, pattern, fcnode, TV, prm=None, spd=True):
+    """Energy minimisation of P on the pattern on the GPU (chronos_emin;
+    replaces EMIN_Prolong_compute / EMIN_ImpProl, matrix-free path, Jacobi,
+    SPD).  Returns (P n x nc, info[12]): info[7] CG iterations, info[6] rows
+    whose constraint block took the SVD branch."""
+    prm = prm or params()
+    n, ip, ix, dv = _csr(A)
+    P = sp.csr_matrix(P)
+    P.sort_indices()
+    nc = P.shape[1]
+    T = sp.csr_matrix(pattern)
+    T.sort_indices()
+    if P.shape[0] != n or T.shape != P.shape or np.size(fcnode) != n:
+        raise ValueError("P and the pattern must be n x nc, fcnode of length n")
+    TV = np.asarray(TV, dtype=np.float64).reshape(n, -1)
+    ntv = TV.shape[1]
+    tvc = np.ascontiguousarray(TV.T).ravel()           # column-major
+    fc = np.ascontiguousarray(fcnode, dtype=np.int32)
+    pi, px, pv = (P.indptr.astype(np.int32), P.indices.astype(np.int32),
+                  np.ascontiguousarray(P.data, np.float64))
+    ti, tx = T.indptr.astype(np.int32), T.indices.astype(np.int32)
+    info = np.zeros(12)
+    h = C.c_void_p()
+    check(load().chronos_emin(C.byref(prm), n, _pi(ip), _pi(ix), _pd(dv), nc, _pi(pi), _pi(px),
+                              _pd(pv), _pi(ti), _pi(tx), _pi(fc), ntv, _pd(tvc),
+                              1 if spd else 0, C.byref(h), _pd(info)))
+    return _CsrHandle.take(h), info
 
 
 def galerkin(A, P):

@@ -36,6 +36,9 @@ class chronos_params(C.Structure):
         ("itmax_vol", C.c_int), ("tol_vol", C.c_double), ("dist_min", C.c_int),
         ("dist_max", C.c_int), ("maxcond", C.c_double), ("maxrownrm", C.c_double),
         ("eps_prol", C.c_double), ("updateCF", C.c_int),
+        ("patt_pow", C.c_int), ("patt_tau", C.c_double), ("nnzr_max", C.c_int),
+        ("itmax_emin", C.c_int), ("energ_tol", C.c_double), ("condmax_emin", C.c_double),
+        ("prec_emin", C.c_int), ("solv_emin", C.c_int),
         ("filt_np", C.c_int), ("filt_wgt", C.c_double), ("filt_tol", C.c_double),
         ("filt_tau", C.c_double), ("min_patt", C.c_int),
         ("ascii_input", C.c_int), ("rhs_build", C.c_char * 16), ("symmetric", C.c_int),
@@ -105,6 +108,9 @@ SIGNATURES = {
     "chronos_bamg": [C.POINTER(chronos_params), _i, _pi, _pi, _pi, _i, _pd, _pi, _pp],
     "chronos_bamg_device": [C.POINTER(chronos_params), _i, _pi, _pi, _pi, _i, _pd, _pi, _i, _pp,
                             _pi],
+    "chronos_emin_pattern": [_i, _i, _i, _pi, _pi, _pd, _pi, _pi, _pd, _pi, _i, _i, _pp, _pi],
+    "chronos_emin": [C.POINTER(chronos_params), _i, _pi, _pi, _pd, _i, _pi, _pi, _pd, _pi, _pi,
+                     _pi, _i, _pd, _i, _pp, _pd],
     "chronos_fsai_compute": [_i, _i, _i, _d, _d, _i, _i, _i64, _pi64, _pi, _pd, _pi64, _pi64,
                              _pi, _pd, _pi],
     "chronos_fsai_numeric": [_i, _i, _pi64, _pi, _pd, _pi64, _pi, _i, _vp, _pi, _vp],

@@ -24,12 +24,12 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["setup_kernels.cu", "hier.cu", "block.cu", "batch.cu", "group.cu", "capi.cu",
-              "coarsen_gpu.cu", "gmres.cu", "bamg_gpu.cu"]
+              "coarsen_gpu.cu", "gmres.cu", "bamg_gpu.cu", "emin_gpu.cu"]
 # per-file flags: the GPU BAMG reproduces the host restatement (built with
 # -ffp-contract=off) bit for bit, so its products and sums are not fused
 CU_EXTRA = {"bamg_gpu.cu": ["-fmad=false"]}
 CPP_SOURCES = ["host/params.cpp", "host/coarsen.cpp", "host/bamg.cpp", "host/fsai_pattern.cpp",
-               "host/formats.cpp"]
+               "host/formats.cpp", "host/emin.cpp"]
 HEADERS = ["common.cuh", "errors.h", "internal.h", "hier.h", "group.h", "spmv.cuh", "host/host.h"]
 
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]

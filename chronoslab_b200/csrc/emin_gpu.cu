@@ -1,0 +1,915 @@
+// Energy-minimised prolongation (prolong.m:207-235, prol_emin = EMIN) on the
+// GPU: the pattern of MEX_EMIN/MEX_cptProlPatt.cpp and the energy
+// minimisation of Cpp_EMIN/EMIN_matfree.cpp with solv_emin = 4 (products
+// with A on the stored pattern), prec_emin = 1 (Jacobi) and an SPD A.
+//
+// Unknowns are the entries of P's fine rows on the pattern, row-major (the
+// pattern has no coarse rows; coarse rows of P are unit rows).  Layout in HBM:
+// the pattern (rp, ci; int32) and one FP64 value per pattern entry for each
+// vector of the projected CG (p0, f, D^-1, residual, z, search direction,
+// K p, correction), and the orthonormal constraint bases Q, one m x ntv
+// column-major block per fine row of m pattern entries, at offset
+// ntv * rp[i] -- the reference's mat_Q layout.
+//
+// Kernels:
+//  * k_emin_pattern: a warp per row; candidate columns of (S P)(i, :) in a
+//    per-warp shared-memory table, summed in S's row order one S entry per
+//    step (each column gets its contributions in the reference's order, the
+//    products and sums rounded on their own: bit-identical); selection of the
+//    budget's largest by rank counting; output by column.  S comes as a CSR
+//    with values or is computed on the fly from A as DOM strength
+//    |a_ij| / sqrt(a_ii a_jj) > tau (cpt_SoC_dom.m:26-47).  Rows whose
+//    candidate count could outgrow the table go to emin_pattern_row (host).
+//  * k_emin_constraints: a thread per fine row; gathers B = TV(coarse nodes
+//    of the row, :), corrects p0 so that B' p0 = TV(i, :)' and leaves the
+//    orthonormal basis of range(B) in Q -- Householder QR when m > ntv and
+//    max|R_kk| / min|R_kk| <= condmax, else a one-sided Jacobi SVD with the
+//    reference's rank rule (gather_B_QR.cpp:183-454).
+//  * k_emin_kp: a warp per fine row; (A X)(i, c) for the row's pattern
+//    columns, X the unknowns on the pattern, summed in A's row order
+//    (KP_spmat.cpp:11-73's order; products and sums rounded on their own).
+//  * k_emin_orth: a warp per fine row; y = x - Q (Q' x) (Orth_Q.cpp) with
+//    the optional Jacobi scaling before it and a dot product after it
+//    (per-block partial sums, added on the host in block order).
+//  * k_emin_xpby, k_emin_step, k_emin_sub: the CG's vector updates.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "hier.h"
+#include "internal.h"
+
+namespace chronos {
+
+namespace {
+
+constexpr int kEminMaxTv = 16;          // test vectors
+constexpr int kPattMaxTable = 4096;     // slots of a warp's candidate table
+constexpr int kEminWarps = 4;           // warps per block of the warp-per-row kernels
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ unsigned col_hash(int c) { return (unsigned)c * 2654435761u; }
+
+// Whether c is among the n ascending columns at p.
+__device__ __forceinline__ bool has_col(const int *__restrict__ p, int n, int c) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const int v = __ldg(p + mid);
+    if (v < c) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < n && __ldg(p + lo) == c;
+}
+
+// Columns among the n ascending ones at p that are smaller than c.
+__device__ __forceinline__ int count_below(const int *__restrict__ p, int n, int c) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(p + mid) < c) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// One power step of the pattern for rows [0, n).  Row i is written at
+// out_off[i] (capacity max(nnzr, |P0(i,:)|)); out_len[i] = its length, or -1
+// when it is left to the host (candidate bound above table / 2).
+template <bool FROM_A>
+__global__ void __launch_bounds__(32 * kEminWarps)
+k_emin_pattern(int n, const int *__restrict__ srp, const int *__restrict__ sci,
+               const double *__restrict__ sv, const double *__restrict__ diag, double tau,
+               const int *__restrict__ crp, const int *__restrict__ cci,
+               const double *__restrict__ cv, const int *__restrict__ p0rp,
+               const int *__restrict__ p0ci, const int *__restrict__ fc, int nnzr, int last,
+               int table, const int64_t *__restrict__ out_off, int *__restrict__ out_ci,
+               double *__restrict__ out_v, int *__restrict__ out_len) {
+  extern __shared__ double emin_smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  // per warp: vals[table], cval[table/2] (doubles), keys[table], ccol[table/2]
+  // (ints), keep[table/2] (chars)
+  const size_t per_warp = (size_t)table * 8 + (size_t)table / 2 * 8 + (size_t)table * 4 +
+                          (size_t)table / 2 * 4 + (size_t)table / 2;
+  const size_t per_warp_al = (per_warp + 15) & ~(size_t)15;
+  char *base = reinterpret_cast<char *>(emin_smem) + per_warp_al * wib;
+  double *vals = reinterpret_cast<double *>(base);
+  double *cval = vals + table;
+  int *keys = reinterpret_cast<int *>(cval + table / 2);
+  int *ccol = keys + table;
+  char *keep = reinterpret_cast<char *>(ccol + table / 2);
+  const int half = table / 2;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = gwarp; i < n; i += nwarps) {
+    const int s0 = __ldg(p0rp + i), n0 = __ldg(p0rp + i + 1) - s0;
+    const int budget = max(0, nnzr - n0);
+    int *oc = out_ci + out_off[i];
+    double *ov = out_v + out_off[i];
+    if (last && __ldg(fc + i) >= 0) {
+      if (lane == 0) out_len[i] = 0;
+      continue;
+    }
+    if (budget == 0) {
+      for (int k = lane; k < n0; k += 32) {
+        oc[k] = __ldg(p0ci + s0 + k);
+        ov[k] = 1.0;
+      }
+      if (lane == 0) out_len[i] = n0;
+      continue;
+    }
+    // bound on the candidates: the entries of Pc in the rows S(i, :) can reach
+    int bound = 0;
+    const int sb = __ldg(srp + i), se = __ldg(srp + i + 1);
+    for (int k = sb + lane; k < se; k += 32) {
+      const int j = __ldg(sci + k);
+      bound += __ldg(crp + j + 1) - __ldg(crp + j);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bound += __shfl_xor_sync(kFull, bound, o);
+    if (bound > half) {
+      if (lane == 0) out_len[i] = -1;
+      continue;
+    }
+    // this row's table: at least twice its candidate bound
+    int tb = 64;
+    while (tb < 2 * bound) tb <<= 1;
+    const unsigned rmask = (unsigned)tb - 1u;
+    for (int s = lane; s < tb; s += 32) keys[s] = -1;
+    __syncwarp();
+    const double di = FROM_A ? __ldg(diag + i) : 0.0;
+    for (int ks = sb; ks < se; ++ks) {
+      const int j = __ldg(sci + ks);
+      double sij = __ldg(sv + ks);
+      if (FROM_A) {
+        // cpt_SoC_dom.m:26-47: S keeps s_ij unless s_ij <= tau
+        sij = __ddiv_rn(fabs(sij), __dsqrt_rn(__dmul_rn(di, __ldg(diag + j))));
+        if (sij <= tau) continue;                      // the same for every lane
+      }
+      const int cb = __ldg(crp + j), ce = __ldg(crp + j + 1);
+      for (int kp = cb + lane; kp < ce; kp += 32) {
+        const int c = __ldg(cci + kp);
+        if (has_col(p0ci + s0, n0, c)) continue;
+        const double t = __dmul_rn(sij, __ldg(cv + kp));
+        unsigned h = col_hash(c) & rmask;
+        while (true) {                                 // ends: fewer keys than slots
+          const int prev = atomicCAS(&keys[h], -1, c);
+          if (prev == -1) { vals[h] = t; break; }
+          if (prev == c) { vals[h] = __dadd_rn(vals[h], t); break; }
+          h = (h + 1) & rmask;
+        }
+      }
+      __syncwarp();
+    }
+    __syncwarp();
+    // nonzero candidates, compacted
+    int ncand = 0;
+    for (int s0_ = 0; s0_ < tb; s0_ += 32) {
+      const int s = s0_ + lane;
+      const bool is = keys[s] >= 0 && vals[s] != 0.0;
+      const unsigned b = __ballot_sync(kFull, is);
+      if (is) {
+        const int p = ncand + __popc(b & ((1u << lane) - 1u));
+        ccol[p] = keys[s];
+        cval[p] = vals[s];
+      }
+      ncand += __popc(b);
+    }
+    __syncwarp();
+    // the budget's largest magnitudes, ties to the lower column
+    for (int p = lane; p < ncand; p += 32) {
+      char k = 1;
+      if (ncand > budget) {
+        const double ap = fabs(cval[p]);
+        const int cp = ccol[p];
+        int beat = 0;
+        for (int q = 0; q < ncand; ++q) {
+          const double aq = fabs(cval[q]);
+          beat += (aq > ap) || (aq == ap && ccol[q] < cp);
+        }
+        k = beat < budget;
+      }
+      keep[p] = k;
+    }
+    __syncwarp();
+    for (int p = lane; p < ncand; p += 32) {
+      if (!keep[p]) continue;
+      const int c = ccol[p];
+      int pos = count_below(p0ci + s0, n0, c);
+      for (int q = 0; q < ncand; ++q) pos += keep[q] && ccol[q] < c;
+      oc[pos] = c;
+      ov[pos] = cval[p];
+    }
+    for (int k = lane; k < n0; k += 32) {
+      const int c = __ldg(p0ci + s0 + k);
+      int pos = k;
+      for (int q = 0; q < ncand; ++q) pos += keep[q] && ccol[q] < c;
+      oc[pos] = c;
+      ov[pos] = 1.0;
+    }
+    if (lane == 0) out_len[i] = n0 + min(ncand, budget);
+    __syncwarp();
+  }
+}
+
+// ---- energy minimisation ----------------------------------------------------
+
+// copy_Prol.cpp:7-53: p0 = P on the pattern of the fine rows (0 elsewhere).
+__global__ void k_emin_copy_prol(int n, const int *__restrict__ fc, const int *__restrict__ prp,
+                                 const int *__restrict__ pci, const double *__restrict__ pv,
+                                 const int *__restrict__ trp, const int *__restrict__ tci,
+                                 double *__restrict__ p0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int a = trp[i], b = trp[i + 1];
+  for (int k = a; k < b; ++k) p0[k] = 0.0;
+  if (fc[i] >= 0) return;
+  int jj = a;
+  for (int ii = prp[i]; ii < prp[i + 1]; ++ii) {
+    const int c = pci[ii];
+    while (jj < b && tci[jj] < c) ++jj;
+    if (jj < b && tci[jj] == c) {
+      p0[jj] = pv[ii];
+      ++jj;
+    }
+  }
+}
+
+// Householder QR of the m x nt column-major block B (m > nt), as LAPACK's
+// dgeqr2: R on and above the diagonal, the reflectors below, tau[k].
+__device__ void emin_qr(double *B, int m, int nt, double *tau) {
+  for (int k = 0; k < nt; ++k) {
+    double *col = B + (size_t)k * m;
+    double xn = 0.0;
+    for (int r = k + 1; r < m; ++r) xn += col[r] * col[r];
+    xn = sqrt(xn);
+    const double alpha = col[k];
+    if (xn == 0.0) {
+      tau[k] = 0.0;
+      continue;
+    }
+    const double beta = -copysign(hypot(alpha, xn), alpha);
+    tau[k] = (beta - alpha) / beta;
+    const double sc = 1.0 / (alpha - beta);
+    for (int r = k + 1; r < m; ++r) col[r] *= sc;
+    col[k] = beta;
+    for (int j = k + 1; j < nt; ++j) {
+      double *cj = B + (size_t)j * m;
+      double w = cj[k];
+      for (int r = k + 1; r < m; ++r) w += col[r] * cj[r];
+      w *= tau[k];
+      cj[k] -= w;
+      for (int r = k + 1; r < m; ++r) cj[r] -= w * col[r];
+    }
+  }
+}
+
+// The explicit Q of emin_qr's reflectors, in place (LAPACK's dorg2r).
+__device__ void emin_form_q(double *B, int m, int nt, const double *tau) {
+  for (int k = nt - 1; k >= 0; --k) {
+    double *col = B + (size_t)k * m;
+    for (int j = k + 1; j < nt; ++j) {
+      double *cj = B + (size_t)j * m;
+      double w = cj[k];
+      for (int r = k + 1; r < m; ++r) w += col[r] * cj[r];
+      w *= tau[k];
+      cj[k] -= w;
+      for (int r = k + 1; r < m; ++r) cj[r] -= w * col[r];
+    }
+    for (int r = k + 1; r < m; ++r) col[r] *= -tau[k];
+    col[k] = 1.0 - tau[k];
+    for (int r = 0; r < k; ++r) col[r] = 0.0;
+  }
+}
+
+// One-sided Jacobi SVD of the m x nt column-major block W: on return W's
+// columns are u_k s_k and V (nt x nt, column-major) the right singular
+// vectors, columns sorted by s_k descending (s[k] = s_k).
+__device__ void emin_jacobi_svd(double *W, int m, int nt, double *V, double *s) {
+  for (int a = 0; a < nt; ++a)
+    for (int b = 0; b < nt; ++b) V[a + b * nt] = a == b ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    bool rotated = false;
+    for (int p = 0; p < nt - 1; ++p)
+      for (int q = p + 1; q < nt; ++q) {
+        double *wp = W + (size_t)p * m, *wq = W + (size_t)q * m;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (int r = 0; r < m; ++r) {
+          al += wp[r] * wp[r];
+          be += wq[r] * wq[r];
+          ga += wp[r] * wq[r];
+        }
+        if (ga == 0.0 || !(fabs(ga) > 1e-15 * sqrt(al * be))) continue;
+        rotated = true;
+        const double zeta = (be - al) / (2.0 * ga);
+        const double t = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
+        for (int r = 0; r < m; ++r) {
+          const double x = wp[r], y = wq[r];
+          wp[r] = c * x - sn * y;
+          wq[r] = sn * x + c * y;
+        }
+        for (int r = 0; r < nt; ++r) {
+          const double x = V[r + p * nt], y = V[r + q * nt];
+          V[r + p * nt] = c * x - sn * y;
+          V[r + q * nt] = sn * x + c * y;
+        }
+      }
+    if (!rotated) break;
+  }
+  for (int k = 0; k < nt; ++k) {
+    double a = 0.0;
+    for (int r = 0; r < m; ++r) a += W[(size_t)k * m + r] * W[(size_t)k * m + r];
+    s[k] = sqrt(a);
+  }
+  for (int k = 0; k < nt; ++k) {                     // selection sort, columns swapped along
+    int best = k;
+    for (int j = k + 1; j < nt; ++j)
+      if (s[j] > s[best]) best = j;
+    if (best == k) continue;
+    const double t = s[k];
+    s[k] = s[best];
+    s[best] = t;
+    for (int r = 0; r < m; ++r) {
+      const double x = W[(size_t)k * m + r];
+      W[(size_t)k * m + r] = W[(size_t)best * m + r];
+      W[(size_t)best * m + r] = x;
+    }
+    for (int r = 0; r < nt; ++r) {
+      const double x = V[r + k * nt];
+      V[r + k * nt] = V[r + best * nt];
+      V[r + best * nt] = x;
+    }
+  }
+}
+
+// gather_B_QR.cpp:183-454 for each fine row: the constraint block, the
+// correction of p0 and the basis Q.  svd_rows counts the rows that took the
+// SVD branch.
+__global__ void k_emin_constraints(int n, int nt, double condmax, const int *__restrict__ trp,
+                                   const int *__restrict__ tci, const int *__restrict__ fc,
+                                   const int *__restrict__ c2glo, const double *__restrict__ TV,
+                                   double *__restrict__ Q, double *__restrict__ p0,
+                                   int *__restrict__ svd_rows) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || fc[i] >= 0) return;
+  const int a = trp[i], m = trp[i + 1] - a;
+  if (m == 0) return;
+  double *B = Q + (size_t)a * nt;
+  auto load_b = [&] {
+    for (int r = 0; r < m; ++r) {
+      const double *tv = TV + (size_t)c2glo[tci[a + r]] * nt;
+      for (int k = 0; k < nt; ++k) B[(size_t)k * m + r] = tv[k];
+    }
+  };
+  load_b();
+  double g[kEminMaxTv];
+  for (int k = 0; k < nt; ++k) {
+    double s = 0.0;
+    for (int r = 0; r < m; ++r) s += B[(size_t)k * m + r] * p0[a + r];
+    g[k] = TV[(size_t)i * nt + k] - s;
+  }
+  if (m > nt) {
+    double tau[kEminMaxTv];
+    emin_qr(B, m, nt, tau);
+    double dmax = 0.0, dmin = 1.7976931348623157e308;
+    for (int k = 0; k < nt; ++k) {
+      const double d = fabs(B[(size_t)k * m + k]);
+      dmax = fmax(dmax, d);
+      dmin = fmin(dmin, d);
+    }
+    if (!(dmax / dmin > condmax)) {
+      double y[kEminMaxTv];
+      for (int k = 0; k < nt; ++k) {                 // R' y = g
+        double s = g[k];
+        for (int l = 0; l < k; ++l) s -= B[(size_t)k * m + l] * y[l];
+        y[k] = s / B[(size_t)k * m + k];
+      }
+      emin_form_q(B, m, nt, tau);
+      for (int r = 0; r < m; ++r) {
+        double s = 0.0;
+        for (int k = 0; k < nt; ++k) s += B[(size_t)k * m + r] * y[k];
+        p0[a + r] += s;
+      }
+      return;
+    }
+    load_b();
+  }
+  atomicAdd(svd_rows, 1);
+  double V[kEminMaxTv * kEminMaxTv], sg[kEminMaxTv];
+  emin_jacobi_svd(B, m, nt, V, sg);
+  const int kmin = min(m, nt);
+  int rank = 0;
+  if (sg[0] > 1e-15) {
+    rank = 1;
+    if (m > 1)
+      while (rank < kmin && sg[0] < condmax * fabs(sg[rank])) {
+        ++rank;
+        if (rank == kmin) break;
+      }
+  }
+  for (int k = 0; k < rank; ++k) {
+    double w = 0.0;
+    for (int l = 0; l < nt; ++l) w += V[l + k * nt] * g[l];
+    w /= sg[k];
+    const double inv = 1.0 / sg[k];
+    double *u = B + (size_t)k * m;
+    for (int r = 0; r < m; ++r) {
+      u[r] *= inv;
+      p0[a + r] += u[r] * w;
+    }
+  }
+  for (int k = rank; k < nt; ++k)
+    for (int r = 0; r < m; ++r) B[(size_t)k * m + r] = 0.0;
+}
+
+// gather_f.cpp (f(i,c) = -A(c2glo[c], i) on the pattern, 0 where A has no
+// entry) and load_Jacobi.cpp (D^-1(i,c) = 1 / a_ii, 1 when |a_ii| <= 1e-15).
+__global__ void k_emin_f_dinv(int n, const int *__restrict__ arp, const int *__restrict__ aci,
+                              const double *__restrict__ av, const int *__restrict__ trp,
+                              const int *__restrict__ tci, const int *__restrict__ c2glo,
+                              double *__restrict__ f, double *__restrict__ dinv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int a = trp[i], b = trp[i + 1];
+  if (a == b) return;
+  const int ab = arp[i], ae = arp[i + 1];
+  const int dpos = ab + count_below(aci + ab, ae - ab, i);
+  const double d = (dpos < ae && aci[dpos] == i) ? av[dpos] : 0.0;
+  const double inv = (dpos < ae && aci[dpos] == i && fabs(d) > 1e-15) ? 1.0 / d : 1.0;
+  for (int k = a; k < b; ++k) {
+    const int r = c2glo[tci[k]];
+    const int rb = arp[r], re = arp[r + 1];
+    const int p = rb + count_below(aci + rb, re - rb, i);
+    f[k] = (p < re && aci[p] == i) ? -av[p] : 0.0;
+    dinv[k] = inv;
+  }
+}
+
+// KP_spmat.cpp:11-73: y(i, c) = sum_j a_ij x(j, c) over the pattern columns
+// c of fine row i, x on the pattern (coarse rows have none).
+__global__ void __launch_bounds__(32 * kEminWarps)
+k_emin_kp(int n, const int *__restrict__ arp, const int *__restrict__ aci,
+          const double *__restrict__ av, const int *__restrict__ trp,
+          const int *__restrict__ tci, const double *__restrict__ x, double *__restrict__ y,
+          int mmax, int hslots) {
+  extern __shared__ double emin_smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double *acc = emin_smem + (size_t)wib * (mmax + hslots);
+  int *hk = reinterpret_cast<int *>(acc + mmax);          // keys, then positions
+  int *hp = hk + hslots;
+  const unsigned mask = (unsigned)hslots - 1u;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = gwarp; i < n; i += nwarps) {
+    const int a = __ldg(trp + i), m = __ldg(trp + i + 1) - a;
+    if (m == 0) continue;
+    for (int s = lane; s < hslots; s += 32) hk[s] = -1;
+    __syncwarp();
+    for (int r = lane; r < m; r += 32) {
+      const int c = __ldg(tci + a + r);
+      unsigned h = col_hash(c) & mask;
+      while (atomicCAS(&hk[h], -1, c) != -1) h = (h + 1) & mask;   // columns distinct
+      hp[h] = r;
+      acc[r] = 0.0;
+    }
+    __syncwarp();
+    const int ab = __ldg(arp + i), ae = __ldg(arp + i + 1);
+    for (int ka = ab; ka < ae; ++ka) {
+      const int j = __ldg(aci + ka);
+      const int b = __ldg(trp + j), e = __ldg(trp + j + 1);
+      if (b == e) continue;                               // coarse row: no unknowns
+      const double aij = __ldg(av + ka);
+      for (int kk = b + lane; kk < e; kk += 32) {
+        const int c = __ldg(tci + kk);
+        unsigned h = col_hash(c) & mask;
+        int key;
+        while ((key = hk[h]) != c && key != -1) h = (h + 1) & mask;
+        if (key == c) {
+          const int r = hp[h];
+          acc[r] = __dadd_rn(acc[r], __dmul_rn(aij, __ldg(x + kk)));
+        }
+      }
+      __syncwarp();
+    }
+    for (int r = lane; r < m; r += 32) y[a + r] = acc[r];
+    __syncwarp();
+  }
+}
+
+// y = (I - Q Q') u per fine row (Orth_Q.cpp:6-74), u = x - sub (sub may be
+// null) scaled by d (may be null); part[block] = sum over the block's rows of
+// y . w (w may be null: no dot; w == y allowed).
+__global__ void __launch_bounds__(32 * kEminWarps)
+k_emin_orth(int n, int nt, const int *__restrict__ trp, const double *__restrict__ Q,
+            const double *x, const double *__restrict__ sub, const double *__restrict__ d,
+            double *y, const double *w, double *__restrict__ part) {
+  __shared__ double red[32];
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  double dacc = 0.0;
+  for (int i = gwarp; i < n; i += nwarps) {
+    const int a = __ldg(trp + i), m = __ldg(trp + i + 1) - a;
+    if (m == 0) continue;
+    const double *q = Q + (size_t)a * nt;
+    double t[kEminMaxTv];
+    for (int k = 0; k < nt; ++k) {
+      double s = 0.0;
+      for (int r = lane; r < m; r += 32) {
+        double u = x[a + r];
+        if (sub) u -= sub[a + r];
+        if (d) u *= d[a + r];
+        s += q[(size_t)k * m + r] * u;
+      }
+      t[k] = warp_sum(s);
+    }
+    for (int r = lane; r < m; r += 32) {
+      double u = x[a + r];
+      if (sub) u -= sub[a + r];
+      if (d) u *= d[a + r];
+      double s = 0.0;
+      for (int k = 0; k < nt; ++k) s += q[(size_t)k * m + r] * t[k];
+      const double v = u - s;
+      y[a + r] = v;
+      if (w) dacc += v * w[a + r];
+    }
+  }
+  if (part) {
+    const double b = block_sum(dacc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = b;
+  }
+}
+
+// y = x + beta y (beta_zero: y = x).
+__global__ void k_emin_xpby(int64_t nt, const double *__restrict__ x, double beta, int beta_zero,
+                            double *__restrict__ y) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nt;
+       k += (int64_t)gridDim.x * blockDim.x)
+    y[k] = beta_zero ? x[k] : x[k] + beta * y[k];
+}
+
+// dp += alpha p; res -= alpha kp.
+__global__ void k_emin_step(int64_t nt, double alpha, const double *__restrict__ p,
+                            const double *__restrict__ kp, double *__restrict__ dp,
+                            double *__restrict__ res) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nt;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    dp[k] += alpha * p[k];
+    res[k] -= alpha * kp[k];
+  }
+}
+
+// out = a - b.
+__global__ void k_emin_sub(int64_t nt, const double *__restrict__ a, const double *__restrict__ b,
+                           double *__restrict__ out) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nt;
+       k += (int64_t)gridDim.x * blockDim.x)
+    out[k] = a[k] - b[k];
+}
+
+__global__ void k_diag_of(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                          const double *__restrict__ v, double *__restrict__ d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int b = rp[i], e = rp[i + 1];
+  const int p = b + count_below(ci + b, e - b, i);
+  d[i] = (p < e && ci[p] == i) ? v[p] : 0.0;
+}
+
+std::vector<int> to_int32(const std::vector<int64_t> &v) {
+  std::vector<int> out(v.size());
+  for (size_t k = 0; k < v.size(); ++k) {
+    CHRONOS_REQUIRE(v[k] <= INT32_MAX, CHRONOS_EINVAL, "EMIN: more than 2^31 - 1 entries");
+    out[k] = (int)v[k];
+  }
+  return out;
+}
+
+double host_sum(const DBuf<double> &part, int nb, cudaStream_t st) {
+  std::vector<double> h(nb);
+  part.download(h.data(), nb, st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  double s = 0.0;
+  for (int b = 0; b < nb; ++b) s += h[b];
+  return s;
+}
+
+int warp_grid(int64_t rows) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(rows, kEminWarps),
+                                                     (int64_t)num_sms() * 16));
+}
+
+}  // namespace
+
+HostCSR emin_pattern_device(int kpow, int n, int nc, const EminStrength &str, const HostCSR &P0,
+                            const std::vector<int> &fc0, int nnzr_max, int nnzr_min,
+                            cudaStream_t st, int *host_rows) {
+  const int nnzr = std::max(nnzr_max, nnzr_min);
+  if (host_rows) *host_rows = 0;
+  if (kpow <= 1) {                                     // P's fine rows as they are
+    HostCSR out;
+    out.nrows = n;
+    out.ncols = nc;
+    out.rp.assign((size_t)n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      if (fc0[i] < 0)
+        for (int64_t k = P0.rp[i]; k < P0.rp[i + 1]; ++k) {
+          out.ci.push_back(P0.ci[k]);
+          out.v.push_back(P0.v[k]);
+        }
+      out.rp[i + 1] = (int64_t)out.ci.size();
+    }
+    return out;
+  }
+  const bool from_a = str.S == nullptr;
+  DBuf<int> srp, sci, p0rp, p0ci, fcd, crp, cci, olen;
+  DBuf<double> sv, diag, cv, ov;
+  DBuf<int64_t> ooff;
+  DBuf<int> ocid;
+  if (from_a) {
+    diag.alloc(n);
+    k_diag_of<<<ceil_div(n, 256), 256, 0, st>>>(n, str.arp, str.aci, str.av, diag.get());
+    CHRONOS_CHECK_LAUNCH();
+  } else {
+    srp.upload(to_int32(str.S->rp), st);
+    sci.upload(str.S->ci, st);
+    sv.upload(str.S->v, st);
+  }
+  const int *srp_d = from_a ? str.arp : srp.get();
+  const int *sci_d = from_a ? str.aci : sci.get();
+  const double *sv_d = from_a ? str.av : sv.get();
+  p0rp.upload(to_int32(P0.rp), st);
+  p0ci.upload(P0.ci, st);
+  fcd.upload(fc0, st);
+  HostCSR cur = P0;                                    // P_cur of MEX_cptProlPatt
+  std::vector<int> cols;
+  std::vector<double> vals;
+  HostCSR S_host;                                      // for host rows, built when needed
+  bool have_s_host = false;
+  for (int ipow = 2; ipow <= kpow; ++ipow) {
+    const bool last = ipow == kpow;
+    crp.upload(to_int32(cur.rp), st);
+    cci.upload(cur.ci, st);
+    cv.upload(cur.v, st);
+    // capacities and the candidate table
+    std::vector<int64_t> off((size_t)n + 1, 0);
+    int maxlen = 0;
+    for (int i = 0; i < n; ++i) {
+      const int n0 = (int)(P0.rp[i + 1] - P0.rp[i]);
+      const int cap = (last && fc0[i] >= 0) ? 0 : std::max(nnzr, n0);
+      off[i + 1] = off[i] + cap;
+    }
+    for (int i = 0; i < n; ++i) maxlen = std::max<int>(maxlen, (int)(cur.rp[i + 1] - cur.rp[i]));
+    int64_t maxs = from_a ? str.max_row : 0;
+    if (!from_a)
+      for (int i = 0; i < n; ++i) maxs = std::max<int64_t>(maxs, str.S->rp[i + 1] - str.S->rp[i]);
+    const int64_t bound = maxs * (int64_t)maxlen;
+    int table = 64;
+    while (table < kPattMaxTable && table < 2 * bound) table <<= 1;
+    ooff.upload(off, st);
+    ocid.alloc(std::max<int64_t>(off[n], 1));
+    ov.alloc(std::max<int64_t>(off[n], 1));
+    olen.alloc(n);
+    const size_t per_warp = (size_t)table * 8 + (size_t)table / 2 * 8 + (size_t)table * 4 +
+                            (size_t)table / 2 * 4 + (size_t)table / 2;
+    const size_t per_warp_al = (per_warp + 15) & ~(size_t)15;
+    // warps per block: as many as 200 KB of shared memory hold (at most 4)
+    const int wpb = (int)std::max<size_t>(1, std::min<size_t>(kEminWarps, (200u << 10) / per_warp_al));
+    const size_t smem = per_warp_al * wpb;
+    const int grid = (int)std::max<int64_t>(
+        1, std::min<int64_t>(ceil_div(n, wpb), (int64_t)num_sms() * 16));
+    if (from_a) {
+      CHRONOS_CUDA(cudaFuncSetAttribute(k_emin_pattern<true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_emin_pattern<true><<<grid, 32 * wpb, smem, st>>>(
+          n, srp_d, sci_d, sv_d, diag.get(), str.tau, crp.get(), cci.get(), cv.get(),
+          p0rp.get(), p0ci.get(), fcd.get(), nnzr, last ? 1 : 0, table, ooff.get(), ocid.get(),
+          ov.get(), olen.get());
+    } else {
+      CHRONOS_CUDA(cudaFuncSetAttribute(k_emin_pattern<false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_emin_pattern<false><<<grid, 32 * wpb, smem, st>>>(
+          n, srp_d, sci_d, sv_d, nullptr, 0.0, crp.get(), cci.get(), cv.get(), p0rp.get(),
+          p0ci.get(), fcd.get(), nnzr, last ? 1 : 0, table, ooff.get(), ocid.get(), ov.get(),
+          olen.get());
+    }
+    CHRONOS_CHECK_LAUNCH();
+    std::vector<int> len = olen.to_host(st);
+    std::vector<int> oci(off[n]);
+    std::vector<double> oval(off[n]);
+    ocid.download(oci.data(), off[n], st);
+    ov.download(oval.data(), off[n], st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    HostCSR next;
+    next.nrows = n;
+    next.ncols = nc;
+    next.rp.assign((size_t)n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+      if (len[i] < 0) {
+        if (!have_s_host) {
+          S_host = from_a ? str.host_strength() : *str.S;
+          have_s_host = true;
+        }
+        emin_pattern_row(i, S_host, cur, P0, nnzr, cols, vals);
+        if (host_rows) ++*host_rows;
+        next.ci.insert(next.ci.end(), cols.begin(), cols.end());
+        next.v.insert(next.v.end(), vals.begin(), vals.end());
+      } else {
+        next.ci.insert(next.ci.end(), oci.begin() + off[i], oci.begin() + off[i] + len[i]);
+        next.v.insert(next.v.end(), oval.begin() + off[i], oval.begin() + off[i] + len[i]);
+      }
+      next.rp[i + 1] = (int64_t)next.ci.size();
+    }
+    cur.rp.swap(next.rp);
+    cur.ci.swap(next.ci);
+    cur.v.swap(next.v);
+  }
+  cur.nrows = n;
+  cur.ncols = nc;
+  return cur;
+}
+
+HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const int *aci,
+                    const double *av, const HostCSR &Pin, const HostCSR &patt,
+                    const std::vector<int> &fc0, const double *TVr, int ntv, cudaStream_t st,
+                    double *info) {
+  using clk = std::chrono::steady_clock;
+  const auto t_glob = clk::now();
+  CHRONOS_REQUIRE(prm.prec == 1, CHRONOS_ENOTSUP,
+                  "EMIN preconditioner " + std::to_string(prm.prec) +
+                      " is outside this path (1: Jacobi)");
+  CHRONOS_REQUIRE(prm.solv == 3 || prm.solv == 4, CHRONOS_ENOTSUP,
+                  "EMIN solver " + std::to_string(prm.solv) +
+                      " is outside this path (3, 4: products with A)");
+  CHRONOS_REQUIRE(prm.spd, CHRONOS_ENOTSUP, "EMIN for a nonsymmetric A is outside this path");
+  CHRONOS_REQUIRE(ntv >= 1 && ntv <= kEminMaxTv, CHRONOS_ENOTSUP,
+                  "EMIN takes 1 to 16 test vectors");
+  CHRONOS_REQUIRE(patt.nrows == n && Pin.nrows == n && (int)fc0.size() == n, CHRONOS_EINVAL,
+                  "EMIN: pattern, P and fcnode must have n rows");
+  std::vector<int> c2glo(std::max(nc, 1), -1);
+  for (int i = 0; i < n; ++i) {
+    if (fc0[i] >= 0) {
+      CHRONOS_REQUIRE(fc0[i] < nc, CHRONOS_EINVAL, "EMIN: coarse index out of range");
+      c2glo[fc0[i]] = i;
+    }
+  }
+  int mmax = 0;
+  for (int i = 0; i < n; ++i) {
+    const int64_t m = patt.rp[i + 1] - patt.rp[i];
+    CHRONOS_REQUIRE(m == 0 || fc0[i] < 0, CHRONOS_EINVAL,
+                    "EMIN: the pattern must have no coarse rows");
+    mmax = std::max<int>(mmax, (int)m);
+    for (int64_t k = patt.rp[i]; k < patt.rp[i + 1]; ++k)
+      CHRONOS_REQUIRE(patt.ci[k] >= 0 && patt.ci[k] < nc &&
+                          (k == patt.rp[i] || patt.ci[k] > patt.ci[k - 1]),
+                      CHRONOS_EINVAL, "EMIN: pattern columns must be ascending in [0, nc)");
+  }
+  for (int c = 0; c < nc; ++c)
+    CHRONOS_REQUIRE(c2glo[c] >= 0, CHRONOS_EINVAL, "EMIN: coarse index without a node");
+  CHRONOS_REQUIRE(mmax <= 4096, CHRONOS_ENOTSUP, "EMIN: pattern rows beyond 4096 entries");
+  const int64_t nt = patt.rp[n];
+  DBuf<int> trp, tci, prp, pci, fcd, c2g;
+  DBuf<double> pv, tvd;
+  trp.upload(to_int32(patt.rp), st);
+  tci.upload(patt.ci, st);
+  prp.upload(to_int32(Pin.rp), st);
+  pci.upload(Pin.ci, st);
+  pv.upload(Pin.v, st);
+  fcd.upload(fc0, st);
+  c2g.upload(c2glo, st);
+  tvd.upload(TVr, (size_t)n * ntv, st);
+  const int64_t ntv_ = std::max<int64_t>(nt, 1);
+  DBuf<double> p0(ntv_), Qd(ntv_ * ntv), f(ntv_), dinv(ntv_), res(ntv_), z(ntv_), pvec(ntv_),
+      kp(ntv_), dp(ntv_);
+  DBuf<int> svd_rows(1);
+  svd_rows.zero(st);
+  const int tpb = 128;
+  // copy_Prol, gather_B_QR
+  const auto t_b = clk::now();
+  k_emin_copy_prol<<<ceil_div(n, tpb), tpb, 0, st>>>(n, fcd.get(), prp.get(), pci.get(), pv.get(),
+                                                      trp.get(), tci.get(), p0.get());
+  CHRONOS_CHECK_LAUNCH();
+  k_emin_constraints<<<ceil_div(n, tpb), tpb, 0, st>>>(n, ntv, prm.condmax, trp.get(), tci.get(),
+                                                        fcd.get(), c2g.get(), tvd.get(), Qd.get(),
+                                                        p0.get(), svd_rows.get());
+  CHRONOS_CHECK_LAUNCH();
+  k_emin_f_dinv<<<ceil_div(n, tpb), tpb, 0, st>>>(n, arp, aci, av, trp.get(), tci.get(), c2g.get(),
+                                                   f.get(), dinv.get());
+  CHRONOS_CHECK_LAUNCH();
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  const double t_gath = std::chrono::duration<double>(clk::now() - t_b).count();
+  // products with A on the pattern, projections
+  int hslots = 64;
+  while (hslots < 2 * mmax) hslots <<= 1;
+  // per warp: the row's accumulators and its column -> position table; as
+  // many warps per block as 200 KB hold (at most 4)
+  const size_t kp_warp = (size_t)std::max(mmax, 1) * 8 + (size_t)hslots * 8;
+  const int kp_wpb = (int)std::max<size_t>(1, std::min<size_t>(kEminWarps, (200u << 10) / kp_warp));
+  const size_t kp_smem = kp_warp * kp_wpb;
+  CHRONOS_CUDA(cudaFuncSetAttribute(k_emin_kp, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)kp_smem));
+  const int kp_grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>(ceil_div(n, kp_wpb), (int64_t)num_sms() * 16));
+  const int wg = warp_grid(n);
+  DBuf<double> part(wg);
+  auto kp_apply = [&](const double *x, double *y) {
+    k_emin_kp<<<kp_grid, 32 * kp_wpb, kp_smem, st>>>(n, arp, aci, av, trp.get(), tci.get(), x, y,
+                                                      std::max(mmax, 1), hslots);
+    CHRONOS_CHECK_LAUNCH();
+  };
+  auto orth = [&](const double *x, const double *sub, const double *d, double *y,
+                  const double *w) {
+    k_emin_orth<<<wg, 32 * kEminWarps, 0, st>>>(n, ntv, trp.get(), Qd.get(), x, sub, d, y, w,
+                                                 w ? part.get() : nullptr);
+    CHRONOS_CHECK_LAUNCH();
+    return w ? host_sum(part, wg, st) : 0.0;
+  };
+  const int vg = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(ntv_, 256),
+                                                             (int64_t)num_sms() * 8));
+  const auto t_pcg = clk::now();
+  dp.zero(st);
+  pvec.zero(st);
+  kp_apply(p0.get(), kp.get());
+  // rhs = res = (I - QQ') (K p0 - f)
+  const double rn2 = orth(kp.get(), f.get(), nullptr, res.get(), res.get());
+  int iter = 0;
+  bool exit_test = prm.itmax <= 0 || std::sqrt(rn2) < 1e-15;
+  double gamma_old = 0.0, de0 = 1.0;
+  while (!exit_test) {
+    ++iter;
+    const double gamma = orth(res.get(), nullptr, dinv.get(), z.get(), res.get());
+    const double beta = iter == 1 ? 0.0 : gamma / gamma_old;
+    k_emin_xpby<<<vg, 256, 0, st>>>(nt, z.get(), beta, iter == 1 ? 1 : 0, pvec.get());
+    CHRONOS_CHECK_LAUNCH();
+    gamma_old = gamma;
+    kp_apply(pvec.get(), kp.get());
+    const double denom = orth(kp.get(), nullptr, nullptr, kp.get(), pvec.get());
+    if (std::fabs(denom) < 1e-18) break;
+    const double dek = gamma * gamma / denom, alpha = gamma / denom;
+    k_emin_step<<<vg, 256, 0, st>>>(nt, alpha, pvec.get(), kp.get(), dp.get(), res.get());
+    CHRONOS_CHECK_LAUNCH();
+    if (iter == 1) de0 = dek;
+    exit_test = iter == prm.itmax || dek / de0 < prm.energ_tol;
+  }
+  k_emin_sub<<<vg, 256, 0, st>>>(nt, p0.get(), dp.get(), p0.get());
+  CHRONOS_CHECK_LAUNCH();
+  std::vector<double> pf(nt);
+  p0.download(pf.data(), nt, st);
+  std::vector<int> nsvd = svd_rows.to_host(st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  const double t_solve = std::chrono::duration<double>(clk::now() - t_pcg).count();
+  // Prol_add_Cnodes + sparse(): unit coarse rows, exact zeros dropped
+  HostCSR out;
+  out.nrows = n;
+  out.ncols = nc;
+  out.rp.assign((size_t)n + 1, 0);
+  out.ci.reserve(nt + nc);
+  out.v.reserve(nt + nc);
+  for (int i = 0; i < n; ++i) {
+    if (fc0[i] >= 0) {
+      out.ci.push_back(fc0[i]);
+      out.v.push_back(1.0);
+    } else {
+      for (int64_t k = patt.rp[i]; k < patt.rp[i + 1]; ++k)
+        if (pf[k] != 0.0) {
+          out.ci.push_back(patt.ci[k]);
+          out.v.push_back(pf[k]);
+        }
+    }
+    out.rp[i + 1] = (int64_t)out.ci.size();
+  }
+  if (info) {
+    const double t_all = std::chrono::duration<double>(clk::now() - t_glob).count();
+    for (int k = 0; k < 12; ++k) info[k] = 0.0;
+    info[2] = t_gath;
+    info[3] = t_solve;
+    info[4] = std::max(0.0, t_all - t_gath - t_solve);
+    info[5] = t_all;
+    info[7] = iter;
+    info[10] = (double)nt;
+    info[11] = (double)nt * ntv;
+    info[6] = nsvd[0];                      // rows whose constraint block took the SVD branch
+  }
+  return out;
+}
+
+HostCSR EminStrength::host_strength() const {
+  // DOM strength of A with values (cpt_SoC_dom.m:26-47), for the rows the
+  // pattern kernel leaves to the host.
+  std::vector<int> rp(n + 1), ci(nnz);
+  std::vector<double> v(nnz);
+  CHRONOS_CUDA(cudaMemcpy(rp.data(), arp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+  CHRONOS_CUDA(cudaMemcpy(ci.data(), aci, sizeof(int) * nnz, cudaMemcpyDeviceToHost));
+  CHRONOS_CUDA(cudaMemcpy(v.data(), av, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
+  HostCSR A;
+  A.nrows = A.ncols = n;
+  A.rp.assign(rp.begin(), rp.end());
+  A.ci = std::move(ci);
+  A.v = std::move(v);
+  return soc_matrix(A, "DOM", tau);
+}
+
+}  // namespace chronos

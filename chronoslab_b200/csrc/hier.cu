@@ -864,8 +864,16 @@ HierBuilder::HierBuilder(const chronos_params &prm_in, const HostCSR &A0, int nt
   if (!prolong) {   // with a caller-supplied P these choices are the caller's
     CHRONOS_REQUIRE(tmeth == "NONE", CHRONOS_ENOTSUP, "test-space method " + tmeth + " is outside this path");
     CHRONOS_REQUIRE(ptype == "BAMG", CHRONOS_ENOTSUP, "prolongation " + ptype + " is outside this path");
-    CHRONOS_REQUIRE(pemin == "NONE" || pemin == "SMOOTH", CHRONOS_ENOTSUP,
+    CHRONOS_REQUIRE(pemin == "NONE" || pemin == "SMOOTH" || pemin == "EMIN", CHRONOS_ENOTSUP,
                     "prolongation post-process " + pemin + " is outside this path");
+    if (pemin == "EMIN") {
+      CHRONOS_REQUIRE(prm.symmetric, CHRONOS_ENOTSUP,
+                      "EMIN for a nonsymmetric problem (DEFL_GMRES_matfree) is outside this path");
+      CHRONOS_REQUIRE(prm.prec_emin == 1 && (prm.solv_emin == 3 || prm.solv_emin == 4),
+                      CHRONOS_ENOTSUP,
+                      "EMIN is on this path with prec_emin 1 (Jacobi) and solv_emin 3 or 4");
+      CHRONOS_REQUIRE(prm.ntv <= 16, CHRONOS_ENOTSUP, "EMIN takes at most 16 test vectors");
+    }
     CHRONOS_REQUIRE(prm.nl_agg == 0, CHRONOS_ENOTSUP, "aggressive coarsening is outside this path");
     CHRONOS_REQUIRE(prm.updateCF == 0, CHRONOS_ENOTSUP, "updateCF != 0 is outside this path");
   }
@@ -1114,6 +1122,35 @@ void HierBuilder::end_level(int fl) {
            ? bamg_prolongation_device(bp, S, fc0, nc, TVr.data(), ntv, c_mark, st)
                   : bamg_prolongation(bp, S, fc0, nc, TVr.data(), ntv, c_mark);
   if (pemin == "SMOOTH") Ph = smooth_prolongation(Al, L.A, Ph, st);
+  if (pemin == "EMIN") {
+    // prolong.m:207-235: S_emin is DOM strength of A with threshold patt_tau
+    // either way (the coarsening's S when it is DOM with tau = patt_tau,
+    // cpt_SoC_dom(patt_tau, A) otherwise), computed on the fly on the GPU
+    EminStrength str;
+    str.arp = L.A.rp.get();
+    str.aci = L.A.ci.get();
+    str.av = L.A.v64.get();
+    str.n = n;
+    str.nnz = L.A.nnz;
+    str.tau = prm.patt_tau;
+    for (int i = 0; i < n; ++i)
+      str.max_row = std::max<int>(str.max_row, (int)(Al.rp[i + 1] - Al.rp[i]));
+    HostCSR patt = emin_pattern_device(prm.patt_pow, n, nc, str, Ph, fc0, prm.nnzr_max, ntv, st);
+    EminParams ep;
+    ep.itmax = prm.itmax_emin;
+    ep.energ_tol = prm.energ_tol;
+    ep.condmax = prm.condmax_emin;
+    ep.prec = prm.prec_emin;
+    ep.solv = prm.solv_emin;
+    ep.spd = true;
+    double info[12];
+    Ph = emin_device(ep, n, nc, L.A.rp.get(), L.A.ci.get(), L.A.v64.get(), Ph, patt, fc0,
+                     TVr.data(), ntv, st, info);
+    if (std::getenv("CHRONOS_TUNE_VERBOSE"))
+      std::fprintf(stderr, "chronos setup: level %d EMIN pattern %lld entries, %d CG steps, "
+                   "%d SVD rows, %.3f s\n", level, (long long)patt.nnz(), (int)info[7],
+                   (int)info[6], info[5]);
+  }
   std::vector<double> TVn((size_t)nc * ntv);
   for (int j = 0; j < ntv; ++j)
     for (int c = 0; c < nc; ++c) TVn[(size_t)j * nc + c] = TV[(size_t)j * n + clist[c]];

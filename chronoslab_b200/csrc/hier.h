@@ -152,6 +152,47 @@ HostCSR bamg_prolongation_device(const BamgParams &prm, const HostCSR &S,
 // Whether the setup runs BAMG on the GPU: when CHRONOS_GPU_BAMG=1.
 bool gpu_bamg();
 
+// Strength rows for the EMIN pattern (emin_gpu.cu): an explicit S with values
+// (S != nullptr, host), or DOM strength with threshold tau computed on the
+// fly from the device CSR (arp, aci, av) of an n x n A with nnz entries and
+// rows of at most max_row entries (cpt_SoC_dom.m:26-47, prolong.m:213-217).
+struct EminStrength {
+  const HostCSR *S = nullptr;
+  const int *arp = nullptr, *aci = nullptr;
+  const double *av = nullptr;
+  int n = 0, max_row = 0;
+  int64_t nnz = 0;
+  double tau = 0.0;
+  HostCSR host_strength() const;    // the DOM S of A with values, on the host
+};
+// MEX_cptProlPatt (MEX_EMIN/MEX_cptProlPatt.cpp:234-490) on the GPU: the
+// n x nc EMIN pattern (values as the MEX returns them) from P0 (n x nc,
+// ascending columns), fc0 (coarse index or -1) and kpow power steps, with at
+// most max(nnzr_max, nnzr_min) entries per row beyond P0's own.  Bit-identical
+// to the reference; rows whose candidates outgrow a warp's table are computed
+// by emin_pattern_row on the host (their count in *host_rows, may be null).
+HostCSR emin_pattern_device(int kpow, int n, int nc, const EminStrength &str, const HostCSR &P0,
+                            const std::vector<int> &fc0, int nnzr_max, int nnzr_min,
+                            cudaStream_t st, int *host_rows = nullptr);
+// EMIN parameters of parm_PROLONG (read_prolong.m): itmax_emin, energ_tol,
+// condmax_emin, prec_emin, solv_emin, and whether A is symmetric.
+struct EminParams {
+  int itmax = 10;
+  double energ_tol = 1e-3, condmax = 1e10;
+  int prec = 1, solv = 4;
+  bool spd = true;
+};
+// EMIN_ImpProl (Cpp_EMIN/EMIN_ImpProl.cpp:84-410) with the matrix-free path
+// of EMIN_matfree.cpp on the GPU: P (n x nc) improved on the pattern patt
+// (no coarse rows) for the device CSR A (FP64), TVr row-major n x ntv.
+// Returns P with unit coarse rows and exact zeros dropped; info[12] as the
+// reference's info array (info[6]: rows whose constraint block took the SVD
+// branch; info[7]: iterations).
+HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const int *aci,
+                    const double *av, const HostCSR &Pin, const HostCSR &patt,
+                    const std::vector<int> &fc0, const double *TVr, int ntv, cudaStream_t st,
+                    double *info);
+
 // Source of a level's prolongation outside the library: given the 1-based
 // level number and the level's operator (FP64, from the GPU Galerkin product
 // on levels > 1), returns P (n x nc, 0-based CSR, sorted rows).

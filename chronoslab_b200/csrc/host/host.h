@@ -63,6 +63,17 @@ void bamg_rows_host(const BamgParams &prm, const HostCSR &S, const std::vector<i
                     std::vector<std::vector<int>> &rcols, std::vector<std::vector<double>> &rvals,
                     std::vector<int> &c_mark);
 
+// ---- EMIN prolongation pattern (MEX_cptProlPatt.cpp) -------------------------
+// One row of a power step of the EMIN pattern (MEX_cptProlPatt.cpp:356-443):
+// the columns of (S * Pc)(i, :) that are not in P0's row i, summed in S's row
+// order and Pc's, the nonzero ones only; beyond the budget nnzr - |P0(i,:)|
+// the budget's worth of largest magnitude (ties: lower column first); then
+// P0's own columns with value 1; by column.  S with values, rows of P0 and
+// Pc with ascending columns.  The GPU pattern kernel hands rows whose
+// candidate lists outgrow its per-warp table to this function.
+void emin_pattern_row(int i, const HostCSR &S, const HostCSR &Pc, const HostCSR &P0, int nnzr,
+                      std::vector<int> &cols, std::vector<double> &vals);
+
 // ---- adaptive FSAI pattern search (cpt_afsai_coef.cpp) ----------------------
 // Rows of G hold their strictly-lower columns ascending, then the diagonal.
 // vals receives the host FP64 values of the final per-row solve (the GPU

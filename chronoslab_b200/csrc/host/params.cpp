@@ -81,6 +81,14 @@ void params_default(chronos_params *p) {
   p->maxrownrm = 5.0;
   p->eps_prol = 1e-10;
   p->updateCF = 0;
+  p->patt_pow = 2;
+  p->patt_tau = 0.01;
+  p->nnzr_max = 30;
+  p->itmax_emin = 10;
+  p->energ_tol = 1e-3;
+  p->condmax_emin = 1e10;
+  p->prec_emin = 1;
+  p->solv_emin = 4;
   p->filt_np = 0;
   p->filt_wgt = 170.0;
   p->filt_tol = 0.1;
@@ -144,6 +152,14 @@ void params_read(const char *fnames_path, chronos_params *p) {
   p->maxrownrm = num(pro[8], path(4));
   p->eps_prol = num(pro[9], path(4));
   p->updateCF = (int)num(pro[10], path(4));
+  p->patt_pow = (int)num(pro[11], path(4));
+  p->patt_tau = num(pro[12], path(4));
+  p->nnzr_max = (int)num(pro[13], path(4));
+  p->itmax_emin = (int)num(pro[14], path(4));
+  p->energ_tol = num(pro[15], path(4));
+  p->condmax_emin = num(pro[16], path(4));
+  p->prec_emin = (int)num(pro[17], path(4));
+  p->solv_emin = (int)num(pro[18], path(4));
   auto fil = first_tokens(path(5), 5);
   p->filt_np = (int)num(fil[0], path(5));
   p->filt_wgt = num(fil[1], path(5));

@@ -78,6 +78,12 @@ typedef struct chronos_params {
   int dist_min, dist_max;
   double maxcond, maxrownrm, eps_prol;
   int updateCF;
+  /* parm_PROLONG, the EMIN lines (prol_emin = EMIN, prolong.m:207-235) */
+  int patt_pow;                   /* power steps of the EMIN pattern (2) */
+  double patt_tau;                /* DOM threshold of its strength matrix (0.01) */
+  int nnzr_max, itmax_emin;       /* entries per pattern row (30); CG steps (10) */
+  double energ_tol, condmax_emin; /* energy-decrease exit (1e-3); constraint blocks' condition (1e10) */
+  int prec_emin, solv_emin;       /* 1 (Jacobi); 4 (products with A) */
   /* parm_FILTER (read_filter.m) */
   int filt_np;
   double filt_wgt, filt_tol, filt_tau;
@@ -264,6 +270,37 @@ int chronos_bamg(const chronos_params *prm, int n, const int *iat_S_h, const int
 int chronos_bamg_device(const chronos_params *prm, int n, const int *iat_S_h, const int *ja_S_h,
                         const int *fcnode_h, int ntv, const double *TV_h, int *c_mark_h,
                         int max_neigh, chronos_csr **P, int *host_rows);
+/* EMIN prolongation pattern on the GPU, replaces MEX_cptProlPatt
+ * (MEX_EMIN/MEX_cptProlPatt.cpp:234-490) as prolong.m:222 calls it:
+ * Ppatt = MEX_cptProlPatt(kpow, S, P, fcnode, nnzr, nnzr_min, np).  S (n x n,
+ * strength values), P (n x nc) 0-based CSR with ascending columns, fcnode as
+ * chronos_coarsen returns it.  The n x nc pattern (coarse rows empty; values
+ * as the MEX returns them: 1 on P's own entries, those of S*P on the added
+ * ones) is bit-identical to the reference's.  *host_rows (may be NULL):
+ * rows computed on the host because their candidates outgrew a GPU warp's
+ * table. */
+int chronos_emin_pattern(int kpow, int n, int nc, const int *iat_S_h, const int *ja_S_h,
+                         const double *coef_S_h, const int *iat_P_h, const int *ja_P_h,
+                         const double *coef_P_h, const int *fcnode_h, int nnzr_max, int nnzr_min,
+                         chronos_csr **patt, int *host_rows);
+/* Energy minimisation of a prolongation on the GPU, replaces
+ * EMIN_Prolong_compute / EMIN_ImpProl (Cpp_EMIN/EMIN_ImpProl.cpp:84-410,
+ * MEX_EMIN/EMIN_Prolong_compute.cpp:73-209) with prm->solv_emin 3 or 4
+ * (products with A, EMIN_matfree.cpp:69-308), prm->prec_emin 1 (Jacobi) and
+ * spd != 0 (DEFL_PCG_matfree.cpp; the GMRES variant for a nonsymmetric A is
+ * outside this path: CHRONOS_ENOTSUP).  A (n x n), P (n x nc) and the pattern
+ * (n x nc, no coarse rows, e.g. from chronos_emin_pattern) as 0-based CSR with
+ * ascending columns; fcnode as chronos_coarsen returns it; TV_h n x ntv
+ * column-major (ntv <= 16).  Returns P with unit coarse rows and exact zeros
+ * dropped (as sparse() does in MEX_EMIN_enhance_prol.m:102) and info[12] (may
+ * be NULL) as the reference's info array: [2] constraint setup s, [3] CG s,
+ * [5] total s, [6] rows whose constraint block took the SVD branch, [7] CG
+ * iterations, [10] pattern entries, [11] entries of Q. */
+int chronos_emin(const chronos_params *prm, int n, const int *iat_A_h, const int *ja_A_h,
+                 const double *coef_A_h, int nc, const int *iat_P_h, const int *ja_P_h,
+                 const double *coef_P_h, const int *iat_patt_h, const int *ja_patt_h,
+                 const int *fcnode_h, int ntv, const double *TV_h, int spd, chronos_csr **P,
+                 double *info);
 
 /* ---- Galerkin product P'*(A*P) on the GPU (0-based CSR, FP64) --------- */
 typedef struct chronos_galerkin_plan chronos_galerkin_plan;

@@ -1,0 +1,156 @@
+"""Energy-minimised prolongation (prol_emin = EMIN, prolong.m:207-235) on the
+GPU against the reference's own C++ built into oracle/_ref:
+
+* chronos_emin_pattern against MEX_cptProlPatt (MEX_EMIN/MEX_cptProlPatt.cpp):
+  pattern and values bit for bit, with one to three power steps, a budget of
+  zero, and rows beyond a GPU warp's candidate table (computed on the host);
+* chronos_emin against EMIN_ImpProl (Cpp_EMIN/EMIN_ImpProl.cpp, matrix-free
+  path, Jacobi, SPD): the same CG iteration count and P within 1e-12 of its
+  largest entry, on Cubo_4820, elasticity and Poisson with short pattern rows
+  (SVD branch) and with a rank-deficient test space;
+* the setup with prol_emin = EMIN on Cubo_4820: the reference's pinned
+  regression, 20 SQMR iterations to 1e-6 with tolerance max(5%, 2)
+  (Tests/CubeBAMG_EMIN.m:3,34), and within one of the oracle's count.
+"""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import chronoslab_b200 as cb
+from chronoslab_b200 import problems as PB
+from oracle import amg_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _level1(A, TV, tau=0.01):
+    """S (DOM with values), fcnode, the reference's BAMG P, orthonormal TV."""
+    prm = O.default_params(2)
+    prm["coarsen"]["tau"] = tau
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    fc, clist, _, S = O.coarsen(prm["coarsen"], A, O.MatlabRand())
+    TV = O.qr_thin(np.asarray(TV, dtype=np.float64).reshape(A.shape[0], -1))
+    P, _ = O.ref_bamg(prm["prolong"], clist.size, fc, S, TV)
+    return A, prm, S, fc, P, TV
+
+
+def _arrow(n2d=50):
+    """2-D Poisson shifted by 20 I with two extra nodes, each strongly coupled
+    to every grid node and to each other (SPD): one of them becomes fine, and
+    its candidate list outgrows a GPU warp's table, so its row is computed on
+    the host."""
+    m = n2d * n2d
+    I = sp.identity(n2d)
+    T1 = sp.diags([-np.ones(n2d - 1), 2 * np.ones(n2d), -np.ones(n2d - 1)], [-1, 0, 1])
+    A = (sp.kron(I, T1) + sp.kron(T1, I) + 20.0 * sp.identity(m)).tolil()
+    A.resize((m + 2, m + 2))
+    for a in (m, m + 1):
+        A[a, :m] = -4.0
+        A[:m, a] = -4.0
+        A[a, a] = 2.0 * m
+    A[m, m + 1] = A[m + 1, m] = -500.0
+    A = A.tocsr()
+    A.sort_indices()
+    return A
+
+
+@pytest.fixture(scope="module")
+def cubo_level1(cubo):
+    return _level1(cubo["Af"], cubo["TV0"])
+
+
+def _pattern_cases(cubo_level1):
+    A, prm, S, fc, P, TV = cubo_level1
+    cases = [("cubo", 2, S, P, fc, 30, TV.shape[1])]
+    Ae, X = PB.elasticity_q1(5, return_coords=True)
+    _, _, S2, fc2, P2, TV2 = _level1(Ae, PB.rbm_test_space(X))
+    for kpow, nnzr in ((1, 30), (2, 12), (3, 20), (2, 1)):
+        cases.append((f"elasticity k{kpow} n{nnzr}", kpow, S2, P2, fc2, nnzr, TV2.shape[1]))
+    Aa = _arrow()
+    _, _, S3, fc3, P3, TV3 = _level1(Aa, np.ones(Aa.shape[0]))
+    cases.append(("arrow", 2, S3, P3, fc3, 30, 1))
+    return cases
+
+
+def test_emin_pattern_matches_reference(lib, cubo_level1):
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    host_rows_seen = {}
+    for name, kpow, S, P, fc, nnzr, ntv in _pattern_cases(cubo_level1):
+        R = O.ref_emin_pattern(kpow, S, P, fc, nnzr, ntv, 2)
+        G, host_rows = cb.emin_pattern(S, P, fc, kpow=kpow, nnzr_max=nnzr, nnzr_min=ntv)
+        host_rows_seen[name] = host_rows
+        assert G.shape == R.shape, name
+        assert np.array_equal(G.indptr, R.indptr) and np.array_equal(G.indices, R.indices), name
+        assert np.array_equal(G.data, R.data), name
+    assert host_rows_seen["arrow"] >= 1 and host_rows_seen["cubo"] == 0
+
+
+def _emin_cases(cubo_level1):
+    A, prm, S, fc, P, TV = cubo_level1
+    cases = [("cubo", A, S, fc, P, TV, 30)]
+    Ae, X = PB.elasticity_q1(5, return_coords=True)
+    Ae_, _, Se, fce, Pe, TVe = _level1(Ae, PB.rbm_test_space(X))
+    cases.append(("elasticity short rows", Ae_, Se, fce, Pe, TVe, 5))
+    Ap = PB.poisson7(9)
+    rng = np.random.default_rng(3)
+    TVd = np.column_stack([np.ones(Ap.shape[0]), np.ones(Ap.shape[0]), rng.random(Ap.shape[0])])
+    Ap_, _, Sp, fcp, Pp, _ = _level1(Ap, TVd)
+    cases.append(("poisson rank-deficient", Ap_, Sp, fcp, Pp, TVd, 5))
+    return cases
+
+
+def test_emin_matches_reference(lib, cubo_level1):
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    prm = cb.params()
+    pro = O.default_params(2)["prolong"]
+    svd_rows = {}
+    for name, A, S, fc, P, TV, nnzr in _emin_cases(cubo_level1):
+        patt = O.ref_emin_pattern(2, S, P, fc, nnzr, TV.shape[1], 2)
+        R, rinfo = O.ref_emin(pro, A, patt, P, TV, fc)
+        G, info = cb.emin(A, P, patt, fc, TV, prm)
+        assert int(info[7]) == int(rinfo[7]), (name, info[7], rinfo[7])
+        scale = abs(R).max()
+        assert abs(G - R).max() <= 1e-12 * scale, (name, abs(G - R).max(), scale)
+        svd_rows[name] = int(info[6])
+    assert svd_rows["elasticity short rows"] > 0 and svd_rows["poisson rank-deficient"] > 0
+
+
+def test_emin_errors(lib, cubo_level1):
+    A, prm, S, fc, P, TV = cubo_level1
+    patt = O.emin_pattern(2, S, P, fc, 30, TV.shape[1])
+    held = cb.device_bytes()
+    bad = cb.params(prec_emin=2)
+    with pytest.raises(cb.ChronosError):          # SGS preconditioner: not on this path
+        cb.emin(A, P, patt, fc, TV, bad)
+    with pytest.raises(cb.ChronosError):          # nonsymmetric variant
+        cb.emin(A, P, patt, fc, TV, cb.params(), spd=False)
+    coarse_row = patt.tolil()
+    c = int(np.flatnonzero(fc > 0)[0])
+    coarse_row[c, 0] = 1.0
+    with pytest.raises(cb.ChronosError):          # the pattern must have no coarse rows
+        cb.emin(A, P, coarse_row.tocsr(), fc, TV, cb.params())
+    assert cb.device_bytes() == held
+
+
+def test_cubo_emin_prolongation_pinned(lib, cubo, cubo_ref):
+    """Tests/CubeBAMG_EMIN.m: SQMR to 1e-6 on Cubo_4820 with prol_emin = EMIN
+    takes 20 iterations, tolerance max(5%, 2); the oracle (reference FSAI,
+    BAMG and EMIN C++) takes the golden count, and this setup within one."""
+    A, Af, TV0 = cubo["A"], cubo["Af"], cubo["TV0"]
+    info = cubo_ref["info"]
+    ref_it = info["reference_sqmr_iterations_emin"]
+    with cb.Hierarchy(Af, TV0, cb.params(precision=cb.CHRONOS_FP64, prol_emin="EMIN")) as h:
+        assert [h.level_info(l)["n"] for l in range(h.nlevels)] == info["levels_emin"]
+        P = h.export(0, "P")
+        x, sinfo, relres, niter = h.sqmr(np.ones(A.shape[0]), 1e-6, 100, A=A)
+        assert sinfo == 0
+        assert abs(niter - info["oracle_sqmr_iterations_emin"]) <= 1
+        assert not (abs(ref_it / niter - 1) > 0.05 and abs(ref_it - niter) > 2)
+        x, it, _, flag, _ = h.pcg(np.ones(A.shape[0]), itmax=200, tol=1e-8)
+        assert flag == 0
+        assert abs(it - info["oracle_pcg_iterations_1e-8_emin"]) <= 1
+    # EMIN widens BAMG's rows to the pattern (up to 30 entries)
+    assert P.nnz > 2 * cubo_ref["P"].nnz
