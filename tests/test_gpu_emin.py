@@ -154,3 +154,32 @@ def test_cubo_emin_prolongation_pinned(lib, cubo, cubo_ref):
         assert abs(it - info["oracle_pcg_iterations_1e-8_emin"]) <= 1
     # EMIN widens BAMG's rows to the pattern (up to 30 entries)
     assert P.nnz > 2 * cubo_ref["P"].nnz
+
+
+def test_emin_elasticity40_matches_reference(lib):
+    """Q1 elasticity 40^3 (201,720 rows, rigid-body test space), the level-1
+    EMIN of the reference's own BAMG prolongation: the GPU pattern equals
+    MEX_cptProlPatt's bit for bit (5.4M entries) and the GPU EMIN takes the
+    reference's CG steps, P within 1e-13 of its largest entry."""
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    from oracle import c_oracle as CO
+    A, X = PB.elasticity_q1(40, return_coords=True)
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    n = A.shape[0]
+    fc0, _ = O.mark_isolated_nodes(A, np.zeros(n, dtype=np.int64))
+    S = O.soc_dom(0.01, A)
+    fc, nc = CO.pmis_c(S, fc0, O.MatlabRand().rand(n))
+    TV = O.qr_thin(PB.rbm_test_space(X))
+    pro = O.default_params(8)["prolong"]
+    P, _ = O.ref_bamg(pro, nc, fc, S, TV)
+    R = O.ref_emin_pattern(2, S, P, fc, 30, 6, 8)
+    G, host_rows = cb.emin_pattern(S, P, fc, kpow=2, nnzr_max=30, nnzr_min=6)
+    assert host_rows == 0
+    assert np.array_equal(G.indptr, R.indptr) and np.array_equal(G.indices, R.indices)
+    assert np.array_equal(G.data, R.data)
+    Pr, rinfo = O.ref_emin(pro, A, R, P, TV, fc)
+    Pg, info = cb.emin(A, P, R, fc, TV, cb.params())
+    assert int(info[7]) == int(rinfo[7])
+    assert abs(Pg - Pr).max() <= 1e-13 * abs(Pr).max()
