@@ -45,10 +45,12 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--itmax", type=int, default=1000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5"], default="c2",
+    ap.add_argument("--workload", choices=["c1", "c2", "c3", "c4", "c5", "emin"], default="c2",
                     help="c2: elasticity (default, the headline); c1: Poisson 32^3; c3: "
                          "diffusion 128^3 with a block of 16 right-hand sides; c4: 64 batched "
-                         "problems; c5: adjoint gradient on log-normal diffusion 64^3")
+                         "problems; c5: adjoint gradient on log-normal diffusion 64^3; emin: the "
+                         "energy-minimised prolongation of the elasticity's first level "
+                         "(pattern + minimisation) against the reference's EMIN C++")
     ap.add_argument("--profile-solve", choices=["fp32", "fp64"], default=None,
                     help="for ncu --profile-from-start off: build one hierarchy, warm up, "
                          "then bracket exactly one solve with the profiler range and exit")
@@ -705,6 +707,93 @@ def run_c1_or_c5(args):
     return 0
 
 
+def run_emin(args):
+    """prolong.m:207-235 on the first level of the C2 elasticity (--ne): the
+    pattern (chronos_emin_pattern) and the energy minimisation (chronos_emin)
+    of the library's own BAMG prolongation, timed end to end through the C
+    ABI with host arrays (value), with the device phases of the minimisation
+    from its info array; the reference's MEX_cptProlPatt and EMIN_ImpProl
+    (oracle/_ref, all host threads) on the same inputs as cpu_baseline, and
+    the parity of the two (pattern bit for bit, P's largest difference)."""
+    import numpy as np
+    import scipy.sparse as sp
+    import chronoslab_b200 as cb
+    A, TV0, _ = build_problem(args.ne, seed=0)
+    A = sp.csr_matrix(A)
+    A.sort_indices()
+    n = A.shape[0]
+    prm = cb.params()
+    fc, nc, S = cb.coarsen(A, prm, 0)
+    S = sp.csr_matrix(S)
+    S.sort_indices()
+    d = A.diagonal()
+    rows = np.repeat(np.arange(n), np.diff(S.indptr))
+    a = np.asarray(A[rows, S.indices]).ravel()
+    S = sp.csr_matrix((np.abs(a) / np.sqrt(d[rows] * d[S.indices]), S.indices, S.indptr),
+                      shape=(n, n))                     # cpt_SoC_dom.m:26-47 values
+    TV, _ = np.linalg.qr(TV0)
+    P, _ = cb.bamg(S, fc, TV, prm)
+    ntv = TV.shape[1]
+
+    def step():
+        t0 = time.perf_counter()
+        patt, host_rows = cb.emin_pattern(S, P, fc, kpow=prm.patt_pow, nnzr_max=prm.nnzr_max,
+                                          nnzr_min=ntv)
+        t1 = time.perf_counter()
+        Pe, info = cb.emin(A, P, patt, fc, TV, prm)
+        t2 = time.perf_counter()
+        return patt, Pe, info, host_rows, (t1 - t0) * 1e3, (t2 - t1) * 1e3
+
+    for _ in range(args.warmup):
+        step()
+    rec = [step() for _ in range(args.steps)]
+    patt, Pe, info, host_rows = rec[-1][:4]
+    t_patt = sum(r[4] for r in rec) / len(rec)
+    t_emin = sum(r[5] for r in rec) / len(rec)
+    iters = int(info[7])
+    out = {"metric": "EMIN prolongation time (pattern + energy minimisation), level 1",
+           "value": t_patt + t_emin, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": t_patt + t_emin, "higher_is_better": False,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded Q1 elasticity, rigid-body test space)",
+           "config": {"workload": f"Q1 elasticity {args.ne}^3 elements, {n} DOF, level-1 EMIN "
+                                  f"(patt_pow {prm.patt_pow}, nnzr_max {prm.nnzr_max}, "
+                                  f"itmax_emin {prm.itmax_emin}, Jacobi) of this library's BAMG P "
+                                  f"({nc} coarse nodes)",
+                      "pattern_entries": int(patt.nnz), "cg_steps": iters,
+                      "host_rows": int(host_rows)},
+           "e2e": {"value": t_patt + t_emin, "unit": "ms",
+                   "h2d_bytes_per_step": int(2 * (A.data.nbytes + A.indices.nbytes + A.indptr.nbytes)
+                                             + S.data.nbytes + S.indices.nbytes + 2 * P.data.nbytes),
+                   "d2h_bytes_per_step": int(12 * patt.nnz + 12 * Pe.nnz)},
+           "detail": {"pattern_ms": t_patt, "minimisation_ms": t_emin,
+                      "device_constraints_ms": info[2] * 1e3, "device_cg_ms": info[3] * 1e3,
+                      "device_total_ms": info[5] * 1e3, "svd_rows": int(info[6])},
+           "gpu_launches": args.steps * (1 + 3 + (iters + 1) + (2 * iters + 1) + 2 * iters + 1)}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, ROOT)
+        from oracle import amg_oracle as O
+        nth = cpu_threads()
+        pro = O.default_params(nth)["prolong"]
+        t0 = time.perf_counter()
+        R = O.ref_emin_pattern(prm.patt_pow, S, P, fc, prm.nnzr_max, ntv, nth)
+        t1 = time.perf_counter()
+        Pr, rinfo = O.ref_emin(pro, A, R, P, TV, fc)
+        t2 = time.perf_counter()
+        out["cpu_baseline"] = {
+            "value": (t2 - t0) * 1e3, "unit": "ms", "cores": nth, "kind": "reference",
+            "sample": "one call each of the reference's MEX_cptProlPatt and EMIN_ImpProl "
+                      "(oracle/_ref) on the same inputs",
+            "pattern_ms": (t1 - t0) * 1e3, "minimisation_ms": (t2 - t1) * 1e3,
+            "cg_steps": int(rinfo[7]),
+            "parity": {"pattern_bit_identical": bool(np.array_equal(R.indptr, patt.indptr) and
+                                                     np.array_equal(R.indices, patt.indices) and
+                                                     np.array_equal(R.data, patt.data)),
+                       "P_max_diff_over_max": float(abs(Pe - Pr).max() / abs(Pr).max())}}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse()
     world, rank, local = dist_env()
@@ -718,6 +807,8 @@ def main():
         return run_profile_solve(args)
     if args.workload in ("c1", "c5"):
         return run_c1_or_c5(args)
+    if args.workload == "emin":
+        return run_emin(args)
     if args.workload != "c2":
         return run_block_or_batch(args, world, rank)
     return run_product(args, world, rank, local)

@@ -20,11 +20,13 @@
 //    with values or is computed on the fly from A as DOM strength
 //    |a_ij| / sqrt(a_ii a_jj) > tau (cpt_SoC_dom.m:26-47).  Rows whose
 //    candidate count could outgrow the table go to emin_pattern_row (host).
-//  * k_emin_constraints: a thread per fine row; gathers B = TV(coarse nodes
-//    of the row, :), corrects p0 so that B' p0 = TV(i, :)' and leaves the
+//  * k_emin_constraints_warp / k_emin_constraints: gather B = TV(coarse nodes
+//    of the row, :), correct p0 so that B' p0 = TV(i, :)' and leave the
 //    orthonormal basis of range(B) in Q -- Householder QR when m > ntv and
 //    max|R_kk| / min|R_kk| <= condmax, else a one-sided Jacobi SVD with the
-//    reference's rank rule (gather_B_QR.cpp:183-454).
+//    reference's rank rule (gather_B_QR.cpp:183-454).  A warp per row (B in
+//    registers, lane r holding row r) for rows of up to 32 entries and 1-4 or
+//    6 test vectors; a thread per row for the rest and the SVD branch.
 //  * k_emin_kp: a warp per fine row; (A X)(i, c) for the row's pattern
 //    columns, X the unknowns on the pattern, summed in A's row order
 //    (KP_spmat.cpp:11-73's order; products and sums rounded on their own).
@@ -352,9 +354,12 @@ __global__ void k_emin_constraints(int n, int nt, double condmax, const int *__r
                                    const int *__restrict__ tci, const int *__restrict__ fc,
                                    const int *__restrict__ c2glo, const double *__restrict__ TV,
                                    double *__restrict__ Q, double *__restrict__ p0,
-                                   int *__restrict__ svd_rows) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || fc[i] >= 0) return;
+                                   int *__restrict__ svd_rows, const int *__restrict__ rows,
+                                   int nrows) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (rows ? t >= nrows : t >= n) return;
+  const int i = rows ? rows[t] : t;
+  if (fc[i] >= 0) return;
   const int a = trp[i], m = trp[i + 1] - a;
   if (m == 0) return;
   double *B = Q + (size_t)a * nt;
@@ -423,6 +428,107 @@ __global__ void k_emin_constraints(int n, int nt, double condmax, const int *__r
   }
   for (int k = rank; k < nt; ++k)
     for (int r = 0; r < m; ++r) B[(size_t)k * m + r] = 0.0;
+}
+
+// The constraint step for fine rows of ntv < m <= 32 pattern entries, a warp
+// per row: lane r holds row r of B (NT test-vector values) in registers; the
+// Householder QR (dgeqr2's reflectors), the condition test, R' y = g, the
+// explicit Q (dorg2r) and p0 += Q y run with warp sums and shuffles, and the
+// lanes write Q's columns coalesced.  Rows of other lengths, and rows whose
+// R fails the condition test, are listed in defer[] for k_emin_constraints
+// (p0 and Q of a deferred row are left untouched).
+template <int NT>
+__global__ void __launch_bounds__(32 * kEminWarps)
+k_emin_constraints_warp(int n, double condmax, const int *__restrict__ trp,
+                        const int *__restrict__ tci, const int *__restrict__ fc,
+                        const int *__restrict__ c2glo, const double *__restrict__ TV,
+                        double *__restrict__ Q, double *__restrict__ p0, int *__restrict__ defer,
+                        int *__restrict__ ndefer) {
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = gwarp; i < n; i += nwarps) {
+    if (__ldg(fc + i) >= 0) continue;
+    const int a = __ldg(trp + i), m = __ldg(trp + i + 1) - a;
+    if (m == 0) continue;
+    if (m <= NT || m > 32) {
+      if (lane == 0) defer[atomicAdd(ndefer, 1)] = i;
+      continue;
+    }
+    const bool act = lane < m;
+    double b[NT];
+    double p = 0.0;
+    if (act) {
+      const double *tv = TV + (size_t)__ldg(c2glo + __ldg(tci + a + lane)) * NT;
+#pragma unroll
+      for (int k = 0; k < NT; ++k) b[k] = tv[k];
+      p = p0[a + lane];
+    } else {
+#pragma unroll
+      for (int k = 0; k < NT; ++k) b[k] = 0.0;
+    }
+    double g[NT], tau[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) g[k] = TV[(size_t)i * NT + k] - warp_sum(b[k] * p);
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+      const double alpha = __shfl_sync(kFull, b[k], k);
+      const double xn = sqrt(warp_sum(lane > k ? b[k] * b[k] : 0.0));
+      if (xn == 0.0) {
+        tau[k] = 0.0;
+        continue;
+      }
+      const double beta = -copysign(hypot(alpha, xn), alpha);
+      tau[k] = (beta - alpha) / beta;
+      const double sc = 1.0 / (alpha - beta);
+      if (lane > k) b[k] *= sc;
+      else if (lane == k) b[k] = beta;
+      const double v = lane > k ? b[k] : (lane == k ? 1.0 : 0.0);
+#pragma unroll
+      for (int j = k + 1; j < NT; ++j) {
+        const double w = warp_sum(v * b[j]) * tau[k];
+        if (lane >= k) b[j] -= w * v;
+      }
+    }
+    double dmax = 0.0, dmin = 1.7976931348623157e308;
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {
+      const double d = fabs(__shfl_sync(kFull, b[k], k));
+      dmax = fmax(dmax, d);
+      dmin = fmin(dmin, d);
+    }
+    if (dmax / dmin > condmax) {
+      if (lane == 0) defer[atomicAdd(ndefer, 1)] = i;
+      continue;
+    }
+    double y[NT];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) {                     // R' y = g
+      double s = g[k];
+#pragma unroll
+      for (int l = 0; l < k; ++l) s -= __shfl_sync(kFull, b[k], l) * y[l];
+      y[k] = s / __shfl_sync(kFull, b[k], k);
+    }
+#pragma unroll
+    for (int k = NT - 1; k >= 0; --k) {                // explicit Q
+      const double v = lane > k ? b[k] : (lane == k ? 1.0 : 0.0);
+#pragma unroll
+      for (int j = k + 1; j < NT; ++j) {
+        const double w = warp_sum(v * b[j]) * tau[k];
+        if (lane >= k) b[j] -= w * v;
+      }
+      b[k] = lane > k ? -tau[k] * v : (lane == k ? 1.0 - tau[k] : 0.0);
+    }
+    if (act) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NT; ++k) s += b[k] * y[k];
+      p0[a + lane] = p + s;
+      double *q = Q + (size_t)a * NT;
+#pragma unroll
+      for (int k = 0; k < NT; ++k) q[(size_t)k * m + lane] = b[k];
+    }
+  }
 }
 
 // gather_f.cpp (f(i,c) = -A(c2glo[c], i) on the pattern, 0 where A has no
@@ -792,10 +898,43 @@ HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const 
   k_emin_copy_prol<<<ceil_div(n, tpb), tpb, 0, st>>>(n, fcd.get(), prp.get(), pci.get(), pv.get(),
                                                       trp.get(), tci.get(), p0.get());
   CHRONOS_CHECK_LAUNCH();
-  k_emin_constraints<<<ceil_div(n, tpb), tpb, 0, st>>>(n, ntv, prm.condmax, trp.get(), tci.get(),
-                                                        fcd.get(), c2g.get(), tvd.get(), Qd.get(),
-                                                        p0.get(), svd_rows.get());
+  // constraint blocks: a warp per row for the common test-space sizes, the
+  // deferred rows (and every row for other sizes) a thread per row
+  DBuf<int> defer(n), ndefer(1);
+  ndefer.zero(st);
+  bool warp_path = true;
+  const int cg = warp_grid(n);
+  switch (ntv) {
+#define CHRONOS_EMIN_CW(NTV)                                                                    \
+  case NTV:                                                                                     \
+    k_emin_constraints_warp<NTV><<<cg, 32 * kEminWarps, 0, st>>>(                              \
+        n, prm.condmax, trp.get(), tci.get(), fcd.get(), c2g.get(), tvd.get(), Qd.get(),        \
+        p0.get(), defer.get(), ndefer.get());                                                   \
+    break;
+    CHRONOS_EMIN_CW(1)
+    CHRONOS_EMIN_CW(2)
+    CHRONOS_EMIN_CW(3)
+    CHRONOS_EMIN_CW(4)
+    CHRONOS_EMIN_CW(6)
+#undef CHRONOS_EMIN_CW
+    default: warp_path = false;
+  }
   CHRONOS_CHECK_LAUNCH();
+  if (warp_path) {
+    const int nd = ndefer.to_host(st)[0];
+    if (nd > 0) {
+      k_emin_constraints<<<ceil_div(nd, tpb), tpb, 0, st>>>(n, ntv, prm.condmax, trp.get(),
+                                                            tci.get(), fcd.get(), c2g.get(),
+                                                            tvd.get(), Qd.get(), p0.get(),
+                                                            svd_rows.get(), defer.get(), nd);
+      CHRONOS_CHECK_LAUNCH();
+    }
+  } else {
+    k_emin_constraints<<<ceil_div(n, tpb), tpb, 0, st>>>(n, ntv, prm.condmax, trp.get(), tci.get(),
+                                                          fcd.get(), c2g.get(), tvd.get(), Qd.get(),
+                                                          p0.get(), svd_rows.get(), nullptr, 0);
+    CHRONOS_CHECK_LAUNCH();
+  }
   k_emin_f_dinv<<<ceil_div(n, tpb), tpb, 0, st>>>(n, arp, aci, av, trp.get(), tci.get(), c2g.get(),
                                                    f.get(), dinv.get());
   CHRONOS_CHECK_LAUNCH();
