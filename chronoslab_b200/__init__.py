@@ -322,10 +322,9 @@ def emin_pattern(S, P, fcnode, kpow=2, nnzr_max=30, nnzr_min=None):
     if nnzr_min is None:
         raise ValueError("nnzr_min (the number of test vectors) is required")
     fc = np.ascontiguousarray(fcnode, dtype=np.int32)
-    si, sx, sv = (S.indptr.astype(np.int32), S.indices.astype(np.int32),
-                  np.ascontiguousarray(S.data, np.float64))
-    pi, px, pv = (P.indptr.astype(np.int32), P.indices.astype(np.int32),
-                  np.ascontiguousarray(P.data, np.float64))
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+    si, sx, sv = i32(S.indptr), i32(S.indices), np.ascontiguousarray(S.data, np.float64)
+    pi, px, pv = i32(P.indptr), i32(P.indices), np.ascontiguousarray(P.data, np.float64)
     h = C.c_void_p()
     hr = C.c_int(0)
     check(load().chronos_emin_pattern(kpow, n, nc, _pi(si), _pi(sx), _pd(sv), _pi(pi), _pi(px),
@@ -352,9 +351,9 @@ def emin(A, P, pattern, fcnode, TV, prm=None, spd=True):
     ntv = TV.shape[1]
     tvc = np.ascontiguousarray(TV.T).ravel()           # column-major
     fc = np.ascontiguousarray(fcnode, dtype=np.int32)
-    pi, px, pv = (P.indptr.astype(np.int32), P.indices.astype(np.int32),
-                  np.ascontiguousarray(P.data, np.float64))
-    ti, tx = T.indptr.astype(np.int32), T.indices.astype(np.int32)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)  # noqa: E731
+    pi, px, pv = i32(P.indptr), i32(P.indices), np.ascontiguousarray(P.data, np.float64)
+    ti, tx = i32(T.indptr), i32(T.indices)
     info = np.zeros(12)
     h = C.c_void_p()
     check(load().chronos_emin(C.byref(prm), n, _pi(ip), _pi(ix), _pd(dv), nc, _pi(pi), _pi(px),

@@ -366,30 +366,6 @@ int chronos_bamg_device(const chronos_params *prm, int n, const int *iat_S_h, co
                     max_neigh);
 }
 
-// n x ncols host CSR from caller arrays (values 1 when v is null): row
-// pointers nondecreasing from 0, columns ascending in [0, ncols).
-static HostCSR caller_csr(int n, int ncols, const int *iat, const int *ja, const double *v,
-                          const char *what) {
-  CHRONOS_REQUIRE(iat && ja && iat[0] == 0, CHRONOS_EINVAL,
-                  std::string(what) + ": row pointers must start at 0");
-  HostCSR M;
-  M.nrows = n;
-  M.ncols = ncols;
-  M.rp.assign(iat, iat + n + 1);
-  for (int i = 0; i < n; ++i) {
-    CHRONOS_REQUIRE(M.rp[i + 1] >= M.rp[i], CHRONOS_EINVAL,
-                    std::string(what) + ": decreasing row pointers");
-    for (int64_t k = M.rp[i]; k < M.rp[i + 1]; ++k)
-      CHRONOS_REQUIRE(ja[k] >= 0 && ja[k] < ncols && (k == M.rp[i] || ja[k] > ja[k - 1]),
-                      CHRONOS_EINVAL,
-                      std::string(what) + ": columns must be ascending in [0, ncols)");
-  }
-  M.ci.assign(ja, ja + M.rp[n]);
-  if (v) M.v.assign(v, v + M.rp[n]);
-  else M.v.assign(M.rp[n], 1.0);
-  return M;
-}
-
 // fcnode as chronos_coarsen numbers it (coarse k -> k in 1..nc, fine < 0)
 // -> coarse index or -1; nc counted.
 static std::vector<int> coarse_index(int n, const int *fcnode_h, int *nc) {
@@ -410,16 +386,20 @@ int chronos_emin_pattern(int kpow, int n, int nc, const int *iat_S_h, const int 
     CallRange range_("chronos_emin_pattern");
     CHRONOS_REQUIRE(n > 0 && nc > 0 && nc <= n && fcnode_h && coef_S_h && coef_P_h && patt,
                     CHRONOS_EINVAL, "bad argument");
-    HostCSR S = caller_csr(n, n, iat_S_h, ja_S_h, coef_S_h, "S");
-    HostCSR P = caller_csr(n, nc, iat_P_h, ja_P_h, coef_P_h, "P");
+    const CsrRef S{n, n, iat_S_h, ja_S_h, coef_S_h};
+    const CsrRef P{n, nc, iat_P_h, ja_P_h, coef_P_h};
+    validate_ref(S, "S");
+    validate_ref(P, "P");
     int ncf = 0;
     std::vector<int> fc0 = coarse_index(n, fcnode_h, &ncf);
     CHRONOS_REQUIRE(ncf == nc, CHRONOS_EINVAL, "fcnode must mark exactly nc coarse nodes");
     EminStrength str;
     str.S = &S;
     ScopedStream ss;
-    *patt = wrap_csr(emin_pattern_device(kpow, n, nc, str, P, fc0, nnzr_max, nnzr_min, ss.st,
-                                         host_rows));
+    DevPattern dp;
+    emin_pattern_device(kpow, n, nc, str, P, fc0, nnzr_max, nnzr_min, true, dp, ss.st,
+                        host_rows);
+    *patt = wrap_csr(dp.to_host(ss.st));
   });
 }
 
@@ -433,13 +413,17 @@ int chronos_emin(const chronos_params *prm, int n, const int *iat_A_h, const int
     CHRONOS_REQUIRE(prm && n > 0 && nc > 0 && nc <= n && coef_A_h && coef_P_h && fcnode_h &&
                         TV_h && P && ntv >= 1,
                     CHRONOS_EINVAL, "bad argument");
-    HostCSR A = caller_csr(n, n, iat_A_h, ja_A_h, coef_A_h, "A");
-    HostCSR Pin = caller_csr(n, nc, iat_P_h, ja_P_h, coef_P_h, "P");
-    HostCSR patt = caller_csr(n, nc, iat_patt_h, ja_patt_h, nullptr, "pattern");
+    const CsrRef A{n, n, iat_A_h, ja_A_h, coef_A_h};
+    const CsrRef Pin{n, nc, iat_P_h, ja_P_h, coef_P_h};
+    const CsrRef T{n, nc, iat_patt_h, ja_patt_h, nullptr};
+    validate_ref(A, "A");
+    validate_ref(Pin, "P");
     int ncf = 0;
     std::vector<int> fc0 = coarse_index(n, fcnode_h, &ncf);
     CHRONOS_REQUIRE(ncf == nc, CHRONOS_EINVAL, "fcnode must mark exactly nc coarse nodes");
+    validate_ref(T, "pattern", &fc0);
     std::vector<double> TVr((size_t)n * ntv);
+#pragma omp parallel for schedule(static, 8192)
     for (int i = 0; i < n; ++i)
       for (int j = 0; j < ntv; ++j) TVr[(size_t)i * ntv + j] = TV_h[(size_t)j * n + i];
     EminParams ep;
@@ -452,11 +436,22 @@ int chronos_emin(const chronos_params *prm, int n, const int *iat_A_h, const int
     ScopedStream ss;
     DBuf<int> arp, aci;
     DBuf<double> av;
-    std::vector<int> rp32(A.rp.begin(), A.rp.end());
-    arp.upload(rp32, ss.st);
-    aci.upload(A.ci, ss.st);
-    av.upload(A.v, ss.st);
-    *P = wrap_csr(emin_device(ep, n, nc, arp.get(), aci.get(), av.get(), Pin, patt, fc0,
+    arp.upload(iat_A_h, (size_t)n + 1, ss.st);
+    aci.upload(ja_A_h, (size_t)A.nnz(), ss.st);
+    av.upload(coef_A_h, (size_t)A.nnz(), ss.st);
+    DevPattern dp;
+    dp.n = n;
+    dp.nc = nc;
+    dp.rp_h.assign(iat_patt_h, iat_patt_h + n + 1);
+    dp.nnz = T.nnz();
+    dp.mmax = 0;
+    for (int i = 0; i < n; ++i) dp.mmax = std::max(dp.mmax, dp.rp_h[i + 1] - dp.rp_h[i]);
+    dp.rp.upload(dp.rp_h, ss.st);
+    dp.ci.alloc(std::max<int64_t>(dp.nnz, 1));
+    if (dp.nnz)
+      CHRONOS_CUDA(cudaMemcpyAsync(dp.ci.get(), ja_patt_h, sizeof(int) * dp.nnz,
+                                   cudaMemcpyHostToDevice, ss.st));
+    *P = wrap_csr(emin_device(ep, n, nc, arp.get(), aci.get(), av.get(), Pin, dp, fc0,
                               TVr.data(), ntv, ss.st, info));
   });
 }

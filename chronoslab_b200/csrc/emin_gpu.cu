@@ -142,28 +142,76 @@ k_emin_pattern(int n, const int *__restrict__ srp, const int *__restrict__ sci,
     for (int s = lane; s < tb; s += 32) keys[s] = -1;
     __syncwarp();
     const double di = FROM_A ? __ldg(diag + i) : 0.0;
-    for (int ks = sb; ks < se; ++ks) {
-      const int j = __ldg(sci + ks);
-      double sij = __ldg(sv + ks);
-      if (FROM_A) {
-        // cpt_SoC_dom.m:26-47: S keeps s_ij unless s_ij <= tau
-        sij = __ddiv_rn(fabs(sij), __dsqrt_rn(__dmul_rn(di, __ldg(diag + j))));
-        if (sij <= tau) continue;                      // the same for every lane
+    // PT_U entries of S's row at a time: the loads of their P_cur rows and the
+    // own-column tests are issued together, the table updates made one S
+    // entry after the other (each column's sum in S's row order)
+    constexpr int PT_U = 4;
+    auto add = [&](int c, double t) {
+      unsigned h = col_hash(c) & rmask;
+      while (true) {                                   // ends: fewer keys than slots
+        const int prev = atomicCAS(&keys[h], -1, c);
+        if (prev == -1) { vals[h] = t; break; }
+        if (prev == c) { vals[h] = __dadd_rn(vals[h], t); break; }
+        h = (h + 1) & rmask;
       }
-      const int cb = __ldg(crp + j), ce = __ldg(crp + j + 1);
-      for (int kp = cb + lane; kp < ce; kp += 32) {
-        const int c = __ldg(cci + kp);
-        if (has_col(p0ci + s0, n0, c)) continue;
-        const double t = __dmul_rn(sij, __ldg(cv + kp));
-        unsigned h = col_hash(c) & rmask;
-        while (true) {                                 // ends: fewer keys than slots
-          const int prev = atomicCAS(&keys[h], -1, c);
-          if (prev == -1) { vals[h] = t; break; }
-          if (prev == c) { vals[h] = __dadd_rn(vals[h], t); break; }
-          h = (h + 1) & rmask;
+    };
+    for (int ks0 = sb; ks0 < se; ks0 += PT_U) {
+      int cb[PT_U], ce[PT_U];
+      double sij[PT_U];
+#pragma unroll
+      for (int u = 0; u < PT_U; ++u) {
+        cb[u] = ce[u] = 0;
+        sij[u] = 0.0;
+        if (ks0 + u < se) {
+          const int j = __ldg(sci + ks0 + u);
+          double sv_u = __ldg(sv + ks0 + u);
+          bool strong = true;
+          if (FROM_A) {
+            // cpt_SoC_dom.m:26-47: S keeps s_ij unless s_ij <= tau
+            sv_u = __ddiv_rn(fabs(sv_u), __dsqrt_rn(__dmul_rn(di, __ldg(diag + j))));
+            strong = !(sv_u <= tau);
+          }
+          if (strong) {
+            cb[u] = __ldg(crp + j);
+            ce[u] = __ldg(crp + j + 1);
+            sij[u] = sv_u;
+          }
         }
       }
-      __syncwarp();
+      bool wide = false;
+#pragma unroll
+      for (int u = 0; u < PT_U; ++u) wide |= ce[u] - cb[u] > 32;
+      if (!wide) {
+        int cc[PT_U];
+        double tt[PT_U];
+#pragma unroll
+        for (int u = 0; u < PT_U; ++u) {
+          cc[u] = -1;
+          tt[u] = 0.0;
+          const int kp = cb[u] + lane;
+          if (kp < ce[u]) {
+            const int c = __ldg(cci + kp);
+            if (!has_col(p0ci + s0, n0, c)) {
+              cc[u] = c;
+              tt[u] = __dmul_rn(sij[u], __ldg(cv + kp));
+            }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < PT_U; ++u) {
+          if (cc[u] >= 0) add(cc[u], tt[u]);
+          __syncwarp();
+        }
+      } else {
+        for (int u = 0; u < PT_U; ++u) {                  // a P_cur row beyond 32 entries
+          for (int kp = cb[u] + lane; kp < ce[u]; kp += 32) {
+            const int c = __ldg(cci + kp);
+            if (has_col(p0ci + s0, n0, c)) continue;
+            add(c, __dmul_rn(sij[u], __ldg(cv + kp)));
+          }
+          __syncwarp();
+        }
+      }
     }
     __syncwarp();
     // nonzero candidates, compacted
@@ -685,6 +733,42 @@ __global__ void k_diag_of(int n, const int *__restrict__ rp, const int *__restri
   d[i] = (p < e && ci[p] == i) ? v[p] : 0.0;
 }
 
+// Prol_add_Cnodes.cpp + sparse(): entries per row of the final P (a coarse
+// row: its unit entry; a fine row: its nonzero pattern entries) ...
+__global__ void k_emin_out_count(int n, const int *__restrict__ fc, const int *__restrict__ trp,
+                                 const double *__restrict__ pf, int *__restrict__ cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (fc[i] >= 0) {
+    cnt[i] = 1;
+    return;
+  }
+  int c = 0;
+  for (int k = trp[i]; k < trp[i + 1]; ++k) c += pf[k] != 0.0;
+  cnt[i] = c;
+}
+
+// ... and the entries themselves at the row pointers orp.
+__global__ void k_emin_out_fill(int n, const int *__restrict__ fc, const int *__restrict__ trp,
+                                const int *__restrict__ tci, const double *__restrict__ pf,
+                                const int *__restrict__ orp, int *__restrict__ oci,
+                                double *__restrict__ ov) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int o = orp[i];
+  if (fc[i] >= 0) {
+    oci[o] = fc[i];
+    ov[o] = 1.0;
+    return;
+  }
+  for (int k = trp[i]; k < trp[i + 1]; ++k)
+    if (pf[k] != 0.0) {
+      oci[o] = tci[k];
+      ov[o] = pf[k];
+      ++o;
+    }
+}
+
 std::vector<int> to_int32(const std::vector<int64_t> &v) {
   std::vector<int> out(v.size());
   for (size_t k = 0; k < v.size(); ++k) {
@@ -710,68 +794,137 @@ int warp_grid(int64_t rows) {
 
 }  // namespace
 
-HostCSR emin_pattern_device(int kpow, int n, int nc, const EminStrength &str, const HostCSR &P0,
-                            const std::vector<int> &fc0, int nnzr_max, int nnzr_min,
-                            cudaStream_t st, int *host_rows) {
+// Row lengths -> host row pointers and the widest row; compacts the capacity
+// slots into out (rows with len < 0 are left for the host).
+__global__ void k_emin_compact(int n, const int64_t *__restrict__ off, const int *__restrict__ len,
+                               const int *__restrict__ rp, const int *__restrict__ ci_in,
+                               const double *__restrict__ v_in, int *__restrict__ ci_out,
+                               double *__restrict__ v_out) {
+  const int lane = threadIdx.x & 31;
+  const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (int i = gwarp; i < n; i += nwarps) {
+    const int l = len[i];
+    if (l <= 0) continue;
+    const int64_t s = off[i];
+    const int d = rp[i];
+    for (int k = lane; k < l; k += 32) {
+      ci_out[d + k] = ci_in[s + k];
+      if (v_out) v_out[d + k] = v_in[s + k];
+    }
+  }
+}
+
+HostCSR DevPattern::to_host(cudaStream_t st) const {
+  HostCSR h;
+  h.nrows = n;
+  h.ncols = nc;
+  h.rp.assign(rp_h.begin(), rp_h.end());
+  h.ci.resize(nnz);
+  ci.download(h.ci.data(), nnz, st);
+  if (v.get()) {
+    h.v.resize(nnz);
+    v.download(h.v.data(), nnz, st);
+  }
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  return h;
+}
+
+std::vector<int> rp32(const HostCSR &M) { return to_int32(M.rp); }
+
+void validate_ref(const CsrRef &M, const char *what, const std::vector<int> *coarse) {
+  CHRONOS_REQUIRE(M.rp && M.rp[0] == 0 && (M.nnz() == 0 || M.ci), CHRONOS_EINVAL,
+                  std::string(what) + ": row pointers must start at 0");
+  int bad = 0;
+#pragma omp parallel for schedule(static, 4096) reduction(| : bad)
+  for (int i = 0; i < M.nrows; ++i) {
+    const int b = M.rp[i], e = M.rp[i + 1];
+    if (e < b) { bad |= 1; continue; }
+    if (coarse && e > b && (*coarse)[i] >= 0) bad |= 4;
+    for (int k = b; k < e; ++k)
+      if (M.ci[k] < 0 || M.ci[k] >= M.ncols || (k > b && M.ci[k] <= M.ci[k - 1])) bad |= 2;
+  }
+  CHRONOS_REQUIRE(!(bad & 1), CHRONOS_EINVAL, std::string(what) + ": decreasing row pointers");
+  CHRONOS_REQUIRE(!(bad & 2), CHRONOS_EINVAL,
+                  std::string(what) + ": columns must be ascending in [0, ncols)");
+  CHRONOS_REQUIRE(!(bad & 4), CHRONOS_EINVAL, std::string(what) + ": entries in coarse rows");
+}
+
+void emin_pattern_device(int kpow, int n, int nc, const EminStrength &str, const CsrRef &P0,
+                         const std::vector<int> &fc0, int nnzr_max, int nnzr_min, bool values,
+                         DevPattern &out, cudaStream_t st, int *host_rows) {
   const int nnzr = std::max(nnzr_max, nnzr_min);
   if (host_rows) *host_rows = 0;
-  if (kpow <= 1) {                                     // P's fine rows as they are
-    HostCSR out;
-    out.nrows = n;
-    out.ncols = nc;
-    out.rp.assign((size_t)n + 1, 0);
-    for (int i = 0; i < n; ++i) {
-      if (fc0[i] < 0)
-        for (int64_t k = P0.rp[i]; k < P0.rp[i + 1]; ++k) {
-          out.ci.push_back(P0.ci[k]);
-          out.v.push_back(P0.v[k]);
-        }
-      out.rp[i + 1] = (int64_t)out.ci.size();
-    }
-    return out;
-  }
+  out.n = n;
+  out.nc = nc;
   const bool from_a = str.S == nullptr;
-  DBuf<int> srp, sci, p0rp, p0ci, fcd, crp, cci, olen;
-  DBuf<double> sv, diag, cv, ov;
+  DBuf<int> srp, sci, p0rp, p0ci, fcd, olen;
+  DBuf<double> sv, diag, p0v, ov;
   DBuf<int64_t> ooff;
   DBuf<int> ocid;
+  p0rp.upload(P0.rp, (size_t)n + 1, st);
+  p0ci.upload(P0.ci, (size_t)P0.nnz(), st);
+  p0v.upload(P0.v, (size_t)P0.nnz(), st);
+  fcd.upload(fc0, st);
+  if (kpow <= 1) {                                     // P's fine rows as they are
+    std::vector<int64_t> off((size_t)n + 1, 0);
+    std::vector<int> len(n);
+    out.rp_h.assign((size_t)n + 1, 0);
+    out.mmax = 0;
+    for (int i = 0; i < n; ++i) {
+      off[i] = P0.rp[i];
+      len[i] = fc0[i] < 0 ? P0.rp[i + 1] - P0.rp[i] : 0;
+      out.rp_h[i + 1] = out.rp_h[i] + len[i];
+      out.mmax = std::max(out.mmax, len[i]);
+    }
+    out.nnz = out.rp_h[n];
+    ooff.upload(off, st);
+    olen.upload(len, st);
+    out.rp.upload(out.rp_h, st);
+    out.ci.alloc(std::max<int64_t>(out.nnz, 1));
+    if (values) out.v.alloc(std::max<int64_t>(out.nnz, 1));
+    k_emin_compact<<<warp_grid(n), 32 * kEminWarps, 0, st>>>(
+        n, ooff.get(), olen.get(), out.rp.get(), p0ci.get(), p0v.get(), out.ci.get(),
+        values ? out.v.get() : nullptr);
+    CHRONOS_CHECK_LAUNCH();
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
   if (from_a) {
     diag.alloc(n);
     k_diag_of<<<ceil_div(n, 256), 256, 0, st>>>(n, str.arp, str.aci, str.av, diag.get());
     CHRONOS_CHECK_LAUNCH();
   } else {
-    srp.upload(to_int32(str.S->rp), st);
-    sci.upload(str.S->ci, st);
-    sv.upload(str.S->v, st);
+    srp.upload(str.S->rp, (size_t)n + 1, st);
+    sci.upload(str.S->ci, (size_t)str.S->nnz(), st);
+    sv.upload(str.S->v, (size_t)str.S->nnz(), st);
   }
   const int *srp_d = from_a ? str.arp : srp.get();
   const int *sci_d = from_a ? str.aci : sci.get();
   const double *sv_d = from_a ? str.av : sv.get();
-  p0rp.upload(to_int32(P0.rp), st);
-  p0ci.upload(P0.ci, st);
-  fcd.upload(fc0, st);
-  HostCSR cur = P0;                                    // P_cur of MEX_cptProlPatt
+  int64_t maxs = from_a ? str.max_row : 0;
+  if (!from_a)
+    for (int i = 0; i < n; ++i) maxs = std::max<int64_t>(maxs, str.S->rp[i + 1] - str.S->rp[i]);
+  // P_cur of MEX_cptProlPatt: P0 for the first step, then the previous step's
+  // output (device; its host copy made only when a host row needs it)
+  const int *crp = p0rp.get(), *cci = p0ci.get();
+  const double *cv = p0v.get();
+  std::vector<int> cur_rp(P0.rp, P0.rp + n + 1);
+  DevPattern prev;
+  HostCSR cur_h, S_h;
+  bool have_cur_h = false, have_s_h = false;
   std::vector<int> cols;
   std::vector<double> vals;
-  HostCSR S_host;                                      // for host rows, built when needed
-  bool have_s_host = false;
   for (int ipow = 2; ipow <= kpow; ++ipow) {
     const bool last = ipow == kpow;
-    crp.upload(to_int32(cur.rp), st);
-    cci.upload(cur.ci, st);
-    cv.upload(cur.v, st);
-    // capacities and the candidate table
     std::vector<int64_t> off((size_t)n + 1, 0);
     int maxlen = 0;
     for (int i = 0; i < n; ++i) {
-      const int n0 = (int)(P0.rp[i + 1] - P0.rp[i]);
+      const int n0 = P0.rp[i + 1] - P0.rp[i];
       const int cap = (last && fc0[i] >= 0) ? 0 : std::max(nnzr, n0);
       off[i + 1] = off[i] + cap;
+      maxlen = std::max(maxlen, cur_rp[i + 1] - cur_rp[i]);
     }
-    for (int i = 0; i < n; ++i) maxlen = std::max<int>(maxlen, (int)(cur.rp[i + 1] - cur.rp[i]));
-    int64_t maxs = from_a ? str.max_row : 0;
-    if (!from_a)
-      for (int i = 0; i < n; ++i) maxs = std::max<int64_t>(maxs, str.S->rp[i + 1] - str.S->rp[i]);
     const int64_t bound = maxs * (int64_t)maxlen;
     int table = 64;
     while (table < kPattMaxTable && table < 2 * bound) table <<= 1;
@@ -791,55 +944,110 @@ HostCSR emin_pattern_device(int kpow, int n, int nc, const EminStrength &str, co
       CHRONOS_CUDA(cudaFuncSetAttribute(k_emin_pattern<true>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_emin_pattern<true><<<grid, 32 * wpb, smem, st>>>(
-          n, srp_d, sci_d, sv_d, diag.get(), str.tau, crp.get(), cci.get(), cv.get(),
-          p0rp.get(), p0ci.get(), fcd.get(), nnzr, last ? 1 : 0, table, ooff.get(), ocid.get(),
-          ov.get(), olen.get());
+          n, srp_d, sci_d, sv_d, diag.get(), str.tau, crp, cci, cv, p0rp.get(), p0ci.get(),
+          fcd.get(), nnzr, last ? 1 : 0, table, ooff.get(), ocid.get(), ov.get(), olen.get());
     } else {
       CHRONOS_CUDA(cudaFuncSetAttribute(k_emin_pattern<false>,
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_emin_pattern<false><<<grid, 32 * wpb, smem, st>>>(
-          n, srp_d, sci_d, sv_d, nullptr, 0.0, crp.get(), cci.get(), cv.get(), p0rp.get(),
-          p0ci.get(), fcd.get(), nnzr, last ? 1 : 0, table, ooff.get(), ocid.get(), ov.get(),
-          olen.get());
+          n, srp_d, sci_d, sv_d, nullptr, 0.0, crp, cci, cv, p0rp.get(), p0ci.get(), fcd.get(),
+          nnzr, last ? 1 : 0, table, ooff.get(), ocid.get(), ov.get(), olen.get());
     }
     CHRONOS_CHECK_LAUNCH();
     std::vector<int> len = olen.to_host(st);
-    std::vector<int> oci(off[n]);
-    std::vector<double> oval(off[n]);
-    ocid.download(oci.data(), off[n], st);
-    ov.download(oval.data(), off[n], st);
-    CHRONOS_CUDA(cudaStreamSynchronize(st));
-    HostCSR next;
-    next.nrows = n;
-    next.ncols = nc;
-    next.rp.assign((size_t)n + 1, 0);
-    for (int i = 0; i < n; ++i) {
-      if (len[i] < 0) {
-        if (!have_s_host) {
-          S_host = from_a ? str.host_strength() : *str.S;
-          have_s_host = true;
+    // rows left to the host
+    std::vector<int> hrows;
+    std::vector<std::vector<int>> hcols;
+    std::vector<std::vector<double>> hvals;
+    for (int i = 0; i < n; ++i)
+      if (len[i] < 0) hrows.push_back(i);
+    if (!hrows.empty()) {
+      if (!have_s_h) {
+        if (from_a) {
+          std::vector<int> arp_h(n + 1), aci_h(str.nnz);
+          std::vector<double> av_h(str.nnz);
+          CHRONOS_CUDA(cudaMemcpy(arp_h.data(), str.arp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
+          CHRONOS_CUDA(cudaMemcpy(aci_h.data(), str.aci, sizeof(int) * str.nnz, cudaMemcpyDeviceToHost));
+          CHRONOS_CUDA(cudaMemcpy(av_h.data(), str.av, sizeof(double) * str.nnz, cudaMemcpyDeviceToHost));
+          HostCSR A;
+          A.nrows = A.ncols = n;
+          A.rp.assign(arp_h.begin(), arp_h.end());
+          A.ci = std::move(aci_h);
+          A.v = std::move(av_h);
+          S_h = soc_matrix(A, "DOM", str.tau);     // cpt_SoC_dom.m:26-47 with values
         }
-        emin_pattern_row(i, S_host, cur, P0, nnzr, cols, vals);
-        if (host_rows) ++*host_rows;
-        next.ci.insert(next.ci.end(), cols.begin(), cols.end());
-        next.v.insert(next.v.end(), vals.begin(), vals.end());
-      } else {
-        next.ci.insert(next.ci.end(), oci.begin() + off[i], oci.begin() + off[i] + len[i]);
-        next.v.insert(next.v.end(), oval.begin() + off[i], oval.begin() + off[i] + len[i]);
+        have_s_h = true;
       }
-      next.rp[i + 1] = (int64_t)next.ci.size();
+      if (ipow > 2 && !have_cur_h) {
+        cur_h = prev.to_host(st);
+        have_cur_h = true;
+      }
+      std::vector<int> srp32;
+      CsrRef Sref;
+      if (from_a) {
+        srp32 = to_int32(S_h.rp);
+        Sref = CsrRef{n, n, srp32.data(), S_h.ci.data(), S_h.v.data()};
+      } else {
+        Sref = *str.S;
+      }
+      std::vector<int> crp32;
+      CsrRef Cref = P0;
+      if (ipow > 2) {
+        crp32 = to_int32(cur_h.rp);
+        Cref = CsrRef{n, nc, crp32.data(), cur_h.ci.data(), cur_h.v.data()};
+      }
+      hcols.resize(hrows.size());
+      hvals.resize(hrows.size());
+      for (size_t h = 0; h < hrows.size(); ++h) {
+        emin_pattern_row(hrows[h], Sref, Cref, P0, nnzr, hcols[h], hvals[h]);
+        len[hrows[h]] = (int)hcols[h].size();
+      }
+      if (host_rows) *host_rows += (int)hrows.size();
     }
-    cur.rp.swap(next.rp);
-    cur.ci.swap(next.ci);
-    cur.v.swap(next.v);
+    // compact into the step's output
+    DevPattern next;
+    next.n = n;
+    next.nc = nc;
+    next.rp_h.assign((size_t)n + 1, 0);
+    next.mmax = 0;
+    for (int i = 0; i < n; ++i) {
+      next.rp_h[i + 1] = next.rp_h[i] + len[i];
+      next.mmax = std::max(next.mmax, len[i]);
+    }
+    next.nnz = next.rp_h[n];
+    const bool keep_v = values || !last;
+    next.rp.upload(next.rp_h, st);
+    next.ci.alloc(std::max<int64_t>(next.nnz, 1));
+    if (keep_v) next.v.alloc(std::max<int64_t>(next.nnz, 1));
+    for (int h : hrows) len[h] = -1;
+    olen.upload(len, st);
+    k_emin_compact<<<warp_grid(n), 32 * kEminWarps, 0, st>>>(
+        n, ooff.get(), olen.get(), next.rp.get(), ocid.get(), ov.get(), next.ci.get(),
+        keep_v ? next.v.get() : nullptr);
+    CHRONOS_CHECK_LAUNCH();
+    for (size_t h = 0; h < hrows.size(); ++h) {
+      const int i = hrows[h];
+      const size_t l = hcols[h].size();
+      if (!l) continue;
+      CHRONOS_CUDA(cudaMemcpyAsync(next.ci.get() + next.rp_h[i], hcols[h].data(), sizeof(int) * l,
+                                   cudaMemcpyHostToDevice, st));
+      if (keep_v)
+        CHRONOS_CUDA(cudaMemcpyAsync(next.v.get() + next.rp_h[i], hvals[h].data(),
+                                     sizeof(double) * l, cudaMemcpyHostToDevice, st));
+    }
+    CHRONOS_CUDA(cudaStreamSynchronize(st));            // the host rows' buffers end here
+    prev = std::move(next);
+    have_cur_h = false;
+    crp = prev.rp.get();
+    cci = prev.ci.get();
+    cv = prev.v.get();
+    cur_rp = prev.rp_h;
   }
-  cur.nrows = n;
-  cur.ncols = nc;
-  return cur;
+  out = std::move(prev);
 }
 
 HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const int *aci,
-                    const double *av, const HostCSR &Pin, const HostCSR &patt,
+                    const double *av, const CsrRef &Pin, const DevPattern &patt,
                     const std::vector<int> &fc0, const double *TVr, int ntv, cudaStream_t st,
                     double *info) {
   using clk = std::chrono::steady_clock;
@@ -853,7 +1061,7 @@ HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const 
   CHRONOS_REQUIRE(prm.spd, CHRONOS_ENOTSUP, "EMIN for a nonsymmetric A is outside this path");
   CHRONOS_REQUIRE(ntv >= 1 && ntv <= kEminMaxTv, CHRONOS_ENOTSUP,
                   "EMIN takes 1 to 16 test vectors");
-  CHRONOS_REQUIRE(patt.nrows == n && Pin.nrows == n && (int)fc0.size() == n, CHRONOS_EINVAL,
+  CHRONOS_REQUIRE(patt.n == n && Pin.nrows == n && (int)fc0.size() == n, CHRONOS_EINVAL,
                   "EMIN: pattern, P and fcnode must have n rows");
   std::vector<int> c2glo(std::max(nc, 1), -1);
   for (int i = 0; i < n; ++i) {
@@ -862,28 +1070,17 @@ HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const 
       c2glo[fc0[i]] = i;
     }
   }
-  int mmax = 0;
-  for (int i = 0; i < n; ++i) {
-    const int64_t m = patt.rp[i + 1] - patt.rp[i];
-    CHRONOS_REQUIRE(m == 0 || fc0[i] < 0, CHRONOS_EINVAL,
-                    "EMIN: the pattern must have no coarse rows");
-    mmax = std::max<int>(mmax, (int)m);
-    for (int64_t k = patt.rp[i]; k < patt.rp[i + 1]; ++k)
-      CHRONOS_REQUIRE(patt.ci[k] >= 0 && patt.ci[k] < nc &&
-                          (k == patt.rp[i] || patt.ci[k] > patt.ci[k - 1]),
-                      CHRONOS_EINVAL, "EMIN: pattern columns must be ascending in [0, nc)");
-  }
+  const int mmax = patt.mmax;
   for (int c = 0; c < nc; ++c)
     CHRONOS_REQUIRE(c2glo[c] >= 0, CHRONOS_EINVAL, "EMIN: coarse index without a node");
   CHRONOS_REQUIRE(mmax <= 4096, CHRONOS_ENOTSUP, "EMIN: pattern rows beyond 4096 entries");
-  const int64_t nt = patt.rp[n];
-  DBuf<int> trp, tci, prp, pci, fcd, c2g;
+  const int64_t nt = patt.nnz;
+  const DBuf<int> &trp = patt.rp, &tci = patt.ci;
+  DBuf<int> prp, pci, fcd, c2g;
   DBuf<double> pv, tvd;
-  trp.upload(to_int32(patt.rp), st);
-  tci.upload(patt.ci, st);
-  prp.upload(to_int32(Pin.rp), st);
-  pci.upload(Pin.ci, st);
-  pv.upload(Pin.v, st);
+  prp.upload(Pin.rp, (size_t)n + 1, st);
+  pci.upload(Pin.ci, (size_t)Pin.nnz(), st);
+  pv.upload(Pin.v, (size_t)Pin.nnz(), st);
   fcd.upload(fc0, st);
   c2g.upload(c2glo, st);
   tvd.upload(TVr, (size_t)n * ntv, st);
@@ -995,31 +1192,35 @@ HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const 
   }
   k_emin_sub<<<vg, 256, 0, st>>>(nt, p0.get(), dp.get(), p0.get());
   CHRONOS_CHECK_LAUNCH();
-  std::vector<double> pf(nt);
-  p0.download(pf.data(), nt, st);
   std::vector<int> nsvd = svd_rows.to_host(st);
-  CHRONOS_CUDA(cudaStreamSynchronize(st));
   const double t_solve = std::chrono::duration<double>(clk::now() - t_pcg).count();
-  // Prol_add_Cnodes + sparse(): unit coarse rows, exact zeros dropped
+  // Prol_add_Cnodes + sparse(): unit coarse rows, exact zeros dropped,
+  // assembled on the device (counts, host prefix sum, fill)
+  DBuf<int> cnt(n);
+  k_emin_out_count<<<ceil_div(n, tpb), tpb, 0, st>>>(n, fcd.get(), trp.get(), p0.get(), cnt.get());
+  CHRONOS_CHECK_LAUNCH();
+  std::vector<int> ch = cnt.to_host(st);
   HostCSR out;
   out.nrows = n;
   out.ncols = nc;
   out.rp.assign((size_t)n + 1, 0);
-  out.ci.reserve(nt + nc);
-  out.v.reserve(nt + nc);
+  std::vector<int> orp_h((size_t)n + 1, 0);
   for (int i = 0; i < n; ++i) {
-    if (fc0[i] >= 0) {
-      out.ci.push_back(fc0[i]);
-      out.v.push_back(1.0);
-    } else {
-      for (int64_t k = patt.rp[i]; k < patt.rp[i + 1]; ++k)
-        if (pf[k] != 0.0) {
-          out.ci.push_back(patt.ci[k]);
-          out.v.push_back(pf[k]);
-        }
-    }
-    out.rp[i + 1] = (int64_t)out.ci.size();
+    out.rp[i + 1] = out.rp[i] + ch[i];
+    orp_h[i + 1] = (int)out.rp[i + 1];
   }
+  const int64_t onnz = out.rp[n];
+  DBuf<int> orp, oci(std::max<int64_t>(onnz, 1));
+  DBuf<double> ov(std::max<int64_t>(onnz, 1));
+  orp.upload(orp_h, st);
+  k_emin_out_fill<<<ceil_div(n, tpb), tpb, 0, st>>>(n, fcd.get(), trp.get(), tci.get(), p0.get(),
+                                                     orp.get(), oci.get(), ov.get());
+  CHRONOS_CHECK_LAUNCH();
+  out.ci.resize(onnz);
+  out.v.resize(onnz);
+  oci.download(out.ci.data(), onnz, st);
+  ov.download(out.v.data(), onnz, st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
   if (info) {
     const double t_all = std::chrono::duration<double>(clk::now() - t_glob).count();
     for (int k = 0; k < 12; ++k) info[k] = 0.0;
@@ -1033,22 +1234,6 @@ HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const 
     info[6] = nsvd[0];                      // rows whose constraint block took the SVD branch
   }
   return out;
-}
-
-HostCSR EminStrength::host_strength() const {
-  // DOM strength of A with values (cpt_SoC_dom.m:26-47), for the rows the
-  // pattern kernel leaves to the host.
-  std::vector<int> rp(n + 1), ci(nnz);
-  std::vector<double> v(nnz);
-  CHRONOS_CUDA(cudaMemcpy(rp.data(), arp, sizeof(int) * (n + 1), cudaMemcpyDeviceToHost));
-  CHRONOS_CUDA(cudaMemcpy(ci.data(), aci, sizeof(int) * nnz, cudaMemcpyDeviceToHost));
-  CHRONOS_CUDA(cudaMemcpy(v.data(), av, sizeof(double) * nnz, cudaMemcpyDeviceToHost));
-  HostCSR A;
-  A.nrows = A.ncols = n;
-  A.rp.assign(rp.begin(), rp.end());
-  A.ci = std::move(ci);
-  A.v = std::move(v);
-  return soc_matrix(A, "DOM", tau);
 }
 
 }  // namespace chronos

@@ -1135,7 +1135,10 @@ void HierBuilder::end_level(int fl) {
     str.tau = prm.patt_tau;
     for (int i = 0; i < n; ++i)
       str.max_row = std::max<int>(str.max_row, (int)(Al.rp[i + 1] - Al.rp[i]));
-    HostCSR patt = emin_pattern_device(prm.patt_pow, n, nc, str, Ph, fc0, prm.nnzr_max, ntv, st);
+    const std::vector<int> prp = rp32(Ph);
+    const CsrRef P0{n, nc, prp.data(), Ph.ci.data(), Ph.v.data()};
+    DevPattern patt;
+    emin_pattern_device(prm.patt_pow, n, nc, str, P0, fc0, prm.nnzr_max, ntv, false, patt, st);
     EminParams ep;
     ep.itmax = prm.itmax_emin;
     ep.energ_tol = prm.energ_tol;
@@ -1144,11 +1147,11 @@ void HierBuilder::end_level(int fl) {
     ep.solv = prm.solv_emin;
     ep.spd = true;
     double info[12];
-    Ph = emin_device(ep, n, nc, L.A.rp.get(), L.A.ci.get(), L.A.v64.get(), Ph, patt, fc0,
+    Ph = emin_device(ep, n, nc, L.A.rp.get(), L.A.ci.get(), L.A.v64.get(), P0, patt, fc0,
                      TVr.data(), ntv, st, info);
     if (std::getenv("CHRONOS_TUNE_VERBOSE"))
       std::fprintf(stderr, "chronos setup: level %d EMIN pattern %lld entries, %d CG steps, "
-                   "%d SVD rows, %.3f s\n", level, (long long)patt.nnz(), (int)info[7],
+                   "%d SVD rows, %.3f s\n", level, (long long)patt.nnz, (int)info[7],
                    (int)info[6], info[5]);
   }
   std::vector<double> TVn((size_t)nc * ntv);

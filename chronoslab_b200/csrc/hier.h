@@ -157,13 +157,22 @@ bool gpu_bamg();
 // fly from the device CSR (arp, aci, av) of an n x n A with nnz entries and
 // rows of at most max_row entries (cpt_SoC_dom.m:26-47, prolong.m:213-217).
 struct EminStrength {
-  const HostCSR *S = nullptr;
+  const CsrRef *S = nullptr;
   const int *arp = nullptr, *aci = nullptr;
   const double *av = nullptr;
   int n = 0, max_row = 0;
   int64_t nnz = 0;
   double tau = 0.0;
-  HostCSR host_strength() const;    // the DOM S of A with values, on the host
+};
+// An n x nc EMIN pattern in device memory (values kept when asked for), with
+// its row pointers on the host.
+struct DevPattern {
+  int n = 0, nc = 0, mmax = 0;
+  int64_t nnz = 0;
+  DBuf<int> rp, ci;
+  DBuf<double> v;
+  std::vector<int> rp_h;
+  HostCSR to_host(cudaStream_t st) const;
 };
 // MEX_cptProlPatt (MEX_EMIN/MEX_cptProlPatt.cpp:234-490) on the GPU: the
 // n x nc EMIN pattern (values as the MEX returns them) from P0 (n x nc,
@@ -171,9 +180,9 @@ struct EminStrength {
 // most max(nnzr_max, nnzr_min) entries per row beyond P0's own.  Bit-identical
 // to the reference; rows whose candidates outgrow a warp's table are computed
 // by emin_pattern_row on the host (their count in *host_rows, may be null).
-HostCSR emin_pattern_device(int kpow, int n, int nc, const EminStrength &str, const HostCSR &P0,
-                            const std::vector<int> &fc0, int nnzr_max, int nnzr_min,
-                            cudaStream_t st, int *host_rows = nullptr);
+void emin_pattern_device(int kpow, int n, int nc, const EminStrength &str, const CsrRef &P0,
+                         const std::vector<int> &fc0, int nnzr_max, int nnzr_min, bool values,
+                         DevPattern &out, cudaStream_t st, int *host_rows = nullptr);
 // EMIN parameters of parm_PROLONG (read_prolong.m): itmax_emin, energ_tol,
 // condmax_emin, prec_emin, solv_emin, and whether A is symmetric.
 struct EminParams {
@@ -189,9 +198,15 @@ struct EminParams {
 // reference's info array (info[6]: rows whose constraint block took the SVD
 // branch; info[7]: iterations).
 HostCSR emin_device(const EminParams &prm, int n, int nc, const int *arp, const int *aci,
-                    const double *av, const HostCSR &Pin, const HostCSR &patt,
+                    const double *av, const CsrRef &Pin, const DevPattern &patt,
                     const std::vector<int> &fc0, const double *TVr, int ntv, cudaStream_t st,
                     double *info);
+// Row pointers, columns ascending in [0, ncols) and (when coarse is given)
+// no entries in coarse rows, or CHRONOS_EINVAL naming what; rows checked in
+// parallel.
+void validate_ref(const CsrRef &M, const char *what, const std::vector<int> *coarse = nullptr);
+// int32 row pointers of a HostCSR, for a CsrRef over it.
+std::vector<int> rp32(const HostCSR &M);
 
 // Source of a level's prolongation outside the library: given the 1-based
 // level number and the level's operator (FP64, from the GPU Galerkin product

@@ -9,14 +9,14 @@
 
 namespace chronos {
 
-void emin_pattern_row(int i, const HostCSR &S, const HostCSR &Pc, const HostCSR &P0, int nnzr,
+void emin_pattern_row(int i, const CsrRef &S, const CsrRef &Pc, const CsrRef &P0, int nnzr,
                       std::vector<int> &cols, std::vector<double> &vals) {
   const int64_t s0 = P0.rp[i], e0 = P0.rp[i + 1];
   const int n0 = (int)(e0 - s0);
   const int budget = std::max(0, nnzr - n0);
   cols.clear();
   vals.clear();
-  auto own = [&](int c) { return std::binary_search(P0.ci.begin() + s0, P0.ci.begin() + e0, c); };
+  auto own = [&](int c) { return std::binary_search(P0.ci + s0, P0.ci + e0, c); };
   std::vector<std::pair<int, double>> cand;       // first-seen order
   if (budget > 0) {
     std::unordered_map<int, size_t> at;

@@ -63,6 +63,15 @@ void bamg_rows_host(const BamgParams &prm, const HostCSR &S, const std::vector<i
                     std::vector<std::vector<int>> &rcols, std::vector<std::vector<double>> &rvals,
                     std::vector<int> &c_mark);
 
+// A CSR borrowed from its owner: int32 row pointers, v may be null.
+struct CsrRef {
+  int nrows = 0, ncols = 0;
+  const int *rp = nullptr;
+  const int *ci = nullptr;
+  const double *v = nullptr;
+  int64_t nnz() const { return rp ? rp[nrows] : 0; }
+};
+
 // ---- EMIN prolongation pattern (MEX_cptProlPatt.cpp) -------------------------
 // One row of a power step of the EMIN pattern (MEX_cptProlPatt.cpp:356-443):
 // the columns of (S * Pc)(i, :) that are not in P0's row i, summed in S's row
@@ -71,7 +80,7 @@ void bamg_rows_host(const BamgParams &prm, const HostCSR &S, const std::vector<i
 // P0's own columns with value 1; by column.  S with values, rows of P0 and
 // Pc with ascending columns.  The GPU pattern kernel hands rows whose
 // candidate lists outgrow its per-warp table to this function.
-void emin_pattern_row(int i, const HostCSR &S, const HostCSR &Pc, const HostCSR &P0, int nnzr,
+void emin_pattern_row(int i, const CsrRef &S, const CsrRef &Pc, const CsrRef &P0, int nnzr,
                       std::vector<int> &cols, std::vector<double> &vals);
 
 // ---- adaptive FSAI pattern search (cpt_afsai_coef.cpp) ----------------------
