@@ -183,3 +183,33 @@ def test_emin_elasticity40_matches_reference(lib):
     Pg, info = cb.emin(A, P, R, fc, TV, cb.params())
     assert int(info[7]) == int(rinfo[7])
     assert abs(Pg - Pr).max() <= 1e-13 * abs(Pr).max()
+
+
+def test_setup_with_emin_elasticity20_against_the_reference_path(lib):
+    """Q1 elasticity 20^3 with the rigid-body test space and prol_emin = EMIN:
+    the GPU setup against the CPU path built with the reference's FSAI, BAMG
+    and EMIN C++ (oracle/_ref): level sizes within 2 %, and PCG_CJ to 1e-8
+    within the reference's regression tolerance max(5 %, 2) of that path's
+    iterations (the two BAMG prolongations pick different, equally exact,
+    interpolation sets in about 1 % of the rows, see the BAMG golden test),
+    each solve with a true relative residual of at most 1e-8."""
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built")
+    from oracle import c_oracle as CO
+    A, X = PB.elasticity_q1(20, return_coords=True)
+    TV = PB.rbm_test_space(X)
+    b = PB.elasticity_rhs(A, X, seed=0)
+    prm = O.default_params(8)
+    prm["prolong"]["prol_emin"] = "EMIN"
+    H = O.cpt_aspamg(prm, A, TV)
+    _, ito, _, flo = CO.CHierarchy(H).pcg(b, itmax=1000, tol=1e-8)
+    assert flo == 0
+    with cb.Hierarchy(A, TV, cb.params(precision=cb.CHRONOS_FP64, prol_emin="EMIN")) as h:
+        sizes = [h.level_info(l)["n"] for l in range(h.nlevels)]
+        ref_sizes = [L.A.shape[0] for L in H.levels]
+        assert len(sizes) == len(ref_sizes)
+        assert all(abs(s - r) <= 0.02 * r for s, r in zip(sizes, ref_sizes)), (sizes, ref_sizes)
+        x, it, _, flag, _ = h.pcg(b, itmax=1000, tol=1e-8)
+    assert flag == 0
+    assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
+    assert not (abs(ito / it - 1) > 0.05 and abs(ito - it) > 2), (it, ito)
