@@ -121,8 +121,8 @@ def test_params_files(lib, tmp_path):
         "parm_SMOOTH": "20 %\n1 %\n1 %\n15 %\n1 %\n1.e-3 %\nAFSAI_SYM %\n",
         "parm_TSPACE": "6 %\n40 %\n1.e-4 %\nNONE %\n5 %\n\nAvailable Methods:\n",
         "parm_COARSEN": "CLA %\n0.2 %\n0 %\n",
-        "parm_PROLONG": "BAMG\nNONE\n20\n100\n0.01\n1\n10\n1.e+13\n5.0\n1.e-10\n0\n2\n0.010\n30\n10\n"
-                        "0.001\n1.e+10\n1\n4\n0\n20\n5\n",
+        "parm_PROLONG": "BAMG\nEMIN\n20\n100\n0.01\n1\n10\n1.e+13\n5.0\n1.e-10\n0\n3\n0.020\n25\n8\n"
+                        "0.002\n1.e+9\n1\n3\n0\n20\n5\n",
         "parm_FILTER": "10\n170.0\n0.1\n0.000\n0\n",
         "parm_GENERAL": "false\nunit_rhs\ntrue\nPCG\n15000\n1.e-8\n100\n",
     }
@@ -133,9 +133,14 @@ def test_params_files(lib, tmp_path):
     assert p.SoC_type == b"CLA" and p.soc_tau == 0.2 and p.nthread == 20 and p.nstep == 15
     assert p.maxcond == 1e13 and p.itmax == 15000 and p.tol == 1e-8 and p.symmetric == 1
     assert p.tspace_method == b"NONE" and p.proltype == b"BAMG" and p.filt_wgt == 170.0
+    # the EMIN lines of parm_PROLONG (read_prolong.m)
+    assert p.prol_emin == b"EMIN" and p.patt_pow == 3 and p.patt_tau == 0.02
+    assert p.nnzr_max == 25 and p.itmax_emin == 8 and p.energ_tol == 0.002
+    assert p.condmax_emin == 1e9 and p.prec_emin == 1 and p.solv_emin == 3
     # the oracle reads the same files the same way
     q = O.read_params(str(tmp_path / "aspAMG.fnames"))
     assert q["coarsen"]["tau"] == p.soc_tau and q["smoother"]["nstep"] == p.nstep
+    assert (q["prolong"]["patt_pow"], q["prolong"]["nnzr_max"], q["prolong"]["solv_emin"]) == (3, 25, 3)
     (tmp_path / "parm_AMG").write_text("10\n")
     with pytest.raises(cb.ChronosError) as e:
         cb.readDefaultParams(tmp_path / "aspAMG.fnames")
