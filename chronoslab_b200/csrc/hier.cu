@@ -543,9 +543,40 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
         CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
         tmin = std::min(tmin, 4 * ms);
       }
-      if (std::getenv("CHRONOS_TUNE_VERBOSE"))
-        std::fprintf(stderr, "chronos tune: block form T=%d  %.4f ms per residual pair + outer\n",
-                     t, tmin / 4);
+      if (std::getenv("CHRONOS_TUNE_VERBOSE")) {
+        // the two parts alone, for the record
+        auto part_time = [&](bool outer) {
+          float m = 1e30f;
+          for (int r = 0; r < 3; ++r) {
+            CHRONOS_CUDA(cudaMemsetAsync(flush.get(), r, kL2FlushBytes, st));
+            CHRONOS_CUDA(cudaEventRecord(e0, st));
+            if (outer)
+              launch_pcg_spmv(st, probe, fp32, p64.get(), p64.get(), q64.get(), part.get(),
+                              tick.get(), sc.get());
+            else if (fp32)
+              sell3_apply<float, float, float, float, MODE_PLAIN, false>(
+                  st, t, probe.nb, probe.nchunk, probe.choff, probe.chw, probe.sci,
+                  probe.bv32.get(), probe.nslots, x32.get(), (const float *)nullptr, y32.get(),
+                  1.0f);
+            else
+              sell3_apply<double, double, double, double, MODE_PLAIN, false>(
+                  st, t, probe.nb, probe.nchunk, probe.choff, probe.chw, probe.sci,
+                  probe.bv64.get(), probe.nslots, x64.get(), (const double *)nullptr,
+                  y64.get(), 1.0);
+            CHRONOS_CUDA(cudaEventRecord(e1, st));
+            CHRONOS_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            CHRONOS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            m = std::min(m, ms);
+          }
+          return m;
+        };
+        const float tr = part_time(false), to = part_time(true);
+        std::fprintf(stderr,
+                     "chronos tune: block form T=%d  %.4f ms per residual pair + outer "
+                     "(residual %.4f, outer %.4f ms alone)\n",
+                     t, tmin / 4, tr, to);
+      }
       if (tmin < best) {
         best = tmin;
         T = t;
