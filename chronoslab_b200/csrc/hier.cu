@@ -390,8 +390,8 @@ void autotune_lanes(DMat &m, bool fp32, cudaStream_t st, int format) {
 }
 
 // Sliced 3x3 block form of a CSR matrix whose row triples share a pattern of
-// whole, aligned 3x3 blocks (structural zeros included).  Returns false
-// otherwise.  Layout as k_sell3_apply reads it.
+// whole, aligned 3x3 blocks (structural zeros included); layout as
+// k_sell3_apply reads it.
 // Block lengths of the 3x3 block form, or empty when A has none.
 static std::vector<int> block_row_lengths(const HostCSR &A) {
   if (A.nrows % 3 != 0 || A.ncols % 3 != 0 || A.nrows == 0) return {};
@@ -419,10 +419,10 @@ static std::vector<int> block_row_lengths(const HostCSR &A) {
 
 // Layout for T threads per block row: chunks of C = 32/T block rows, each
 // padded to its longest row rounded up to a multiple of T; slot j of row l
-// at off_c + (j/T)*32 + (j%T)*C + l; chw = padded width / T.
-static bool build_sell3(const HostCSR &A, const std::vector<int> &blen, int T,
-                        std::vector<int> &choff, std::vector<int> &chw, std::vector<int> &sci,
-                        std::vector<double> &planes) {
+// at off_c + (j/T)*32 + (j%T)*C + l; chw = padded width / T.  Returns false
+// when the slot count does not fit int32.
+static bool sell3_offsets(const std::vector<int> &blen, int T, std::vector<int> &choff,
+                          std::vector<int> &chw) {
   const int nb = (int)blen.size();
   const int C = 32 / T;
   const int nchunk = (nb + C - 1) / C;
@@ -437,42 +437,65 @@ static bool build_sell3(const HostCSR &A, const std::vector<int> &blen, int T,
     if (next >= INT32_MAX) return false;
     choff[c + 1] = (int)next;
   }
-  const int64_t nslots = choff[nchunk];
-  sci.assign(nslots, 0);
-  planes.assign((size_t)9 * nslots, 0.0);
-#pragma omp parallel for schedule(static, 4096)
-  for (int I = 0; I < nb; ++I) {
-    const int c = I / C, l = I % C;
-    const int64_t s0 = A.rp[3 * I];
-    for (int j = 0; j < blen[I]; ++j) {
-      const int64_t slot = choff[c] + 32LL * (j / T) + (int64_t)(j % T) * C + l;
-      sci[slot] = A.ci[s0 + 3 * j] / 3;
-      for (int r = 0; r < 3; ++r)
-        for (int cc = 0; cc < 3; ++cc)
-          planes[(size_t)(3 * r + cc) * nslots + slot] = A.v[A.rp[3 * I + r] + 3 * j + cc];
-    }
-  }
   return true;
 }
 
-static void upload_sell3(const HostCSR &A, const std::vector<int> &blen, int T, DMat &d,
+// Block row I's blocks into their slots (a thread per block row): the block
+// column and the nine values, plane-major, from the device CSR whose row
+// triples share one pattern of aligned 3x3 blocks.  Padding slots stay as
+// set before (zero values, block column 0).
+__global__ void k_fill_sell3(int nb, int T, const int *__restrict__ blen,
+                             const int *__restrict__ choff, const int *__restrict__ rp,
+                             const int *__restrict__ ci, const double *__restrict__ v,
+                             int64_t nslots, int *__restrict__ sci, double *__restrict__ planes) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nb) return;
+  const int C = 32 / T;
+  const int c = I / C, l = I % C;
+  const int r0 = rp[3 * I], r1 = rp[3 * I + 1], r2 = rp[3 * I + 2];
+  const int64_t base = choff[c];
+  for (int j = 0; j < blen[I]; ++j) {
+    const int64_t slot = base + 32LL * (j / T) + (int64_t)(j % T) * C + l;
+    sci[slot] = ci[r0 + 3 * j] / 3;
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc) {
+      planes[(int64_t)cc * nslots + slot] = v[r0 + 3 * j + cc];
+      planes[(int64_t)(3 + cc) * nslots + slot] = v[r1 + 3 * j + cc];
+      planes[(int64_t)(6 + cc) * nslots + slot] = v[r2 + 3 * j + cc];
+    }
+  }
+}
+
+// Builds d's sliced 3x3 block form for T threads per block row on the
+// device, from src's device CSR (src and d may be the same matrix).
+static void upload_sell3(const DMat &src, const std::vector<int> &blen, int T, DMat &d,
                          bool fp32, cudaStream_t st) {
-  std::vector<int> choff, chw, sci;
-  std::vector<double> planes;
-  if (!build_sell3(A, blen, T, choff, chw, sci, planes)) return;
-  d.nb = A.nrows / 3;
+  std::vector<int> choff, chw;
+  if (!sell3_offsets(blen, T, choff, chw)) return;
+  const int nb = (int)blen.size();
+  const int64_t nslots = choff.back();
+  DBuf<int> blen_d;
+  blen_d.upload(blen, st);
+  d.nb = nb;
   d.sell_T = T;
   d.nchunk = (int)chw.size();
   d.nnzb = 0;
   for (int l : blen) d.nnzb += l;
-  d.nslots = choff.back();
+  d.nslots = nslots;
   d.choff.upload(choff, st);
   d.chw.upload(chw, st);
-  d.sci.upload(sci, st);
-  d.bv64.upload(planes, st);
+  d.sci.alloc(std::max<int64_t>(nslots, 1));
+  d.bv64.alloc(std::max<int64_t>(9 * nslots, 1));
+  CHRONOS_CUDA(cudaMemsetAsync(d.sci.get(), 0, sizeof(int) * std::max<int64_t>(nslots, 1), st));
+  CHRONOS_CUDA(cudaMemsetAsync(d.bv64.get(), 0,
+                               sizeof(double) * std::max<int64_t>(9 * nslots, 1), st));
+  k_fill_sell3<<<ceil_div(nb, 256), 256, 0, st>>>(nb, T, blen_d.get(), d.choff.get(), src.rp.get(),
+                                                  src.ci.get(), src.v64.get(), nslots,
+                                                  d.sci.get(), d.bv64.get());
+  CHRONOS_CHECK_LAUNCH();
   if (fp32) {
-    d.bv32.alloc(planes.size());
-    convert_f64_to_f32((int64_t)planes.size(), d.bv64.get(), d.bv32.get(), st);
+    d.bv32.alloc(std::max<int64_t>(9 * nslots, 1));
+    convert_f64_to_f32(9 * nslots, d.bv64.get(), d.bv32.get(), st);
   }
   CHRONOS_CUDA(cudaStreamSynchronize(st));
 }
@@ -514,7 +537,7 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
     DMat winner;                                    // the fastest layout, kept for d
     for (int t : {1, 2, 4}) {
       DMat probe;
-      upload_sell3(A, blen, t, probe, fp32, st);
+      upload_sell3(d, blen, t, probe, fp32, st);
       auto launch = [&] {
         for (int k = 0; k < 2; ++k) {
           if (fp32)
@@ -602,7 +625,7 @@ static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) 
     d.bv32 = std::move(winner.bv32);
     return;
   }
-  upload_sell3(A, blen, T, d, fp32, st);
+  upload_sell3(d, blen, T, d, fp32, st);
 }
 
 template <typename T> inline const T *bvals(const DMat &m);
