@@ -618,6 +618,13 @@ class Hierarchy:
         check(self._lib.chronos_vcycle(self._h, _pd(bc), _pd(x), nrhs, _stream(stream)))
         return x if b.ndim == 1 else x.reshape(nrhs, self.n).T
 
+    def vcycle_dev(self, b_ptr, x_ptr, precision=CHRONOS_FP64, nrhs=1, stream=None):
+        """AMG_Vcycle on device vectors (chronos_vcycle_dev): b_ptr, x_ptr are
+        device addresses of n x nrhs column-major double (CHRONOS_FP64) or
+        float (CHRONOS_FP32) arrays; ordered on stream."""
+        check(self._lib.chronos_vcycle_dev(self._h, precision, C.c_void_p(b_ptr),
+                                           C.c_void_p(x_ptr), nrhs, _stream(stream)))
+
     def pcg(self, b, x0=None, itmax=1000, tol=1e-8, A=None, stream=None):
         """PCG_CJ; A (optional) is the operator prodA (0-based CSR of the
         level-1 size), else the hierarchy's level-1 operator."""

@@ -136,6 +136,7 @@ SIGNATURES = {
     "chronos_hier_profile": [_vp, _i, C.POINTER(chronos_profile)],
     "chronos_diag_fix": [_i, _pi, _pi, _pd],
     "chronos_vcycle": [_vp, _pd, _pd, _i, _vp],
+    "chronos_vcycle_dev": [_vp, _i, _vp, _vp, _i, _vp],
     "chronos_pcg": [_vp, _pi, _pi, _pd, _pd, _pd, _i, _d, _pi, _pd, _pi, _pd, _vp],
     "chronos_pcg_dev": [_vp, _vp, _vp, _i, _d, _pi, _pd, _pi, _pd, _vp],
     "chronos_pcg_block": [_vp, _i, _pd, _pd, _i, _d, _pi, _pi, _pd, _vp],

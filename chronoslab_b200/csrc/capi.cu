@@ -917,6 +917,26 @@ int chronos_vcycle(chronos_hier *hh, const double *b_h, double *x_h, int nrhs, v
   });
 }
 
+int chronos_vcycle_dev(chronos_hier *hh, int io_precision, const void *b_d, void *x_d, int nrhs,
+                       void *stream) {
+  return guard([&] {
+    CallRange range_("chronos_vcycle_dev");
+    CHRONOS_REQUIRE(hh && b_d && x_d && nrhs >= 1, CHRONOS_EINVAL, "bad argument");
+    CHRONOS_REQUIRE(io_precision == CHRONOS_FP64 || io_precision == CHRONOS_FP32, CHRONOS_EINVAL,
+                    "io_precision must be CHRONOS_FP64 or CHRONOS_FP32");
+    Hier &h = *hh->h;
+    const size_t n = (size_t)h.levels[0].n;
+    CallerStream order(h, stream);
+    for (int c = 0; c < nrhs; ++c) {
+      if (io_precision == CHRONOS_FP64)
+        h.vcycle(static_cast<const double *>(b_d) + c * n, static_cast<double *>(x_d) + c * n,
+                 nullptr, nullptr);
+      else
+        h.vcycle_f32(static_cast<const float *>(b_d) + c * n, static_cast<float *>(x_d) + c * n);
+    }
+  });
+}
+
 int chronos_pcg_dev(chronos_hier *hh, const double *b_d, double *x_d, int itmax, double tol,
                     int *iters, double *resvec_h, int *flag, double *seconds, void *stream) {
   return guard([&] {

@@ -1549,6 +1549,30 @@ void Hier::vcycle(const double *b, double *out, const double *dw, double *dot_ou
     vcycle_level<double, double, double, true>(*this, 0, b, out, dw, dot_out);
 }
 
+__global__ void k_f32_to_f64(int64_t n, const float *__restrict__ a, double *__restrict__ b) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (double)a[i];
+}
+
+void Hier::vcycle_f32(const float *b, float *out) {
+  if (precision == CHRONOS_FP32) {
+    vcycle_level<float, float, float, true>(*this, 0, b, out, nullptr, nullptr);
+    return;
+  }
+  // FP64 hierarchy: FP64 copies of the vectors around the cycle
+  const int n = levels[0].n;
+  if (stage_b.size() < (size_t)n) {
+    stage_b.alloc(n);
+    stage_x.alloc(n);
+  }
+  k_f32_to_f64<<<std::min<int64_t>(ceil_div(n, 256), (int64_t)num_sms() * 8), 256, 0, st>>>(
+      n, b, stage_b.get());
+  CHRONOS_CHECK_LAUNCH();
+  vcycle(stage_b.get(), stage_x.get(), nullptr, nullptr);
+  convert_f64_to_f32(n, stage_x.get(), out, st);
+}
+
 void Hier::apply_A(const double *x, double *y) {
   op_apply<double, double, double, double, MODE_PLAIN, false>(st, levels[0].A, x,
                                                               (const double *)nullptr, y, 1.0);

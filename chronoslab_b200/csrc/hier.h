@@ -123,6 +123,9 @@ struct Hier {
   // one V-cycle: out = M^{-1} b on device FP64 vectors of length n0;
   // when dw != nullptr also *dot_out = out . dw (deterministic).
   void vcycle(const double *b, double *out, const double *dw, double *dot_out);
+  // the same on FP32 device vectors (an FP32 hierarchy reads and writes them
+  // directly; an FP64 one through FP64 copies)
+  void vcycle_f32(const float *b, float *out);
   // PCG_CJ to tolerance on device vectors; returns iterations, flag.
   void pcg_solve(const double *b, double *x, int itmax, double tol, int *iters, int *flag,
                  std::vector<double> *resvec, double *seconds);

@@ -20,7 +20,7 @@
  *   chronos_fsai_numeric   <- numeric half of the same MEX (cpt_afsai_coef.cpp:440-541)
  *   chronos_amg_setup      <- cpt_aspAMG(param,A,TV0)   (aspAMG/cpt_aspAMG.m:1,54; called at
  *                             Drivers/driver_AMG/aspAMG_main.m:175, utils/computeAMG.m:46)
- *   chronos_vcycle         <- AMG_Vcycle(hrc,A,b)       (aspAMG/AMG_Vcycle.m:1-54)
+ *   chronos_vcycle(_dev)   <- AMG_Vcycle(hrc,A,b)       (aspAMG/AMG_Vcycle.m:1-54)
  *   chronos_pcg            <- PCG_CJ(prodM,prodA,b,x0,itmax,tol) (LinearSolver/PCG_CJ.m:1-73;
  *                             called at aspAMG_main.m:199-202)
  *   chronos_sqmr           <- SQMR(Afun,rhs,tol,itmax,lprec,rprec) (LinearSolver/SQMR.m:1-108;
@@ -29,6 +29,9 @@
  *   chronos_dense_chol     <- [L,p,S] = chol(A,'lower') (aspAMG/cpt_aspAMG.m:109) and the
  *                             coarsest solve S*(L'\(L\(S'*b))) (AMG_Vcycle.m:9-10)
  *   chronos_params_read    <- readDefaultParams.m / aspAMG_main.m:17-59 and read_*.m
+ *   chronos_emin_pattern   <- MEX_cptProlPatt          (prolong/EMIN/MEX_EMIN/MEX_cptProlPatt.cpp)
+ *   chronos_emin           <- EMIN_Prolong_compute / EMIN_ImpProl (prolong/EMIN/Cpp_EMIN/
+ *                             EMIN_ImpProl.cpp:84-410; called from prolong.m:224-225)
  */
 #ifndef CHRONOS_B200_H
 #define CHRONOS_B200_H
@@ -72,7 +75,7 @@ typedef struct chronos_params {
   int nl_agg;
   /* parm_PROLONG (read_prolong.m; the BAMG lines) */
   char proltype[16];              /* BAMG */
-  char prol_emin[16];             /* NONE */
+  char prol_emin[16];             /* NONE, SMOOTH or EMIN */
   int prol_np, itmax_vol;
   double tol_vol;
   int dist_min, dist_max;
@@ -448,6 +451,13 @@ int chronos_diag_fix(int n, const int *iat_h, const int *ja_h, double *val_h);
 /* One V(nupre,nupost) cycle x = M^{-1} b (x0 absent), host vectors, FP64 in/out.
  * nrhs columns, column-major (leading dimension n). */
 int chronos_vcycle(chronos_hier *h, const double *b_h, double *x_h, int nrhs, void *stream);
+/* The same V-cycle on device vectors (column-major n x nrhs): io_precision
+ * CHRONOS_FP64 (double) or CHRONOS_FP32 (float).  An FP32 hierarchy reads and
+ * writes float vectors directly (AMG_Vcycle.m:1-54 in FP32 end to end, the
+ * coarsest solve in FP64 as always); an FP64 hierarchy runs on FP64 copies.
+ * Work is ordered on stream with no host synchronisation. */
+int chronos_vcycle_dev(chronos_hier *h, int io_precision, const void *b_d, void *x_d, int nrhs,
+                       void *stream);
 
 /* PCG_CJ with the V-cycle preconditioner, x0 = x_h on input.  The operator is
  * PCG_CJ's prodA (PCG_CJ.m:1; aspAMG_main.m:199-202 passes @(x)A*x): the

@@ -186,3 +186,37 @@ def test_setup_from_device_memory(lib):
         xd, itd, _, _, _ = dev_h.pcg(b)
         xh, ith, _, _, _ = host_h.pcg(b)
         assert itd == ith and np.array_equal(xd, xh)
+
+
+def test_vcycle_on_device_vectors_fp64_and_fp32(lib):
+    """chronos_vcycle_dev: FP64 device vectors give chronos_vcycle's result
+    bit for bit; FP32 vectors on an FP32 hierarchy (read and written
+    directly) agree with the FP64-vector V-cycle to 2e-5; on an FP64
+    hierarchy FP32 vectors give the FP64 cycle of the same input rounded once
+    to FP32.  Two columns at once."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    A, TV, b_np, ntv = _problems()[1]
+    B = np.stack([b_np, np.roll(b_np, 7)], axis=1)
+    for prec in (cb.CHRONOS_FP32, cb.CHRONOS_FP64):
+        with cb.Hierarchy(A, TV, cb.params(precision=prec, ntv=ntv)) as h:
+            ref = h.vcycle(B)
+            bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(dev)
+            xd = torch.zeros_like(bd)
+            h.vcycle_dev(bd.data_ptr(), xd.data_ptr(), cb.CHRONOS_FP64, nrhs=2)
+            torch.cuda.synchronize()
+            assert np.array_equal(xd.cpu().numpy().T, ref)
+            b32 = bd.to(torch.float32)
+            x32 = torch.zeros_like(b32)
+            h.vcycle_dev(b32.data_ptr(), x32.data_ptr(), cb.CHRONOS_FP32, nrhs=2)
+            torch.cuda.synchronize()
+            got = x32.cpu().numpy().T.astype(np.float64)
+            if prec == cb.CHRONOS_FP32:
+                for j in range(2):
+                    assert np.linalg.norm(got[:, j] - ref[:, j]) <= 2e-5 * np.linalg.norm(ref[:, j])
+            else:
+                want = h.vcycle(b32.cpu().numpy().T.astype(np.float64)).astype(np.float32)
+                assert np.array_equal(x32.cpu().numpy().T, want)
+            with pytest.raises(cb.ChronosError):
+                h.vcycle_dev(bd.data_ptr(), xd.data_ptr(), 7)
+
