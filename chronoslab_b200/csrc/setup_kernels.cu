@@ -395,14 +395,15 @@ __device__ __forceinline__ unsigned hash_insert(int *keys, unsigned mask, int ke
 }
 
 // Symbolic: unique columns per row (warp per row, rows [r0, r1)).
-__global__ void k_spgemm_symbolic(int r0, int r1, const int *xrp, const int *xci, const int *yrp,
-                                  const int *yci, const int64_t *toff, const unsigned *tcap,
-                                  int *keys, int *cnt) {
+__global__ void k_spgemm_symbolic(int r0, int r1, const int *rows, const int *xrp, const int *xci,
+                                  const int *yrp, const int *yci, const int64_t *toff,
+                                  const unsigned *tcap, int *keys, int *cnt) {
   const int lane = threadIdx.x & 31;
-  const int i = r0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (i >= r1) return;
-  int *tk = keys + toff[i - r0];
-  const unsigned cap = tcap[i - r0], mask = cap - 1;
+  const int t = r0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (t >= r1) return;
+  const int i = rows[t];
+  int *tk = keys + toff[t - r0];
+  const unsigned cap = tcap[t - r0], mask = cap - 1;
   for (unsigned s = lane; s < cap; s += 32) tk[s] = -1;
   __syncwarp();
   int mine = 0;
@@ -421,17 +422,18 @@ __global__ void k_spgemm_symbolic(int r0, int r1, const int *xrp, const int *xci
 // Numeric: accumulate in the order of row i of X (products rounded, then
 // added), emit the nonzero entries unsorted into [crp_sym[i], ...); cnt_out[i]
 // = number emitted.
-__global__ void k_spgemm_numeric(int r0, int r1, const int *xrp, const int *xci, const double *xv,
-                                 const int *yrp, const int *yci, const double *yv,
-                                 const int64_t *toff, const unsigned *tcap, int *keys,
-                                 double *vals, const int64_t *crp_sym, int *cci, double *cv,
-                                 int *cnt_out) {
+__global__ void k_spgemm_numeric(int r0, int r1, const int *rows, const int *xrp, const int *xci,
+                                 const double *xv, const int *yrp, const int *yci,
+                                 const double *yv, const int64_t *toff, const unsigned *tcap,
+                                 int *keys, double *vals, const int64_t *crp_sym, int *cci,
+                                 double *cv, int *cnt_out) {
   const int lane = threadIdx.x & 31;
-  const int i = r0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (i >= r1) return;
-  int *tk = keys + toff[i - r0];
-  double *tv = vals + toff[i - r0];
-  const unsigned cap = tcap[i - r0], mask = cap - 1;
+  const int t = r0 + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (t >= r1) return;
+  const int i = rows[t];
+  int *tk = keys + toff[t - r0];
+  double *tv = vals + toff[t - r0];
+  const unsigned cap = tcap[t - r0], mask = cap - 1;
   for (unsigned s = lane; s < cap; s += 32) { tk[s] = -1; tv[s] = 0.0; }
   __syncwarp();
   for (int k = xrp[i]; k < xrp[i + 1]; ++k) {
@@ -468,6 +470,119 @@ __global__ void k_spgemm_numeric(int r0, int r1, const int *xrp, const int *xci,
   if (lane == 0) cnt_out[i] = emitted;
 }
 
+// Shared-memory variants for rows whose distinct columns fit a warp's table
+// of kSpgemmSmSlots: the same insertion order and sums as the global-table
+// kernels (each output column gets its products in X's row order), so the
+// results are bit-identical; only the table's place and size differ.
+constexpr int kSpgemmSmSlots = 4096;
+constexpr int kSpgemmSmWarps = 4;
+
+__device__ __forceinline__ unsigned spgemm_cap(int64_t prod, int ncols) {
+  const uint64_t want = (uint64_t)2 * (uint64_t)prod + 1, colcap = (uint64_t)2 * (uint64_t)max(ncols, 1);
+  uint64_t p = 32, v = want < colcap ? want : colcap;
+  while (p < v) p <<= 1;
+  return (unsigned)p;
+}
+
+// Symbolic in shared memory: cnt[i] = distinct columns of row i, or -1 when
+// they outgrow half the warp's table (the row then goes to the global table).
+__global__ void __launch_bounds__(32 * kSpgemmSmWarps)
+k_spgemm_symbolic_sm(int m, int ncols, const int *__restrict__ xrp, const int *__restrict__ xci,
+                     const int *__restrict__ yrp, const int *__restrict__ yci,
+                     const int64_t *__restrict__ prod, int *__restrict__ cnt) {
+  extern __shared__ int spg_keys[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  int *tk = spg_keys + wib * kSpgemmSmSlots;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = gw; i < m; i += nw) {
+    const unsigned cap = spgemm_cap(prod[i], ncols);
+    const unsigned tsz = cap < (unsigned)kSpgemmSmSlots ? cap : (unsigned)kSpgemmSmSlots;
+    const unsigned mask = tsz - 1;
+    for (unsigned s = lane; s < tsz; s += 32) tk[s] = -1;
+    __syncwarp();
+    int count = 0;
+    bool over = false;
+    for (int k = xrp[i]; k < xrp[i + 1] && !over; ++k) {
+      const int j = xci[k];
+      for (int kk0 = yrp[j]; kk0 < yrp[j + 1]; kk0 += 32) {
+        const int kk = kk0 + lane;
+        int fresh_n = 0;
+        if (kk < yrp[j + 1]) {
+          bool fresh;
+          hash_insert(tk, mask, yci[kk], &fresh);
+          fresh_n = fresh;
+        }
+        count += warp_sum(fresh_n);
+        if (2 * count > (int)tsz) {                    // the same for every lane
+          over = true;
+          break;
+        }
+      }
+    }
+    if (lane == 0) cnt[i] = over ? -1 : count;
+    __syncwarp();
+  }
+}
+
+// Numeric in shared memory for the rows with 0 <= cnt[i] <= kSpgemmSmSlots/2
+// (others skipped): emits row i's nonzero entries unsorted at crp_sym[i].
+__global__ void __launch_bounds__(32 * kSpgemmSmWarps)
+k_spgemm_numeric_sm(int m, const int *__restrict__ xrp, const int *__restrict__ xci,
+                    const double *__restrict__ xv, const int *__restrict__ yrp,
+                    const int *__restrict__ yci, const double *__restrict__ yv,
+                    const int *__restrict__ cnt, const int64_t *__restrict__ crp_sym,
+                    int *__restrict__ cci, double *__restrict__ cv, int *__restrict__ cnt_out) {
+  extern __shared__ double spg_vals[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  double *tv = spg_vals + (size_t)wib * kSpgemmSmSlots;
+  int *tk = reinterpret_cast<int *>(spg_vals + (size_t)kSpgemmSmWarps * kSpgemmSmSlots) +
+            wib * kSpgemmSmSlots;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int i = gw; i < m; i += nw) {
+    const int c = cnt[i];
+    if (c < 0 || 2 * c > kSpgemmSmSlots) continue;
+    unsigned tsz = 32;
+    while (tsz < (unsigned)(2 * c + 1)) tsz <<= 1;
+    const unsigned mask = tsz - 1;
+    for (unsigned s = lane; s < tsz; s += 32) { tk[s] = -1; tv[s] = 0.0; }
+    __syncwarp();
+    for (int k = xrp[i]; k < xrp[i + 1]; ++k) {
+      const int j = xci[k];
+      const double a = xv[k];
+      for (int kk = yrp[j] + lane; kk < yrp[j + 1]; kk += 32) {
+        bool fresh;
+        const unsigned s = hash_insert(tk, mask, yci[kk], &fresh);
+        tv[s] = __dadd_rn(tv[s], __dmul_rn(a, yv[kk]));
+      }
+      __syncwarp();
+    }
+    const int64_t base = crp_sym[i];
+    int emitted = 0;
+    for (unsigned s0 = 0; s0 < tsz; s0 += 32) {
+      const unsigned s = s0 + lane;
+      bool keep = false;
+      int key = -1;
+      double val = 0.0;
+      if (s < tsz) {
+        key = tk[s];
+        val = tv[s];
+        keep = key != -1 && val != 0.0;
+      }
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int off = __popc(bal & ((1u << lane) - 1u));
+        cci[base + emitted + off] = key;
+        cv[base + emitted + off] = val;
+      }
+      emitted += __popc(bal);
+    }
+    if (lane == 0) cnt_out[i] = emitted;
+    __syncwarp();
+  }
+}
+
 __global__ void k_compact_rows(int m, const int64_t *src_rp, const int *cnt, const int *crp,
                                const int *sci, const double *sv, int *dci, double *dv) {
   const int i = blockIdx.x;
@@ -498,46 +613,72 @@ void spgemm_device(int m, int ncols, const int *xrp, const int *xci, const doubl
   DBuf<int64_t> dprod(m);
   k_spgemm_products<<<ceil_div(m, 256), 256, 0, st>>>(m, xrp, xci, yrp, dprod.get());
   CHRONOS_CHECK_LAUNCH();
-  std::vector<int64_t> prod = dprod.to_host(st);
-  std::vector<unsigned> cap(m);
-  const uint64_t colcap = (uint64_t)2 * (uint64_t)std::max(ncols, 1);
-  for (int i = 0; i < m; ++i) cap[i] = next_pow2(std::min<uint64_t>(2 * (uint64_t)prod[i] + 1, colcap));
-  // Chunks of rows whose tables fit the slot budget.
-  const uint64_t budget = (uint64_t)1 << 24;     // 16M slots (192 MB with values)
-  std::vector<int> bounds{0};
-  {
-    uint64_t acc = 0;
-    for (int i = 0; i < m; ++i) {
-      if (acc + cap[i] > budget && i > bounds.back()) { bounds.push_back(i); acc = 0; }
-      acc += cap[i];
-    }
-    bounds.push_back(m);
-  }
-  uint64_t maxchunk = 0;
-  for (size_t c = 0; c + 1 < bounds.size(); ++c) {
-    uint64_t acc = 0;
-    for (int i = bounds[c]; i < bounds[c + 1]; ++i) acc += cap[i];
-    maxchunk = std::max(maxchunk, acc);
-  }
-  DBuf<int> keys(maxchunk);
-  DBuf<double> vals(maxchunk);
-  DBuf<int64_t> toff(m);
-  DBuf<unsigned> tcap(m);
-  std::vector<int64_t> toff_h(m);
-  for (size_t c = 0; c + 1 < bounds.size(); ++c) {
-    int64_t acc = 0;
-    for (int i = bounds[c]; i < bounds[c + 1]; ++i) { toff_h[i] = acc; acc += cap[i]; }
-  }
-  toff.upload(toff_h, st);
-  tcap.upload(cap.data(), m, st);
+  // symbolic: in each warp's shared table first; rows whose distinct columns
+  // outgrow it (cnt = -1) again in global tables sized from their products
+  const size_t sym_smem = (size_t)kSpgemmSmWarps * kSpgemmSmSlots * sizeof(int);
+  const size_t num_smem = (size_t)kSpgemmSmWarps * kSpgemmSmSlots * (sizeof(int) + sizeof(double));
+  static const bool attrs = [&] {
+    CHRONOS_CUDA(cudaFuncSetAttribute(k_spgemm_symbolic_sm,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sym_smem));
+    CHRONOS_CUDA(cudaFuncSetAttribute(k_spgemm_numeric_sm,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)num_smem));
+    return true;
+  }();
+  (void)attrs;
+  const int sm_grid = (int)std::max<int64_t>(
+      1, std::min<int64_t>(ceil_div(m, kSpgemmSmWarps), (int64_t)num_sms() * 8));
   DBuf<int> cnt(m);
-  for (size_t c = 0; c + 1 < bounds.size(); ++c) {
-    const int r0 = bounds[c], r1 = bounds[c + 1];
-    k_spgemm_symbolic<<<ceil_div((int64_t)(r1 - r0) * 32, 256), 256, 0, st>>>(
-        r0, r1, xrp, xci, yrp, yci, toff.get() + r0, tcap.get() + r0, keys.get(), cnt.get());
-    CHRONOS_CHECK_LAUNCH();
-  }
+  k_spgemm_symbolic_sm<<<sm_grid, 32 * kSpgemmSmWarps, sym_smem, st>>>(m, ncols, xrp, xci, yrp,
+                                                                       yci, dprod.get(), cnt.get());
+  CHRONOS_CHECK_LAUNCH();
   std::vector<int> cnt_h = cnt.to_host(st);
+  std::vector<int> big;                                // rows for the global tables
+  for (int i = 0; i < m; ++i)
+    if (cnt_h[i] < 0) big.push_back(i);
+  const int nbig = (int)big.size();
+  DBuf<int> dbig;
+  std::vector<int> bounds{0};
+  DBuf<int> keys;
+  DBuf<double> vals;
+  DBuf<int64_t> toff;
+  DBuf<unsigned> tcap;
+  if (nbig > 0) {
+    std::vector<int64_t> prod(m);
+    dprod.download(prod.data(), m, st);
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+    std::vector<unsigned> cap(nbig);
+    const uint64_t colcap = (uint64_t)2 * (uint64_t)std::max(ncols, 1);
+    for (int t = 0; t < nbig; ++t)
+      cap[t] = next_pow2(std::min<uint64_t>(2 * (uint64_t)prod[big[t]] + 1, colcap));
+    // chunks of rows whose tables fit the slot budget
+    const uint64_t budget = (uint64_t)1 << 24;     // 16M slots (192 MB with values)
+    uint64_t acc = 0;
+    for (int t = 0; t < nbig; ++t) {
+      if (acc + cap[t] > budget && t > bounds.back()) { bounds.push_back(t); acc = 0; }
+      acc += cap[t];
+    }
+    bounds.push_back(nbig);
+    uint64_t maxchunk = 0;
+    std::vector<int64_t> toff_h(nbig);
+    for (size_t c = 0; c + 1 < bounds.size(); ++c) {
+      int64_t a = 0;
+      for (int t = bounds[c]; t < bounds[c + 1]; ++t) { toff_h[t] = a; a += cap[t]; }
+      maxchunk = std::max<uint64_t>(maxchunk, (uint64_t)a);
+    }
+    keys.alloc(maxchunk);
+    vals.alloc(maxchunk);
+    toff.upload(toff_h, st);
+    tcap.upload(cap.data(), nbig, st);
+    dbig.upload(big, st);
+    for (size_t c = 0; c + 1 < bounds.size(); ++c) {
+      const int t0 = bounds[c], t1 = bounds[c + 1];
+      k_spgemm_symbolic<<<ceil_div((int64_t)(t1 - t0) * 32, 256), 256, 0, st>>>(
+          t0, t1, dbig.get(), xrp, xci, yrp, yci, toff.get() + t0, tcap.get() + t0, keys.get(),
+          cnt.get());
+      CHRONOS_CHECK_LAUNCH();
+    }
+    cnt_h = cnt.to_host(st);
+  }
   std::vector<int64_t> rps(m + 1, 0);
   for (int i = 0; i < m; ++i) rps[i + 1] = rps[i] + cnt_h[i];
   DBuf<int64_t> drps(m + 1);
@@ -545,11 +686,14 @@ void spgemm_device(int m, int ncols, const int *xrp, const int *xci, const doubl
   DBuf<int> sci(std::max<int64_t>(rps[m], 1));
   DBuf<double> sv(std::max<int64_t>(rps[m], 1));
   DBuf<int> cnt2(m);
-  for (size_t c = 0; c + 1 < bounds.size(); ++c) {
-    const int r0 = bounds[c], r1 = bounds[c + 1];
-    k_spgemm_numeric<<<ceil_div((int64_t)(r1 - r0) * 32, 256), 256, 0, st>>>(
-        r0, r1, xrp, xci, xv, yrp, yci, yv, toff.get() + r0, tcap.get() + r0, keys.get(),
-        vals.get(), drps.get(), sci.get(), sv.get(), cnt2.get());
+  k_spgemm_numeric_sm<<<sm_grid, 32 * kSpgemmSmWarps, num_smem, st>>>(
+      m, xrp, xci, xv, yrp, yci, yv, cnt.get(), drps.get(), sci.get(), sv.get(), cnt2.get());
+  CHRONOS_CHECK_LAUNCH();
+  for (size_t c = 0; c + 1 < bounds.size() && nbig > 0; ++c) {
+    const int t0 = bounds[c], t1 = bounds[c + 1];
+    k_spgemm_numeric<<<ceil_div((int64_t)(t1 - t0) * 32, 256), 256, 0, st>>>(
+        t0, t1, dbig.get(), xrp, xci, xv, yrp, yci, yv, toff.get() + t0, tcap.get() + t0,
+        keys.get(), vals.get(), drps.get(), sci.get(), sv.get(), cnt2.get());
     CHRONOS_CHECK_LAUNCH();
   }
   std::vector<int> cnt2_h = cnt2.to_host(st);
