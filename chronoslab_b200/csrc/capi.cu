@@ -722,7 +722,7 @@ int chronos_amg_setup(const chronos_params *prm, int n, const int *iat_h, const 
     }
     auto *hh = new chronos_hier();
     try {
-      hh->h = build_hierarchy(*prm, A, ntv0, TV0_h);
+      hh->h = build_hierarchy(*prm, std::move(A), ntv0, TV0_h);
     } catch (...) {
       delete hh;
       throw;

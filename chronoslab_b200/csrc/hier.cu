@@ -786,15 +786,23 @@ void validate_csr(const HostCSR &A) {
   CHRONOS_REQUIRE(A.nrows > 0 && A.ncols == A.nrows, CHRONOS_EINVAL, "matrix must be square, n > 0");
   CHRONOS_REQUIRE((int64_t)A.rp.size() == (int64_t)A.nrows + 1 && A.rp[0] == 0, CHRONOS_EINVAL,
                   "malformed CSR row pointers");
+  CHRONOS_REQUIRE((int64_t)A.ci.size() >= A.rp[A.nrows] && (int64_t)A.v.size() >= A.rp[A.nrows],
+                  CHRONOS_EINVAL, "malformed CSR row pointers");
+  // rows checked in parallel; the first failure kind found is reported
+  int bad = 0;
+#pragma omp parallel for schedule(static, 4096) reduction(| : bad)
   for (int i = 0; i < A.nrows; ++i) {
-    CHRONOS_REQUIRE(A.rp[i + 1] >= A.rp[i], CHRONOS_EINVAL, "CSR row pointers must not decrease");
+    if (A.rp[i + 1] < A.rp[i]) { bad |= 1; continue; }
     for (int64_t k = A.rp[i]; k < A.rp[i + 1]; ++k) {
-      CHRONOS_REQUIRE(A.ci[k] >= 0 && A.ci[k] < A.ncols, CHRONOS_EINVAL, "CSR column out of range");
-      CHRONOS_REQUIRE(k == A.rp[i] || A.ci[k] > A.ci[k - 1], CHRONOS_EINVAL,
-                      "CSR columns must be strictly increasing within a row");
-      CHRONOS_REQUIRE(std::isfinite(A.v[k]), CHRONOS_EINVAL, "non-finite matrix entry");
+      if (A.ci[k] < 0 || A.ci[k] >= A.ncols) bad |= 2;
+      else if (k > A.rp[i] && A.ci[k] <= A.ci[k - 1]) bad |= 4;
+      if (!std::isfinite(A.v[k])) bad |= 8;
     }
   }
+  CHRONOS_REQUIRE(!(bad & 1), CHRONOS_EINVAL, "CSR row pointers must not decrease");
+  CHRONOS_REQUIRE(!(bad & 2), CHRONOS_EINVAL, "CSR column out of range");
+  CHRONOS_REQUIRE(!(bad & 4), CHRONOS_EINVAL, "CSR columns must be strictly increasing within a row");
+  CHRONOS_REQUIRE(!(bad & 8), CHRONOS_EINVAL, "non-finite matrix entry");
 }
 
 // Jacobi-smoothed prolongation (prolong.m:180-196, prol_emin = SMOOTH):
@@ -902,7 +910,7 @@ struct HierBuilder::Active {
   ~Active() { acc += now_s() - t0; }
 };
 
-HierBuilder::HierBuilder(const chronos_params &prm_in, const HostCSR &A0, int ntv0,
+HierBuilder::HierBuilder(const chronos_params &prm_in, HostCSR A0, int ntv0,
                          const double *TV0, const ProlongFn *prolong)
     : prm_(prm_in), prolong_(prolong),
       rng_((uint32_t)(prm_in.seed ? prm_in.seed : 5489)) {
@@ -964,7 +972,7 @@ HierBuilder::HierBuilder(const chronos_params &prm_in, const HostCSR &A0, int nt
     SetupPhase ph3("chronos setup: coarsening", &h_->times[3]);
     qr_orthonormalize(n, ntv_, TV_.data());
   }
-  Al_ = A0;
+  Al_ = std::move(A0);
 }
 
 HierBuilder::~HierBuilder() = default;
@@ -1253,9 +1261,9 @@ std::unique_ptr<Hier> HierBuilder::finish(bool tune) {
   return std::move(h_);
 }
 
-std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A0, int ntv0,
+std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, HostCSR A0, int ntv0,
                                       const double *TV0, bool tune, const ProlongFn *prolong) {
-  HierBuilder b(prm, A0, ntv0, TV0, prolong);
+  HierBuilder b(prm, std::move(A0), ntv0, TV0, prolong);
   while (b.begin_level()) b.end_level(b.fsai_numeric_single());
   return b.finish(tune);
 }

@@ -238,7 +238,7 @@ class CallerStream {
 // prolong != nullptr takes every level's P from it (coarsening, C/F splitting
 // and the prolongation stay with the caller; TV0 is unused); otherwise the
 // library's own coarsening and BAMG build P from the test space.
-std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, const HostCSR &A,
+std::unique_ptr<Hier> build_hierarchy(const chronos_params &prm, HostCSR A,
                                       int ntv0, const double *TV0, bool tune = true,
                                       const ProlongFn *prolong = nullptr);
 void tune_hierarchy(Hier &h);
@@ -251,7 +251,7 @@ void tune_hierarchy(Hier &h);
 // (omega, coarsening, prolongation, Galerkin product of the next level).
 class HierBuilder {
  public:
-  HierBuilder(const chronos_params &prm, const HostCSR &A0, int ntv0, const double *TV0,
+  HierBuilder(const chronos_params &prm, HostCSR A0, int ntv0, const double *TV0,
               const ProlongFn *prolong = nullptr);
   ~HierBuilder();
   bool begin_level();
