@@ -98,6 +98,12 @@ def _emin_cases(cubo_level1):
     TVd = np.column_stack([np.ones(Ap.shape[0]), np.ones(Ap.shape[0]), rng.random(Ap.shape[0])])
     Ap_, _, Sp, fcp, Pp, _ = _level1(Ap, TVd)
     cases.append(("poisson rank-deficient", Ap_, Sp, fcp, Pp, TVd, 5))
+    # one and four test vectors (the warp kernel's other widths)
+    A1, _, S1, fc1, P1, TV1 = _level1(PB.poisson7(12), np.ones(12 ** 3))
+    cases.append(("poisson ntv 1", A1, S1, fc1, P1, TV1, 30))
+    T4 = np.column_stack([np.ones(Ap.shape[0]), rng.random((Ap.shape[0], 3))])
+    A4, _, S4, fc4, P4, TV4 = _level1(Ap, T4)
+    cases.append(("poisson ntv 4", A4, S4, fc4, P4, TV4, 12))
     return cases
 
 
