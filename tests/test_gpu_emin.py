@@ -222,3 +222,30 @@ def test_setup_with_emin_elasticity20_against_the_reference_path(lib):
     assert flag == 0
     assert np.linalg.norm(b - A @ x) <= 1e-8 * np.linalg.norm(b)
     assert not (abs(ito / it - 1) > 0.05 and abs(ito - it) > 2), (it, ito)
+
+
+def test_batch_with_emin_matches_single_setups(lib):
+    """A batch of independent problems (Poisson and log-normal diffusion, one
+    test vector) set up with prol_emin = EMIN: every problem's hierarchy has
+    the levels of its own single EMIN setup, and the batch solve takes the
+    single solve's iterations within one, each to a true relative residual
+    of 1e-8."""
+    rng = np.random.default_rng(5)
+    As, bs = [], []
+    for p in range(4):
+        e = int(rng.integers(10, 18))
+        A = PB.poisson7(e) if p % 2 == 0 else PB.diffusion7(e, sigma=1.0, corr_len=4.0,
+                                                            seed=40 + p)[0]
+        As.append(A)
+        bs.append(PB.uniform_rhs(A.shape[0], seed=60 + p))
+    prm = cb.params(precision=cb.CHRONOS_FP64, ntv=1, prol_emin="EMIN")
+    with cb.Batch(As, prm) as Bt:
+        xs, its, fl, _ = Bt.solve(bs, itmax=1000, tol=1e-8)
+        nlev = [Bt.nlevels(p) for p in range(len(As))]
+    assert np.all(fl == 0)
+    for p, (A, b) in enumerate(zip(As, bs)):
+        with cb.Hierarchy(A, np.ones(A.shape[0]), prm) as h:
+            assert h.nlevels == nlev[p]
+            x, it, _, flag, _ = h.pcg(b, itmax=1000, tol=1e-8)
+        assert flag == 0 and abs(int(its[p]) - it) <= 1, (p, int(its[p]), it)
+        assert np.linalg.norm(b - A @ xs[p]) <= 1e-8 * np.linalg.norm(b)
