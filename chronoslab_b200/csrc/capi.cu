@@ -619,12 +619,11 @@ int chronos_galerkin_compute(int n, int nc, const int *iat_A_h, const int *ja_A_
     for (int i = 0; i < n; ++i)
       for (int64_t k = A.rp[i] + 1; k < A.rp[i + 1]; ++k)
         CHRONOS_REQUIRE(A.ci[k] > A.ci[k - 1], CHRONOS_EINVAL, "A rows must be sorted");
-    HostCSR Pt = csr_transpose(P);
     ScopedStream s;
     DMat dA, dP, dPt;
     upload_csr(A, dA, false, s.st);
     upload_csr(P, dP, false, s.st);
-    upload_csr(Pt, dPt, false, s.st);
+    upload_transpose(dP, dPt, false, s.st);
     DBuf<int> aprp, apci;
     DBuf<double> apv;
     int64_t nnz_ap = 0;

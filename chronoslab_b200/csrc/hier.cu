@@ -91,6 +91,24 @@ CallerStream::~CallerStream() {
 // Device matrices
 // ---------------------------------------------------------------------------
 
+// FP32 copy, 16-bit column offsets (every row spanning fewer than 65536
+// columns: 2 index bytes per entry plus a 4-byte base per row) and the lane
+// heuristic of a CSR whose arrays are on the device and whose row pointers
+// are in rp_h.
+static void finish_csr(DMat &d, bool fp32, cudaStream_t st) {
+  if (fp32) {
+    d.v32.alloc(std::max<int64_t>(d.nnz, 1));
+    convert_f64_to_f32(d.nnz, d.v64.get(), d.v32.get(), st);
+  }
+  d.idx16 = csr_offsets16_device(d.nrows, d.nnz, d.rp.get(), d.ci.get(), d.cbase, d.c16, st);
+  if (!d.idx16) {
+    d.cbase.release();
+    d.c16.release();
+  }
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  set_lanes(d, heuristic_lanes(d), st);
+}
+
 void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st) {
   CHRONOS_REQUIRE(h.nnz() < INT32_MAX, CHRONOS_ENOTSUP, "matrix with 2^31 or more entries");
   d.nrows = h.nrows;
@@ -100,39 +118,21 @@ void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st) {
   d.rp.upload(d.rp_h, st);
   d.ci.upload(h.ci, st);
   d.v64.upload(h.v, st);
-  if (fp32) {
-    d.v32.alloc(std::max<int64_t>(d.nnz, 1));
-    convert_f64_to_f32(d.nnz, d.v64.get(), d.v32.get(), st);
-  }
-  // 16-bit column offsets when every row spans fewer than 65536 columns
-  std::vector<int> base(std::max(h.nrows, 1), 0);
-  int fits = h.nrows > 0;
-#pragma omp parallel for schedule(static, 4096) reduction(&& : fits)
-  for (int i = 0; i < h.nrows; ++i) {
-    if (h.rp[i] == h.rp[i + 1]) continue;
-    int lo = h.ci[h.rp[i]], hi = lo;
-    for (int64_t k = h.rp[i] + 1; k < h.rp[i + 1]; ++k) {
-      lo = std::min(lo, h.ci[k]);
-      hi = std::max(hi, h.ci[k]);
-    }
-    base[i] = lo;
-    fits = fits && hi - lo <= 0xffff;
-  }
-  d.idx16 = fits;
-  if (fits) {
-    std::vector<uint16_t> off(std::max<int64_t>(d.nnz, 1), 0);
-#pragma omp parallel for schedule(static, 4096)
-    for (int i = 0; i < h.nrows; ++i)
-      for (int64_t k = h.rp[i]; k < h.rp[i + 1]; ++k) off[k] = (uint16_t)(h.ci[k] - base[i]);
-    d.cbase.upload(base, st);
-    d.c16.upload(off, st);
-    CHRONOS_CUDA(cudaStreamSynchronize(st));
-  } else {
-    d.cbase.release();
-    d.c16.release();
-    CHRONOS_CUDA(cudaStreamSynchronize(st));
-  }
-  set_lanes(d, heuristic_lanes(d), st);
+  finish_csr(d, fp32, st);
+}
+
+// M' of a device CSR, built on the device: the pattern and values that
+// uploading csr_transpose of the host matrix gives.
+void upload_transpose(const DMat &M, DMat &T, bool fp32, cudaStream_t st) {
+  T.nrows = M.ncols;
+  T.ncols = M.nrows;
+  T.nnz = M.nnz;
+  csr_transpose_device(M.nrows, M.ncols, M.nnz, M.rp.get(), M.ci.get(), M.v64.get(), T.rp, T.ci,
+                       T.v64, st);
+  T.rp_h.resize((size_t)T.nrows + 1);
+  T.rp.download(T.rp_h.data(), (size_t)T.nrows + 1, st);
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  finish_csr(T, fp32, st);
 }
 
 int heuristic_lanes(const DMat &m) {
@@ -1092,13 +1092,7 @@ void HierBuilder::end_level(int fl) {
     if (fixed) L.G.v64.upload(gv, st);
     ph1.end();
     SetupPhase ph9("chronos setup: layouts", &T[9]);
-    std::vector<int64_t> perm;
-    HostCSR Gt = csr_transpose_map(Gh, perm);
-    Gt.v.assign(Gt.ci.size(), 0.0);
-    upload_csr(Gt, L.Gt, false, st);
-    DBuf<int64_t> dperm;
-    dperm.upload(perm, st);
-    gather_values(L.G.nnz, L.G.v64.get(), dperm.get(), L.Gt.v64.get(), st);
+    upload_transpose(L.G, L.Gt, false, st);
     if (fp32) {
       L.G.v32.alloc(std::max<int64_t>(L.G.nnz, 1));
       L.Gt.v32.alloc(std::max<int64_t>(L.Gt.nnz, 1));
@@ -1226,9 +1220,7 @@ void HierBuilder::end_level(int fl) {
   SetupPhase ph9("chronos setup: layouts", &T[9]);
   L.nc = nc;
   upload_csr(Ph, L.P, fp32, st);
-  HostCSR Pt = csr_transpose(Ph);
-  upload_csr(Pt, L.Pt, fp32, st);
-  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  upload_transpose(L.P, L.Pt, fp32, st);
   ph9.end();
   SetupPhase ph5("chronos setup: galerkin", &T[5]);
   DBuf<int> aprp, apci, acrp, acci;
@@ -1462,9 +1454,9 @@ std::unique_ptr<Hier> load_hierarchy(const char *path) {
                           L.nc > 0 && L.nc < L.n,
                       CHRONOS_EIO, "smoother or prolongation size differs in the hierarchy file");
       upload_csr(G, L.G, fp32, st);
-      upload_csr(csr_transpose(G), L.Gt, fp32, st);
+      upload_transpose(L.G, L.Gt, fp32, st);
       upload_csr(P, L.P, fp32, st);
-      upload_csr(csr_transpose(P), L.Pt, fp32, st);
+      upload_transpose(L.P, L.Pt, fp32, st);
     }
     alloc_vectors(L, h->precision, st);
     nprev = L.coarsest ? -1 : L.nc;

@@ -55,9 +55,8 @@ uint32_t MT19937::next_u32() {
 // Transpose of A with rows ascending in each column.  Parallel over blocks
 // of rows: every thread counts the columns of its block, the positions are
 // laid out column by column in block order, and every thread scatters its
-// block -- the same output as the sequential pass.  perm (when given)
-// receives, for each entry of the transpose, its index in A.
-static HostCSR transpose_impl(const HostCSR &A, std::vector<int64_t> *perm) {
+// block -- the same output as the sequential pass.
+HostCSR csr_transpose(const HostCSR &A) {
   HostCSR T;
   T.nrows = A.ncols;
   T.ncols = A.nrows;
@@ -85,7 +84,6 @@ static HostCSR transpose_impl(const HostCSR &A, std::vector<int64_t> *perm) {
   }
   T.ci.resize(nnz);
   T.v.resize(nnz);
-  if (perm) perm->resize(nnz);
   const bool vals = !A.v.empty();
 #pragma omp parallel for num_threads(nt) schedule(static, 1)
   for (int t = 0; t < nt; ++t) {
@@ -95,17 +93,11 @@ static HostCSR transpose_impl(const HostCSR &A, std::vector<int64_t> *perm) {
         const int64_t d = p[A.ci[k]]++;
         T.ci[d] = i;
         T.v[d] = vals ? A.v[k] : 0.0;
-        if (perm) (*perm)[d] = k;
       }
   }
   return T;
 }
 
-HostCSR csr_transpose_map(const HostCSR &A, std::vector<int64_t> &perm) {
-  return transpose_impl(A, &perm);
-}
-
-HostCSR csr_transpose(const HostCSR &A) { return transpose_impl(A, nullptr); }
 
 // ---- strength of connection ------------------------------------------------
 static std::vector<double> diagonal(const HostCSR &A) {

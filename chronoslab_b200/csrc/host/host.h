@@ -108,7 +108,5 @@ void write_tv_ext_bin(const std::string &path, int nrows, int ntv, const double 
 
 // CSR utilities
 HostCSR csr_transpose(const HostCSR &A);
-// Transpose with the permutation map: At.v[k] = A.v[perm[k]].
-HostCSR csr_transpose_map(const HostCSR &A, std::vector<int64_t> &perm);
 
 }  // namespace chronos

@@ -105,9 +105,18 @@ template <typename TI, typename TO>
 void dense_matvec(int n, const double *W, const TI *b, TO *x, cudaStream_t st);
 
 // ---- vector helpers (setup_kernels.cu) ---------------------------------------
-void gather_values(int64_t nnz, const double *src, const int64_t *perm, double *dst,
-                   cudaStream_t st);
 void convert_f64_to_f32(int64_t n, const double *src, float *dst, cudaStream_t st);
+// Transpose (ncols x nrows) of a device CSR: its row pointers, columns and
+// values as the host transpose orders them (rows of the transpose in
+// ascending order of the original row).  Synchronises st.
+void csr_transpose_device(int nrows, int ncols, int64_t nnz, const int *rp, const int *ci,
+                          const double *v, DBuf<int> &trp, DBuf<int> &tci, DBuf<double> &tv,
+                          cudaStream_t st);
+// 16-bit column offsets from each row's smallest column (rows without
+// entries: base 0), when every row spans fewer than 65536 columns; returns
+// false (nothing kept) otherwise.
+bool csr_offsets16_device(int nrows, int64_t nnz, const int *rp, const int *ci, DBuf<int> &base,
+                          DBuf<uint16_t> &off, cudaStream_t st);
 double device_dot(int n, const double *a, const double *b, double *scratch, cudaStream_t st);
 void device_axpby(int n, double a, const double *x, double b, double *y, cudaStream_t st);
 void device_scale_copy(int n, double a, const double *x, double *y, cudaStream_t st);

@@ -853,19 +853,6 @@ template void dense_matvec<double, double>(int, const double *, const double *, 
 // Vector helpers
 // =============================================================================
 
-__global__ void k_gather(int64_t nnz, const double *src, const int64_t *perm, double *dst) {
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz;
-       k += (int64_t)gridDim.x * blockDim.x)
-    dst[k] = src[perm[k]];
-}
-
-void gather_values(int64_t nnz, const double *src, const int64_t *perm, double *dst,
-                   cudaStream_t st) {
-  if (nnz <= 0) return;
-  k_gather<<<std::min<int64_t>(ceil_div(nnz, 256), 4096), 256, 0, st>>>(nnz, src, perm, dst);
-  CHRONOS_CHECK_LAUNCH();
-}
-
 __global__ void k_f64_to_f32(int64_t n, const double *s, float *d) {
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n;
        k += (int64_t)gridDim.x * blockDim.x)
@@ -876,6 +863,128 @@ void convert_f64_to_f32(int64_t n, const double *src, float *dst, cudaStream_t s
   if (n <= 0) return;
   k_f64_to_f32<<<std::min<int64_t>(ceil_div(n, 256), 4096), 256, 0, st>>>(n, src, dst);
   CHRONOS_CHECK_LAUNCH();
+}
+
+// =============================================================================
+// CSR layouts on the device: transpose, 16-bit column offsets
+// =============================================================================
+
+__global__ void k_row_ids(int n, const int *__restrict__ rp, int *__restrict__ rid) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int k = rp[i]; k < rp[i + 1]; ++k) rid[k] = i;
+}
+
+__global__ void k_col_count(int nnz, const int *__restrict__ ci, int *__restrict__ cnt) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nnz; k += gridDim.x * blockDim.x)
+    atomicAdd(cnt + ci[k], 1);
+}
+
+__global__ void k_iota(int n, int *__restrict__ a) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) a[k] = k;
+}
+
+__global__ void k_transpose_fill(int nnz, const int *__restrict__ perm, const int *__restrict__ rid,
+                                 const double *__restrict__ v, int *__restrict__ tci,
+                                 double *__restrict__ tv) {
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < nnz; d += gridDim.x * blockDim.x) {
+    const int k = perm[d];
+    tci[d] = rid[k];
+    tv[d] = v[k];
+  }
+}
+
+// Entry k of row i lands in row ci[k] of the transpose; a stable radix sort
+// of the row-major entries by column keeps each transposed row in ascending
+// order of i (then of k), which is the order the host transpose fills.
+void csr_transpose_device(int nrows, int ncols, int64_t nnz64, const int *rp, const int *ci,
+                          const double *v, DBuf<int> &trp, DBuf<int> &tci, DBuf<double> &tv,
+                          cudaStream_t st) {
+  CHRONOS_REQUIRE(nnz64 < INT32_MAX, CHRONOS_ENOTSUP, "matrix with 2^31 or more entries");
+  const int nnz = (int)nnz64;
+  trp.alloc((size_t)ncols + 1);
+  tci.alloc(std::max(nnz, 1));
+  tv.alloc(std::max(nnz, 1));
+  DBuf<int> cnt((size_t)ncols + 1);
+  cnt.zero(st);
+  const int grid = std::max(1, std::min<int>(ceil_div(std::max(nnz, 1), 256), num_sms() * 16));
+  if (nnz > 0) {
+    k_col_count<<<grid, 256, 0, st>>>(nnz, ci, cnt.get());
+    CHRONOS_CHECK_LAUNCH();
+  }
+  size_t bytes = 0;
+  CHRONOS_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cnt.get(), trp.get(), ncols + 1, st));
+  {
+    DBuf<unsigned char> tmp(std::max<size_t>(bytes, 1));
+    CHRONOS_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, cnt.get(), trp.get(), ncols + 1,
+                                               st));
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+  }
+  if (nnz == 0) return;
+  DBuf<int> rid(nnz), idx(nnz), perm(nnz), keys(nnz);
+  k_row_ids<<<std::max(1, std::min<int>(ceil_div(std::max(nrows, 1), 256), num_sms() * 16)), 256,
+              0, st>>>(nrows, rp, rid.get());
+  CHRONOS_CHECK_LAUNCH();
+  k_iota<<<grid, 256, 0, st>>>(nnz, idx.get());
+  CHRONOS_CHECK_LAUNCH();
+  int end_bit = 1;
+  while (end_bit < 31 && (1LL << end_bit) < (long long)ncols) ++end_bit;
+  bytes = 0;
+  CHRONOS_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, ci, keys.get(), idx.get(),
+                                               perm.get(), nnz, 0, end_bit, st));
+  {
+    DBuf<unsigned char> tmp(std::max<size_t>(bytes, 1));
+    CHRONOS_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, ci, keys.get(), idx.get(),
+                                                 perm.get(), nnz, 0, end_bit, st));
+    k_transpose_fill<<<grid, 256, 0, st>>>(nnz, perm.get(), rid.get(), v, tci.get(), tv.get());
+    CHRONOS_CHECK_LAUNCH();
+    CHRONOS_CUDA(cudaStreamSynchronize(st));
+  }
+}
+
+__global__ void k_row_span(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                           int *__restrict__ base, int *__restrict__ wide) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int s = rp[i], e = rp[i + 1];
+    int lo = 0;
+    if (e > s) {
+      lo = ci[s];
+      int hi = lo;
+      for (int k = s + 1; k < e; ++k) {
+        lo = min(lo, ci[k]);
+        hi = max(hi, ci[k]);
+      }
+      if (hi - lo > 0xffff) atomicOr(wide, 1);
+    }
+    base[i] = lo;
+  }
+}
+
+__global__ void k_col_offsets16(int n, const int *__restrict__ rp, const int *__restrict__ ci,
+                                const int *__restrict__ base, uint16_t *__restrict__ off) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    for (int k = rp[i]; k < rp[i + 1]; ++k) off[k] = (uint16_t)(ci[k] - base[i]);
+}
+
+bool csr_offsets16_device(int nrows, int64_t nnz, const int *rp, const int *ci, DBuf<int> &base,
+                          DBuf<uint16_t> &off, cudaStream_t st) {
+  if (nrows <= 0) return false;
+  base.alloc(nrows);
+  DBuf<int> wide(1);
+  wide.zero(st);
+  const int grid = std::max(1, std::min<int>(ceil_div(nrows, 256), num_sms() * 16));
+  k_row_span<<<grid, 256, 0, st>>>(nrows, rp, ci, base.get(), wide.get());
+  CHRONOS_CHECK_LAUNCH();
+  int w = 0;
+  CHRONOS_CUDA(cudaMemcpyAsync(&w, wide.get(), sizeof(int), cudaMemcpyDeviceToHost, st));
+  CHRONOS_CUDA(cudaStreamSynchronize(st));
+  if (w) {
+    base.release();
+    return false;
+  }
+  off.alloc(std::max<int64_t>(nnz, 1));
+  k_col_offsets16<<<grid, 256, 0, st>>>(nrows, rp, ci, base.get(), off.get());
+  CHRONOS_CHECK_LAUNCH();
+  return true;
 }
 
 __global__ void k_dot_partial(int n, const double *a, const double *b, double *part) {
