@@ -91,16 +91,56 @@ CallerStream::~CallerStream() {
 // Device matrices
 // ---------------------------------------------------------------------------
 
+// Matrices of at least this many entries get their 16-bit column offsets and
+// their transposes built on the device; smaller ones on the host, where the
+// device path's temporary allocations and synchronisations cost more (the
+// batch setup builds many small levels from several host threads).
+constexpr int64_t kDeviceLayoutNnz = 1 << 20;
+
+// 16-bit column offsets on the host (rows without entries: base 0); false
+// when a row spans 65536 columns or more.
+static bool offsets16_host(const HostCSR &h, std::vector<int> &base, std::vector<uint16_t> &off) {
+  base.assign(std::max(h.nrows, 1), 0);
+  int fits = h.nrows > 0;
+#pragma omp parallel for schedule(static, 4096) reduction(&& : fits)
+  for (int i = 0; i < h.nrows; ++i) {
+    if (h.rp[i] == h.rp[i + 1]) continue;
+    int lo = h.ci[h.rp[i]], hi = lo;
+    for (int64_t k = h.rp[i] + 1; k < h.rp[i + 1]; ++k) {
+      lo = std::min(lo, h.ci[k]);
+      hi = std::max(hi, h.ci[k]);
+    }
+    base[i] = lo;
+    fits = fits && hi - lo <= 0xffff;
+  }
+  if (!fits) return false;
+  off.assign(std::max<int64_t>(h.nnz(), 1), 0);
+#pragma omp parallel for schedule(static, 4096)
+  for (int i = 0; i < h.nrows; ++i)
+    for (int64_t k = h.rp[i]; k < h.rp[i + 1]; ++k) off[k] = (uint16_t)(h.ci[k] - base[i]);
+  return true;
+}
+
 // FP32 copy, 16-bit column offsets (every row spanning fewer than 65536
-// columns: 2 index bytes per entry plus a 4-byte base per row) and the lane
-// heuristic of a CSR whose arrays are on the device and whose row pointers
-// are in rp_h.
-static void finish_csr(DMat &d, bool fp32, cudaStream_t st) {
+// columns: 2 index bytes per entry plus a 4-byte base per row; from the host
+// arrays h when given, else on the device) and the lane heuristic of a CSR
+// whose arrays are on the device and whose row pointers are in rp_h.
+static void finish_csr(DMat &d, const HostCSR *h, bool fp32, cudaStream_t st) {
   if (fp32) {
     d.v32.alloc(std::max<int64_t>(d.nnz, 1));
     convert_f64_to_f32(d.nnz, d.v64.get(), d.v32.get(), st);
   }
-  d.idx16 = csr_offsets16_device(d.nrows, d.nnz, d.rp.get(), d.ci.get(), d.cbase, d.c16, st);
+  if (h) {
+    std::vector<int> base;
+    std::vector<uint16_t> off;
+    d.idx16 = offsets16_host(*h, base, off);
+    if (d.idx16) {
+      d.cbase.upload(base, st);
+      d.c16.upload(off, st);
+    }
+  } else {
+    d.idx16 = csr_offsets16_device(d.nrows, d.nnz, d.rp.get(), d.ci.get(), d.cbase, d.c16, st);
+  }
   if (!d.idx16) {
     d.cbase.release();
     d.c16.release();
@@ -118,12 +158,20 @@ void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st) {
   d.rp.upload(d.rp_h, st);
   d.ci.upload(h.ci, st);
   d.v64.upload(h.v, st);
-  finish_csr(d, fp32, st);
+  finish_csr(d, d.nnz >= kDeviceLayoutNnz ? nullptr : &h, fp32, st);
 }
 
-// M' of a device CSR, built on the device: the pattern and values that
-// uploading csr_transpose of the host matrix gives.
+static HostCSR download_csr(int nrows, int ncols, const DBuf<int> &rp, const DBuf<int> &ci,
+                            const DBuf<double> &v, int64_t nnz, cudaStream_t st);
+
+// M' of a device CSR: the pattern and values that uploading csr_transpose of
+// the host matrix gives (built on the device for large matrices).
 void upload_transpose(const DMat &M, DMat &T, bool fp32, cudaStream_t st) {
+  if (M.nnz < kDeviceLayoutNnz) {
+    upload_csr(csr_transpose(download_csr(M.nrows, M.ncols, M.rp, M.ci, M.v64, M.nnz, st)), T,
+               fp32, st);
+    return;
+  }
   T.nrows = M.ncols;
   T.ncols = M.nrows;
   T.nnz = M.nnz;
@@ -132,7 +180,7 @@ void upload_transpose(const DMat &M, DMat &T, bool fp32, cudaStream_t st) {
   T.rp_h.resize((size_t)T.nrows + 1);
   T.rp.download(T.rp_h.data(), (size_t)T.nrows + 1, st);
   CHRONOS_CUDA(cudaStreamSynchronize(st));
-  finish_csr(T, fp32, st);
+  finish_csr(T, nullptr, fp32, st);
 }
 
 int heuristic_lanes(const DMat &m) {
