@@ -97,6 +97,27 @@ def test_galerkin_bitexact_cubo(lib, cubo, cubo_ref):
     assert np.array_equal(Ac.data, ref.data)
 
 
+def test_galerkin_bitexact_device_transpose(lib):
+    """A prolongation of 2M entries: P' is built on the device (stable radix
+    sort by column) and the 16-bit column offsets of A and P there too; the
+    product is still bit-identical to the row-wise Gustavson one."""
+    A = PB.poisson7(100)
+    n = A.shape[0]
+    nc = n // 8
+    rng = np.random.default_rng(17)
+    rows = np.repeat(np.arange(n), 2)
+    cols = np.stack([np.arange(n) // 8, (np.arange(n) // 8 + 1 + np.arange(n) % 5) % nc], 1).ravel()
+    P = sp.csr_matrix((rng.uniform(0.1, 1.0, 2 * n), (rows, cols)), shape=(n, nc))
+    P.sum_duplicates()
+    P.sort_indices()
+    assert P.nnz >= 1 << 20
+    Ac = cb.galerkin(A, P)
+    ref = _scipy_galerkin(A, P)
+    assert np.array_equal(Ac.indptr, ref.indptr)
+    assert np.array_equal(Ac.indices, ref.indices)
+    assert np.array_equal(Ac.data, ref.data)
+
+
 def test_galerkin_cancellation_drops_zeros(lib):
     """Exact cancellations are dropped from the pattern, as MATLAB does."""
     A = PB.poisson7(6)
