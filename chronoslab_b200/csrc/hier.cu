@@ -301,11 +301,14 @@ static void drop_sell(DMat &m) {
 
 // Autotuner of the lanes per row (CSR) or per block row (BSR3): times each
 // candidate on the matrix itself and keeps the fastest.  Decisions are cached
-// per matrix signature (format, rows, entries, columns, precision) in memory
-// and in a text file (CHRONOS_TUNE_CACHE, default ~/.cache/chronos_b200_tune.txt)
-// so later processes on the machine -- a profiler run included -- reuse them.
+// per matrix signature (format, rows, entries, columns, precision, longest
+// row -- G and G' share the first five but not their row lengths) in memory
+// and in a text file (CHRONOS_TUNE_CACHE, default ~/.cache/chronos_b200_tune.txt;
+// lines "v2 kind rows entries columns fp32 longest decision", other lines
+// ignored) so later processes on the machine -- a profiler run included --
+// reuse them.
 namespace {
-using TuneKey = std::tuple<char, int, int64_t, int, bool>;
+using TuneKey = std::tuple<char, int, int64_t, int, bool, int>;
 std::mutex g_tune_mu;
 std::map<TuneKey, int> g_tune;
 bool g_tune_loaded = false;
@@ -321,11 +324,14 @@ void tune_load_locked() {
   g_tune_loaded = true;
   FILE *f = std::fopen(tune_path().c_str(), "r");
   if (!f) return;
-  char kind;
-  int nr, nc, fp, L;
-  long long nnz;
-  while (std::fscanf(f, " %c %d %lld %d %d %d", &kind, &nr, &nnz, &nc, &fp, &L) == 6)
-    g_tune[TuneKey(kind, nr, (int64_t)nnz, nc, fp != 0)] = L;
+  char line[256];
+  while (std::fgets(line, sizeof(line), f)) {
+    char kind;
+    int nr, nc, fp, mx, L;
+    long long nnz;
+    if (std::sscanf(line, "v2 %c %d %lld %d %d %d %d", &kind, &nr, &nnz, &nc, &fp, &mx, &L) == 7)
+      g_tune[TuneKey(kind, nr, (int64_t)nnz, nc, fp != 0, mx)] = L;
+  }
   std::fclose(f);
 }
 
@@ -340,8 +346,9 @@ void tune_store_locked(const TuneKey &k, int L) {
       if (i == dir.size() || dir[i] == '/') mkdir(dir.substr(0, i).c_str(), 0755);
   }
   if (FILE *f = std::fopen(path.c_str(), "a")) {
-    std::fprintf(f, "%c %d %lld %d %d %d\n", std::get<0>(k), std::get<1>(k),
-                 (long long)std::get<2>(k), std::get<3>(k), std::get<4>(k) ? 1 : 0, L);
+    std::fprintf(f, "v2 %c %d %lld %d %d %d %d\n", std::get<0>(k), std::get<1>(k),
+                 (long long)std::get<2>(k), std::get<3>(k), std::get<4>(k) ? 1 : 0,
+                 std::get<5>(k), L);
     std::fclose(f);
   }
 }
@@ -352,7 +359,9 @@ void autotune_lanes(DMat &m, bool fp32, cudaStream_t st, int format) {
   if (m.nrows <= 0) return;
   // 'H': the hybrid CSR kernel (k_csrh_apply); the index width is part of the
   // shape.  A cached value is lanes + 100 * form (decoded at the end).
-  const TuneKey key(m.idx16 ? 'h' : 'H', m.nrows, m.nnz, m.ncols, fp32);
+  int maxrow = 0;
+  for (int i = 0; i < m.nrows; ++i) maxrow = std::max(maxrow, m.rp_h[i + 1] - m.rp_h[i]);
+  const TuneKey key(m.idx16 ? 'h' : 'H', m.nrows, m.nnz, m.ncols, fp32, maxrow);
   int L = -1;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -560,7 +569,8 @@ static void launch_pcg_spmv(cudaStream_t st, const DMat &A, bool fp32vals, const
 static void attach_sell3(const HostCSR &A, DMat &d, bool fp32, cudaStream_t st) {
   const std::vector<int> blen = block_row_lengths(A);
   if (blen.empty()) return;
-  const TuneKey key('B', (int)blen.size(), A.nnz(), A.ncols, fp32);
+  const TuneKey key('B', (int)blen.size(), A.nnz(), A.ncols, fp32,
+                    *std::max_element(blen.begin(), blen.end()));
   int T = -1;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
