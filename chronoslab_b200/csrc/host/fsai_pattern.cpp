@@ -18,6 +18,7 @@
 // ref_abs = false uses fabs.
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <vector>
 
 #include "host.h"
@@ -57,9 +58,13 @@ void select_largest(int n, int ncut, double *R, int *I, bool ref_abs) {
 }
 
 struct Work {
-  std::vector<int> pat;        // pattern (IWN[0..mrow)) followed by candidates
+  // pattern (IWN[0..mrow)) followed by candidates, and the candidates'
+  // gradients: n slots each, written before they are read, so left
+  // uninitialised (zero-filling 12 bytes per row and thread was a visible
+  // share of the search at a million rows)
+  std::unique_ptr<int[]> pat;
+  std::unique_ptr<double[]> grad;
   std::vector<int> mark;       // per column: -1 in pattern, >0 candidate slot, 0 free
-  std::vector<double> grad;    // candidate gradients
   std::vector<double> M;       // mmax x mmax, column-major lower triangle
   std::vector<double> y, ysav; // current solution / saved right-hand side
 };
@@ -68,8 +73,8 @@ struct Work {
 // pattern; keeps the lfil largest and appends them to the pattern (sorted).
 void grow_pattern(const HostCSR &A, int i, int lfil, int &mrow, Work &w, bool ref_abs) {
   int nw = 0;
-  auto *pat = w.pat.data();
-  auto *mark = w.mark.data();
+  int *pat = w.pat.get();
+  int *mark = w.mark.data();
   for (int64_t k = A.rp[i]; k < A.rp[i + 1] && A.ci[k] < i; ++k) {
     const int c = A.ci[k];
     if (mark[c] >= 0) {
@@ -97,7 +102,7 @@ void grow_pattern(const HostCSR &A, int i, int lfil, int &mrow, Work &w, bool re
     }
   }
   const int ncut = std::min(lfil, nw);
-  select_largest(nw, ncut, w.grad.data(), pat + mrow, ref_abs);
+  select_largest(nw, ncut, w.grad.get(), pat + mrow, ref_abs);
   for (int p = mrow; p < mrow + ncut; ++p) mark[pat[p]] = -1;
   for (int p = mrow + ncut; p < mrow + nw; ++p) mark[pat[p]] = 0;
   mrow += ncut;
@@ -108,7 +113,7 @@ void grow_pattern(const HostCSR &A, int i, int lfil, int &mrow, Work &w, bool re
 // M (ld = mmax), and rhs = -A[i, P].  Returns false when row i holds no entry
 // left of the diagonal (the null right-hand side).
 bool gather_system(const HostCSR &A, int i, int mrow, int mmax, Work &w) {
-  const int *P = w.pat.data();
+  const int *P = w.pat.get();
   for (int c = 0; c < mrow; ++c) {
     const int r = P[c];
     int64_t k = A.rp[r];
@@ -180,9 +185,9 @@ FsaiResult fsai_adaptive(const HostCSR &A, int nstep, int step_size, double eps,
 #pragma omp parallel num_threads(std::max(1, nthreads)) reduction(& : posdef_all)
   {
     Work w;
-    w.pat.assign((size_t)n, 0);
+    w.pat.reset(new int[std::max(n, 1)]);
+    w.grad.reset(new double[std::max(n, 1)]);
     w.mark.assign((size_t)n, 0);
-    w.grad.assign((size_t)n, 0.0);
     w.M.assign((size_t)std::max(mmax, 1) * std::max(mmax, 1), 0.0);
     w.y.assign((size_t)mmax + 1, 0.0);
     w.ysav.assign((size_t)mmax + 1, 0.0);
