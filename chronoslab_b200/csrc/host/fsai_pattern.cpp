@@ -178,8 +178,10 @@ FsaiResult fsai_adaptive(const HostCSR &A, int nstep, int step_size, double eps,
   const int mmax = nstep * step_size;
   const int kmax = 1 + mmax;
   std::vector<int> rowlen(n, 0);
-  std::vector<int> cols((size_t)n * kmax);
-  std::vector<double> vals((size_t)n * kmax);
+  // each row's columns and values, written before they are read (not zeroed:
+  // n * kmax * 12 bytes)
+  std::unique_ptr<int[]> cols(new int[(size_t)std::max(n, 1) * kmax]);
+  std::unique_ptr<double[]> vals(new double[(size_t)std::max(n, 1) * kmax]);
   int posdef_all = 1;
 
 #pragma omp parallel num_threads(std::max(1, nthreads)) reduction(& : posdef_all)
@@ -244,8 +246,8 @@ FsaiResult fsai_adaptive(const HostCSR &A, int nstep, int step_size, double eps,
       }
       if (scal <= 0.0) { posdef = 0; scal = 1.0; }
       scal = 1.0 / std::sqrt(scal);
-      int *oc = cols.data() + (size_t)i * kmax;
-      double *ov = vals.data() + (size_t)i * kmax;
+      int *oc = cols.get() + (size_t)i * kmax;
+      double *ov = vals.get() + (size_t)i * kmax;
       for (int p = 0; p < mrow; ++p) {
         oc[p] = w.pat[p];
         ov[p] = scal * w.y[p];
@@ -267,9 +269,9 @@ FsaiResult fsai_adaptive(const HostCSR &A, int nstep, int step_size, double eps,
   G.v.resize(G.rp[n]);
 #pragma omp parallel for num_threads(std::max(1, nthreads)) schedule(static)
   for (int i = 0; i < n; ++i) {
-    std::copy(cols.begin() + (size_t)i * kmax, cols.begin() + (size_t)i * kmax + rowlen[i],
+    std::copy(cols.get() + (size_t)i * kmax, cols.get() + (size_t)i * kmax + rowlen[i],
               G.ci.begin() + G.rp[i]);
-    std::copy(vals.begin() + (size_t)i * kmax, vals.begin() + (size_t)i * kmax + rowlen[i],
+    std::copy(vals.get() + (size_t)i * kmax, vals.get() + (size_t)i * kmax + rowlen[i],
               G.v.begin() + G.rp[i]);
   }
   return out;
