@@ -623,7 +623,7 @@ int chronos_galerkin_compute(int n, int nc, const int *iat_A_h, const int *ja_A_
     DMat dA, dP, dPt;
     upload_csr(A, dA, false, s.st);
     upload_csr(P, dP, false, s.st);
-    upload_transpose(dP, dPt, false, s.st);
+    upload_transpose(dP, dPt, false, s.st, &P);
     DBuf<int> aprp, apci;
     DBuf<double> apv;
     int64_t nnz_ap = 0;

@@ -165,11 +165,16 @@ static HostCSR download_csr(int nrows, int ncols, const DBuf<int> &rp, const DBu
                             const DBuf<double> &v, int64_t nnz, cudaStream_t st);
 
 // M' of a device CSR: the pattern and values that uploading csr_transpose of
-// the host matrix gives (built on the device for large matrices).
-void upload_transpose(const DMat &M, DMat &T, bool fp32, cudaStream_t st) {
+// the host matrix gives (built on the device for large matrices).  Mh, when
+// given, is the same matrix on the host (values included), which spares a
+// small matrix its download.
+void upload_transpose(const DMat &M, DMat &T, bool fp32, cudaStream_t st, const HostCSR *Mh) {
   if (M.nnz < kDeviceLayoutNnz) {
-    upload_csr(csr_transpose(download_csr(M.nrows, M.ncols, M.rp, M.ci, M.v64, M.nnz, st)), T,
-               fp32, st);
+    if (Mh)
+      upload_csr(csr_transpose(*Mh), T, fp32, st);
+    else
+      upload_csr(csr_transpose(download_csr(M.nrows, M.ncols, M.rp, M.ci, M.v64, M.nnz, st)), T,
+                 fp32, st);
     return;
   }
   T.nrows = M.ncols;
@@ -1278,7 +1283,7 @@ void HierBuilder::end_level(int fl) {
   SetupPhase ph9("chronos setup: layouts", &T[9]);
   L.nc = nc;
   upload_csr(Ph, L.P, fp32, st);
-  upload_transpose(L.P, L.Pt, fp32, st);
+  upload_transpose(L.P, L.Pt, fp32, st, &Ph);
   ph9.end();
   SetupPhase ph5("chronos setup: galerkin", &T[5]);
   DBuf<int> aprp, apci, acrp, acci;
@@ -1512,9 +1517,9 @@ std::unique_ptr<Hier> load_hierarchy(const char *path) {
                           L.nc > 0 && L.nc < L.n,
                       CHRONOS_EIO, "smoother or prolongation size differs in the hierarchy file");
       upload_csr(G, L.G, fp32, st);
-      upload_transpose(L.G, L.Gt, fp32, st);
+      upload_transpose(L.G, L.Gt, fp32, st, &G);
       upload_csr(P, L.P, fp32, st);
-      upload_transpose(L.P, L.Pt, fp32, st);
+      upload_transpose(L.P, L.Pt, fp32, st, &P);
     }
     alloc_vectors(L, h->precision, st);
     nprev = L.coarsest ? -1 : L.nc;

@@ -292,8 +292,9 @@ void params_read(const char *fnames_path, chronos_params *p);
 // Upload a host CSR (FP64) to a device matrix, with FP32 values when fp32.
 void upload_csr(const HostCSR &h, DMat &d, bool fp32, cudaStream_t st);
 // T = M' built on the device from M's device arrays (as upload_csr of the
-// host transpose would give).
-void upload_transpose(const DMat &M, DMat &T, bool fp32, cudaStream_t st);
+// host transpose would give); Mh: the same matrix on the host, if at hand.
+void upload_transpose(const DMat &M, DMat &T, bool fp32, cudaStream_t st,
+                      const HostCSR *Mh = nullptr);
 // SpMV lane count by timing the candidates (cached per shape).
 // format: 0 tuned (row-grouped CSR or sliced ELL), 1 CSR only, 2 sliced ELL
 // whenever the rows average at most 16 entries.
