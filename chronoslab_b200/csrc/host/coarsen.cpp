@@ -314,11 +314,32 @@ std::vector<int> pmis_split(const HostCSR &A, const HostCSR &S, MT19937 &rng, in
 
 // ---- thin QR ------------------------------------------------------------------
 // Householder QR with LAPACK's sign convention (beta = -sign(x1)*||x||); Q is
-// accumulated explicitly into X (n x k, column-major).
+// accumulated explicitly into X (n x k, column-major).  Each reflector's
+// projections on the other columns are independent: they run in parallel
+// over the columns, each dot product summed in index order as a sequential
+// loop would, and the column updates in parallel over the rows, so the result
+// does not depend on the thread count.
 void qr_orthonormalize(int n, int k, double *X) {
   if (k == 0 || n == 0) return;
-  std::vector<double> V((size_t)n * k, 0.0), tau(k, 0.0);
+  std::vector<double> V((size_t)n * k, 0.0), tau(k, 0.0), s(k, 0.0);
   std::vector<double> R(X, X + (size_t)n * k);
+  const bool big = n > 65536;
+  // s[jj] = tau_j * (v_j . M_jj) over rows j.. for columns jj0..k-1 of M
+  auto project = [&](const double *v, const double *M, int j, int jj0) {
+#pragma omp parallel for schedule(static, 1) if (big && k - jj0 > 1)
+    for (int jj = jj0; jj < k; ++jj) {
+      const double *cc = M + (size_t)jj * n;
+      double t = 0;
+      for (int i = j; i < n; ++i) t += v[i] * cc[i];
+      s[jj] = t * tau[j];
+    }
+  };
+  // M_jj -= s[jj] v_j over rows j.. for columns jj0..k-1
+  auto update = [&](const double *v, double *M, int j, int jj0) {
+#pragma omp parallel for schedule(static) if (big)
+    for (int i = j; i < n; ++i)
+      for (int jj = jj0; jj < k; ++jj) M[(size_t)jj * n + i] -= s[jj] * v[i];
+  };
   for (int j = 0; j < k && j < n; ++j) {
     double *c = &R[(size_t)j * n];
     double nrm2 = 0;
@@ -330,29 +351,25 @@ void qr_orthonormalize(int n, int k, double *X) {
     tau[j] = (beta - alpha) / beta;
     double scal = 1.0 / (alpha - beta);
     v[j] = 1.0;
-    for (int i = j + 1; i < n; ++i) v[i] = c[i] * scal;
+#pragma omp parallel for schedule(static) if (big)
+    for (int i = j + 1; i < n; ++i) {
+      v[i] = c[i] * scal;
+      c[i] = 0.0;
+    }
     c[j] = beta;
-    for (int i = j + 1; i < n; ++i) c[i] = 0.0;
-    for (int jj = j + 1; jj < k; ++jj) {
-      double *cc = &R[(size_t)jj * n];
-      double s = 0;
-      for (int i = j; i < n; ++i) s += v[i] * cc[i];
-      s *= tau[j];
-      for (int i = j; i < n; ++i) cc[i] -= s * v[i];
+    if (j + 1 < k) {
+      project(v, R.data(), j, j + 1);
+      update(v, R.data(), j, j + 1);
     }
   }
   // Q = H_0 H_1 ... H_{k-1} applied to the first k columns of I
-  for (int j = 0; j < k; ++j)
-    for (int i = 0; i < n; ++i) X[(size_t)j * n + i] = (i == j) ? 1.0 : 0.0;
+#pragma omp parallel for schedule(static) if (big)
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < k; ++j) X[(size_t)j * n + i] = (i == j) ? 1.0 : 0.0;
   for (int j = std::min(k, n) - 1; j >= 0; --j) {
     const double *v = &V[(size_t)j * n];
-    for (int jj = 0; jj < k; ++jj) {
-      double *cc = &X[(size_t)jj * n];
-      double s = 0;
-      for (int i = j; i < n; ++i) s += v[i] * cc[i];
-      s *= tau[j];
-      for (int i = j; i < n; ++i) cc[i] -= s * v[i];
-    }
+    project(v, X, j, 0);
+    update(v, X, j, 0);
   }
 }
 
