@@ -154,3 +154,57 @@ def test_reference_parameter_files_if_present(lib):
         pytest.skip("reference tree not mounted")
     p = cb.readDefaultParams(fn)
     assert p.SoC_type == b"DOM" and p.soc_tau == 0.01 and p.nupre == 1 and p.ntv == 6
+
+
+QR_CALLER = r"""
+#include <cstdio>
+#include <cstdlib>
+#include <random>
+#include <vector>
+namespace chronos { void qr_orthonormalize(int n, int k, double *X); }
+int main(int argc, char **argv) {
+  const int n = std::atoi(argv[1]), k = std::atoi(argv[2]);
+  std::vector<double> X((size_t)n * k);
+  std::mt19937_64 g(12345);
+  std::uniform_real_distribution<double> u(-1.0, 1.0);
+  for (auto &x : X) x = u(g);
+  std::FILE *f = std::fopen(argv[3], "wb");
+  std::fwrite(X.data(), sizeof(double), X.size(), f);
+  chronos::qr_orthonormalize(n, k, X.data());
+  std::fwrite(X.data(), sizeof(double), X.size(), f);
+  std::fclose(f);
+  return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("n,k", [(200000, 6), (70000, 1), (5, 6)])
+def test_test_space_qr_thread_independent(lib, tmp_path, n, k):
+    """The setup's Householder QR of the test space (threaded over columns
+    and rows) gives the same bytes on 1 and 4 threads, orthonormal columns,
+    and LAPACK's Q (numpy's QR) to rounding."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "qr.cpp"
+    src.write_text(QR_CALLER)
+    exe = tmp_path / "qr"
+    libdir = os.path.join(ROOT, "chronoslab_b200")
+    subprocess.run([gxx, "-O2", "-std=c++17", str(src), "-L", libdir, "-lchronos_b200",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    outs = []
+    for threads in ("1", "4"):
+        out = tmp_path / f"q{threads}.bin"
+        env = dict(os.environ, OMP_NUM_THREADS=threads)
+        subprocess.run([str(exe), str(n), str(k), str(out)], check=True, env=env, timeout=300)
+        outs.append(out.read_bytes())
+    assert outs[0] == outs[1]
+    data = np.frombuffer(outs[0], dtype=np.float64)
+    X0 = data[:n * k].reshape(k, n).T
+    Q = data[n * k:].reshape(k, n).T
+    m = min(n, k)
+    assert np.allclose(Q[:, :m].T @ Q[:, :m], np.eye(m), atol=1e-12)
+    Qn, _ = np.linalg.qr(X0)
+    assert np.allclose(Q[:, :m], Qn[:, :m], atol=1e-10)
