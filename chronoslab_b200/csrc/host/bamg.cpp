@@ -338,6 +338,7 @@ HostCSR bamg_prolongation(const BamgParams &p, const HostCSR &S, const std::vect
   for (int i = 0; i < n; ++i) P.rp[i + 1] = P.rp[i] + (int64_t)rcols[i].size();
   P.ci.resize(P.rp[n]);
   P.v.resize(P.rp[n]);
+#pragma omp parallel for num_threads(p.nthreads) schedule(static, 4096)
   for (int i = 0; i < n; ++i) {
     std::copy(rcols[i].begin(), rcols[i].end(), P.ci.begin() + P.rp[i]);
     std::copy(rvals[i].begin(), rvals[i].end(), P.v.begin() + P.rp[i]);
